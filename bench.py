@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""Benchmark: FP64 BiCGSTAB to 1e-8 relative residual on one B200, plus the
+H-matvec HBM throughput, on the plain-FP64 workload (configuration C1):
+
+  Laplace single layer 1/(4 pi r), unit icosphere level 5 (20,480 flat
+  triangles), piecewise-constant collocation at centroids with the analytic
+  flat-triangle integral (self term included), HACApK cluster tree with leaf
+  size 32, admissibility eta = 2.0, ACA+ tolerance 1e-5; rhs = 1 + N(0,1e-3^2)
+  per element (seed 0); BiCGSTAB from x0 = 0 to ||r||/||b|| < 1e-8.
+
+A step is one complete solve.  `value` is seconds per solve with b resident in
+HBM (CUDA events on the launching stream, max over ranks); `e2e` is the same
+solve through the host-vector C-ABI call (hbx_bicgstab_host: b and x0 copied
+in, the solution copied out, inside the timed region).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank solves its own replica: the solve is one
+shared H-matrix per GPU and no data moves between ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hacapk-magma_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "BiCGSTAB s to 1e-8 rel. residual; H-matvec HBM GB/s (% peak), 1 B200"
+WORKLOAD = ("C1 plain FP64: Laplace single layer on a unit icosphere L5 (20,480 triangles), "
+            "leaf 32, eta 2.0, ACA+ 1e-5, rhs 1+N(0,1e-3^2) seed 0, BiCGSTAB to 1e-8 from x0=0")
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == kernel and parts[1] == "C1":
+            return float(parts[2])
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl" if os.environ.get("HBX_BENCH_BACKEND", "nccl") == "nccl" else "gloo",
+                                timeout=timedelta(seconds=300))
+    return world, rank, local
+
+
+def reduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def vector_bytes_per_iteration(n: int) -> int:
+    """HBM bytes of the vector traffic of one iteration launch besides the two
+    H-matvecs: p update (r, p, Ap read, p write), rh.Ap, t = r - alpha Ap,
+    At.t / At.At, u and r updates with rh.r / r.r."""
+    return 8 * n * (4 + 2 + 3 + 2 + 8)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from hacapk_b200 import configs
+    from hacapk_b200.engine import Engine
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    t0 = time.time()
+    H, b = configs.c1(args.level)
+    t_build = time.time() - t0
+    E = Engine(H.st, H.nd)
+    info = E.info
+    n = H.nd
+    stream = torch.cuda.current_stream(dev)
+    s = stream.cuda_stream
+    bd = torch.from_numpy(b).to(dev)
+    ud = torch.zeros(n, dtype=torch.float64, device=dev)
+    # ---- warm-up solves (untimed)
+    for _ in range(max(args.warmup, 3)):
+        ud.zero_()
+        E.bicgstab_dev(bd.data_ptr(), ud.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
+    torch.cuda.synchronize(dev)
+    # ---- timed region: K device-resident solves
+    clocks = Clocks(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    infos = []
+    for _ in range(args.steps):
+        ud.zero_()
+        infos.append(E.bicgstab_dev(bd.data_ptr(), ud.data_ptr(), tol=args.tol, max_iter=args.max_iter,
+                                    stream=s))
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = reduce_max(ms, world)
+    iters = infos[-1]["iterations"]
+    launches = int(sum(i["launches"] for i in infos)) + args.steps  # + the u.zero_() memsets are torch's
+    # ---- e2e: the same solve through the host-vector C-ABI call
+    b_host = torch.from_numpy(b).pin_memory().numpy()
+    u_host = torch.zeros(n, dtype=torch.float64).pin_memory().numpy()
+    E.bicgstab_host(b_host, u_host, tol=args.tol, max_iter=args.max_iter)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    te0 = time.perf_counter()
+    for _ in range(args.steps):
+        u_host[:] = 0.0
+        u_sol, inf_h = E.bicgstab_host(b_host, u_host, tol=args.tol, max_iter=args.max_iter)
+    torch.cuda.synchronize(dev)
+    e2e_s = (time.perf_counter() - te0) / args.steps
+    e2e_s = reduce_max(e2e_s, world)
+    # ---- iteration-kernel roofline (device time of the iteration launches)
+    it_s = sum(i["iter_kernel_seconds"] for i in infos)
+    it_n = sum(i["iterations"] for i in infos)
+    per_iter_s = it_s / max(1, it_n)
+    bytes_iter = 2 * info["alg_bytes"] + vector_bytes_per_iteration(n)
+    peak, peak_kind = peaks()
+    achieved = bytes_iter / per_iter_s / 1e9
+    # ---- standalone H-matvec throughput (secondary metric)
+    x = torch.randn(n, dtype=torch.float64, device=dev)
+    y = torch.empty_like(x)
+    for _ in range(5):
+        E.matvec_dev(x.data_ptr(), y.data_ptr(), stream=s)
+    torch.cuda.synchronize(dev)
+    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 50
+    m0.record(stream)
+    for _ in range(reps):
+        E.matvec_dev(x.data_ptr(), y.data_ptr(), stream=s)
+    m1.record(stream)
+    torch.cuda.synchronize(dev)
+    E.sync(s)
+    mv_us = m0.elapsed_time(m1) / reps * 1e3
+    mv_gbs = info["alg_bytes"] / (mv_us * 1e-6) / 1e9
+    out = {
+        "metric": METRIC,
+        "value": ms / 1e3,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded icosphere mesh and rhs)",
+        "config": {
+            "workload": WORKLOAD,
+            "n": n,
+            "iterations": iters,
+            "true_relres": infos[-1]["true_relres"],
+            "h_alg_bytes": info["alg_bytes"],
+            "dense_words": info["dense_words"],
+            "lowrank_words": info["lowrank_words"],
+            "l2": "inputs larger than L2: the packed H-matrix is %.0f MB > 126 MB" % (info["stream_bytes"] / 1e6),
+            "parallelism": "replicas" if world > 1 else "1 GPU",
+            "build_seconds": t_build,
+            "setup_seconds": info["setup_seconds"],
+        },
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n},
+        "hmatvec": {"us": mv_us, "gbs": mv_gbs, "frac_of_" + peak_kind + "_peak": mv_gbs / peak},
+        "roofline": {
+            "kernel": "k_bicg_iter (one BiCGSTAB step: 2 H-matvecs + vector updates + dots)",
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": ncu_traffic("k_bicg_iter"),
+            "alg_bytes_per_launch": bytes_iter,
+            "avg_launch_us": per_iter_s * 1e6,
+        },
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(H, b, args)
+    return out
+
+
+def cpu_baseline(H, b, args):
+    """The compiled reference CPU H-matvec (HACApK_MAGMA.c:5-57, one thread as
+    written) inside the BiCGSTAB of HACApK_SOLVER.c:254-417: one full solve."""
+    import oracle
+    kind = "ref" if oracle.have_ref() else "restated"
+    t0 = time.perf_counter()
+    u, n, hist, mv_s = oracle.bicgstab(H.st, b, tol=args.tol, max_iter=args.max_iter, kind=kind)
+    dt = time.perf_counter() - t0
+    return {"value": dt, "unit": "s", "cores": 1, "kind": "reference" if kind == "ref" else "port",
+            "sample": f"one full C1 solve on the host: {n} iterations, matvec time {mv_s:.2f} s",
+            "iterations": n}
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the reference's own CPU path on the host cores."""
+    if rank != 0:
+        return None
+    from hacapk_b200 import configs
+    import oracle
+    H, b = configs.c1(args.level)
+    kind = "ref" if oracle.have_ref() else "restated"
+    for _ in range(args.warmup):
+        oracle.bicgstab(H.st, b, tol=args.tol, max_iter=args.max_iter, kind=kind)
+    times, n = [], 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, n, _, _ = oracle.bicgstab(H.st, b, tol=args.tol, max_iter=args.max_iter, kind=kind)
+        times.append(time.perf_counter() - t0)
+    v = float(np.mean(times))
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded icosphere mesh and rhs)",
+        "config": {"workload": WORKLOAD, "n": H.nd, "iterations": n},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": 1,
+                         "kind": "reference" if kind == "ref" else "port",
+                         "sample": "full C1 solves: compiled HACApK_MAGMA.c CPU matvec (one thread, as written) "
+                                   "in the BiCGSTAB of HACApK_SOLVER.c:254-417"},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--level", type=int, default=5)
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--max-iter", type=int, default=2000)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        out = run_reference(args, world, rank)
+    else:
+        out = run_ours(args, world, rank, local)
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,674 @@
+// hbx_api.cu -- the hbx_* C API and the HACApK drop-in entry points.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/hacapk_b200.h"
+#include "hbx_engine.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int status, const std::string &msg) {
+  g_last_error = msg;
+  return status;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  return fail(e == cudaErrorMemoryAllocation ? HBX_ERR_NOMEM : HBX_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define HBX_CUDA(call)                               \
+  do {                                               \
+    cudaError_t e_ = (call);                         \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+void free_engine(hbx_hmat *h) {
+  if (!h) return;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != h->device) cudaSetDevice(h->device);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  cudaFree(h->d_stream);
+  cudaFree(h->d_terms);
+  cudaFree(h->d_runs);
+  cudaFree(h->d_ctas);
+  cudaFree(h->d_atoms);
+  cudaFree(h->d_zbu);
+  cudaFree(h->d_gbar);
+  cudaFree(h->d_err);
+  cudaFree(h->d_prof);
+  cudaFree(h->d_x);
+  cudaFree(h->d_y);
+  cudaFree(h->d_work);
+  cudaFree(h->d_part);
+  cudaFree(h->d_dot);
+  cudaFree(h->d_state);
+  cudaFree(h->d_hist);
+  if (h->h_pin) cudaFreeHost(h->h_pin);
+  if (h->h_state) cudaFreeHost(h->h_state);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->ev2) cudaEventDestroy(h->ev2);
+  if (h->ev3) cudaEventDestroy(h->ev3);
+  if (h->ev4) cudaEventDestroy(h->ev4);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  if (cur >= 0 && cur != h->device) cudaSetDevice(cur);
+  delete h;
+}
+
+// Reads and clears the device error word; resets the grid barrier after a
+// failure so the next launch starts from a clean state.
+int check_device_error(hbx_hmat *h, cudaStream_t s) {
+  int err = 0;
+  cudaError_t e = cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "device error readback");
+  if (err != 0) {
+    cudaMemsetAsync(h->d_err, 0, sizeof(int), s);
+    cudaMemsetAsync(h->d_gbar, 0, 2 * sizeof(unsigned), s);
+    cudaStreamSynchronize(s);
+    return fail(HBX_ERR_TIMEOUT, "a bounded device wait expired (error bits " + std::to_string(err) + ")");
+  }
+  return HBX_OK;
+}
+
+hbx::MatvecArgs matvec_args(hbx_hmat *h, double alpha, const double *x, double beta, const double *yin, double *y) {
+  hbx::MatvecArgs a{};
+  a.stream = h->d_stream;
+  a.terms = h->d_terms;
+  a.runs = h->d_runs;
+  a.ctas = h->d_ctas;
+  a.x = x;
+  a.yin = yin;
+  a.y = y;
+  a.zbu = h->d_zbu;
+  a.alpha = alpha;
+  a.beta = beta;
+  a.gbar = h->d_gbar;
+  a.err = h->d_err;
+  a.timeout_ns = h->timeout_ns;
+  a.prof = h->d_prof;
+  return a;
+}
+
+int ensure_host_staging(hbx_hmat *h) {
+  const size_t n = (size_t)h->plan.nd;
+  if (!h->d_x) HBX_CUDA(cudaMalloc(&h->d_x, n * sizeof(double)));
+  if (!h->d_y) HBX_CUDA(cudaMalloc(&h->d_y, n * sizeof(double)));
+  if (!h->h_pin) HBX_CUDA(cudaHostAlloc(&h->h_pin, 2 * n * sizeof(double), cudaHostAllocDefault));
+  return HBX_OK;
+}
+
+int ensure_solver(hbx_hmat *h, int max_iter) {
+  const size_t n = (size_t)h->plan.nd;
+  if (!h->d_work) HBX_CUDA(cudaMalloc(&h->d_work, 8 * n * sizeof(double)));
+  if (!h->d_part) HBX_CUDA(cudaMalloc(&h->d_part, (size_t)h->num_ctas * hbx::kSlots * 2 * sizeof(double)));
+  if (!h->d_dot) HBX_CUDA(cudaMalloc(&h->d_dot, 4 * sizeof(double)));
+  if (!h->d_state) HBX_CUDA(cudaMalloc(&h->d_state, sizeof(hbx::BicgState)));
+  if (!h->h_state) HBX_CUDA(cudaHostAlloc(&h->h_state, sizeof(hbx::BicgState), cudaHostAllocDefault));
+  if (h->hist_cap < max_iter + 1) {
+    cudaFree(h->d_hist);
+    h->d_hist = nullptr;
+    HBX_CUDA(cudaMalloc(&h->d_hist, (size_t)(max_iter + 1) * sizeof(double)));
+    h->hist_cap = max_iter + 1;
+  }
+  return HBX_OK;
+}
+
+std::mutex g_table_mu;
+std::unordered_map<const void *, hbx_hmat *> g_table;
+
+}  // namespace
+
+extern "C" {
+
+const char *hbx_status_string(int status) {
+  switch (status) {
+    case HBX_OK: return "HBX_OK";
+    case HBX_ERR_INVALID: return "HBX_ERR_INVALID";
+    case HBX_ERR_NOMEM: return "HBX_ERR_NOMEM";
+    case HBX_ERR_CUDA: return "HBX_ERR_CUDA";
+    case HBX_ERR_TIMEOUT: return "HBX_ERR_TIMEOUT";
+    case HBX_ERR_BREAKDOWN: return "HBX_ERR_BREAKDOWN";
+    case HBX_ERR_NOT_CONVERGED: return "HBX_ERR_NOT_CONVERGED";
+    case HBX_ERR_NONFINITE: return "HBX_ERR_NONFINITE";
+    case HBX_ERR_UNSUPPORTED: return "HBX_ERR_UNSUPPORTED";
+    default: return "HBX_ERR_UNKNOWN";
+  }
+}
+
+const char *hbx_last_error(void) { return g_last_error.c_str(); }
+
+int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hbx_hmat **out) {
+  if (!out) return fail(HBX_ERR_INVALID, "hbx_create: out is NULL");
+  *out = nullptr;
+  if (!st) return fail(HBX_ERR_INVALID, "hbx_create: container is NULL");
+  if (nd <= 0) return fail(HBX_ERR_INVALID, "hbx_create: nd <= 0");
+  if (opt && opt->precision != HBX_FP64) return fail(HBX_ERR_UNSUPPORTED, "hbx_create: only HBX_FP64 is supported");
+  const double t0 = now_s();
+  hbx_hmat *h = new (std::nothrow) hbx_hmat();
+  if (!h) return fail(HBX_ERR_NOMEM, "hbx_create: host allocation");
+  auto bail = [&](int st_) { free_engine(h); return st_; };
+  cudaError_t e;
+  if ((e = cudaGetDevice(&h->device)) != cudaSuccess) return bail(cuda_fail(e, "cudaGetDevice"));
+  cudaDeviceProp prop;
+  if ((e = cudaGetDeviceProperties(&prop, h->device)) != cudaSuccess) return bail(cuda_fail(e, "cudaGetDeviceProperties"));
+  if (prop.major < 10) return bail(fail(HBX_ERR_UNSUPPORTED, "hbx_create: needs an sm_100 device"));
+  if ((e = hbx::configure_kernels()) != cudaSuccess) return bail(cuda_fail(e, "configure_kernels"));
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->device);
+  if (!coop) return bail(fail(HBX_ERR_UNSUPPORTED, "hbx_create: device lacks cooperative launch"));
+  const int max_ctas = prop.multiProcessorCount;  // one CTA per SM (shared-memory bound)
+  int nc = (opt && opt->num_ctas > 0) ? opt->num_ctas : max_ctas;
+  if (nc > max_ctas) return bail(fail(HBX_ERR_INVALID, "hbx_create: num_ctas exceeds co-resident CTAs"));
+  h->num_ctas = nc;
+  const char *tmo = std::getenv("HBX_TIMEOUT_MS");
+  if (tmo) h->timeout_ns = (unsigned long long)(std::atof(tmo) * 1e6);
+  const char *prof = std::getenv("HBX_PROFILE");
+  if (prof && std::atoi(prof) > 0) {
+    if ((e = cudaMalloc(&h->d_prof, (size_t)nc * 8 * sizeof(unsigned long long))) != cudaSuccess)
+      return bail(cuda_fail(e, "cudaMalloc(prof)"));
+    cudaMemset(h->d_prof, 0, (size_t)nc * 8 * sizeof(unsigned long long));
+  }
+
+  std::string err;
+  int st_plan = hbx::make_plan(st, nd, nc, h->plan, err);
+  if (st_plan != HBX_OK) return bail(fail(st_plan, "hbx_create: " + err));
+  const hbx::Plan &P = h->plan;
+
+  std::vector<uint8_t> host;
+  try {
+    host.resize(P.total_bytes);
+  } catch (...) {
+    return bail(fail(HBX_ERR_NOMEM, "hbx_create: host staging buffer"));
+  }
+  hbx::pack_plan(st, P, host.data());
+
+  if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(cuda_fail(e, "stream"));
+  cudaEventCreate(&h->ev0);
+  cudaEventCreate(&h->ev1);
+  cudaEventCreate(&h->ev2);
+  cudaEventCreate(&h->ev3);
+  cudaEventCreate(&h->ev4);
+  if ((e = cudaMalloc(&h->d_stream, P.total_bytes)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(stream)"));
+  if ((e = cudaMalloc(&h->d_terms, std::max<size_t>(1, P.terms.size()) * sizeof(hbx::Term))) != cudaSuccess)
+    return bail(cuda_fail(e, "cudaMalloc(terms)"));
+  if ((e = cudaMalloc(&h->d_runs, std::max<size_t>(1, P.runs.size()) * sizeof(hbx::Run))) != cudaSuccess)
+    return bail(cuda_fail(e, "cudaMalloc(runs)"));
+  if ((e = cudaMalloc(&h->d_ctas, P.ctas.size() * sizeof(hbx::CtaInfo))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(ctas)"));
+  if ((e = cudaMalloc(&h->d_atoms, std::max<size_t>(1, P.atoms.size()) * sizeof(hbx::Atom))) != cudaSuccess)
+    return bail(cuda_fail(e, "cudaMalloc(atoms)"));
+  if ((e = cudaMalloc(&h->d_zbu, std::max<uint64_t>(1, P.zbu_len) * sizeof(double))) != cudaSuccess)
+    return bail(cuda_fail(e, "cudaMalloc(zbu)"));
+  if ((e = cudaMalloc(&h->d_gbar, 4 * sizeof(unsigned))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(gbar)"));
+  if ((e = cudaMalloc(&h->d_err, sizeof(int))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(err)"));
+  if ((e = cudaMemcpy(h->d_stream, host.data(), P.total_bytes, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return bail(cuda_fail(e, "upload stream"));
+  if (!P.terms.empty() &&
+      (e = cudaMemcpy(h->d_terms, P.terms.data(), P.terms.size() * sizeof(hbx::Term), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return bail(cuda_fail(e, "upload terms"));
+  if (!P.runs.empty() &&
+      (e = cudaMemcpy(h->d_runs, P.runs.data(), P.runs.size() * sizeof(hbx::Run), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return bail(cuda_fail(e, "upload runs"));
+  if ((e = cudaMemcpy(h->d_ctas, P.ctas.data(), P.ctas.size() * sizeof(hbx::CtaInfo), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return bail(cuda_fail(e, "upload ctas"));
+  if (!P.atoms.empty() &&
+      (e = cudaMemcpy(h->d_atoms, P.atoms.data(), P.atoms.size() * sizeof(hbx::Atom), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return bail(cuda_fail(e, "upload atoms"));
+  cudaMemset(h->d_gbar, 0, 4 * sizeof(unsigned));
+  cudaMemset(h->d_err, 0, sizeof(int));
+  cudaMemset(h->d_zbu, 0, std::max<uint64_t>(1, P.zbu_len) * sizeof(double));
+  if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(cuda_fail(e, "hbx_create sync"));
+  // the term list stays on the host only for hbx_get_info
+  h->plan.terms.clear();
+  h->plan.terms.shrink_to_fit();
+  h->plan.runs.clear();
+  h->plan.runs.shrink_to_fit();
+  h->setup_seconds = now_s() - t0;
+  *out = h;
+  return HBX_OK;
+}
+
+int hbx_destroy(hbx_hmat *h) {
+  if (!h) return fail(HBX_ERR_INVALID, "hbx_destroy: NULL handle");
+  free_engine(h);
+  return HBX_OK;
+}
+
+// Diagnostics: copies the per-CTA phase stamps of the last k_matvec
+// (HBX_PROFILE=1 at create time) into out[num_ctas*8]; returns the count.
+int hbx_debug_phase_stamps(hbx_hmat *h, unsigned long long *out, int cap) {
+  if (!h || !out || !h->d_prof) return 0;
+  const int n = std::min(cap, h->num_ctas * 8);
+  cudaDeviceSynchronize();
+  cudaMemcpy(out, h->d_prof, (size_t)n * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+  return n;
+}
+
+int hbx_get_info(const hbx_hmat *h, hbx_info *info) {
+  if (!h || !info) return fail(HBX_ERR_INVALID, "hbx_get_info: NULL argument");
+  std::memset(info, 0, sizeof(*info));
+  const hbx::Plan &P = h->plan;
+  info->nd = P.nd;
+  info->nlf = P.nlf;
+  info->nlfkt = P.nlfkt;
+  info->ktmax = P.ktmax;
+  info->num_ctas = h->num_ctas;
+  info->num_atoms = (int)P.atoms.size();
+  uint64_t nt = 0;
+  for (const auto &c : P.ctas) nt += c.n_p + c.n_d + c.n_u;
+  info->num_terms = (int)nt;
+  info->precision = HBX_FP64;
+  uint64_t sb = 0;
+  for (const auto &c : P.ctas) sb += c.stream_bytes;
+  info->stream_bytes = (long long)sb;
+  info->alg_bytes = (long long)P.alg_bytes;
+  info->alg_flops = (long long)P.alg_flops;
+  info->zbu_len = (long long)P.zbu_len;
+  info->dense_words = (long long)P.dense_words;
+  info->lowrank_words = (long long)P.lowrank_words;
+  info->setup_seconds = h->setup_seconds;
+  return HBX_OK;
+}
+
+int hbx_matvec(hbx_hmat *h, double alpha, const double *x, double beta, const double *yin, double *y, void *stream) {
+  if (!h || !x || !y) return fail(HBX_ERR_INVALID, "hbx_matvec: NULL argument");
+  if (beta != 0.0 && !yin) return fail(HBX_ERR_INVALID, "hbx_matvec: beta != 0 needs yin");
+  cudaError_t e = hbx::launch_matvec(matvec_args(h, alpha, x, beta, yin, y), h->num_ctas, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "hbx_matvec launch");
+  return HBX_OK;
+}
+
+int hbx_sync(hbx_hmat *h, void *stream) {
+  if (!h) return fail(HBX_ERR_INVALID, "hbx_sync: NULL handle");
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "hbx_sync");
+  return check_device_error(h, (cudaStream_t)stream);
+}
+
+int hbx_matvec_host(hbx_hmat *h, const double *zu, double *zau, int accumulate, double *kernel_seconds,
+                    double *copy_seconds) {
+  if (!h || !zu || !zau) return fail(HBX_ERR_INVALID, "hbx_matvec_host: NULL argument");
+  int st = ensure_host_staging(h);
+  if (st != HBX_OK) return st;
+  const size_t n = (size_t)h->plan.nd, bytes = n * sizeof(double);
+  cudaStream_t s = h->stream;
+  const double t0 = now_s();
+  HBX_CUDA(cudaMemcpyAsync(h->d_x, zu, bytes, cudaMemcpyHostToDevice, s));
+  if (accumulate) HBX_CUDA(cudaMemcpyAsync(h->d_y, zau, bytes, cudaMemcpyHostToDevice, s));
+  HBX_CUDA(cudaEventRecord(h->ev0, s));
+  HBX_CUDA(hbx::launch_matvec(matvec_args(h, 1.0, h->d_x, accumulate ? 1.0 : 0.0, h->d_y, h->d_y), h->num_ctas, s));
+  HBX_CUDA(cudaEventRecord(h->ev1, s));
+  HBX_CUDA(cudaMemcpyAsync(zau, h->d_y, bytes, cudaMemcpyDeviceToHost, s));
+  HBX_CUDA(cudaStreamSynchronize(s));
+  const double t1 = now_s();
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  if (kernel_seconds) *kernel_seconds += ms * 1e-3;
+  if (copy_seconds) *copy_seconds += (t1 - t0) - ms * 1e-3;
+  return check_device_error(h, s);
+}
+
+static hbx::BicgArgs bicg_args(hbx_hmat *h, const double *b, double *u, double tol, int max_iter) {
+  const size_t n = (size_t)h->plan.nd;
+  hbx::BicgArgs a{};
+  a.stream = h->d_stream;
+  a.terms = h->d_terms;
+  a.runs = h->d_runs;
+  a.ctas = h->d_ctas;
+  a.atoms = h->d_atoms;
+  a.zbu = h->d_zbu;
+  a.gbar = h->d_gbar;
+  a.err = h->d_err;
+  a.timeout_ns = h->timeout_ns;
+  a.b = b;
+  a.u = u;
+  a.r = h->d_work;
+  a.rh = h->d_work + n;
+  a.p = h->d_work + 2 * n;
+  a.ap = h->d_work + 3 * n;
+  a.t = h->d_work + 4 * n;
+  a.at = h->d_work + 5 * n;
+  a.part = h->d_part;
+  a.state = h->d_state;
+  a.hist = h->d_hist;
+  a.tol = tol;
+  a.max_iter = max_iter;
+  return a;
+}
+
+// Captures `batch` iteration launches into one graph (re-captured when the
+// vectors or the stopping parameters change).
+static int get_graph(hbx_hmat *h, const hbx::BicgArgs &a, int batch) {
+  const void *key[4] = {a.b, a.u, (const void *)(uintptr_t)a.max_iter, nullptr};
+  double tolkey = a.tol;
+  std::memcpy(&key[3], &tolkey, sizeof(double));
+  if (h->graph && h->graph_batch == batch && std::memcmp(key, h->graph_key, sizeof(key)) == 0) return HBX_OK;
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  cudaStream_t s = h->stream;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return HBX_ERR_CUDA;
+  for (int i = 0; i < batch; ++i) hbx::launch_bicg_iter(a, h->num_ctas, s);
+  cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (e != cudaSuccess || !g) {
+    cudaGetLastError();
+    return HBX_ERR_CUDA;
+  }
+  e = cudaGraphInstantiate(&h->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    h->graph = nullptr;
+    return HBX_ERR_CUDA;
+  }
+  h->graph_batch = batch;
+  std::memcpy(h->graph_key, key, sizeof(key));
+  return HBX_OK;
+}
+
+// BiCGSTAB on device vectors b, u (u: x0 in / solution out), all on h->stream.
+static int bicgstab_dev(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info) {
+  const double tol = opts ? opts->tol : 1e-8;
+  const int max_iter = opts ? opts->max_iter : 1000;
+  const int verbose = opts ? opts->verbose : 0;
+  int batch = (opts && opts->batch > 0) ? opts->batch : 8;
+  if (max_iter < 0 || !(tol >= 0.0)) return fail(HBX_ERR_INVALID, "hbx_bicgstab: bad tol or max_iter");
+  int st = ensure_solver(h, max_iter);
+  if (st != HBX_OK) return st;
+  cudaStream_t s = h->stream;
+  const hbx::BicgArgs a = bicg_args(h, b, u, tol, max_iter);
+  HBX_CUDA(cudaEventRecord(h->ev0, s));
+  // r = b - H u  (HACApK_SOLVER.c:562-573)
+  HBX_CUDA(hbx::launch_matvec(matvec_args(h, -1.0, u, 1.0, b, a.r), h->num_ctas, s));
+  HBX_CUDA(hbx::launch_bicg_setup(a, h->num_ctas, s));
+  const bool use_graph = get_graph(h, a, batch) == HBX_OK;
+  int launched = 0;
+  double iter_s = 0.0;
+  for (;;) {
+    HBX_CUDA(cudaEventRecord(h->ev3, s));
+    if (use_graph) {
+      HBX_CUDA(cudaGraphLaunch(h->graph, s));
+    } else {
+      for (int i = 0; i < batch; ++i) HBX_CUDA(hbx::launch_bicg_iter(a, h->num_ctas, s));
+    }
+    HBX_CUDA(cudaEventRecord(h->ev4, s));
+    launched += batch;
+    HBX_CUDA(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(hbx::BicgState), cudaMemcpyDeviceToHost, s));
+    HBX_CUDA(cudaStreamSynchronize(s));
+    float bms = 0.f;
+    cudaEventElapsedTime(&bms, h->ev3, h->ev4);
+    iter_s += bms * 1e-3;
+    if (h->h_state->done || launched > max_iter + batch) break;
+    int derr = 0;
+    HBX_CUDA(cudaMemcpy(&derr, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (derr) break;
+  }
+  HBX_CUDA(cudaEventRecord(h->ev1, s));
+  const hbx::BicgState S = *h->h_state;
+  // true residual ||b - H u|| (HACApK_SOLVER.c:737-746)
+  HBX_CUDA(hbx::launch_matvec(matvec_args(h, -1.0, u, 1.0, b, a.t), h->num_ctas, s));
+  HBX_CUDA(hbx::launch_dot(a, a.t, a.t, hbx::kSlotAux, h->d_dot, h->num_ctas, s));
+  double tr2 = 0.0;
+  HBX_CUDA(cudaMemcpyAsync(&tr2, h->d_dot, sizeof(double), cudaMemcpyDeviceToHost, s));
+  HBX_CUDA(cudaStreamSynchronize(s));
+  int dst = check_device_error(h, s);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  if (info) {
+    std::memset(info, 0, sizeof(*info));
+    info->iterations = S.iter;
+    info->status = dst != HBX_OK ? dst : S.status;
+    info->bnorm = S.bnorm;
+    info->relres = S.relres;
+    info->true_relres = S.bnorm > 0 ? std::sqrt(tr2) / S.bnorm : std::sqrt(tr2);
+    info->seconds = ms * 1e-3;
+    info->iter_kernel_seconds = iter_s;
+    info->iter_launches = launched;
+    info->launches = launched + 5;  // r0 matvec, setup, residual matvec, two dot kernels
+  }
+  if (verbose > 0) {
+    std::vector<double> hist(S.iter + 1, 0.0);
+    if (S.iter > 0) cudaMemcpy(hist.data(), h->d_hist, S.iter * sizeof(double), cudaMemcpyDeviceToHost);
+    hist[S.iter] = S.relres;
+    std::printf("\n ** BICG (B200 persistent kernel) **\n");
+    std::printf("\nOriginal relative residual norm = %.2e\n", hist[0]);
+    for (int i = 1; i <= S.iter; ++i) std::printf(" %d: log10(zrnorm/bnorm)=%.2e\n", i, std::log10(hist[i]));
+    std::printf("       BiCG        = %.5e\n", ms * 1e-3);
+    std::printf(" resnorm=%.2e\n", std::sqrt(tr2));
+    std::fflush(stdout);
+  }
+  if (dst != HBX_OK) return dst;
+  if (!S.done) return fail(HBX_ERR_NOT_CONVERGED, "hbx_bicgstab: iteration limit");
+  if (S.status != HBX_OK) return fail(S.status, std::string("hbx_bicgstab: ") + hbx_status_string(S.status));
+  return HBX_OK;
+}
+
+int hbx_bicgstab(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info,
+                 void *stream) {
+  if (!h || !b || !u) return fail(HBX_ERR_INVALID, "hbx_bicgstab: NULL argument");
+  cudaStream_t us = (cudaStream_t)stream;
+  HBX_CUDA(cudaEventRecord(h->ev2, us));
+  HBX_CUDA(cudaStreamWaitEvent(h->stream, h->ev2, 0));
+  int st = bicgstab_dev(h, b, u, opts, info);
+  cudaEventRecord(h->ev2, h->stream);
+  cudaStreamWaitEvent(us, h->ev2, 0);
+  return st;
+}
+
+int hbx_bicgstab_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info) {
+  if (!h || !b || !u) return fail(HBX_ERR_INVALID, "hbx_bicgstab_host: NULL argument");
+  const int max_iter = opts ? opts->max_iter : 1000;
+  int st = ensure_solver(h, max_iter < 0 ? 0 : max_iter);
+  if (st != HBX_OK) return st;
+  const size_t n = (size_t)h->plan.nd, bytes = n * sizeof(double);
+  double *db = h->d_work + 6 * n, *du = h->d_work + 7 * n;
+  cudaStream_t s = h->stream;
+  HBX_CUDA(cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, s));
+  HBX_CUDA(cudaMemcpyAsync(du, u, bytes, cudaMemcpyHostToDevice, s));
+  st = bicgstab_dev(h, db, du, opts, info);
+  cudaError_t e = cudaMemcpyAsync(u, du, bytes, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "hbx_bicgstab_host copy-out");
+  return st;
+}
+
+// ------------------------------------------------------------------------
+// HACApK drop-in entry points
+// ------------------------------------------------------------------------
+
+static hbx_hmat *lookup(const stc_HACApK_leafmtxp *st) {
+  std::lock_guard<std::mutex> lk(g_table_mu);
+  auto it = g_table.find(st);
+  return it == g_table.end() ? nullptr : it->second;
+}
+
+static hbx_hmat *create_for(stc_HACApK_leafmtxp *st, int nd) {
+  hbx_hmat *h = nullptr;
+  int rc = hbx_create(st, nd, nullptr, &h);
+  if (rc != HBX_OK) {
+    std::fprintf(stderr, "!!!! hacapk_b200: setup failed: %s (%s)\n", hbx_status_string(rc), hbx_last_error());
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(g_table_mu);
+  auto it = g_table.find(st);
+  if (it != g_table.end()) hbx_destroy(it->second);
+  g_table[st] = h;
+  return h;
+}
+
+static void release_for(stc_HACApK_leafmtxp *st) {
+  hbx_hmat *h = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_table_mu);
+    auto it = g_table.find(st);
+    if (it == g_table.end()) return;
+    h = it->second;
+    g_table.erase(it);
+  }
+  hbx_destroy(h);
+}
+
+void magma_init_(void) { cudaFree(nullptr); }
+
+void magma_finalize_(void) {}
+
+void c_hacapk_adot_body_lfcpy_batch_sorted_(int *nd, stc_HACApK_leafmtxp *st_leafmtxp) {
+  if (!nd || !st_leafmtxp) return;
+  create_for(st_leafmtxp, *nd);
+}
+
+void c_hacapk_adot_body_lfmtx_batch_(double *zau, stc_HACApK_leafmtxp *st_leafmtxp, double *zu, double *zbu,
+                                     double *time_batch, double *time_set, double *time_copy) {
+  (void)zbu;
+  (void)time_set;
+  if (!st_leafmtxp || !zau || !zu) return;
+  hbx_hmat *h = lookup(st_leafmtxp);
+  if (!h) h = create_for(st_leafmtxp, st_leafmtxp->nd);
+  if (!h) return;
+  int rc = hbx_matvec_host(h, zu, zau, 1, time_batch, time_copy);
+  if (rc != HBX_OK)
+    std::fprintf(stderr, "!!!! hacapk_b200: matvec failed: %s (%s)\n", hbx_status_string(rc), hbx_last_error());
+}
+
+void c_hacapk_adot_body_lfdel_batch_(stc_HACApK_leafmtxp *st_leafmtxp) { release_for(st_leafmtxp); }
+
+void c_hacapk_adot_body_lfcpy_gpu_(int *nd, stc_HACApK_leafmtxp *st_leafmtxp) {
+  c_hacapk_adot_body_lfcpy_batch_sorted_(nd, st_leafmtxp);
+}
+
+void c_hacapk_adot_body_lfmtx_gpu_(double *zau, stc_HACApK_leafmtxp *st_leafmtxp, double *zu, double *zbu) {
+  c_hacapk_adot_body_lfmtx_batch_(zau, st_leafmtxp, zu, zbu, nullptr, nullptr, nullptr);
+}
+
+void c_hacapk_adot_body_lfdel_gpu_(stc_HACApK_leafmtxp *st_leafmtxp) { release_for(st_leafmtxp); }
+
+static int ctl_nrank(const stc_HACApK_lcontrol *ctl) {
+  if (!ctl || !ctl->param) return 1;
+  const int *lpmd = reinterpret_cast<const int *>(reinterpret_cast<const char *>(ctl->param) + ctl->lpmd_offset);
+  return lpmd[1];
+}
+
+void c_hacapk_bicgstab_cax_lfmtx_gpu_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl, double *u,
+                                      double *b, double *param, int *nd, int *nstp, int *lrtrn) {
+  if (lrtrn) *lrtrn = HBX_OK;
+  if (!st_leafmtxp || !u || !b || !param || !nd) {
+    if (lrtrn) *lrtrn = HBX_ERR_INVALID;
+    return;
+  }
+  if (ctl_nrank(st_ctl) > 1) {
+    std::fprintf(stderr, "!!!! hacapk_b200: one MPI rank per solve only (nrank=%d)\n", ctl_nrank(st_ctl));
+    if (lrtrn) *lrtrn = HBX_ERR_UNSUPPORTED;
+    return;
+  }
+  hbx_hmat *h = lookup(st_leafmtxp);
+  const bool own = (h == nullptr);
+  if (own) h = create_for(st_leafmtxp, *nd);
+  if (!h) {
+    if (lrtrn) *lrtrn = HBX_ERR_CUDA;
+    return;
+  }
+  hbx_solve_opts o{};
+  o.tol = param[90];
+  o.max_iter = (int)param[82];
+  o.verbose = param[0] > 0 ? 1 : 0;
+  hbx_solve_info info{};
+  int rc = hbx_bicgstab_host(h, b, u, &o, &info);
+  if (nstp) *nstp = info.iterations;
+  if (lrtrn) *lrtrn = rc;
+  if (own) release_for(st_leafmtxp);
+}
+
+// Host-vector BiCGSTAB with one GPU matvec per product (HACApK_SOLVER.c:254-417).
+void c_hacapk_bicgstab_cax_lfmtx_flat_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl, double *u,
+                                       double *b, double *param, int *nd, int *nstp, int *lrtrn) {
+  if (lrtrn) *lrtrn = HBX_OK;
+  if (!st_leafmtxp || !u || !b || !param || !nd || *nd <= 0) {
+    if (lrtrn) *lrtrn = HBX_ERR_INVALID;
+    return;
+  }
+  if (ctl_nrank(st_ctl) > 1) {
+    if (lrtrn) *lrtrn = HBX_ERR_UNSUPPORTED;
+    return;
+  }
+  hbx_hmat *h = lookup(st_leafmtxp);
+  const bool own = (h == nullptr);
+  if (own) h = create_for(st_leafmtxp, *nd);
+  if (!h) {
+    if (lrtrn) *lrtrn = HBX_ERR_CUDA;
+    return;
+  }
+  const int n = *nd, mstep = (int)param[82];
+  const double eps = param[90];
+  std::vector<double> zr(n), zshdw(n), zp(n), zt(n), zkp(n), zakp(n), zkt(n), zakt(n);
+  auto dot = [&](const std::vector<double> &x, const std::vector<double> &y) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s += x[i] * y[i];
+    return s;
+  };
+  auto mv = [&](const double *x, std::vector<double> &y) {
+    std::fill(y.begin(), y.end(), 0.0);
+    int rc = hbx_matvec_host(h, x, y.data(), 0, nullptr, nullptr);
+    if (rc != HBX_OK && lrtrn) *lrtrn = rc;
+  };
+  double alpha = 0.0, beta = 0.0, zeta = 0.0, znorm, zden, znormold = 1.0;
+  const double bnorm = std::sqrt(dot(std::vector<double>(b, b + n), std::vector<double>(b, b + n)));
+  for (int i = 0; i < n; ++i) zr[i] = b[i];
+  mv(u, zshdw);
+  for (int i = 0; i < n; ++i) zr[i] -= zshdw[i];
+  zshdw = zr;
+  double zrnorm = std::sqrt(dot(zr, zr));
+  int steps = 0;
+  for (int step = 1; step <= mstep; ++step) {
+    if (zrnorm / bnorm < eps) break;
+    if (beta == 0.0) {
+      zp = zr;
+    } else {
+      for (int i = 0; i < n; ++i) zp[i] = (zp[i] + zeta * zakp[i]) * beta + zr[i];
+    }
+    zkp = zp;
+    mv(zkp.data(), zakp);
+    znorm = dot(zshdw, zr);
+    zden = dot(zshdw, zakp);
+    alpha = -znorm / zden;
+    znormold = znorm;
+    for (int i = 0; i < n; ++i) zt[i] = zr[i] + alpha * zakp[i];
+    alpha = -alpha;
+    zkt = zt;
+    mv(zkt.data(), zakt);
+    znorm = dot(zakt, zt);
+    zden = dot(zakt, zakt);
+    zeta = znorm / zden;
+    for (int i = 0; i < n; ++i) u[i] = u[i] + alpha * zkp[i] + zeta * zkt[i];
+    zeta = -zeta;
+    for (int i = 0; i < n; ++i) zr[i] = zt[i] + zeta * zakt[i];
+    beta = dot(zshdw, zr);
+    zrnorm = std::sqrt(dot(zr, zr));
+    beta = -alpha / zeta * beta / znormold;
+    steps = step;
+    if (param[0] > 0) std::printf(" %d: log10(zrnorm/bnorm)=%.2e\n", step, std::log10(zrnorm / bnorm));
+  }
+  if (nstp) *nstp = steps;
+  if (own) release_for(st_leafmtxp);
+}
+
+}  // extern "C"

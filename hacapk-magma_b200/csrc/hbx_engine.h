@@ -1,0 +1,112 @@
+// hbx_engine.h -- engine state behind the opaque hbx_hmat handle, and the
+// kernel launchers shared by the hbx_* API and the HACApK drop-in symbols.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "hbx_plan.h"
+
+namespace hbx {
+
+// Partial-sum slots of the BiCGSTAB reductions (per CTA, compensated pairs).
+enum : int {
+  kSlotRhoR = 0,   // rh . r
+  kSlotRR = 1,     // r . r
+  kSlotRhAp = 2,   // rh . Ap
+  kSlotAtT = 3,    // At . t
+  kSlotAtAt = 4,   // At . At
+  kSlotBB = 5,     // b . b
+  kSlotAux = 6,    // scratch (true residual)
+  kSlots = 8
+};
+
+// Solver scalars carried from one iteration launch to the next.
+struct BicgState {
+  double alpha, zeta, rho, beta;
+  double relres, bnorm;
+  int iter, done, status, breakdown;
+};
+
+struct MatvecArgs {
+  const uint8_t *stream;
+  const Term *terms;
+  const Run *runs;
+  const CtaInfo *ctas;
+  const double *x;
+  const double *yin;
+  double *y;
+  double *zbu;
+  double alpha, beta;
+  unsigned *gbar;
+  int *err;
+  unsigned long long timeout_ns;
+  unsigned long long *prof;  // optional: per-CTA %globaltimer stamps [num_ctas][8]
+};
+
+struct BicgArgs {
+  const uint8_t *stream;
+  const Term *terms;
+  const Run *runs;
+  const CtaInfo *ctas;
+  const Atom *atoms;
+  double *zbu;
+  unsigned *gbar;
+  int *err;
+  unsigned long long timeout_ns;
+  const double *b;
+  double *u, *r, *rh, *p, *ap, *t, *at;
+  double *part;   // [num_ctas][kSlots][2]
+  BicgState *state;
+  double *hist;   // relres per iteration (max_iter + 1 entries)
+  double tol;
+  int max_iter;
+};
+
+// Kernel launchers (hbx_kernels.cu).
+size_t kernel_smem_bytes();
+cudaError_t configure_kernels();
+cudaError_t launch_matvec(const MatvecArgs &a, int num_ctas, cudaStream_t s);
+cudaError_t launch_bicg_setup(const BicgArgs &a, int num_ctas, cudaStream_t s);
+cudaError_t launch_bicg_iter(const BicgArgs &a, int num_ctas, cudaStream_t s);
+// part[.][slot] = sum over own rows of x.y; then out[0] = the total (one block).
+cudaError_t launch_dot(const BicgArgs &a, const double *x, const double *y, int slot, double *out,
+                       int num_ctas, cudaStream_t s);
+
+}  // namespace hbx
+
+struct hbx_hmat {
+  int device = 0;
+  int num_ctas = 0;
+  hbx::Plan plan;
+  uint8_t *d_stream = nullptr;
+  hbx::Term *d_terms = nullptr;
+  hbx::Run *d_runs = nullptr;
+  hbx::CtaInfo *d_ctas = nullptr;
+  hbx::Atom *d_atoms = nullptr;
+  double *d_zbu = nullptr;
+  unsigned *d_gbar = nullptr;
+  int *d_err = nullptr;
+  unsigned long long timeout_ns = 2000000000ull;
+  unsigned long long *d_prof = nullptr;  // phase stamps of the last matvec (HBX_PROFILE=1)
+  double setup_seconds = 0.0;
+  cudaStream_t stream = nullptr;  // used by the host-vector calls
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr, ev4 = nullptr;
+  // host-vector staging
+  double *d_x = nullptr, *d_y = nullptr;
+  double *h_pin = nullptr;        // pinned staging, 2*nd doubles
+  // solver workspace
+  double *d_work = nullptr;       // r, rh, p, ap, t, at, b, u  (8*nd)
+  double *d_part = nullptr;
+  double *d_dot = nullptr;
+  hbx::BicgState *d_state = nullptr;
+  hbx::BicgState *h_state = nullptr;  // pinned
+  double *d_hist = nullptr;
+  int hist_cap = 0;
+  // captured iteration batch
+  cudaGraphExec_t graph = nullptr;
+  int graph_batch = 0;
+  const void *graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
+};

@@ -1,0 +1,554 @@
+// hbx_kernels.cu -- persistent sm_100a kernels of the H-matvec / BiCGSTAB path.
+//
+// k_matvec      one H-matvec: y = alpha*H*x + beta*yin (HACApK_BATCH.c:47-255
+//               replaced: one launch instead of ceil(n/5000) vbatched GEMVs per
+//               phase, no atomics, no zeroing of zbu/zau).
+// k_bicg_setup  r = b - H u has been formed by k_matvec; sets rh = r, p = Ap = 0
+//               and the first reduction partials (HACApK_SOLVER.c:533-594).
+// k_bicg_iter   one BiCGSTAB step of HACApK_SOLVER.c:602-732 in one launch:
+//               both H-matvecs, the vector updates and all dot products, with
+//               compensated (Dot2) partial sums reduced in a fixed order.
+//
+// All kernels run one CTA per SM: 8 consumer warps + 1 producer warp.  The
+// producer streams the CTA's packed terms through a shared-memory ring with
+// cp.async.bulk; consumer warps own disjoint columns of every term (rotated
+// so the work stays balanced) and accumulate in registers.  Grid-wide
+// dependencies (zbu complete, dot products complete) use a bounded grid
+// barrier; the launch is cooperative so every CTA is resident.
+#include "hbx_device.cuh"
+#include "hbx_engine.h"
+
+namespace hbx {
+namespace {
+
+constexpr int NW = kConsumerWarps;
+constexpr int kConsumerThreads = NW * 32;
+
+struct Smem {
+  uint8_t *ring;
+  uint64_t *full, *empty;
+  double *red;    // [2][NW][32]
+  double *scal;   // 64 doubles
+  double *stage;  // [2][kStageCap]
+  uint8_t *desc;  // descriptor queue
+  uint64_t *dfull, *dempty;
+  uint64_t *hbar;
+  Run *hdr;
+};
+
+__device__ __forceinline__ Smem smem_layout(uint8_t *base) {
+  Smem s;
+  s.ring = base + SharedLayout::ring;
+  s.full = reinterpret_cast<uint64_t *>(base + SharedLayout::full);
+  s.empty = reinterpret_cast<uint64_t *>(base + SharedLayout::empty);
+  s.red = reinterpret_cast<double *>(base + SharedLayout::red);
+  s.scal = reinterpret_cast<double *>(base + SharedLayout::scal);
+  s.stage = reinterpret_cast<double *>(base + SharedLayout::stage);
+  s.desc = base + SharedLayout::desc;
+  s.dfull = reinterpret_cast<uint64_t *>(base + SharedLayout::dfull);
+  s.dempty = reinterpret_cast<uint64_t *>(base + SharedLayout::dempty);
+  s.hbar = reinterpret_cast<uint64_t *>(base + SharedLayout::hbar);
+  s.hdr = reinterpret_cast<Run *>(base + SharedLayout::hdr);
+  return s;
+}
+
+__device__ __forceinline__ void init_barriers(const Smem &s) {
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kRingChunks; ++i) {
+      mbar_init(&s.full[i], 1);
+      mbar_init(&s.empty[i], NW);
+    }
+    for (int i = 0; i < kDescSlots; ++i) {
+      mbar_init(&s.dfull[i], 1);
+      mbar_init(&s.dempty[i], NW);
+    }
+    mbar_init(s.hbar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+}
+
+// Cross-warp reduction of one atom (rows r0..r0+h-1): sum the 8 warp
+// partials in warp order.  mode 0: y = alpha*s + beta*yin;  mode 1: y += alpha*s.
+__device__ __forceinline__ uint32_t term_end(const Term &T) { return T.pos + T.nrow * T.ncol * 8u; }
+__device__ __forceinline__ uint32_t run_end(const Run &r) { return r.pos + r.nrow * r.ncol * 8u; }
+
+// Before a named barrier a warp gives back every ring chunk it will not read
+// again, so that warps still working on the same atom or section can get the
+// chunks they need from the producer (no warp waits at a barrier while holding
+// chunks the others depend on).
+__device__ __forceinline__ void atom_end(const Run &T, double &acc, int &buf, double *red, double alpha,
+                                         double beta, const double *yin, double *y, int mode, Ring &R) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t h = T.nrow;
+  R.release_below(R.base + (run_end(T) >> kChunkLog));
+  double *rb = red + buf * (NW * 32);
+  if ((uint32_t)lane < h) rb[w * 32 + lane] = acc;
+  named_bar(2, kConsumerThreads);
+  if (w == 0 && (uint32_t)lane < h) {
+    double s = rb[lane];
+#pragma unroll
+    for (int q = 1; q < NW; ++q) s += rb[q * 32 + lane];
+    const uint32_t r = T.out + lane;
+    if (mode == 0) {
+      double v = alpha * s;
+      if (beta != 0.0) v = fma(beta, yin[r], v);
+      y[r] = v;
+    } else {
+      y[r] = fma(alpha, s, y[r]);
+    }
+  }
+  acc = 0.0;
+  buf ^= 1;
+}
+
+// Runs a section: gathers run k+1's vector segments while computing run k.
+// One named barrier per run makes run k's gathers visible to every warp and
+// guarantees that nobody still reads the buffer run k+1 is gathered into.
+// Run headers and terms come from the descriptor queue.  process(run, terms,
+// stage) returns the stream position where the run ends.
+template <class F>
+__device__ __forceinline__ void run_section(uint32_t nruns, DescQ &Q, const double *x, const double *zbu,
+                                            const Smem &sm, int &sbuf, Ring &R, F &&process) {
+  if (nruns == 0) return;
+  {
+    const Run *r0 = Q.get(0, R.bad);
+    gather_run(*r0, reinterpret_cast<const Term *>(r0 + 1), x, zbu, sm.stage + sbuf * kStageCap);
+  }
+  uint32_t rend = 0;
+  for (uint32_t k = 0; k < nruns; ++k) {
+    // give back the ring chunks of the previous run before blocking
+    if (k > 0) R.release_below(R.base + (rend >> kChunkLog));
+    cp_async_wait_all();
+    named_bar(3, kConsumerThreads);
+    if (k + 1 < nruns) {
+      const Run *rn = Q.get(k + 1, R.bad);
+      gather_run(*rn, reinterpret_cast<const Term *>(rn + 1), x, zbu, sm.stage + (sbuf ^ 1) * kStageCap);
+    }
+    const Run *rc = Q.get(k, R.bad);
+    rend = process(*rc, reinterpret_cast<const Term *>(rc + 1), sm.stage + sbuf * kStageCap);
+    Q.release(k);
+    sbuf ^= 1;
+  }
+  Q.g += nruns;
+}
+
+// One H-matvec over this CTA's stream (pass starting at absolute chunk R.base,
+// K chunks long).  Contains one grid-barrier instance (arrive after P, wait
+// before U); every warp has released the whole pass when it returns.
+__device__ __forceinline__ void matvec_body(Ring &R, DescQ &Q, uint32_t K, const CtaInfo &ci, const double *x,
+                                            double alpha, double beta,
+                                            const double *yin, double *y, double *zbu, unsigned *gbar, int *err,
+                                            uint64_t timeout_ns, const Smem &sm, int &buf, int &sbuf,
+                                            unsigned long long *prof = nullptr) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto stamp = [&](int k) {
+    if (prof && w == 0 && lane == 0) prof[blockIdx.x * 8 + k] = gtimer();
+  };
+  stamp(0);
+  // ---- P: zbu = V^T x for this CTA's panels
+  double pacc = 0.0;
+  uint32_t pend = 0;
+  run_section(ci.nr_p, Q, x, zbu, sm, sbuf, R, [&](const Run &run, const Term *dt, const double *stage) {
+    for (uint32_t q = 0; q < run.nterm; ++q) {
+      const Term T = dt[q];
+      term_panel(T, smem_u32(stage), zbu, R, pacc);
+      pend = term_end(T);
+    }
+    return pend;
+  });
+  R.release_below(R.base + (pend >> kChunkLog));
+  stamp(1);
+  if (lane == 0) __threadfence();
+  named_bar(1, kConsumerThreads);
+  stamp(2);
+  unsigned gen = 0;
+  if (w == 0 && lane == 0) {
+    gen = ld_acquire(&gbar[1]);
+    grid_arrive(gbar, gridDim.x);
+  }
+  // ---- D: dense rows of the owned atoms (hides the barrier latency)
+  double acc = 0.0;
+  uint32_t dend = pend;
+  run_section(ci.nr_d, Q, x, zbu, sm, sbuf, R, [&](const Run &run, const Term *, const double *stage) {
+    run_rows(run, smem_u32(stage), R, acc);
+    if (run.flags & kAtomEnd) atom_end(run, acc, buf, sm.red, alpha, beta, yin, y, 0, R);
+    dend = run_end(run);
+    return dend;
+  });
+  R.release_below(R.base + (dend >> kChunkLog));
+  stamp(3);
+  // ---- wait for every CTA's zbu
+  if (w == 0) {
+    int ok = 1;
+    if (lane == 0) {
+      ok = grid_wait(gbar, gen, timeout_ns) ? 1 : 0;
+      if (!ok) atomicOr(err, kErrGridBarrier);
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    if (lane == 0) sm.scal[63] = ok ? 1.0 : 0.0;
+  }
+  named_bar(1, kConsumerThreads);
+  stamp(4);
+  if (sm.scal[63] == 0.0) R.bad = true;
+  // ---- U: U rows of the owned atoms times zbu
+  run_section(ci.nr_u, Q, x, zbu, sm, sbuf, R, [&](const Run &run, const Term *, const double *stage) {
+    run_rows(run, smem_u32(stage), R, acc);
+    if (run.flags & kAtomEnd) atom_end(run, acc, buf, sm.red, alpha, beta, yin, y, 1, R);
+    return run_end(run);
+  });
+  R.release_below(R.base + K);
+  stamp(5);
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  const Smem sm = smem_layout(smem_raw);
+  const CtaInfo ci = a.ctas[blockIdx.x];
+  init_barriers(sm);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
+  const uint32_t nruns = ci.nr_p + ci.nr_d + ci.nr_u;
+  if (w == kProducerWarp) {
+    if (lane == 0 && K > 0)
+      producer_run(a.stream + ci.stream_off, ci.stream_bytes, 1, sm.ring, sm.full, sm.empty, a.err, a.timeout_ns);
+    return;
+  }
+  if (w == kDescWarp) {
+    if (nruns > 0)
+      desc_run(a.runs + ci.run_begin, nruns, 1, a.terms, sm.desc, sm.dfull, sm.dempty, sm.hdr, sm.hbar, a.err,
+               a.timeout_ns);
+    return;
+  }
+  Ring R{sm.ring, sm.full, sm.empty, 0, 0, 0, a.timeout_ns, a.err, false};
+  DescQ Q{sm.desc, sm.dfull, sm.dempty, 0, a.timeout_ns, a.err};
+  int buf = 0, sbuf = 0;
+  matvec_body(R, Q, K, ci, a.x, a.alpha, a.beta, a.yin, a.y, a.zbu, a.gbar, a.err, a.timeout_ns, sm, buf, sbuf,
+              a.prof);
+  R.drain(K);
+}
+
+// ---------------------------------------------------------------- BiCGSTAB
+template <class F>
+__device__ __forceinline__ void for_own_rows(const Atom *atoms, const CtaInfo &ci, F f) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t q = w; q < ci.n_atoms; q += NW) {
+    const Atom A = atoms[ci.atom_begin + q];
+    if ((uint32_t)lane < A.h) f(A.r0 + lane);
+  }
+}
+
+// Per-CTA compensated partial sums of NS dot products over the owned rows.
+// acc[] holds the calling thread's partials; the result goes to part[cta][slot0+k].
+template <int NSL>
+__device__ __forceinline__ void cta_partials(Acc2 (&acc)[NSL], double *part, int slot0, const Smem &sm) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < NSL; ++k) acc[k] = warp_merge(acc[k]);
+  double *sc = sm.red;  // reuse: [NW][NSL][2]
+  named_bar(1, kConsumerThreads);  // red may still be read by an atom reduction
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NSL; ++k) {
+      sc[(w * NSL + k) * 2 + 0] = acc[k].s;
+      sc[(w * NSL + k) * 2 + 1] = acc[k].c;
+    }
+  }
+  named_bar(1, kConsumerThreads);
+  if (w == 0 && lane < NSL) {
+    Acc2 t{sc[lane * 2], sc[lane * 2 + 1]};
+    for (int q = 1; q < NW; ++q) t = acc2_merge(t, Acc2{sc[(q * NSL + lane) * 2], sc[(q * NSL + lane) * 2 + 1]});
+    double *dst = part + ((size_t)blockIdx.x * kSlots + slot0 + lane) * 2;
+    dst[0] = t.s;
+    dst[1] = t.c;
+    __threadfence();
+  }
+  named_bar(1, kConsumerThreads);
+}
+
+// Total of one slot over all CTAs, same operation order in every CTA (full warp).
+__device__ __forceinline__ double reduce_slot(const double *part, int ncta, int slot) {
+  const int lane = threadIdx.x & 31;
+  Acc2 a{0.0, 0.0};
+  for (int c = lane; c < ncta; c += 32) {
+    const double *src = part + ((size_t)c * kSlots + slot) * 2;
+    a = acc2_merge(a, Acc2{__ldcg(src), __ldcg(src + 1)});
+  }
+  a = warp_merge(a);
+  return a.s + a.c;
+}
+
+// Full grid barrier among the consumer warps of every CTA.
+__device__ __forceinline__ bool grid_sync(unsigned *gbar, int *err, uint64_t timeout_ns, const Smem &sm) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  named_bar(1, kConsumerThreads);
+  if (w == 0 && lane == 0) {
+    const unsigned gen = ld_acquire(&gbar[1]);
+    grid_arrive(gbar, gridDim.x);
+    const bool ok = grid_wait(gbar, gen, timeout_ns);
+    if (!ok) atomicOr(err, kErrGridBarrier);
+    sm.scal[62] = ok ? 1.0 : 0.0;
+  }
+  named_bar(1, kConsumerThreads);
+  return sm.scal[62] != 0.0;
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_bicg_setup(BicgArgs a) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  const Smem sm = smem_layout(smem_raw);
+  if ((threadIdx.x >> 5) >= NW) return;
+  const CtaInfo ci = a.ctas[blockIdx.x];
+  Acc2 acc[3] = {{0, 0}, {0, 0}, {0, 0}};
+  for_own_rows(a.atoms, ci, [&](uint32_t r) {
+    const double rv = a.r[r];
+    a.rh[r] = rv;
+    a.p[r] = 0.0;
+    a.ap[r] = 0.0;
+    dot2_add(acc[0], rv, rv);
+    dot2_add(acc[1], rv, rv);
+    const double bv = a.b[r];
+    dot2_add(acc[2], bv, bv);
+  });
+  // slots 0,1 then 5
+  Acc2 a01[2] = {acc[0], acc[1]};
+  cta_partials<2>(a01, a.part, kSlotRhoR, sm);
+  Acc2 a5[1] = {acc[2]};
+  cta_partials<1>(a5, a.part, kSlotBB, sm);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    BicgState st{};
+    *a.state = st;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  const Smem sm = smem_layout(smem_raw);
+  const CtaInfo ci = a.ctas[blockIdx.x];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ncta = gridDim.x;
+  init_barriers(sm);
+
+  // ---- S0: scalars of the previous step; stop test at the top of the loop
+  // (HACApK_SOLVER.c:602-603).  Every CTA computes identical values.
+  if (w == 0) {
+    const double rho_new = reduce_slot(a.part, ncta, kSlotRhoR);
+    const double rr = reduce_slot(a.part, ncta, kSlotRR);
+    const double bb = reduce_slot(a.part, ncta, kSlotBB);
+    if (lane == 0) {
+      BicgState st;
+      st.alpha = __ldcg(&a.state->alpha);
+      st.zeta = __ldcg(&a.state->zeta);
+      st.rho = __ldcg(&a.state->rho);
+      st.iter = __ldcg(&a.state->iter);
+      st.done = __ldcg(&a.state->done);
+      st.status = __ldcg(&a.state->status);
+      st.breakdown = __ldcg(&a.state->breakdown);
+      const double bnorm = sqrt(bb);
+      const double relres = (bnorm > 0.0) ? sqrt(rr) / bnorm : 0.0;
+      int done = st.done, status = st.status;
+      double beta = 0.0;
+      if (!done) {
+        if (st.breakdown) { done = 1; status = HBX_ERR_BREAKDOWN; }
+        else if (relres < a.tol) { done = 1; status = HBX_OK; }
+        else if (!isfinite(relres)) { done = 1; status = HBX_ERR_BREAKDOWN; }
+        else if (st.iter >= a.max_iter) { done = 1; status = HBX_ERR_NOT_CONVERGED; }
+        else if (st.iter > 0) {
+          // beta = -alpha/zeta * (rh.r_new)/znormold with the reference's sign
+          // flips (HACApK_SOLVER.c:650-655, :699, :724) = (alpha/zeta) rho_new/rho_old
+          beta = (st.alpha / st.zeta) * (rho_new / st.rho);
+          if (!isfinite(beta)) { done = 1; status = HBX_ERR_BREAKDOWN; }
+        }
+      }
+      sm.scal[0] = done;
+      sm.scal[1] = status;
+      sm.scal[2] = beta;
+      sm.scal[3] = st.zeta;
+      sm.scal[4] = rho_new;
+      sm.scal[5] = relres;
+      sm.scal[6] = st.iter;
+      sm.scal[7] = bnorm;
+      if (done && blockIdx.x == 0) {
+        a.state->done = 1;
+        a.state->status = status;
+        a.state->relres = relres;
+        a.state->bnorm = bnorm;
+      }
+    }
+  }
+  __syncthreads();
+  if (sm.scal[0] != 0.0) return;
+  const double beta = sm.scal[2], zeta_prev = sm.scal[3], rho = sm.scal[4];
+  const double relres = sm.scal[5], bnorm = sm.scal[7];
+  const int iter = (int)sm.scal[6];
+
+  const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
+  const uint32_t nruns = ci.nr_p + ci.nr_d + ci.nr_u;
+  if (w == kProducerWarp) {
+    if (lane == 0 && K > 0)
+      producer_run(a.stream + ci.stream_off, ci.stream_bytes, 2, sm.ring, sm.full, sm.empty, a.err, a.timeout_ns);
+    return;
+  }
+  if (w == kDescWarp) {
+    if (nruns > 0)
+      desc_run(a.runs + ci.run_begin, nruns, 2, a.terms, sm.desc, sm.dfull, sm.dempty, sm.hdr, sm.hbar, a.err,
+               a.timeout_ns);
+    return;
+  }
+  Ring R{sm.ring, sm.full, sm.empty, 0, 0, 0, a.timeout_ns, a.err, false};
+  DescQ Q{sm.desc, sm.dfull, sm.dempty, 0, a.timeout_ns, a.err};
+  int buf = 0, sbuf = 0;
+
+  // ---- S1: p = r + beta*(p - zeta*Ap)  (p = r on the first step)
+  if (beta == 0.0) {
+    for_own_rows(a.atoms, ci, [&](uint32_t r) { a.p[r] = a.r[r]; });
+  } else {
+    for_own_rows(a.atoms, ci, [&](uint32_t r) {
+      const double v = fma(-zeta_prev, a.ap[r], a.p[r]) * beta;
+      a.p[r] = v + a.r[r];
+    });
+  }
+  __threadfence();
+  grid_sync(a.gbar, a.err, a.timeout_ns, sm);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.state->iter = iter + 1;
+    a.state->beta = beta;
+    a.state->rho = rho;
+    a.state->relres = relres;
+    a.state->bnorm = bnorm;
+    a.hist[iter] = relres;
+  }
+
+  // ---- S2: Ap = H p;  rh . Ap
+  matvec_body(R, Q, K, ci, a.p, 1.0, 0.0, nullptr, a.ap, a.zbu, a.gbar, a.err, a.timeout_ns, sm, buf, sbuf);
+  {
+    Acc2 acc[1] = {{0, 0}};
+    named_bar(1, kConsumerThreads);
+    for_own_rows(a.atoms, ci, [&](uint32_t r) { dot2_add(acc[0], a.rh[r], a.ap[r]); });
+    cta_partials<1>(acc, a.part, kSlotRhAp, sm);
+  }
+  grid_sync(a.gbar, a.err, a.timeout_ns, sm);
+  if (w == 0) {
+    const double zden = reduce_slot(a.part, ncta, kSlotRhAp);
+    if (lane == 0) sm.scal[8] = rho / zden;
+  }
+  named_bar(1, kConsumerThreads);
+  const double alpha = sm.scal[8];
+
+  // ---- S3: t = r - alpha*Ap
+  for_own_rows(a.atoms, ci, [&](uint32_t r) { a.t[r] = fma(-alpha, a.ap[r], a.r[r]); });
+  __threadfence();
+  grid_sync(a.gbar, a.err, a.timeout_ns, sm);
+
+  // ---- S4: At = H t;  At . t,  At . At
+  R.base = K;
+  matvec_body(R, Q, K, ci, a.t, 1.0, 0.0, nullptr, a.at, a.zbu, a.gbar, a.err, a.timeout_ns, sm, buf, sbuf);
+  {
+    Acc2 acc[2] = {{0, 0}, {0, 0}};
+    named_bar(1, kConsumerThreads);
+    for_own_rows(a.atoms, ci, [&](uint32_t r) {
+      const double atv = a.at[r];
+      dot2_add(acc[0], atv, a.t[r]);
+      dot2_add(acc[1], atv, atv);
+    });
+    cta_partials<2>(acc, a.part, kSlotAtT, sm);
+  }
+  grid_sync(a.gbar, a.err, a.timeout_ns, sm);
+  if (w == 0) {
+    const double s3 = reduce_slot(a.part, ncta, kSlotAtT);
+    const double s4 = reduce_slot(a.part, ncta, kSlotAtAt);
+    if (lane == 0) {
+      const double zeta = (s4 != 0.0) ? s3 / s4 : 0.0;
+      sm.scal[9] = zeta;
+      const bool bad = !isfinite(alpha) || !isfinite(zeta);
+      if (blockIdx.x == 0) {
+        a.state->alpha = alpha;
+        a.state->zeta = zeta;
+        if (bad) a.state->breakdown = 1;
+      }
+    }
+  }
+  named_bar(1, kConsumerThreads);
+  const double zeta = sm.scal[9];
+
+  // ---- S5: u += alpha*p + zeta*t;  r = t - zeta*At;  rh . r,  r . r
+  {
+    Acc2 acc[2] = {{0, 0}, {0, 0}};
+    for_own_rows(a.atoms, ci, [&](uint32_t r) {
+      const double uv = fma(alpha, a.p[r], a.u[r]);
+      a.u[r] = fma(zeta, a.t[r], uv);
+      const double rv = fma(-zeta, a.at[r], a.t[r]);
+      a.r[r] = rv;
+      dot2_add(acc[0], a.rh[r], rv);
+      dot2_add(acc[1], rv, rv);
+    });
+    cta_partials<2>(acc, a.part, kSlotRhoR, sm);
+  }
+  R.drain(2 * K);
+}
+
+// part[cta][slot] over own rows, then (block 0 of a second launch) the total.
+__global__ void __launch_bounds__(kThreads, 1) k_dot_partial(BicgArgs a, const double *x, const double *y, int slot) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  const Smem sm = smem_layout(smem_raw);
+  if ((threadIdx.x >> 5) >= NW) return;
+  const CtaInfo ci = a.ctas[blockIdx.x];
+  Acc2 acc[1] = {{0, 0}};
+  for_own_rows(a.atoms, ci, [&](uint32_t r) { dot2_add(acc[0], x[r], y[r]); });
+  cta_partials<1>(acc, a.part, slot, sm);
+}
+
+__global__ void k_dot_total(const double *part, int ncta, int slot, double *out) {
+  const double v = reduce_slot(part, ncta, slot);
+  if (threadIdx.x == 0) *out = v;
+}
+
+}  // namespace
+
+size_t kernel_smem_bytes() { return SharedLayout::bytes; }
+
+cudaError_t configure_kernels() {
+  const int smem = (int)SharedLayout::bytes;
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_matvec, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_bicg_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_bicg_iter, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_dot_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+template <class Args>
+static cudaError_t launch_coop(void (*kern)(Args), const Args &a, int num_ctas, cudaStream_t s) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(num_ctas);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = SharedLayout::bytes;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, a);
+}
+
+cudaError_t launch_matvec(const MatvecArgs &a, int num_ctas, cudaStream_t s) {
+  return launch_coop(k_matvec, a, num_ctas, s);
+}
+
+cudaError_t launch_bicg_setup(const BicgArgs &a, int num_ctas, cudaStream_t s) {
+  k_bicg_setup<<<num_ctas, kThreads, SharedLayout::bytes, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bicg_iter(const BicgArgs &a, int num_ctas, cudaStream_t s) {
+  return launch_coop(k_bicg_iter, a, num_ctas, s);
+}
+
+cudaError_t launch_dot(const BicgArgs &a, const double *x, const double *y, int slot, double *out, int num_ctas,
+                       cudaStream_t s) {
+  k_dot_partial<<<num_ctas, kThreads, SharedLayout::bytes, s>>>(a, x, y, slot);
+  k_dot_total<<<1, 32, 0, s>>>(a.part, num_ctas, slot, out);
+  return cudaGetLastError();
+}
+
+}  // namespace hbx

@@ -1,0 +1,110 @@
+"""Python handle on the sm_100a engine (libhacapk_b200.so) through its C ABI.
+
+Every call goes through the hbx_* entry points of include/hacapk_b200.h; the
+library fails loudly (RuntimeError) when it is missing or when the device
+reports an error.  There is no host fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+
+class HbxError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        lib = abi.engine_lib()
+        msg = lib.hbx_last_error().decode(errors="replace")
+        super().__init__(f"{where}: {abi.STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _check(status: int, where: str):
+    if status != 0:
+        raise HbxError(status, where)
+
+
+class Engine:
+    """Packed H-matrix resident on the current CUDA device."""
+
+    def __init__(self, st, nd: int, num_ctas: int = 0):
+        self.lib = abi.engine_lib()
+        opt = abi.Options()
+        opt.precision = 0
+        opt.num_ctas = num_ctas
+        h = C.c_void_p()
+        _check(self.lib.hbx_create(st, nd, C.byref(opt), C.byref(h)), "hbx_create")
+        self._h = h
+        self.nd = nd
+        inf = abi.Info()
+        _check(self.lib.hbx_get_info(h, C.byref(inf)), "hbx_get_info")
+        self.info = {f: getattr(inf, f) for f, _ in abi.Info._fields_ if f != "reserved"}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.hbx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- matvec -------------------------------------------------------------
+    def matvec_host(self, zu: np.ndarray, zau: np.ndarray | None = None):
+        """zau + H zu (zau=None: H zu) with host vectors; returns (y, kernel_s, copy_s)."""
+        zu = np.ascontiguousarray(zu, np.float64)
+        acc = zau is not None
+        y = np.array(zau, np.float64, copy=True) if acc else np.zeros(self.nd)
+        tk, tc = C.c_double(0.0), C.c_double(0.0)
+        _check(self.lib.hbx_matvec_host(self._h, abi.dptr(zu), abi.dptr(y), 1 if acc else 0,
+                                        C.byref(tk), C.byref(tc)), "hbx_matvec_host")
+        return y, tk.value, tc.value
+
+    def matvec_dev(self, x_ptr: int, y_ptr: int, alpha: float = 1.0, beta: float = 0.0,
+                   yin_ptr: int | None = None, stream: int = 0):
+        """y = alpha H x + beta yin on device pointers (async on `stream`)."""
+        _check(self.lib.hbx_matvec(self._h, alpha, C.c_void_p(x_ptr), beta,
+                                   C.c_void_p(yin_ptr) if yin_ptr else None, C.c_void_p(y_ptr),
+                                   C.c_void_p(stream) if stream else None), "hbx_matvec")
+
+    def sync(self, stream: int = 0):
+        _check(self.lib.hbx_sync(self._h, C.c_void_p(stream) if stream else None), "hbx_sync")
+
+    # -- BiCGSTAB -------------------------------------------------------------
+    @staticmethod
+    def _opts(tol, max_iter, verbose, batch):
+        o = abi.SolveOpts()
+        o.tol = tol
+        o.max_iter = max_iter
+        o.verbose = verbose
+        o.batch = batch
+        return o
+
+    @staticmethod
+    def _info(si: abi.SolveInfo) -> dict:
+        return {f: getattr(si, f) for f, _ in abi.SolveInfo._fields_ if f != "reserved"}
+
+    def bicgstab_host(self, b: np.ndarray, u0: np.ndarray | None = None, tol: float = 1e-8,
+                      max_iter: int = 1000, verbose: int = 0, batch: int = 8, check: bool = True):
+        b = np.ascontiguousarray(b, np.float64)
+        u = np.zeros(self.nd) if u0 is None else np.array(u0, np.float64, copy=True)
+        o = self._opts(tol, max_iter, verbose, batch)
+        si = abi.SolveInfo()
+        st = self.lib.hbx_bicgstab_host(self._h, abi.dptr(b), abi.dptr(u), C.byref(o), C.byref(si))
+        if check:
+            _check(st, "hbx_bicgstab_host")
+        return u, self._info(si)
+
+    def bicgstab_dev(self, b_ptr: int, u_ptr: int, tol: float = 1e-8, max_iter: int = 1000,
+                     verbose: int = 0, batch: int = 8, stream: int = 0, check: bool = True) -> dict:
+        o = self._opts(tol, max_iter, verbose, batch)
+        si = abi.SolveInfo()
+        st = self.lib.hbx_bicgstab(self._h, C.c_void_p(b_ptr), C.c_void_p(u_ptr), C.byref(o),
+                                   C.byref(si), C.c_void_p(stream) if stream else None)
+        if check:
+            _check(st, "hbx_bicgstab")
+        return self._info(si)

@@ -1,0 +1,240 @@
+/*
+ * hacapk_b200.h -- C ABI of the B200-native H-matrix matvec / BiCGSTAB engine.
+ *
+ * Two layers live behind this header:
+ *
+ *  1. The HACApK drop-in symbols.  They keep the names, argument lists and
+ *     by-reference (Fortran) calling convention of the HACApK-MAGMA C layer so
+ *     that the Fortran driver (m_HACApK_solve.f90 / m_HACApK_use.f90) links
+ *     against libhacapk_b200.so instead of the MAGMA batched-GEMV objects.
+ *     Each declaration cites the reference function it replaces.
+ *
+ *  2. The hbx_* API: status-returning, stream-aware calls on an opaque
+ *     engine handle.  The drop-in symbols are thin wrappers around it.
+ *
+ * All vectors are in HACApK's cluster (permuted) order and all leaf offsets
+ * (nstrtl, nstrtt) are 1-based, exactly as in the reference leaf list.
+ * No torch or CUDA types appear in any signature; streams are passed as
+ * `void *` holding a cudaStream_t (NULL = the legacy default stream).
+ */
+#ifndef HACAPK_B200_H
+#define HACAPK_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HBX_ABI_VERSION 1
+
+/* ------------------------------------------------------------------------ */
+/* Leaf-matrix layout (mirrors HACApK_MAGMA.h:12-121, HAVE_MAGMA_BATCH build) */
+/* ------------------------------------------------------------------------ */
+
+/* One leaf of the H-matrix (HACApK_MAGMA.h:12-20, m_HACApK_base.f90:54-61).
+ *  ltmtx = 1: low-rank, A ~= U V^T with V = a1 (ndt x kt, column-major) and
+ *             U = a2 (ndl x kt, column-major) found at (char*)a1 + a1size.
+ *  ltmtx = 2: dense, a1 is ndt x ndl column-major, A(il,it) = a1[it + il*ndt].
+ * Only a1 (the first word of the Fortran pointer descriptor) and a1size are
+ * read; `a2` is never dereferenced, matching HACApK_MAGMA.c:27. */
+typedef struct stc_HACApK_leafmtx {
+  int ltmtx;
+  int kt;
+  int nstrtl, ndl;
+  int nstrtt, ndt;
+  long long int a1size;
+  double *a1;
+  double *a2;
+} stc_HACApK_leafmtx;
+
+/* Container (HACApK_MAGMA.h:28-106, m_HACApK_base.f90:64-235).  The GPU/batch
+ * fields are kept only so that `st_lf` sits at the offset a MAGMA build of the
+ * Fortran type expects; this engine keeps its own state in a side table keyed
+ * by the container address and never writes these fields.  The leaves are
+ * found at (char*)st_lf + ip*st_lf_stride. */
+typedef struct stc_HACApK_leafmtxp {
+  int nd;
+  int nlf;
+  int nlfkt;
+  int ktmax;
+  int st_lf_stride;
+  /* HAVE_MAGMA | HAVE_MAGMA_BATCH block */
+  int m, n, gn, max_block;
+  double gflops;
+  void *mtx1_gpu, *mtx2_gpu, *zu_gpu, *zau_gpu, *zau_pin, *zbu_gpu;
+  int num_batch, total_size_y, transA;
+  void *d_A_array, *d_X_array, *d_Y_array;
+  void *d_M, *d_N, *d_lda, *d_inc;
+  void *batch_order;
+  void *h_A_array, *h_X_array, *h_Y_array;
+  void *h_type, *h_I, *h_J, *h_M, *h_N, *h_lda, *max_M, *max_N, *batch_size;
+  int num_streamed, num_streamed_t;
+  void *h_A_array_streamed, *h_X_array_streamed, *h_Y_array_streamed;
+  void *h_M_streamed, *h_N_streamed, *h_lda_streamed;
+  void *d_A_mgpu, *d_X_mgpu, *d_Y_mgpu, *d_M_mgpu, *d_N_mgpu, *d_lda_mgpu, *d_inc_mgpu;
+  void *zu_mgpu, *zau_mgpu, *zbu_mgpu;
+  void *h_A_mgpu, *h_X_mgpu, *h_Y_mgpu, *h_type_mgpu, *h_I_mgpu, *h_J_mgpu;
+  void *h_M_mgpu, *h_N_mgpu, *h_lda_mgpu, *max_M_mgpu, *max_N_mgpu;
+  void *nlf_mgpu, *num_batch_mgpu, *total_size_y_mgpu;
+  int *iwork;
+  int mpi_rank;
+  /* end of HAVE_MAGMA block */
+  stc_HACApK_leafmtx *st_lf;
+} stc_HACApK_leafmtxp;
+
+/* Control block (HACApK_MAGMA.h:108-121).  `param` is HACApK's param(1:100)
+ * array; lpmd/lod/lsp/lnp/lthr are found at byte offsets from `param`.
+ * C indices used here: param[0] verbosity, param[82] max steps,
+ * param[90] BiCGSTAB tolerance, lpmd[1] nrank, lpmd[2] rank. */
+typedef struct stc_HACApK_lcontrol {
+  int lf_umpi;
+  int lpmd_offset;
+  int lod_offset;
+  int lsp_offset;
+  int lnp_offset;
+  int lthr_offset;
+  double *param;
+} stc_HACApK_lcontrol;
+
+/* ------------------------------------------------------------------------ */
+/* hbx_* API                                                                */
+/* ------------------------------------------------------------------------ */
+
+typedef enum hbx_status {
+  HBX_OK = 0,
+  HBX_ERR_INVALID = 1,       /* bad argument or malformed leaf list        */
+  HBX_ERR_NOMEM = 2,         /* host or device allocation failed           */
+  HBX_ERR_CUDA = 3,          /* CUDA runtime error                         */
+  HBX_ERR_TIMEOUT = 4,       /* a bounded device wait expired              */
+  HBX_ERR_BREAKDOWN = 5,     /* BiCGSTAB breakdown (zero/non-finite scalar)*/
+  HBX_ERR_NOT_CONVERGED = 6, /* iteration limit reached before tolerance   */
+  HBX_ERR_NONFINITE = 7,     /* NaN or Inf in an input vector              */
+  HBX_ERR_UNSUPPORTED = 8    /* e.g. more than one MPI rank                */
+} hbx_status;
+
+enum { HBX_FP64 = 0 };
+
+typedef struct hbx_hmat hbx_hmat;
+
+typedef struct hbx_options {
+  int precision;   /* HBX_FP64 (only value accepted by this ABI version) */
+  int num_ctas;    /* persistent CTAs; 0 = one per SM                     */
+  int reserved[14];
+} hbx_options;
+
+typedef struct hbx_info {
+  int nd, nlf, nlfkt, ktmax;
+  int num_ctas, num_atoms, num_terms, precision;
+  long long stream_bytes;  /* packed factor bytes streamed per matvec        */
+  long long alg_bytes;     /* algorithmic bytes per single-RHS matvec (B_H)  */
+  long long alg_flops;     /* 2*(sum dense ndl*ndt + sum kt*(ndl+ndt))       */
+  long long zbu_len;       /* sum of kt over low-rank leaves                  */
+  long long dense_words, lowrank_words;
+  double setup_seconds;
+  int reserved[8];
+} hbx_info;
+
+typedef struct hbx_solve_opts {
+  double tol;          /* stop when ||r||/||b|| < tol (checked before each step) */
+  int max_iter;        /* iteration limit (param[82] in the drop-in)             */
+  int verbose;         /* >0: print the residual history like the reference     */
+  int batch;           /* iterations per graph replay between host checks (0=8) */
+  int reserved[11];
+} hbx_solve_opts;
+
+typedef struct hbx_solve_info {
+  int iterations;      /* completed BiCGSTAB steps (nstp)                     */
+  int status;          /* hbx_status of the solve                             */
+  double bnorm;        /* ||b||_2                                             */
+  double relres;       /* recursive residual ||r||/||b|| at exit              */
+  double true_relres;  /* ||b - H u|| / ||b|| recomputed after the solve      */
+  double seconds;      /* device time from r0 = b - H u0 to the last step     */
+  double iter_kernel_seconds; /* device time of the iteration launches only   */
+  int iter_launches;   /* iteration-kernel launches (includes the final
+                          launches that only observe convergence)             */
+  int launches;        /* all kernel launches of the solve                    */
+  int reserved[6];
+} hbx_solve_info;
+
+/* Packs the leaf list into the engine's per-CTA streaming layout and uploads
+ * it to the current device.  Replaces the setup half of
+ * c_hacapk_adot_body_lfcpy_batch_sorted_ (HACApK_BATCH_SORT.c:86-858). */
+int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt,
+               hbx_hmat **out);
+/* Frees device and host state (HACApK_BATCH.c:812-859). */
+int hbx_destroy(hbx_hmat *h);
+int hbx_get_info(const hbx_hmat *h, hbx_info *info);
+
+/* y = alpha * H x + beta * yin on device pointers; yin may equal y; beta == 0
+ * ignores yin.  One persistent kernel launch on `stream`.  Replaces
+ * c_hacapk_adot_body_lfmtx_batch_queue with on_gpu=1 (HACApK_BATCH.c:47-255). */
+int hbx_matvec(hbx_hmat *h, double alpha, const double *x, double beta,
+               const double *yin, double *y, void *stream);
+
+/* Waits for `stream` and returns the device error latched by earlier async
+ * calls on this engine (HBX_ERR_TIMEOUT when a bounded device wait expired),
+ * clearing it. */
+int hbx_sync(hbx_hmat *h, void *stream);
+
+/* Host vectors: zau = (accumulate ? zau : 0) + H zu, with the H2D/D2H copies
+ * inside the call (HACApK_BATCH.c:257-271 semantics when accumulate=1).
+ * kernel_seconds / copy_seconds (nullable) are incremented. */
+int hbx_matvec_host(hbx_hmat *h, const double *zu, double *zau, int accumulate,
+                    double *kernel_seconds, double *copy_seconds);
+
+/* BiCGSTAB on device vectors (u holds x0 on entry, the solution on exit).
+ * Algorithm of c_hacapk_bicgstab_cax_lfmtx_gpu_ (HACApK_SOLVER.c:421-807). */
+int hbx_bicgstab(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts,
+                 hbx_solve_info *info, void *stream);
+/* Same with host vectors; copies are inside the call. */
+int hbx_bicgstab_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts,
+                      hbx_solve_info *info);
+
+/* Diagnostics: per-CTA %globaltimer stamps of the phases of the last matvec
+ * (only when the engine was created with HBX_PROFILE=1 in the environment);
+ * copies up to cap values into out, returns how many. */
+int hbx_debug_phase_stamps(hbx_hmat *h, unsigned long long *out, int cap);
+
+const char *hbx_status_string(int status);
+/* Message of the last failing hbx_* call on this host thread. */
+const char *hbx_last_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* HACApK drop-in entry points (Fortran calling convention)                 */
+/* ------------------------------------------------------------------------ */
+
+/* HACApK_MAGMA.c:69-75 -- device initialisation / release. */
+void magma_init_(void);
+void magma_finalize_(void);
+
+/* HACApK_BATCH_SORT.c:86 -- pack and upload the leaf list. */
+void c_hacapk_adot_body_lfcpy_batch_sorted_(int *nd, stc_HACApK_leafmtxp *st_leafmtxp);
+/* HACApK_BATCH.c:257 -- zau += H zu with host vectors; zbu is unused
+ * (host workspace in the reference); the three timers are incremented. */
+void c_hacapk_adot_body_lfmtx_batch_(double *zau, stc_HACApK_leafmtxp *st_leafmtxp,
+                                     double *zu, double *zbu, double *time_batch,
+                                     double *time_set, double *time_copy);
+/* HACApK_BATCH.c:812 -- release device state. */
+void c_hacapk_adot_body_lfdel_batch_(stc_HACApK_leafmtxp *st_leafmtxp);
+
+/* HACApK_MAGMA.c:231 / :79 / :369 -- the per-leaf GPU variants; mapped onto
+ * the same engine (zau += H zu). */
+void c_hacapk_adot_body_lfcpy_gpu_(int *nd, stc_HACApK_leafmtxp *st_leafmtxp);
+void c_hacapk_adot_body_lfmtx_gpu_(double *zau, stc_HACApK_leafmtxp *st_leafmtxp,
+                                   double *zu, double *zbu);
+void c_hacapk_adot_body_lfdel_gpu_(stc_HACApK_leafmtxp *st_leafmtxp);
+
+/* HACApK_SOLVER.c:421 -- BiCGSTAB with all vectors on the GPU.
+ * HACApK_SOLVER.c:254 -- "flat" BiCGSTAB: host vectors, GPU matvec per step.
+ * u: x0 in / solution out; b: rhs; param: HACApK param(1:100); *nstp: steps.
+ * *lrtrn is set to the hbx_status (0 on success); the reference never set it. */
+void c_hacapk_bicgstab_cax_lfmtx_gpu_(stc_HACApK_leafmtxp *st_leafmtxp,
+                                      stc_HACApK_lcontrol *st_ctl, double *u, double *b,
+                                      double *param, int *nd, int *nstp, int *lrtrn);
+void c_hacapk_bicgstab_cax_lfmtx_flat_(stc_HACApK_leafmtxp *st_leafmtxp,
+                                       stc_HACApK_lcontrol *st_ctl, double *u, double *b,
+                                       double *param, int *nd, int *nstp, int *lrtrn);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HACAPK_B200_H */

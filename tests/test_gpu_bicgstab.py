@@ -1,0 +1,111 @@
+"""GPU BiCGSTAB through the C ABI against the CPU restatement of
+HACApK_SOLVER.c:254-417 using the reference matvec.  Bar: the same iteration
+count within +-1, and a true residual ||b - H u||/||b|| below the tolerance."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import sphere
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("level", [3, 4, 5])
+def test_iterations_and_residual_match_oracle(gpu, build_libs, level):
+    import oracle
+    from hacapk_b200 import configs
+    from hacapk_b200.engine import Engine
+    H, b = configs.c1(level)
+    E = Engine(H.st, H.nd)
+    u, info = E.bicgstab_host(b, tol=1e-8, max_iter=1000)
+    u_ref, n_ref, hist, _ = oracle.bicgstab(H.st, b, tol=1e-8, max_iter=1000,
+                                            kind="ref" if oracle.have_ref() else "restated")
+    assert info["status"] == 0
+    assert abs(info["iterations"] - n_ref) <= 1
+    r = b - oracle.matvec(H.st, u)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-8 * 1.01
+    assert info["true_relres"] == pytest.approx(np.linalg.norm(r) / np.linalg.norm(b), rel=1e-3)
+    assert info["relres"] < 1e-8
+    assert np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref) < 1e-5
+    assert info["iter_launches"] >= info["iterations"] + 1
+
+
+def test_repeated_solves_are_bitwise_identical(gpu, build_libs):
+    from hacapk_b200 import configs
+    from hacapk_b200.engine import Engine
+    H, b = configs.c1(4)
+    E = Engine(H.st, H.nd)
+    u1, i1 = E.bicgstab_host(b)
+    u2, i2 = E.bicgstab_host(b)
+    assert i1["iterations"] == i2["iterations"] and np.array_equal(u1, u2)
+
+
+def test_device_vectors_and_initial_guess(gpu, build_libs):
+    import torch
+    from hacapk_b200 import configs
+    from hacapk_b200.engine import Engine
+    H, b = configs.c1(4)
+    E = Engine(H.st, H.nd)
+    bd = torch.from_numpy(b).to(gpu)
+    ud = torch.zeros_like(bd)
+    s = torch.cuda.current_stream().cuda_stream
+    info = E.bicgstab_dev(bd.data_ptr(), ud.data_ptr(), stream=s)
+    assert info["status"] == 0
+    info2 = E.bicgstab_dev(bd.data_ptr(), ud.data_ptr(), stream=s)  # start from the solution
+    assert info2["iterations"] <= 1
+
+
+def test_limits_zero_rhs_and_not_converged(gpu, build_libs):
+    from hacapk_b200.engine import Engine
+    H = sphere(3)
+    E = Engine(H.st, H.nd)
+    b = np.random.default_rng(3).standard_normal(H.nd)
+    u, info = E.bicgstab_host(b, tol=1e-30, max_iter=2, check=False)
+    assert info["status"] == 6 and info["iterations"] == 2
+    u, info = E.bicgstab_host(np.zeros(H.nd), check=False)
+    assert info["status"] == 0 and info["iterations"] == 0 and np.all(u == 0.0)
+
+
+def _control(nrank=1, maxit=1000, tol=1e-8, verbose=0):
+    from hacapk_b200 import abi
+    buf = np.zeros(160, np.float64)              # param(1:100) followed by lpmd(1:30)
+    buf[82], buf[90], buf[0] = maxit, tol, verbose
+    lp = buf[100:].view(np.int32)
+    lp[:] = 0
+    lp[1], lp[2] = nrank, 0
+    ctl = abi.LControl()
+    ctl.lpmd_offset = 800
+    ctl.param = buf.ctypes.data_as(C.POINTER(C.c_double))
+    return ctl, buf
+
+
+@pytest.mark.parametrize("entry", ["c_hacapk_bicgstab_cax_lfmtx_gpu_", "c_hacapk_bicgstab_cax_lfmtx_flat_"])
+def test_legacy_solver_entry_points(gpu, build_libs, entry):
+    """HACApK_SOLVER.c:421 (all on GPU) and :254 (flat): u in/out, nstp, lrtrn."""
+    import oracle
+    from hacapk_b200 import abi, configs
+    lib = abi.engine_lib()
+    H, b = configs.c1(4)
+    ctl, buf = _control()
+    u = np.zeros(H.nd)
+    nd, nstp, lrtrn = C.c_int(H.nd), C.c_int(-1), C.c_int(-1)
+    getattr(lib, entry)(H.st, C.byref(ctl), abi.dptr(u), abi.dptr(b), ctl.param, C.byref(nd), C.byref(nstp),
+                        C.byref(lrtrn))
+    _, n_ref, _, _ = oracle.bicgstab(H.st, b, tol=1e-8, max_iter=1000, kind="restated")
+    assert lrtrn.value == 0
+    assert abs(nstp.value - n_ref) <= 1
+    r = b - oracle.matvec(H.st, u)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1.05e-8
+
+
+def test_legacy_solver_rejects_several_ranks(gpu, build_libs):
+    from hacapk_b200 import abi
+    lib = abi.engine_lib()
+    H = sphere(2)
+    ctl, buf = _control(nrank=2)
+    u, b = np.zeros(H.nd), np.ones(H.nd)
+    nd, nstp, lrtrn = C.c_int(H.nd), C.c_int(-1), C.c_int(-1)
+    lib.c_hacapk_bicgstab_cax_lfmtx_gpu_(H.st, C.byref(ctl), abi.dptr(u), abi.dptr(b), ctl.param, C.byref(nd),
+                                         C.byref(nstp), C.byref(lrtrn))
+    assert lrtrn.value == 8

@@ -1,0 +1,150 @@
+"""CPU tests of the engine's host planner and packer (hbx_plan.cpp): a
+test-only interpreter (tests/emu/plan_emu.cpp) walks the packed per-CTA
+streams exactly as the kernel does, checks the layout invariants the kernel
+relies on, and its result is compared with the oracle."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, sphere
+
+EMU_SRC = os.path.join(ROOT, "tests", "emu", "plan_emu.cpp")
+EMU_LIB = os.path.join(ROOT, "tests", "emu", "_build", "libplanemu.so")
+
+
+@pytest.fixture(scope="module")
+def emu(build_libs):
+    os.makedirs(os.path.dirname(EMU_LIB), exist_ok=True)
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", EMU_LIB, EMU_SRC,
+                    os.path.join(ROOT, "hacapk-magma_b200", "csrc", "hbx_plan.cpp")], check=True)
+    lib = C.CDLL(EMU_LIB)
+    lib.emu_matvec.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                               C.POINTER(C.c_longlong), C.c_char_p, C.c_int]
+    return lib
+
+
+def run_emu(lib, st_ptr, nd, nc, x):
+    y = np.zeros(nd)
+    stats = (C.c_longlong * 8)()
+    msg = C.create_string_buffer(512)
+    rc = lib.emu_matvec(st_ptr, nd, nc, x.ctypes.data_as(C.POINTER(C.c_double)),
+                        y.ctypes.data_as(C.POINTER(C.c_double)), stats, msg, 512)
+    return rc, msg.value.decode(), y, list(stats)
+
+
+@pytest.mark.parametrize("level,leaf,nc", [(2, 32, 148), (3, 32, 148), (3, 32, 1), (3, 15, 7), (4, 32, 148),
+                                           (4, 32, 300)])
+def test_packed_layout_reproduces_oracle(emu, level, leaf, nc):
+    import oracle
+    H = sphere(level, leaf_size=leaf)
+    x = np.random.default_rng(level * 100 + nc).standard_normal(H.nd)
+    rc, msg, y, stats = run_emu(emu, C.cast(H.st, C.c_void_p), H.nd, nc, x)
+    assert rc == 0, msg
+    ref = oracle.matvec(H.st, x)
+    assert np.abs(y - ref).max() <= 1e-14 * np.abs(ref).max()
+    d, lr = H.storage_words()
+    assert stats[6] >= 8 * (d + lr)           # every factor byte is packed ...
+    assert stats[6] <= 8 * (d + lr) + 16 * nc  # ... with at most 16 B padding per CTA
+
+
+def _fortran_like(H, stride):
+    """A copy of the container whose leaves sit `stride` bytes apart (Fortran
+    derived types carry pointer descriptors between the fields the C side
+    reads), to check that st_lf_stride is honoured."""
+    from hacapk_b200 import abi
+    n = H.nlf
+    buf = (C.c_char * (stride * n))()
+    src = H.st.contents.st_lf
+    for ip in range(n):
+        C.memmove(C.addressof(buf) + ip * stride, C.addressof(src[ip]), C.sizeof(abi.LeafMtx))
+    P = abi.LeafMtxP()
+    C.memmove(C.byref(P), H.st, C.sizeof(abi.LeafMtxP))
+    P.st_lf_stride = stride
+    P.st_lf = C.cast(buf, C.POINTER(abi.LeafMtx))
+    return P, buf
+
+
+def test_leaf_stride_is_honoured(emu):
+    import oracle
+    H = sphere(3)
+    P, keep = _fortran_like(H, 160)
+    x = np.random.default_rng(7).standard_normal(H.nd)
+    rc, msg, y, _ = run_emu(emu, C.cast(C.pointer(P), C.c_void_p), H.nd, 148, x)
+    assert rc == 0, msg
+    ref = oracle.matvec(H.st, x)
+    assert np.abs(y - ref).max() <= 1e-14 * np.abs(ref).max()
+
+
+def _custom(leaves, nd):
+    """Container over hand-made leaves: (ltmtx, kt, nstrtl, ndl, nstrtt, ndt, a1 array)."""
+    from hacapk_b200 import abi
+    arr = (abi.LeafMtx * max(1, len(leaves)))()
+    keep = []
+    for i, (lt, kt, l0, ndl, t0, ndt, data) in enumerate(leaves):
+        data = np.ascontiguousarray(data, np.float64)
+        keep.append(data)
+        arr[i].ltmtx, arr[i].kt, arr[i].nstrtl, arr[i].ndl = lt, kt, l0, ndl
+        arr[i].nstrtt, arr[i].ndt = t0, ndt
+        arr[i].a1 = data.ctypes.data_as(C.POINTER(C.c_double)) if data.size else None
+        arr[i].a1size = 8 * (ndt * kt if lt == 1 else ndt * ndl)
+    P = abi.LeafMtxP()
+    P.nd, P.nlf = nd, len(leaves)
+    P.st_lf_stride = C.sizeof(abi.LeafMtx)
+    P.st_lf = arr
+    return P, (arr, keep)
+
+
+def _dense_of(leaves, nd):
+    A = np.zeros((nd, nd))
+    for lt, kt, l0, ndl, t0, ndt, data in leaves:
+        if lt == 2:
+            A[l0 - 1:l0 - 1 + ndl, t0 - 1:t0 - 1 + ndt] += np.asarray(data).reshape(ndl, ndt)
+        elif kt:
+            V = np.asarray(data[:ndt * kt]).reshape(kt, ndt).T
+            U = np.asarray(data[ndt * kt:]).reshape(kt, ndl).T
+            A[l0 - 1:l0 - 1 + ndl, t0 - 1:t0 - 1 + ndt] += U @ V.T
+    return A
+
+
+def test_edge_cases(emu):
+    rng = np.random.default_rng(9)
+    nd = 100
+    leaves = [
+        (2, 0, 1, 40, 1, 100, rng.standard_normal(40 * 100)),        # wide dense leaf (atoms split rows)
+        (1, 0, 41, 30, 1, 50, np.zeros(0)),                          # kt = 0 low-rank leaf: contributes nothing
+        (1, 3, 41, 30, 51, 50, rng.standard_normal(3 * (30 + 50))),  # ordinary low-rank
+        (1, 70, 71, 30, 1, 100, rng.standard_normal(70 * 130)),      # kt > panel width: several panels
+        (2, 0, 41, 30, 1, 50, rng.standard_normal(30 * 50)),
+    ]
+    P, keep = _custom(leaves, nd)
+    x = rng.standard_normal(nd)
+    for nc in (1, 5, 148):
+        rc, msg, y, _ = run_emu(emu, C.cast(C.pointer(P), C.c_void_p), nd, nc, x)
+        assert rc == 0, msg
+        ref = _dense_of(leaves, nd) @ x
+        assert np.abs(y - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_empty_leaf_list_gives_zero(emu):
+    P, keep = _custom([], 37)
+    x = np.ones(37)
+    rc, msg, y, _ = run_emu(emu, C.cast(C.pointer(P), C.c_void_p), 37, 148, x)
+    assert rc == 0, msg
+    assert np.all(y == 0.0)
+
+
+def test_malformed_leaves_are_rejected(emu):
+    rng = np.random.default_rng(10)
+    bad = [
+        [(3, 0, 1, 10, 1, 10, rng.standard_normal(100))],           # unknown ltmtx
+        [(2, 0, 95, 10, 1, 10, rng.standard_normal(100))],          # rows past nd
+        [(2, 0, 0, 10, 1, 10, rng.standard_normal(100))],           # nstrtl < 1
+        [(1, -1, 1, 10, 1, 10, np.zeros(0))],                       # negative kt
+    ]
+    for leaves in bad:
+        P, keep = _custom(leaves, 100)
+        rc, msg, _, _ = run_emu(emu, C.cast(C.pointer(P), C.c_void_p), 100, 4, np.ones(100))
+        assert rc != 0 and "make_plan" in msg
