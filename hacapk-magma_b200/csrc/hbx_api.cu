@@ -14,6 +14,7 @@
 
 #include "../../include/hacapk_b200.h"
 #include "hbx_engine.h"
+#include "hbx_flat.h"
 
 namespace {
 
@@ -617,56 +618,13 @@ void c_hacapk_bicgstab_cax_lfmtx_flat_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HAC
     if (lrtrn) *lrtrn = HBX_ERR_CUDA;
     return;
   }
-  const int n = *nd, mstep = (int)param[82];
-  const double eps = param[90];
-  std::vector<double> zr(n), zshdw(n), zp(n), zt(n), zkp(n), zakp(n), zkt(n), zakt(n);
-  auto dot = [&](const std::vector<double> &x, const std::vector<double> &y) {
-    double s = 0.0;
-    for (int i = 0; i < n; ++i) s += x[i] * y[i];
-    return s;
+  int status = HBX_OK;
+  auto gpu_mv = [](void *ctx, const double *x, double *y) -> int {
+    return hbx_matvec_host(static_cast<hbx_hmat *>(ctx), x, y, 0, nullptr, nullptr);
   };
-  auto mv = [&](const double *x, std::vector<double> &y) {
-    std::fill(y.begin(), y.end(), 0.0);
-    int rc = hbx_matvec_host(h, x, y.data(), 0, nullptr, nullptr);
-    if (rc != HBX_OK && lrtrn) *lrtrn = rc;
-  };
-  double alpha = 0.0, beta = 0.0, zeta = 0.0, znorm, zden, znormold = 1.0;
-  const double bnorm = std::sqrt(dot(std::vector<double>(b, b + n), std::vector<double>(b, b + n)));
-  for (int i = 0; i < n; ++i) zr[i] = b[i];
-  mv(u, zshdw);
-  for (int i = 0; i < n; ++i) zr[i] -= zshdw[i];
-  zshdw = zr;
-  double zrnorm = std::sqrt(dot(zr, zr));
-  int steps = 0;
-  for (int step = 1; step <= mstep; ++step) {
-    if (zrnorm / bnorm < eps) break;
-    if (beta == 0.0) {
-      zp = zr;
-    } else {
-      for (int i = 0; i < n; ++i) zp[i] = (zp[i] + zeta * zakp[i]) * beta + zr[i];
-    }
-    zkp = zp;
-    mv(zkp.data(), zakp);
-    znorm = dot(zshdw, zr);
-    zden = dot(zshdw, zakp);
-    alpha = -znorm / zden;
-    znormold = znorm;
-    for (int i = 0; i < n; ++i) zt[i] = zr[i] + alpha * zakp[i];
-    alpha = -alpha;
-    zkt = zt;
-    mv(zkt.data(), zakt);
-    znorm = dot(zakt, zt);
-    zden = dot(zakt, zakt);
-    zeta = znorm / zden;
-    for (int i = 0; i < n; ++i) u[i] = u[i] + alpha * zkp[i] + zeta * zkt[i];
-    zeta = -zeta;
-    for (int i = 0; i < n; ++i) zr[i] = zt[i] + zeta * zakt[i];
-    beta = dot(zshdw, zr);
-    zrnorm = std::sqrt(dot(zr, zr));
-    beta = -alpha / zeta * beta / znormold;
-    steps = step;
-    if (param[0] > 0) std::printf(" %d: log10(zrnorm/bnorm)=%.2e\n", step, std::log10(zrnorm / bnorm));
-  }
+  const int steps = hbx::flat_bicgstab(*nd, u, b, param[90], (int)param[82], param[0] > 0 ? 1 : 0, gpu_mv, h,
+                                       &status);
+  if (lrtrn) *lrtrn = status;
   if (nstp) *nstp = steps;
   if (own) release_for(st_leafmtxp);
 }

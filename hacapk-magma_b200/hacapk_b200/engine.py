@@ -89,9 +89,15 @@ class Engine:
         return {f: getattr(si, f) for f, _ in abi.SolveInfo._fields_ if f != "reserved"}
 
     def bicgstab_host(self, b: np.ndarray, u0: np.ndarray | None = None, tol: float = 1e-8,
-                      max_iter: int = 1000, verbose: int = 0, batch: int = 8, check: bool = True):
+                      max_iter: int = 1000, verbose: int = 0, batch: int = 8, check: bool = True,
+                      inplace: bool = False):
+        """Solve with host vectors; u0 is copied unless inplace=True (then u0,
+        a contiguous float64 array, receives the solution)."""
         b = np.ascontiguousarray(b, np.float64)
-        u = np.zeros(self.nd) if u0 is None else np.array(u0, np.float64, copy=True)
+        if inplace:
+            u = u0
+        else:
+            u = np.zeros(self.nd) if u0 is None else np.array(u0, np.float64, copy=True)
         o = self._opts(tol, max_iter, verbose, batch)
         si = abi.SolveInfo()
         st = self.lib.hbx_bicgstab_host(self._h, abi.dptr(b), abi.dptr(u), C.byref(o), C.byref(si))

@@ -80,13 +80,22 @@ def _control(nrank=1, maxit=1000, tol=1e-8, verbose=0):
     return ctl, buf
 
 
-@pytest.mark.parametrize("entry", ["c_hacapk_bicgstab_cax_lfmtx_gpu_", "c_hacapk_bicgstab_cax_lfmtx_flat_"])
-def test_legacy_solver_entry_points(gpu, build_libs, entry):
-    """HACApK_SOLVER.c:421 (all on GPU) and :254 (flat): u in/out, nstp, lrtrn."""
+@pytest.mark.parametrize("entry,level,band", [("c_hacapk_bicgstab_cax_lfmtx_gpu_", 4, (1, 1)),
+                                               ("c_hacapk_bicgstab_cax_lfmtx_flat_", 3, (1, 1)),
+                                               ("c_hacapk_bicgstab_cax_lfmtx_flat_", 4, (1, 8))])
+def test_legacy_solver_entry_points(gpu, build_libs, entry, level, band):
+    """HACApK_SOLVER.c:421 (all on GPU) and :254 (flat): u in/out, nstp, lrtrn.
+
+    The flat solver keeps the reference's plain sequential host dots, so its
+    iteration count follows the last bits of each matvec: on the level-4
+    sphere the oracle loop, fed the oracle matvec plus 1e-15*max|y| of noise,
+    takes 20 to 25 iterations (20 without noise), while on level 3 it takes 14
+    whatever the noise.  Level 3 is held to +-1, level 4 to the band below and
+    to the true residual."""
     import oracle
     from hacapk_b200 import abi, configs
     lib = abi.engine_lib()
-    H, b = configs.c1(4)
+    H, b = configs.c1(level)
     ctl, buf = _control()
     u = np.zeros(H.nd)
     nd, nstp, lrtrn = C.c_int(H.nd), C.c_int(-1), C.c_int(-1)
@@ -94,7 +103,7 @@ def test_legacy_solver_entry_points(gpu, build_libs, entry):
                         C.byref(lrtrn))
     _, n_ref, _, _ = oracle.bicgstab(H.st, b, tol=1e-8, max_iter=1000, kind="restated")
     assert lrtrn.value == 0
-    assert abs(nstp.value - n_ref) <= 1
+    assert n_ref - band[0] <= nstp.value <= n_ref + band[1]
     r = b - oracle.matvec(H.st, u)
     assert np.linalg.norm(r) / np.linalg.norm(b) < 1.05e-8
 
