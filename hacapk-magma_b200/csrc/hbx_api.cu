@@ -297,6 +297,54 @@ int hbx_matvec(hbx_hmat *h, double alpha, const double *x, double beta, const do
   return HBX_OK;
 }
 
+// Allocation-free matvec.  Some callers cannot call cudaMalloc once they are
+// running: a host code that has reserved the GPU's memory for its own pool
+// (a later cudaMalloc finds no room) or a loop that must not stall (cudaFree
+// synchronizes the whole device).  This variant launches the same kernel as
+// hbx_matvec but takes its per-call scratch -- the V^T x segments (zbu) and
+// the grid-barrier words -- from a fixed 1 MiB device array compiled into the
+// library, so the call allocates nothing.  The array's address is looked up
+// once per device, with that device current, on its first call (make that
+// first call before any stream capture).
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[128] = {nullptr};
+
+int hbx_matvec_noalloc(hbx_hmat *h, double alpha, const double *x, double beta, const double *yin, double *y,
+                       void *stream) {
+  if (!h || !x || !y) return fail(HBX_ERR_INVALID, "hbx_matvec_noalloc: NULL argument");
+  if (beta != 0.0 && !yin) return fail(HBX_ERR_INVALID, "hbx_matvec_noalloc: beta != 0 needs yin");
+  if (h->plan.zbu_len > hbx::kNoallocZbuMax)
+    return fail(HBX_ERR_INVALID, "hbx_matvec_noalloc: the matrix needs " + std::to_string(h->plan.zbu_len) +
+                                     " zbu doubles; the static scratch holds " +
+                                     std::to_string(hbx::kNoallocZbuMax) + " (use hbx_matvec)");
+  if (h->device < 0 || h->device >= 128) return fail(HBX_ERR_UNSUPPORTED, "hbx_matvec_noalloc: device ordinal");
+  void *base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    base = g_noalloc_ptr[h->device];
+    if (!base) {
+      int cur = -1;
+      cudaError_t e = cudaGetDevice(&cur);
+      if (e == cudaSuccess && cur != h->device) e = cudaSetDevice(h->device);
+      if (e == cudaSuccess) e = hbx::noalloc_scratch_address(&base);
+      if (cur >= 0 && cur != h->device) cudaSetDevice(cur);
+      if (e != cudaSuccess || !base) return cuda_fail(e, "hbx_matvec_noalloc: cudaGetSymbolAddress");
+      g_noalloc_ptr[h->device] = base;
+    }
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  // the barrier words must start at zero; zbu is written before it is read
+  cudaError_t e = cudaMemsetAsync(base, 0, hbx::kNoallocCtlBytes, s);
+  if (e != cudaSuccess) return cuda_fail(e, "hbx_matvec_noalloc: clear barrier words");
+  hbx::MatvecArgs a = matvec_args(h, alpha, x, beta, yin, y);
+  a.gbar = reinterpret_cast<unsigned *>(base);
+  a.zbu = reinterpret_cast<double *>(reinterpret_cast<char *>(base) + hbx::kNoallocCtlBytes);
+  a.prof = nullptr;
+  e = hbx::launch_matvec(a, h->num_ctas, s);
+  if (e != cudaSuccess) return cuda_fail(e, "hbx_matvec_noalloc launch");
+  return HBX_OK;
+}
+
 int hbx_sync(hbx_hmat *h, void *stream) {
   if (!h) return fail(HBX_ERR_INVALID, "hbx_sync: NULL handle");
   cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);

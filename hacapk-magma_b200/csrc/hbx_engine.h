@@ -65,6 +65,13 @@ struct BicgArgs {
   int max_iter;
 };
 
+// Static scratch of hbx_matvec_noalloc (hbx_kernels.cu): 256 bytes of
+// barrier words, then room for kNoallocZbuMax zbu doubles.
+constexpr size_t kNoallocScratchBytes = size_t(1) << 20;
+constexpr size_t kNoallocCtlBytes = 256;
+constexpr uint64_t kNoallocZbuMax = (kNoallocScratchBytes - kNoallocCtlBytes) / sizeof(double);
+cudaError_t noalloc_scratch_address(void **ptr);
+
 // Kernel launchers (hbx_kernels.cu).
 size_t kernel_smem_bytes();
 cudaError_t configure_kernels();

@@ -504,6 +504,14 @@ __global__ void k_dot_total(const double *part, int ncta, int slot, double *out)
 
 }  // namespace
 
+// ---- fixed scratch for hbx_matvec_noalloc -------------------------------
+// One 1 MiB array per device, held by every GPU that loads this library until
+// the process exits: [0, 256) barrier words, [256, end) the zbu segments.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
+
+// Host side: the device address of g_noalloc_scratch on the current device.
+cudaError_t noalloc_scratch_address(void **ptr) { return cudaGetSymbolAddress(ptr, g_noalloc_scratch); }
+
 size_t kernel_smem_bytes() { return SharedLayout::bytes; }
 
 cudaError_t configure_kernels() {

@@ -113,6 +113,7 @@ ENGINE_SYMBOLS = [
     ("hbx_destroy", C.c_int, [_VP]),
     ("hbx_get_info", C.c_int, [_VP, C.POINTER(Info)]),
     ("hbx_matvec", C.c_int, [_VP, C.c_double, _VP, C.c_double, _VP, _VP, _VP]),
+    ("hbx_matvec_noalloc", C.c_int, [_VP, C.c_double, _VP, C.c_double, _VP, _VP, _VP]),
     ("hbx_sync", C.c_int, [_VP, _VP]),
     ("hbx_matvec_host", C.c_int, [_VP, _DP, _DP, C.c_int, _DP, _DP]),
     ("hbx_bicgstab", C.c_int, [_VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),

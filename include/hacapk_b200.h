@@ -170,6 +170,25 @@ int hbx_get_info(const hbx_hmat *h, hbx_info *info);
 int hbx_matvec(hbx_hmat *h, double alpha, const double *x, double beta,
                const double *yin, double *y, void *stream);
 
+/* Allocation-free variant of hbx_matvec (no counterpart in the reference).
+ * For callers that cannot call cudaMalloc once they are running: a host code
+ * that reserves the GPU's memory for its own pool at start-up, where a later
+ * cudaMalloc fails for lack of room, and a time-stepping loop that must not
+ * stall, where cudaFree would synchronize the whole device.  Same kernel and
+ * same result as hbx_matvec, but the per-call scratch (the V^T x segments and
+ * the grid-barrier words) comes from one fixed 1 MiB device array compiled
+ * into the library, reserved when the library's kernels load and held by
+ * every GPU that loads them until the process exits.  Limit: matrices whose
+ * low-rank ranks sum to more than 131040 are rejected with HBX_ERR_INVALID.
+ * The call allocates nothing: it clears the barrier words and launches on
+ * `stream`.  The array's address is looked up on a device's first call: make
+ * that first call before any stream capture.  All calls share the array, so
+ * calls that overlap on the GPU (other streams, other engines) race:
+ * serialize them.  Device-side wait failures latch in the engine's error
+ * word (hbx_sync). */
+int hbx_matvec_noalloc(hbx_hmat *h, double alpha, const double *x, double beta,
+                       const double *yin, double *y, void *stream);
+
 /* Waits for `stream` and returns the device error latched by earlier async
  * calls on this engine (HBX_ERR_TIMEOUT when a bounded device wait expired),
  * clearing it. */
