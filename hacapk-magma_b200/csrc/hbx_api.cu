@@ -47,8 +47,7 @@ void free_engine(hbx_hmat *h) {
   if (cur != h->device) cudaSetDevice(h->device);
   if (h->graph) cudaGraphExecDestroy(h->graph);
   cudaFree(h->d_stream);
-  cudaFree(h->d_terms);
-  cudaFree(h->d_runs);
+  cudaFree(h->d_recs);
   cudaFree(h->d_ctas);
   cudaFree(h->d_atoms);
   cudaFree(h->d_zbu);
@@ -93,8 +92,7 @@ int check_device_error(hbx_hmat *h, cudaStream_t s) {
 hbx::MatvecArgs matvec_args(hbx_hmat *h, double alpha, const double *x, double beta, const double *yin, double *y) {
   hbx::MatvecArgs a{};
   a.stream = h->d_stream;
-  a.terms = h->d_terms;
-  a.runs = h->d_runs;
+  a.recs = h->d_recs;
   a.ctas = h->d_ctas;
   a.x = x;
   a.yin = yin;
@@ -209,10 +207,8 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hb
   cudaEventCreate(&h->ev3);
   cudaEventCreate(&h->ev4);
   if ((e = cudaMalloc(&h->d_stream, P.total_bytes)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(stream)"));
-  if ((e = cudaMalloc(&h->d_terms, std::max<size_t>(1, P.terms.size()) * sizeof(hbx::Term))) != cudaSuccess)
-    return bail(cuda_fail(e, "cudaMalloc(terms)"));
-  if ((e = cudaMalloc(&h->d_runs, std::max<size_t>(1, P.runs.size()) * sizeof(hbx::Run))) != cudaSuccess)
-    return bail(cuda_fail(e, "cudaMalloc(runs)"));
+  if ((e = cudaMalloc(&h->d_recs, std::max<size_t>(1, P.recs.size()) * sizeof(hbx::RunRec))) != cudaSuccess)
+    return bail(cuda_fail(e, "cudaMalloc(run records)"));
   if ((e = cudaMalloc(&h->d_ctas, P.ctas.size() * sizeof(hbx::CtaInfo))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(ctas)"));
   if ((e = cudaMalloc(&h->d_atoms, std::max<size_t>(1, P.atoms.size()) * sizeof(hbx::Atom))) != cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(atoms)"));
@@ -222,12 +218,9 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hb
   if ((e = cudaMalloc(&h->d_err, sizeof(int))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(err)"));
   if ((e = cudaMemcpy(h->d_stream, host.data(), P.total_bytes, cudaMemcpyHostToDevice)) != cudaSuccess)
     return bail(cuda_fail(e, "upload stream"));
-  if (!P.terms.empty() &&
-      (e = cudaMemcpy(h->d_terms, P.terms.data(), P.terms.size() * sizeof(hbx::Term), cudaMemcpyHostToDevice)) != cudaSuccess)
-    return bail(cuda_fail(e, "upload terms"));
-  if (!P.runs.empty() &&
-      (e = cudaMemcpy(h->d_runs, P.runs.data(), P.runs.size() * sizeof(hbx::Run), cudaMemcpyHostToDevice)) != cudaSuccess)
-    return bail(cuda_fail(e, "upload runs"));
+  if (!P.recs.empty() &&
+      (e = cudaMemcpy(h->d_recs, P.recs.data(), P.recs.size() * sizeof(hbx::RunRec), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return bail(cuda_fail(e, "upload run records"));
   if ((e = cudaMemcpy(h->d_ctas, P.ctas.data(), P.ctas.size() * sizeof(hbx::CtaInfo), cudaMemcpyHostToDevice)) != cudaSuccess)
     return bail(cuda_fail(e, "upload ctas"));
   if (!P.atoms.empty() &&
@@ -237,11 +230,14 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hb
   cudaMemset(h->d_err, 0, sizeof(int));
   cudaMemset(h->d_zbu, 0, std::max<uint64_t>(1, P.zbu_len) * sizeof(double));
   if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(cuda_fail(e, "hbx_create sync"));
-  // the term list stays on the host only for hbx_get_info
-  h->plan.terms.clear();
-  h->plan.terms.shrink_to_fit();
-  h->plan.runs.clear();
-  h->plan.runs.shrink_to_fit();
+  // host copies of the records and the packing tables are no longer needed
+  h->num_runs = (long long)P.recs.size();
+  h->plan.recs.clear();
+  h->plan.recs.shrink_to_fit();
+  h->plan.blocks.clear();
+  h->plan.blocks.shrink_to_fit();
+  h->plan.pieces.clear();
+  h->plan.pieces.shrink_to_fit();
   h->setup_seconds = now_s() - t0;
   *out = h;
   return HBX_OK;
@@ -273,9 +269,7 @@ int hbx_get_info(const hbx_hmat *h, hbx_info *info) {
   info->ktmax = P.ktmax;
   info->num_ctas = h->num_ctas;
   info->num_atoms = (int)P.atoms.size();
-  uint64_t nt = 0;
-  for (const auto &c : P.ctas) nt += c.n_p + c.n_d + c.n_u;
-  info->num_terms = (int)nt;
+  info->num_runs = (int)h->num_runs;
   info->precision = HBX_FP64;
   uint64_t sb = 0;
   for (const auto &c : P.ctas) sb += c.stream_bytes;
@@ -379,8 +373,7 @@ static hbx::BicgArgs bicg_args(hbx_hmat *h, const double *b, double *u, double t
   const size_t n = (size_t)h->plan.nd;
   hbx::BicgArgs a{};
   a.stream = h->d_stream;
-  a.terms = h->d_terms;
-  a.runs = h->d_runs;
+  a.recs = h->d_recs;
   a.ctas = h->d_ctas;
   a.atoms = h->d_atoms;
   a.zbu = h->d_zbu;

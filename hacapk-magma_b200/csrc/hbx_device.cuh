@@ -9,7 +9,7 @@
 //  * A sense-reversing grid barrier (count, generation) for the persistent
 //    cooperative grid, with split arrive / wait so work can be placed between
 //    the two, and the same bounded wait.
-//  * Term processors shared by the matvec and BiCGSTAB kernels.
+//  * The block-row processor shared by the matvec and BiCGSTAB kernels.
 #pragma once
 
 #include <cstdint>
@@ -24,8 +24,15 @@ constexpr uint32_t kRingMask = kRingBytes - 1;
 constexpr int kProducerWarp = kConsumerWarps;
 constexpr int kDescWarp = kConsumerWarps + 1;
 constexpr int kThreads = (kConsumerWarps + 2) * 32;
-constexpr uint32_t kDescSlotBytes = 32u * (1u + kRunTerms);  // Run header + its terms
-constexpr uint32_t kHdrWindow = 128;                          // run headers staged at a time
+// Chunks the producer prefetches into L2 beyond the ones in flight into the
+// ring.  The ring alone keeps kRingBytes in flight per SM, about what HBM
+// latency times the per-SM share of bandwidth needs, so any time consumers
+// hold a chunk shows up as lost bandwidth; the L2 prefetch keeps HBM busy
+// further ahead and turns the ring refills into L2 hits.
+#ifndef HBX_L2_AHEAD
+#define HBX_L2_AHEAD 0
+#endif
+constexpr uint32_t kL2Ahead = HBX_L2_AHEAD;
 
 // error bits written to the device error word
 enum : int { kErrPipeline = 1, kErrGridBarrier = 2, kErrProducer = 4 };
@@ -37,12 +44,10 @@ struct SharedLayout {
   static constexpr uint32_t red = empty + 8 * kRingChunks;            // [2][NW][32] double
   static constexpr uint32_t scal = red + 2 * kConsumerWarps * 32 * 8;  // 64 doubles of scratch
   static constexpr uint32_t stage = scal + 64 * 8;                     // [2][kStageCap] double
-  static constexpr uint32_t desc = stage + 2 * kStageCap * 8;          // [kDescSlots] slots
-  static constexpr uint32_t dfull = desc + kDescSlots * kDescSlotBytes;
+  static constexpr uint32_t desc = stage + 2 * kStageCap * 8;          // [kDescSlots] run records
+  static constexpr uint32_t dfull = desc + kDescSlots * kRecBytes;
   static constexpr uint32_t dempty = dfull + 8 * kDescSlots;
-  static constexpr uint32_t hbar = dempty + 8 * kDescSlots;             // header-window barrier
-  static constexpr uint32_t hdr = hbar + 16;                            // [kHdrWindow] Run
-  static constexpr uint32_t bytes = hdr + kHdrWindow * 32;
+  static constexpr uint32_t bytes = dempty + 8 * kDescSlots;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -114,6 +119,11 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 
+// Prefetch `bytes` (multiple of 16) of global memory into L2, no destination.
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 // Ampere-style asynchronous gathers into shared memory (vector staging).
 // 8-byte copies go through L1 (.ca); 16-byte copies bypass it (.cg).
 __device__ __forceinline__ void cp_async8(void *dst, const void *src) {
@@ -140,6 +150,13 @@ __device__ __forceinline__ double ld_cg(const double *p) { return __ldcg(p); }
 __device__ __forceinline__ double lds_f64(uint32_t addr) {
   double v;
   asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(addr));
+  return v;
+}
+
+// 16-byte shared load (address 16-byte aligned).
+__device__ __forceinline__ double2 lds_f64x2(uint32_t addr) {
+  double2 v;
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(addr));
   return v;
 }
 
@@ -175,6 +192,11 @@ __device__ __forceinline__ void producer_run(const uint8_t *src, uint32_t bytes,
                                              uint64_t timeout_ns) {
   const uint32_t K = (bytes + kChunkBytes - 1) >> kChunkLog;
   const uint32_t total = K * npass;
+  auto prefetch = [&](uint32_t g) {
+    const uint32_t off = (g % K) << kChunkLog;
+    bulk_prefetch_l2(src + off, min((uint32_t)kChunkBytes, bytes - off));
+  };
+  for (uint32_t g = kRingChunks; g < min(total, (uint32_t)kRingChunks + kL2Ahead); ++g) prefetch(g);
   uint32_t issued = 0;
   for (uint32_t g = 0; g < total; ++g) {
     const uint32_t s = g & (kRingChunks - 1);
@@ -190,48 +212,31 @@ __device__ __forceinline__ void producer_run(const uint8_t *src, uint32_t bytes,
     mbar_arrive_expect_tx(&full[s], nb);
     bulk_g2s(ring + ((size_t)s << kChunkLog), src + off, nb, &full[s]);
     issued = g + 1;
+    if (kL2Ahead > 0 && g + kRingChunks + kL2Ahead < total) prefetch(g + kRingChunks + kL2Ahead);
   }
   // Copies still in flight must land before the CTA exits.
   const uint32_t g0 = issued > (uint32_t)kRingChunks ? issued - kRingChunks : 0;
   for (uint32_t g = g0; g < issued; ++g) mbar_wait(&full[g & (kRingChunks - 1)], (g / kRingChunks) & 1, timeout_ns);
 }
 
-// ---- descriptor warp: keeps the descriptor queue kDescSlots runs ahead of
-// the consumers.  The CTA's run headers are bulk-copied into a shared window
-// kHdrWindow at a time; each run's terms (contiguous in global memory) are
-// bulk-copied into its queue slot.  Only lane 0 works.
-__device__ __forceinline__ void desc_run(const Run *runs, uint32_t nruns, uint32_t npass, const Term *terms,
-                                         uint8_t *dbuf, uint64_t *dfull, uint64_t *dempty, Run *hdr,
-                                         uint64_t *hbar, int *err, uint64_t timeout_ns) {
+// ---- descriptor warp: keeps the descriptor queue kDescSlots run records
+// ahead of the consumers.  Records are fixed-size (kRecBytes) and contiguous
+// per CTA, so each one is a single bulk copy with no dependent load.  Only
+// lane 0 works.
+__device__ __forceinline__ void desc_run(const RunRec *recs, uint32_t nruns, uint32_t npass, uint8_t *dbuf,
+                                         uint64_t *dfull, uint64_t *dempty, int *err, uint64_t timeout_ns) {
   if ((threadIdx.x & 31) != 0) return;
   const uint32_t total = nruns * npass;
-  uint32_t win0 = 0xffffffffu, hphase = 0;
   for (uint32_t g = 0; g < total; ++g) {
     const uint32_t slot = g % kDescSlots;
-    const uint32_t r = g % nruns;
-    if (r / kHdrWindow != win0) {  // stage the next window of headers
-      win0 = r / kHdrWindow;
-      const uint32_t first = win0 * kHdrWindow;
-      const uint32_t cnt = min(kHdrWindow, nruns - first);
-      mbar_arrive_expect_tx(hbar, cnt * 32u);
-      bulk_g2s(hdr, runs + first, cnt * 32u, hbar);
-      if (!mbar_wait(hbar, hphase & 1, timeout_ns)) {
-        atomicOr(err, kErrProducer);
-        return;
-      }
-      ++hphase;
-    }
     if (g >= (uint32_t)kDescSlots) {
       if (!mbar_wait(&dempty[slot], ((g / kDescSlots) - 1) & 1, timeout_ns)) {
         atomicOr(err, kErrProducer);
         return;
       }
     }
-    const Run h = hdr[r % kHdrWindow];
-    Run *dr = reinterpret_cast<Run *>(dbuf + slot * kDescSlotBytes);
-    *dr = h;
-    mbar_arrive_expect_tx(&dfull[slot], h.nterm * 32u);
-    bulk_g2s(dr + 1, terms + h.term_first, h.nterm * 32u, &dfull[slot]);
+    mbar_arrive_expect_tx(&dfull[slot], (uint32_t)kRecBytes);
+    bulk_g2s(dbuf + slot * kRecBytes, recs + (g % nruns), (uint32_t)kRecBytes, &dfull[slot]);
   }
   // the last slots' copies must land before the CTA exits
   const uint32_t g0 = total > (uint32_t)kDescSlots ? total - kDescSlots : 0;
@@ -245,14 +250,14 @@ struct DescQ {
   uint32_t g;
   uint64_t timeout_ns;
   int *err;
-  __device__ __forceinline__ const Run *get(uint32_t i, bool &bad) {
+  __device__ __forceinline__ const RunRec *get(uint32_t i, bool &bad) {
     const uint32_t gi = g + i;
     const uint32_t slot = gi % kDescSlots;
     if (!bad && !warp_wait(&dfull[slot], (gi / kDescSlots) & 1, timeout_ns)) {
       bad = true;
       if ((threadIdx.x & 31) == 0) atomicOr(err, kErrPipeline);
     }
-    return reinterpret_cast<const Run *>(dbuf + slot * kDescSlotBytes);
+    return reinterpret_cast<const RunRec *>(dbuf + slot * kRecBytes);
   }
   __device__ __forceinline__ void release(uint32_t i) {
     __syncwarp();
@@ -344,96 +349,72 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// ---- vector staging of one run: warp w gathers the segments of the run's
-// terms w, w+NW, ... with 8-byte cp.async (segments start anywhere).  The
-// run header and its terms are read from the shared-memory descriptor queue.
-__device__ __forceinline__ void gather_run(const Run &run, const Term *terms, const double *x,
-                                           const double *zbu, double *stage) {
+// ---- vector staging of one run: warp w gathers segments w, w+NW, ... with
+// 8-byte cp.async (segments start anywhere); an odd-width block's zero
+// column is written directly.  The record is in the descriptor queue.
+__device__ __forceinline__ void gather_run(const RunRec &rec, const double *x, const double *zbu, double *stage) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (uint32_t q = w; q < run.nterm; q += kConsumerWarps) {
-    const Term T = terms[q];
-    const uint32_t len = term_vlen(T);
-    const double *src = ((T.kind & 0xff) == kTermU ? zbu : x) + T.vec;
-    for (uint32_t j = lane; j < len; j += 32) cp_async8(stage + T.voff + j, src + j);
+  const Run &run = rec.hdr;
+  const double *vec = run_kind(run) == kRunU ? zbu : x;
+  for (uint32_t q = w; q < run.nseg; q += kConsumerWarps) {
+    const Seg sg = rec.seg[q];
+    for (uint32_t e = lane; e < sg.len; e += 32) cp_async8(stage + sg.dst + e, vec + sg.src + e);
   }
+  if ((run.flags & kPadCol) && w == 0 && lane == 0) stage[2u * run.npair - 1u] = 0.0;
   cp_async_commit();
 }
 
-__device__ __forceinline__ double ring_ld(const uint8_t *ring, uint32_t abs_byte) {
-  return *reinterpret_cast<const double *>(ring + (abs_byte & kRingMask));
-}
-
-// ---- P chunk term: every panel has at most NW columns, so a warp owns at
-// most one column l = (w - rot) mod NW of it:  acc += sum_t V(t, l) x(t);
-// the warp reduces and writes zbu on the panel's last chunk.
-__device__ __forceinline__ void term_panel(const Term &T, uint32_t stage_s, double *zbu, Ring &R, double &acc) {
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t kc = T.ncol, hv = T.nrow;
-  const uint32_t l = (uint32_t)((w - (int)T.rot) & (kConsumerWarps - 1));
-  if (T.kind & kPanelFirst) acc = 0.0;
-  if (l >= kc) return;
-  const uint32_t p = T.pos + l * hv * 8u;
-  R.ensure(p, p + hv * 8u);
-  const uint32_t ring_s = smem_u32(R.buf);
-  const uint32_t q = ((R.base << kChunkLog) + p + (uint32_t)lane * 8u) & kRingMask;
-  const uint32_t xs = stage_s + (T.voff + (uint32_t)lane) * 8u;
-  double s0 = 0.0, s1 = 0.0;
-  uint32_t t = 0;
-  if (q + hv * 8u <= kRingBytes) {  // column does not wrap around the ring end
-    const uint32_t a = ring_s + q;
-    for (; t + 64 <= hv; t += 64) {
-      s0 = fma(lds_f64(a + 8u * t), lds_f64(xs + 8u * t), s0);
-      s1 = fma(lds_f64(a + 8u * t + 256u), lds_f64(xs + 8u * t + 256u), s1);
-    }
-  }
-  for (; t + 32 <= hv; t += 32) s0 = fma(lds_f64(ring_s + ((q + 8u * t) & kRingMask)), lds_f64(xs + 8u * t), s0);
-  if (t + lane < hv) s1 = fma(lds_f64(ring_s + ((q + 8u * t) & kRingMask)), lds_f64(xs + 8u * t), s1);
-  acc += s0 + s1;
-  if (T.kind & kPanelLast) {
-    const double v = warp_sum(acc);
-    if (lane == 0) zbu[T.out + l] = v;
-  }
-}
-
-// ---- D / U run: acc(lane) += sum_c A(lane, c) v(c) over the run's h x W
-// column-major block, v staged in shared memory.
-__device__ __forceinline__ void run_rows(const Run &run, uint32_t stage_s, Ring &R, double &acc) {
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t h = run.nrow, W = run.ncol;
-  const uint32_t colb = h * 8u;
+// ---- one run of a block: acc(lane) += sum over the run's column pairs of
+// B(lane, c) v(c).  Pair panel j (16h bytes, row i at 16i) is read by warp
+// (rot + j) mod NW, four panels per iteration; lanes >= h repeat row h-1 and
+// their sums are never used.
+__device__ __forceinline__ void run_block(const Run &run, uint32_t stage_s, Ring &R, double &acc) {
   constexpr uint32_t NW = kConsumerWarps;
-  uint32_t c = (uint32_t)((w - (int)run.rot) & (NW - 1));
-  const bool act = (uint32_t)lane < h;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t h = run.nrow, np = run.npair;
+  if (np == 0) return;
+  const uint32_t pb = 16u * h;
+  const uint32_t lrow = 16u * min((uint32_t)lane, h - 1u);
   const uint32_t ring_s = smem_u32(R.buf);
-  const uint32_t lo = (R.base << kChunkLog) + (uint32_t)lane * 8u;
+  const uint32_t q0 = (R.base << kChunkLog) + run.pos + lrow;
+  uint32_t j = (uint32_t)((w - (int)run.rot) & (int)(NW - 1));
   double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-  for (; c + 3 * NW < W; c += 4 * NW) {
-    const uint32_t p0 = run.pos + c * colb;
-    R.ensure(p0, p0 + 3 * NW * colb + colb);
-    const uint32_t vq = stage_s + 8u * c;
-    const double v0 = lds_f64(vq), v1 = lds_f64(vq + 8u * NW);
-    const double v2 = lds_f64(vq + 16u * NW), v3 = lds_f64(vq + 24u * NW);
-    if (act) {
-      const uint32_t q = (lo + p0) & kRingMask;
-      if (q + 3 * NW * colb < kRingBytes) {
-        const uint32_t a = ring_s + q;
-        a0 = fma(lds_f64(a), v0, a0);
-        a1 = fma(lds_f64(a + NW * colb), v1, a1);
-        a2 = fma(lds_f64(a + 2 * NW * colb), v2, a2);
-        a3 = fma(lds_f64(a + 3 * NW * colb), v3, a3);
-      } else {
-        a0 = fma(lds_f64(ring_s + q), v0, a0);
-        a1 = fma(lds_f64(ring_s + ((q + NW * colb) & kRingMask)), v1, a1);
-        a2 = fma(lds_f64(ring_s + ((q + 2 * NW * colb) & kRingMask)), v2, a2);
-        a3 = fma(lds_f64(ring_s + ((q + 3 * NW * colb) & kRingMask)), v3, a3);
-      }
+  for (; j + 3 * NW < np; j += 4 * NW) {
+    const uint32_t p0 = run.pos + j * pb;
+    R.ensure(p0, p0 + 3 * NW * pb + pb);
+    const uint32_t vq = stage_s + 16u * j;
+    const double2 v0 = lds_f64x2(vq), v1 = lds_f64x2(vq + 16 * NW);
+    const double2 v2 = lds_f64x2(vq + 32 * NW), v3 = lds_f64x2(vq + 48 * NW);
+    const uint32_t q = (q0 + j * pb) & kRingMask;
+    double2 m0, m1, m2, m3;
+    if (q + 3 * NW * pb + 16u <= kRingBytes) {  // the four panels do not wrap around the ring end
+      const uint32_t a = ring_s + q;
+      m0 = lds_f64x2(a);
+      m1 = lds_f64x2(a + NW * pb);
+      m2 = lds_f64x2(a + 2 * NW * pb);
+      m3 = lds_f64x2(a + 3 * NW * pb);
+    } else {
+      m0 = lds_f64x2(ring_s + q);
+      m1 = lds_f64x2(ring_s + ((q + NW * pb) & kRingMask));
+      m2 = lds_f64x2(ring_s + ((q + 2 * NW * pb) & kRingMask));
+      m3 = lds_f64x2(ring_s + ((q + 3 * NW * pb) & kRingMask));
     }
+    a0 = fma(m0.x, v0.x, a0);
+    a1 = fma(m0.y, v0.y, a1);
+    a2 = fma(m1.x, v1.x, a2);
+    a3 = fma(m1.y, v1.y, a3);
+    a0 = fma(m2.x, v2.x, a0);
+    a1 = fma(m2.y, v2.y, a1);
+    a2 = fma(m3.x, v3.x, a2);
+    a3 = fma(m3.y, v3.y, a3);
   }
-  for (; c < W; c += NW) {
-    const uint32_t p0 = run.pos + c * colb;
-    R.ensure(p0, p0 + colb);
-    const double vv = lds_f64(stage_s + 8u * c);
-    if (act) a0 = fma(lds_f64(ring_s + ((lo + p0) & kRingMask)), vv, a0);
+  for (; j < np; j += NW) {
+    const uint32_t p0 = run.pos + j * pb;
+    R.ensure(p0, p0 + pb);
+    const double2 v = lds_f64x2(stage_s + 16u * j);
+    const double2 m = lds_f64x2(ring_s + ((q0 + j * pb) & kRingMask));
+    a0 = fma(m.x, v.x, a0);
+    a1 = fma(m.y, v.y, a1);
   }
   acc += (a0 + a1) + (a2 + a3);
 }

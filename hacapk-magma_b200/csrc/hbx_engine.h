@@ -32,8 +32,7 @@ struct BicgState {
 
 struct MatvecArgs {
   const uint8_t *stream;
-  const Term *terms;
-  const Run *runs;
+  const RunRec *recs;
   const CtaInfo *ctas;
   const double *x;
   const double *yin;
@@ -48,8 +47,7 @@ struct MatvecArgs {
 
 struct BicgArgs {
   const uint8_t *stream;
-  const Term *terms;
-  const Run *runs;
+  const RunRec *recs;
   const CtaInfo *ctas;
   const Atom *atoms;
   double *zbu;
@@ -89,8 +87,8 @@ struct hbx_hmat {
   int num_ctas = 0;
   hbx::Plan plan;
   uint8_t *d_stream = nullptr;
-  hbx::Term *d_terms = nullptr;
-  hbx::Run *d_runs = nullptr;
+  hbx::RunRec *d_recs = nullptr;
+  long long num_runs = 0;
   hbx::CtaInfo *d_ctas = nullptr;
   hbx::Atom *d_atoms = nullptr;
   double *d_zbu = nullptr;

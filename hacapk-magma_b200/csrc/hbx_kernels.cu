@@ -9,12 +9,13 @@
 //               both H-matvecs, the vector updates and all dot products, with
 //               compensated (Dot2) partial sums reduced in a fixed order.
 //
-// All kernels run one CTA per SM: 8 consumer warps + 1 producer warp.  The
-// producer streams the CTA's packed terms through a shared-memory ring with
-// cp.async.bulk; consumer warps own disjoint columns of every term (rotated
-// so the work stays balanced) and accumulate in registers.  Grid-wide
-// dependencies (zbu complete, dot products complete) use a bounded grid
-// barrier; the launch is cooperative so every CTA is resident.
+// All kernels run one CTA per SM: 16 consumer warps, one producer warp and
+// one descriptor warp.  The producer streams the CTA's packed runs through a
+// shared-memory ring with cp.async.bulk; consumer warps own interleaved
+// column pairs of every run (rotated so the work stays balanced) and
+// accumulate in registers.  Grid-wide dependencies (zbu complete, dot
+// products complete) use a bounded grid barrier; the launch is cooperative so
+// every CTA is resident.
 #include "hbx_device.cuh"
 #include "hbx_engine.h"
 
@@ -30,10 +31,8 @@ struct Smem {
   double *red;    // [2][NW][32]
   double *scal;   // 64 doubles
   double *stage;  // [2][kStageCap]
-  uint8_t *desc;  // descriptor queue
+  uint8_t *desc;  // descriptor queue (run records)
   uint64_t *dfull, *dempty;
-  uint64_t *hbar;
-  Run *hdr;
 };
 
 __device__ __forceinline__ Smem smem_layout(uint8_t *base) {
@@ -47,8 +46,6 @@ __device__ __forceinline__ Smem smem_layout(uint8_t *base) {
   s.desc = base + SharedLayout::desc;
   s.dfull = reinterpret_cast<uint64_t *>(base + SharedLayout::dfull);
   s.dempty = reinterpret_cast<uint64_t *>(base + SharedLayout::dempty);
-  s.hbar = reinterpret_cast<uint64_t *>(base + SharedLayout::hbar);
-  s.hdr = reinterpret_cast<Run *>(base + SharedLayout::hdr);
   return s;
 }
 
@@ -62,35 +59,37 @@ __device__ __forceinline__ void init_barriers(const Smem &s) {
       mbar_init(&s.dfull[i], 1);
       mbar_init(&s.dempty[i], NW);
     }
-    mbar_init(s.hbar, 1);
     mbar_fence_init();
   }
   __syncthreads();
 }
 
-// Cross-warp reduction of one atom (rows r0..r0+h-1): sum the 8 warp
-// partials in warp order.  mode 0: y = alpha*s + beta*yin;  mode 1: y += alpha*s.
-__device__ __forceinline__ uint32_t term_end(const Term &T) { return T.pos + T.nrow * T.ncol * 8u; }
-__device__ __forceinline__ uint32_t run_end(const Run &r) { return r.pos + r.nrow * r.ncol * 8u; }
+__device__ __forceinline__ uint32_t run_end(const Run &r) { return r.pos + run_bytes(r); }
 
-// Before a named barrier a warp gives back every ring chunk it will not read
-// again, so that warps still working on the same atom or section can get the
-// chunks they need from the producer (no warp waits at a barrier while holding
+// End of a block (rows out..out+h-1): the NW warp partials are summed in warp
+// order by warp (nae mod NW), so the summing work rotates over the warps.
+// kind P: zbu[out+i] = s;  D: y = alpha*s + beta*yin;  U: y += alpha*s.
+// Before the named barrier a warp gives back every ring chunk it will not
+// read again, so that warps still working on the block can get the chunks
+// they need from the producer (no warp waits at a barrier while holding
 // chunks the others depend on).
-__device__ __forceinline__ void atom_end(const Run &T, double &acc, int &buf, double *red, double alpha,
-                                         double beta, const double *yin, double *y, int mode, Ring &R) {
+__device__ __forceinline__ void block_end(const Run &run, double &acc, uint32_t &nae, double *red, double alpha,
+                                          double beta, const double *yin, double *y, double *zbu, Ring &R) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t h = T.nrow;
-  R.release_below(R.base + (run_end(T) >> kChunkLog));
-  double *rb = red + buf * (NW * 32);
+  const uint32_t h = run.nrow;
+  R.release_below(R.base + (run_end(run) >> kChunkLog));
+  double *rb = red + (nae & 1u) * (NW * 32);
   if ((uint32_t)lane < h) rb[w * 32 + lane] = acc;
   named_bar(2, kConsumerThreads);
-  if (w == 0 && (uint32_t)lane < h) {
+  if ((uint32_t)w == (nae & (NW - 1)) && (uint32_t)lane < h) {
     double s = rb[lane];
 #pragma unroll
     for (int q = 1; q < NW; ++q) s += rb[q * 32 + lane];
-    const uint32_t r = T.out + lane;
-    if (mode == 0) {
+    const uint32_t r = run.out + lane;
+    const uint32_t kind = run_kind(run);
+    if (kind == kRunP) {
+      zbu[r] = s;
+    } else if (kind == kRunD) {
       double v = alpha * s;
       if (beta != 0.0) v = fma(beta, yin[r], v);
       y[r] = v;
@@ -99,7 +98,7 @@ __device__ __forceinline__ void atom_end(const Run &T, double &acc, int &buf, do
     }
   }
   acc = 0.0;
-  buf ^= 1;
+  ++nae;
 }
 
 // Runs a section: gathers run k+1's vector segments while computing run k.
@@ -111,22 +110,16 @@ template <class F>
 __device__ __forceinline__ void run_section(uint32_t nruns, DescQ &Q, const double *x, const double *zbu,
                                             const Smem &sm, int &sbuf, Ring &R, F &&process) {
   if (nruns == 0) return;
-  {
-    const Run *r0 = Q.get(0, R.bad);
-    gather_run(*r0, reinterpret_cast<const Term *>(r0 + 1), x, zbu, sm.stage + sbuf * kStageCap);
-  }
+  gather_run(*Q.get(0, R.bad), x, zbu, sm.stage + sbuf * kStageCap);
   uint32_t rend = 0;
   for (uint32_t k = 0; k < nruns; ++k) {
     // give back the ring chunks of the previous run before blocking
     if (k > 0) R.release_below(R.base + (rend >> kChunkLog));
     cp_async_wait_all();
     named_bar(3, kConsumerThreads);
-    if (k + 1 < nruns) {
-      const Run *rn = Q.get(k + 1, R.bad);
-      gather_run(*rn, reinterpret_cast<const Term *>(rn + 1), x, zbu, sm.stage + (sbuf ^ 1) * kStageCap);
-    }
-    const Run *rc = Q.get(k, R.bad);
-    rend = process(*rc, reinterpret_cast<const Term *>(rc + 1), sm.stage + sbuf * kStageCap);
+    if (k + 1 < nruns) gather_run(*Q.get(k + 1, R.bad), x, zbu, sm.stage + (sbuf ^ 1) * kStageCap);
+    const RunRec *rc = Q.get(k, R.bad);
+    rend = process(rc->hdr, smem_u32(sm.stage + sbuf * kStageCap));
     Q.release(k);
     sbuf ^= 1;
   }
@@ -139,24 +132,22 @@ __device__ __forceinline__ void run_section(uint32_t nruns, DescQ &Q, const doub
 __device__ __forceinline__ void matvec_body(Ring &R, DescQ &Q, uint32_t K, const CtaInfo &ci, const double *x,
                                             double alpha, double beta,
                                             const double *yin, double *y, double *zbu, unsigned *gbar, int *err,
-                                            uint64_t timeout_ns, const Smem &sm, int &buf, int &sbuf,
+                                            uint64_t timeout_ns, const Smem &sm, uint32_t &nae, int &sbuf,
                                             unsigned long long *prof = nullptr) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   auto stamp = [&](int k) {
     if (prof && w == 0 && lane == 0) prof[blockIdx.x * 8 + k] = gtimer();
   };
   stamp(0);
-  // ---- P: zbu = V^T x for this CTA's panels
-  double pacc = 0.0;
+  double acc = 0.0;
+  auto block = [&](const Run &run, uint32_t stage_s) {
+    run_block(run, stage_s, R, acc);
+    if (run.flags & kLast) block_end(run, acc, nae, sm.red, alpha, beta, yin, y, zbu, R);
+    return run_end(run);
+  };
+  // ---- P: zbu = V^T x for this CTA's slabs
   uint32_t pend = 0;
-  run_section(ci.nr_p, Q, x, zbu, sm, sbuf, R, [&](const Run &run, const Term *dt, const double *stage) {
-    for (uint32_t q = 0; q < run.nterm; ++q) {
-      const Term T = dt[q];
-      term_panel(T, smem_u32(stage), zbu, R, pacc);
-      pend = term_end(T);
-    }
-    return pend;
-  });
+  run_section(ci.nr_p, Q, x, zbu, sm, sbuf, R, [&](const Run &run, uint32_t st) { return pend = block(run, st); });
   R.release_below(R.base + (pend >> kChunkLog));
   stamp(1);
   if (lane == 0) __threadfence();
@@ -168,14 +159,8 @@ __device__ __forceinline__ void matvec_body(Ring &R, DescQ &Q, uint32_t K, const
     grid_arrive(gbar, gridDim.x);
   }
   // ---- D: dense rows of the owned atoms (hides the barrier latency)
-  double acc = 0.0;
   uint32_t dend = pend;
-  run_section(ci.nr_d, Q, x, zbu, sm, sbuf, R, [&](const Run &run, const Term *, const double *stage) {
-    run_rows(run, smem_u32(stage), R, acc);
-    if (run.flags & kAtomEnd) atom_end(run, acc, buf, sm.red, alpha, beta, yin, y, 0, R);
-    dend = run_end(run);
-    return dend;
-  });
+  run_section(ci.nr_d, Q, x, zbu, sm, sbuf, R, [&](const Run &run, uint32_t st) { return dend = block(run, st); });
   R.release_below(R.base + (dend >> kChunkLog));
   stamp(3);
   // ---- wait for every CTA's zbu
@@ -192,11 +177,7 @@ __device__ __forceinline__ void matvec_body(Ring &R, DescQ &Q, uint32_t K, const
   stamp(4);
   if (sm.scal[63] == 0.0) R.bad = true;
   // ---- U: U rows of the owned atoms times zbu
-  run_section(ci.nr_u, Q, x, zbu, sm, sbuf, R, [&](const Run &run, const Term *, const double *stage) {
-    run_rows(run, smem_u32(stage), R, acc);
-    if (run.flags & kAtomEnd) atom_end(run, acc, buf, sm.red, alpha, beta, yin, y, 1, R);
-    return run_end(run);
-  });
+  run_section(ci.nr_u, Q, x, zbu, sm, sbuf, R, [&](const Run &run, uint32_t st) { return block(run, st); });
   R.release_below(R.base + K);
   stamp(5);
 }
@@ -216,14 +197,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   }
   if (w == kDescWarp) {
     if (nruns > 0)
-      desc_run(a.runs + ci.run_begin, nruns, 1, a.terms, sm.desc, sm.dfull, sm.dempty, sm.hdr, sm.hbar, a.err,
-               a.timeout_ns);
+      desc_run(a.recs + ci.rec_begin, nruns, 1, sm.desc, sm.dfull, sm.dempty, a.err, a.timeout_ns);
     return;
   }
   Ring R{sm.ring, sm.full, sm.empty, 0, 0, 0, a.timeout_ns, a.err, false};
   DescQ Q{sm.desc, sm.dfull, sm.dempty, 0, a.timeout_ns, a.err};
-  int buf = 0, sbuf = 0;
-  matvec_body(R, Q, K, ci, a.x, a.alpha, a.beta, a.yin, a.y, a.zbu, a.gbar, a.err, a.timeout_ns, sm, buf, sbuf,
+  uint32_t nae = 0;
+  int sbuf = 0;
+  matvec_body(R, Q, K, ci, a.x, a.alpha, a.beta, a.yin, a.y, a.zbu, a.gbar, a.err, a.timeout_ns, sm, nae, sbuf,
               a.prof);
   R.drain(K);
 }
@@ -390,13 +371,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
   if (w == kDescWarp) {
     if (nruns > 0)
-      desc_run(a.runs + ci.run_begin, nruns, 2, a.terms, sm.desc, sm.dfull, sm.dempty, sm.hdr, sm.hbar, a.err,
-               a.timeout_ns);
+      desc_run(a.recs + ci.rec_begin, nruns, 2, sm.desc, sm.dfull, sm.dempty, a.err, a.timeout_ns);
     return;
   }
   Ring R{sm.ring, sm.full, sm.empty, 0, 0, 0, a.timeout_ns, a.err, false};
   DescQ Q{sm.desc, sm.dfull, sm.dempty, 0, a.timeout_ns, a.err};
-  int buf = 0, sbuf = 0;
+  uint32_t nae = 0;
+  int sbuf = 0;
 
   // ---- S1: p = r + beta*(p - zeta*Ap)  (p = r on the first step)
   if (beta == 0.0) {
@@ -419,7 +400,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
 
   // ---- S2: Ap = H p;  rh . Ap
-  matvec_body(R, Q, K, ci, a.p, 1.0, 0.0, nullptr, a.ap, a.zbu, a.gbar, a.err, a.timeout_ns, sm, buf, sbuf);
+  matvec_body(R, Q, K, ci, a.p, 1.0, 0.0, nullptr, a.ap, a.zbu, a.gbar, a.err, a.timeout_ns, sm, nae, sbuf);
   {
     Acc2 acc[1] = {{0, 0}};
     named_bar(1, kConsumerThreads);
@@ -441,7 +422,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
 
   // ---- S4: At = H t;  At . t,  At . At
   R.base = K;
-  matvec_body(R, Q, K, ci, a.t, 1.0, 0.0, nullptr, a.at, a.zbu, a.gbar, a.err, a.timeout_ns, sm, buf, sbuf);
+  matvec_body(R, Q, K, ci, a.t, 1.0, 0.0, nullptr, a.at, a.zbu, a.gbar, a.err, a.timeout_ns, sm, nae, sbuf);
   {
     Acc2 acc[2] = {{0, 0}, {0, 0}};
     named_bar(1, kConsumerThreads);

@@ -3,16 +3,19 @@
 // Replaces the setup of c_hacapk_adot_body_lfcpy_batch_sorted_
 // (HACApK_BATCH_SORT.c:86-858): where the reference sorts the GEMVs of the
 // two phases by size (:269-369) and uploads each transposed panel padded to
-// lda=roundup(M,32) (:541-811), this planner splits the leaves into V-panels
-// and row-atom terms, balances them over the persistent CTAs by bytes
-// (longest-processing-time first), and packs every CTA's terms back to back
-// with no padding.
+// lda=roundup(M,32) (:541-811), this planner stacks the V factors of every
+// column cluster into P slabs, cuts the dense and U factors into row-atom
+// blocks, balances the blocks over the persistent CTAs by bytes (longest
+// processing time first), and packs every CTA's runs back to back as
+// column-pair panels (one zero column per odd-width block, nothing else).
 #include "hbx_plan.h"
 
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <numeric>
 #include <queue>
+#include <utility>
 
 #include <omp.h>
 
@@ -28,12 +31,10 @@ const double *a2_of(const stc_HACApK_leafmtx *s) {
   return reinterpret_cast<const double *>(reinterpret_cast<const char *>(s->a1) + s->a1size);
 }
 
-constexpr uint64_t kTermOverhead = 256;  // bytes-equivalent fixed cost of a term
+bool lowrank_active(const stc_HACApK_leafmtx *s) { return s->ltmtx == 1 && s->kt > 0 && s->ndl > 0 && s->ndt > 0; }
+bool dense_active(const stc_HACApK_leafmtx *s) { return s->ltmtx == 2 && s->ndl > 0 && s->ndt > 0; }
 
-struct Panel {
-  int leaf, l0, kc;
-  uint64_t bytes;
-};
+constexpr uint64_t kRunOverhead = 2048;  // bytes-equivalent fixed cost of a run (balancing only)
 
 // Min-heap load balancer (longest processing time first).
 struct Bins {
@@ -52,6 +53,53 @@ struct Bins {
   }
 };
 
+uint64_t block_cost(uint32_t h, uint32_t W) {
+  const uint64_t wp = W + (W & 1u);
+  return 8ull * h * wp + kRunOverhead * (1 + wp / kStageCap);
+}
+
+// Vector index of block column c (c < W): P -> x index, D -> x index, U -> zbu index.
+struct ColumnMap {
+  const Plan &plan;
+  const Block &b;
+  uint32_t p_x0;  // P: x index of column 0
+  // walks the pieces of a D/U block; returns vsrc of column c and the number
+  // of following columns (c included) that stay contiguous in the same piece
+  std::pair<uint32_t, uint32_t> at(uint32_t c, uint32_t &piece, uint32_t &piece_c0) const {
+    if (b.kind == kRunP) return {p_x0 + c, b.W - c};
+    while (piece < b.npiece && c >= piece_c0 + plan.pieces[b.piece_begin + piece].n) {
+      piece_c0 += plan.pieces[b.piece_begin + piece].n;
+      ++piece;
+    }
+    const Piece &P = plan.pieces[b.piece_begin + piece];
+    return {P.vsrc + (c - piece_c0), P.n - (c - piece_c0)};
+  }
+};
+
+// Gather segments of block columns [c0, c1) (c1 <= W): contiguous vector
+// ranges merged, each at most kSegMax long.
+void segments(const ColumnMap &M, uint32_t c0, uint32_t c1, std::vector<Seg> &out) {
+  out.clear();
+  uint32_t piece = 0, piece_c0 = 0;
+  uint32_t c = c0;
+  while (c < c1) {
+    auto [src, avail] = M.at(c, piece, piece_c0);
+    uint32_t n = std::min(avail, c1 - c);
+    if (!out.empty()) {
+      Seg &L = out.back();
+      if (L.src + L.len == src && L.len < (uint32_t)kSegMax) {
+        const uint32_t take = std::min<uint32_t>(n, kSegMax - L.len);
+        L.len = (uint16_t)(L.len + take);
+        c += take;
+        continue;
+      }
+    }
+    const uint32_t take = std::min<uint32_t>(n, kSegMax);
+    out.push_back(Seg{src, (uint16_t)take, (uint16_t)(c - c0)});
+    c += take;
+  }
+}
+
 }  // namespace
 
 int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, std::string &err) {
@@ -66,9 +114,8 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
   plan.nlf = nlf;
   plan.num_ctas = num_ctas;
 
-  // ---- validation, zbu offsets
-  std::vector<uint64_t> zoff(nlf, 0);
-  uint64_t zlen = 0;
+  // ---- validation and storage counts
+  uint64_t ktsum = 0;
   for (int ip = 0; ip < nlf; ++ip) {
     const stc_HACApK_leafmtx *s = leaf_at(st, ip);
     if (s->ltmtx != 1 && s->ltmtx != 2) { err = "leaf " + std::to_string(ip) + ": ltmtx not 1 or 2"; return HBX_ERR_INVALID; }
@@ -79,28 +126,72 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
     }
     if (s->ltmtx == 1) {
       if (s->kt < 0) { err = "leaf " + std::to_string(ip) + ": negative kt"; return HBX_ERR_INVALID; }
-      if (s->kt > 0 && s->ndl > 0 && s->ndt > 0) {
+      if (lowrank_active(s)) {
         if (!s->a1) { err = "leaf " + std::to_string(ip) + ": null a1"; return HBX_ERR_INVALID; }
         if (s->a1size < (long long)s->ndt * s->kt * 8) { err = "leaf " + std::to_string(ip) + ": a1size smaller than ndt*kt*8"; return HBX_ERR_INVALID; }
-        zoff[ip] = zlen;
-        zlen += (uint64_t)s->kt;
+        ktsum += (uint64_t)s->kt;
         plan.lowrank_words += (uint64_t)s->kt * (uint64_t)(s->ndl + s->ndt);
         plan.nlfkt++;
         plan.ktmax = std::max(plan.ktmax, s->kt);
       }
-    } else if (s->ndl > 0 && s->ndt > 0) {
+    } else if (dense_active(s)) {
       if (!s->a1) { err = "leaf " + std::to_string(ip) + ": null a1"; return HBX_ERR_INVALID; }
       plan.dense_words += (uint64_t)s->ndl * (uint64_t)s->ndt;
     }
   }
-  plan.zbu_len = zlen;
-  uint64_t ktsum = 0;
-  for (int ip = 0; ip < nlf; ++ip) {
-    const stc_HACApK_leafmtx *s = leaf_at(st, ip);
-    if (s->ltmtx == 1 && s->kt > 0 && s->ndl > 0 && s->ndt > 0) ktsum += (uint64_t)s->kt;
-  }
+  plan.zbu_len = ktsum;
   plan.alg_bytes = 8 * (plan.dense_words + plan.lowrank_words) + 16ull * nd + 16ull * ktsum;
   plan.alg_flops = 2 * (plan.dense_words + plan.lowrank_words);
+
+  // ---- P column groups (low-rank leaves with the same nstrtt and ndt), zbu order
+  std::map<std::pair<int, int>, uint32_t> gid;
+  std::vector<std::vector<uint32_t>> gl;
+  for (int ip = 0; ip < nlf; ++ip) {
+    const stc_HACApK_leafmtx *s = leaf_at(st, ip);
+    if (!lowrank_active(s)) continue;
+    auto key = std::make_pair(s->nstrtt, s->ndt);
+    auto it = gid.find(key);
+    if (it == gid.end()) {
+      it = gid.emplace(key, (uint32_t)gl.size()).first;
+      gl.emplace_back();
+    }
+    gl[it->second].push_back((uint32_t)ip);
+  }
+  const uint32_t ngroups = (uint32_t)gl.size();
+  plan.zoff.assign(nlf, 0);
+  plan.group_leaf_begin.assign(ngroups + 1, 0);
+  std::vector<uint64_t> gz(ngroups, 0), grows(ngroups, 0);
+  {
+    uint64_t z = 0;
+    for (uint32_t g = 0; g < ngroups; ++g) {
+      plan.group_leaf_begin[g] = (uint32_t)plan.group_leaves.size();
+      gz[g] = z;
+      for (uint32_t ip : gl[g]) {
+        plan.group_leaves.push_back(ip);
+        plan.zoff[ip] = z;
+        z += (uint64_t)leaf_at(st, (int)ip)->kt;
+      }
+      grows[g] = z - gz[g];
+    }
+    plan.group_leaf_begin[ngroups] = (uint32_t)plan.group_leaves.size();
+  }
+  if (ktsum > 0xffffffffull || (uint64_t)nd > 0xffffffffull) { err = "zbu length exceeds 2^32"; return HBX_ERR_INVALID; }
+
+  // ---- P blocks: slabs of <= 32 stacked rows
+  std::vector<uint32_t> pblocks;
+  for (uint32_t g = 0; g < ngroups; ++g) {
+    const uint32_t R = (uint32_t)grows[g];
+    const uint32_t pieces = (R + kAtomMax - 1) / kAtomMax;
+    const uint32_t base = R / pieces, rem = R % pieces;
+    const uint32_t W = (uint32_t)leaf_at(st, (int)gl[g][0])->ndt;
+    uint32_t r = 0;
+    for (uint32_t p = 0; p < pieces; ++p) {
+      const uint32_t h = base + (p < rem ? 1 : 0);
+      pblocks.push_back((uint32_t)plan.blocks.size());
+      plan.blocks.push_back(Block{kRunP, (uint16_t)h, g, r, W, 0, 0});
+      r += h;
+    }
+  }
 
   // ---- row atoms
   std::vector<int> bnd;
@@ -131,14 +222,14 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
   for (int a = 0; a < natoms; ++a)
     for (uint32_t r = atoms[a].r0; r < atoms[a].r0 + atoms[a].h; ++r) row_atom[r] = a;
 
-  // ---- per-atom D and U term lists (CSR, leaf order inside an atom)
+  // ---- per-atom dense and low-rank leaf lists (CSR)
   std::vector<uint32_t> dcnt(natoms + 1, 0), ucnt(natoms + 1, 0);
   for (int ip = 0; ip < nlf; ++ip) {
     const stc_HACApK_leafmtx *s = leaf_at(st, ip);
-    if (s->ndl <= 0 || s->ndt <= 0) continue;
-    if (s->ltmtx == 1 && s->kt <= 0) continue;
+    const bool d = dense_active(s), u = lowrank_active(s);
+    if (!d && !u) continue;
     int a0 = row_atom[s->nstrtl - 1], a1 = row_atom[s->nstrtl - 2 + s->ndl];
-    for (int a = a0; a <= a1; ++a) (s->ltmtx == 2 ? dcnt : ucnt)[a + 1]++;
+    for (int a = a0; a <= a1; ++a) (d ? dcnt : ucnt)[a + 1]++;
   }
   std::partial_sum(dcnt.begin(), dcnt.end(), dcnt.begin());
   std::partial_sum(ucnt.begin(), ucnt.end(), ucnt.begin());
@@ -147,222 +238,193 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
     std::vector<uint32_t> dfill(dcnt.begin(), dcnt.end() - 1), ufill(ucnt.begin(), ucnt.end() - 1);
     for (int ip = 0; ip < nlf; ++ip) {
       const stc_HACApK_leafmtx *s = leaf_at(st, ip);
-      if (s->ndl <= 0 || s->ndt <= 0) continue;
-      if (s->ltmtx == 1 && s->kt <= 0) continue;
+      const bool d = dense_active(s), u = lowrank_active(s);
+      if (!d && !u) continue;
       int a0 = row_atom[s->nstrtl - 1], a1 = row_atom[s->nstrtl - 2 + s->ndl];
       for (int a = a0; a <= a1; ++a) {
-        if (s->ltmtx == 2) dleaf[dfill[a]++] = (uint32_t)ip;
+        if (d) dleaf[dfill[a]++] = (uint32_t)ip;
         else uleaf[ufill[a]++] = (uint32_t)ip;
       }
     }
   }
+  // D blocks (one per atom, possibly empty) and U blocks (atoms with low-rank rows)
+  std::vector<uint32_t> dblock(natoms), ublock(natoms, 0xffffffffu);
   std::vector<uint64_t> acost(natoms, 0);
   for (int a = 0; a < natoms; ++a) {
-    uint64_t c = kTermOverhead;
-    for (uint32_t q = dcnt[a]; q < dcnt[a + 1]; ++q)
-      c += (uint64_t)atoms[a].h * leaf_at(st, dleaf[q])->ndt * 8 + kTermOverhead;
-    for (uint32_t q = ucnt[a]; q < ucnt[a + 1]; ++q)
-      c += (uint64_t)atoms[a].h * leaf_at(st, uleaf[q])->kt * 8 + kTermOverhead;
-    acost[a] = c;
-  }
-
-  // ---- V-panels
-  const uint64_t total_est = 8 * (plan.dense_words + plan.lowrank_words);
-  const uint64_t budget = total_est / (uint64_t)num_ctas + 1;
-  const uint64_t panel_cap = std::max<uint64_t>(64 * 1024, budget / 3);
-  std::vector<Panel> panels;
-  for (int ip = 0; ip < nlf; ++ip) {
-    const stc_HACApK_leafmtx *s = leaf_at(st, ip);
-    if (s->ltmtx != 1 || s->kt <= 0 || s->ndl <= 0 || s->ndt <= 0) continue;
-    int np = (s->kt + kPanelCols - 1) / kPanelCols;
-    while (np < s->kt && (uint64_t)s->ndt * ((s->kt + np - 1) / np) * 8 > panel_cap) np *= 2;
-    np = std::min(np, s->kt);
-    int base = s->kt / np, rem = s->kt % np, l0 = 0;
-    for (int p = 0; p < np; ++p) {
-      int kc = base + (p < rem ? 1 : 0);
-      panels.push_back(Panel{ip, l0, kc, (uint64_t)s->ndt * kc * 8 + kTermOverhead});
-      l0 += kc;
+    Block b{kRunD, (uint16_t)atoms[a].h, (uint32_t)a, 0, 0, (uint32_t)plan.pieces.size(), 0};
+    for (uint32_t q = dcnt[a]; q < dcnt[a + 1]; ++q) {
+      const stc_HACApK_leafmtx *s = leaf_at(st, (int)dleaf[q]);
+      plan.pieces.push_back(Piece{dleaf[q], 0, (uint32_t)s->ndt, (uint32_t)(s->nstrtt - 1)});
+      b.W += (uint32_t)s->ndt;
+      b.npiece++;
+    }
+    dblock[a] = (uint32_t)plan.blocks.size();
+    plan.blocks.push_back(b);
+    acost[a] = block_cost(b.h, b.W);
+    if (ucnt[a + 1] > ucnt[a]) {
+      // zbu order, so that the segments of one column group merge
+      std::sort(uleaf.begin() + ucnt[a], uleaf.begin() + ucnt[a + 1],
+                [&](uint32_t x, uint32_t y) { return plan.zoff[x] < plan.zoff[y]; });
+      Block u{kRunU, (uint16_t)atoms[a].h, (uint32_t)a, 0, 0, (uint32_t)plan.pieces.size(), 0};
+      for (uint32_t q = ucnt[a]; q < ucnt[a + 1]; ++q) {
+        const stc_HACApK_leafmtx *s = leaf_at(st, (int)uleaf[q]);
+        plan.pieces.push_back(Piece{uleaf[q], 0, (uint32_t)s->kt, (uint32_t)plan.zoff[uleaf[q]]});
+        u.W += (uint32_t)s->kt;
+        u.npiece++;
+      }
+      ublock[a] = (uint32_t)plan.blocks.size();
+      plan.blocks.push_back(u);
+      acost[a] += block_cost(u.h, u.W);
     }
   }
 
-  // ---- balance: panels first (they gate the grid barrier), then atoms
+  // ---- balance: P slabs first (they gate the grid barrier), then atoms
   Bins bins(num_ctas);
-  std::vector<int> porder(panels.size());
-  std::iota(porder.begin(), porder.end(), 0);
-  std::stable_sort(porder.begin(), porder.end(), [&](int a, int b) { return panels[a].bytes > panels[b].bytes; });
-  std::vector<std::vector<int>> cta_panels(num_ctas), cta_atoms(num_ctas);
-  for (int q : porder) cta_panels[bins.take(panels[q].bytes)].push_back(q);
-  std::vector<int> aorder(natoms);
-  std::iota(aorder.begin(), aorder.end(), 0);
-  std::stable_sort(aorder.begin(), aorder.end(), [&](int a, int b) { return acost[a] > acost[b]; });
-  for (int a : aorder) cta_atoms[bins.take(acost[a])].push_back(a);
+  std::vector<std::vector<uint32_t>> cta_p(num_ctas), cta_atoms(num_ctas);
+  {
+    std::vector<uint32_t> order(pblocks);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+      return block_cost(plan.blocks[x].h, plan.blocks[x].W) > block_cost(plan.blocks[y].h, plan.blocks[y].W);
+    });
+    for (uint32_t b : order) cta_p[bins.take(block_cost(plan.blocks[b].h, plan.blocks[b].W))].push_back(b);
+    std::vector<int> aorder(natoms);
+    std::iota(aorder.begin(), aorder.end(), 0);
+    std::stable_sort(aorder.begin(), aorder.end(), [&](int x, int y) { return acost[x] > acost[y]; });
+    for (int a : aorder) cta_atoms[bins.take(acost[a])].push_back((uint32_t)a);
+  }
 
-  // ---- emit terms, runs and stream offsets per CTA
+  // ---- emit run records and stream offsets per CTA
   plan.ctas.resize(num_ctas);
   uint64_t off = 0;
+  std::vector<Seg> segs;
   for (int c = 0; c < num_ctas; ++c) {
-    auto &pl = cta_panels[c];
+    auto &pl = cta_p[c];
     auto &al = cta_atoms[c];
-    std::sort(pl.begin(), pl.end(), [&](int a, int b) {
-      return panels[a].leaf != panels[b].leaf ? panels[a].leaf < panels[b].leaf : panels[a].l0 < panels[b].l0;
-    });
+    std::sort(pl.begin(), pl.end());
     std::sort(al.begin(), al.end());
     CtaInfo info{};
     info.stream_off = off;
-    info.term_begin = (uint32_t)plan.terms.size();
+    info.rec_begin = (uint32_t)plan.recs.size();
     info.atom_begin = (uint32_t)plan.atoms.size();
     info.n_atoms = (uint32_t)al.size();
-    uint64_t pos = 0, rot = 0;
-    auto push = [&](uint64_t bytes, uint32_t nrow, uint32_t ncol, uint32_t vec, uint32_t out, uint16_t kind,
-                    uint32_t leaf, uint64_t trot) {
-      Term t{};
-      t.pos = (uint32_t)pos;
-      t.nrow = nrow; t.ncol = ncol; t.vec = vec; t.out = out;
-      t.kind = kind;
-      t.rot = (uint16_t)(trot % kConsumerWarps);
-      t.leaf = leaf;
-      plan.terms.push_back(t);
-      pos += bytes;
-    };
-    // P: one term per panel chunk; a panel keeps one warp rotation
-    for (int q : pl) {
-      const Panel &P = panels[q];
-      const stc_HACApK_leafmtx *s = leaf_at(st, P.leaf);
-      for (int r0 = 0; r0 < s->ndt; r0 += kPanelRows) {
-        const int hv = std::min(kPanelRows, s->ndt - r0);
-        uint16_t k = kTermP | (r0 == 0 ? kPanelFirst : 0) | (r0 + hv == s->ndt ? kPanelLast : 0);
-        push((uint64_t)hv * P.kc * 8, (uint32_t)hv, (uint32_t)P.kc, (uint32_t)(s->nstrtt - 1 + r0),
-             (uint32_t)(zoff[P.leaf] + P.l0), k, (uint32_t)P.leaf, rot);
-        info.n_p++;
+    for (uint32_t a : al) plan.atoms.push_back(atoms[a]);
+    uint64_t pos = 0;
+    uint32_t rot = 0;
+    auto emit_block = [&](uint32_t bi) -> uint32_t {
+      const Block &b = plan.blocks[bi];
+      const uint32_t Wp = b.W + (b.W & 1u);
+      ColumnMap M{plan, b, 0};
+      uint32_t out = 0;
+      if (b.kind == kRunP) {
+        const stc_HACApK_leafmtx *s = leaf_at(st, (int)plan.group_leaves[plan.group_leaf_begin[b.a]]);
+        M.p_x0 = (uint32_t)(s->nstrtt - 1);
+        out = (uint32_t)(gz[b.a] + b.r0);
+      } else {
+        out = atoms[b.a].r0;
       }
-      rot += (uint64_t)P.kc;
-    }
-    // D: dense rows of every owned atom, split into column pieces <= kStageCap
-    for (int a : al) {
-      const Atom &A = atoms[a];
-      plan.atoms.push_back(A);
-      if (dcnt[a + 1] == dcnt[a]) {
-        push(0, A.h, 0, 0, A.r0, kTermD | kAtomEnd, 0xffffffffu, rot);
-        info.n_d++;
-      }
-      for (uint32_t q = dcnt[a]; q < dcnt[a + 1]; ++q) {
-        const stc_HACApK_leafmtx *s = leaf_at(st, dleaf[q]);
-        for (int c0 = 0; c0 < s->ndt; c0 += kStageCap) {
-          const int wc = std::min(kStageCap, s->ndt - c0);
-          const bool last = (q + 1 == dcnt[a + 1]) && (c0 + wc == s->ndt);
-          push((uint64_t)A.h * wc * 8, A.h, (uint32_t)wc, (uint32_t)(s->nstrtt - 1 + c0), A.r0,
-               kTermD | (last ? kAtomEnd : 0), dleaf[q], rot);
-          rot += (uint64_t)wc;
-          info.n_d++;
+      uint32_t nr = 0, col = 0;
+      do {
+        uint32_t nc = std::min<uint32_t>(kStageCap, Wp - col);
+        segments(M, col, std::min(col + nc, b.W), segs);
+        if (segs.size() > (size_t)kRunSegs) {
+          nc = (segs[kRunSegs - 1].dst + segs[kRunSegs - 1].len) & ~1u;
+          segments(M, col, std::min(col + nc, b.W), segs);
         }
-      }
-    }
-    // U: U rows of every owned atom, split into column pieces <= kStageCap
-    for (int a : al) {
-      const Atom &A = atoms[a];
-      for (uint32_t q = ucnt[a]; q < ucnt[a + 1]; ++q) {
-        const stc_HACApK_leafmtx *s = leaf_at(st, uleaf[q]);
-        for (int c0 = 0; c0 < s->kt; c0 += kStageCap) {
-          const int wc = std::min(kStageCap, s->kt - c0);
-          const bool last = (q + 1 == ucnt[a + 1]) && (c0 + wc == s->kt);
-          push((uint64_t)A.h * wc * 8, A.h, (uint32_t)wc, (uint32_t)(zoff[uleaf[q]] + c0), A.r0,
-               kTermU | (last ? kAtomEnd : 0), uleaf[q], rot);
-          rot += (uint64_t)wc;
-          info.n_u++;
-        }
-      }
-    }
-    // runs: consecutive terms whose vector segments fit one stage buffer
-    info.run_begin = (uint32_t)plan.runs.size();
-    auto build_runs = [&](uint32_t first, uint32_t count, bool split_at_atoms) {
-      uint32_t nr = 0, i = first;
-      while (i < first + count) {
-        Run r{};
-        r.term_first = i;
-        while (i < first + count) {
-          Term &t = plan.terms[i];
-          const uint32_t len = term_vlen(t);
-          if (r.nterm > 0 && (r.vlen + len > (uint32_t)kStageCap || r.nterm == (uint32_t)kRunTerms)) break;
-          t.voff = r.vlen;
-          r.vlen += len;
-          r.nterm++;
-          i++;
-          if (split_at_atoms && (t.kind & kAtomEnd)) break;
-        }
-        if (split_at_atoms) {
-          const Term &t0 = plan.terms[r.term_first];
-          const Term &tl = plan.terms[r.term_first + r.nterm - 1];
-          r.pos = t0.pos;
-          r.nrow = t0.nrow;
-          r.ncol = r.vlen;
-          r.out = t0.out;
-          r.flags = (uint16_t)(tl.kind & kAtomEnd);
-          r.rot = t0.rot;
-        }
-        plan.runs.push_back(r);
-        nr++;
-      }
+        RunRec rec{};
+        Run &r = rec.hdr;
+        r.pos = (uint32_t)pos;
+        r.out = out;
+        r.nrow = b.h;
+        r.npair = (uint16_t)(nc / 2);
+        const bool last = (col + nc == Wp);
+        r.flags = (uint16_t)(b.kind | (col == 0 ? kFirst : 0) | (last ? kLast : 0) |
+                             (last && (b.W & 1u) ? kPadCol : 0));
+        r.rot = (uint16_t)rot;
+        r.nseg = (uint16_t)segs.size();
+        r.vlen = (uint16_t)nc;
+        r.block = bi;
+        r.col0 = col;
+        std::copy(segs.begin(), segs.end(), rec.seg);
+        plan.recs.push_back(rec);
+        if (r.flags & kPadCol) plan.pad_bytes += 8ull * b.h;
+        pos += 16ull * b.h * r.npair;
+        rot = (rot + r.npair) % kConsumerWarps;
+        col += nc;
+        ++nr;
+      } while (col < Wp);
       return nr;
     };
-    info.nr_p = build_runs(info.term_begin, info.n_p, false);
-    info.nr_d = build_runs(info.term_begin + info.n_p, info.n_d, true);
-    info.nr_u = build_runs(info.term_begin + info.n_p + info.n_d, info.n_u, true);
-    uint64_t bytes = (pos + 15) & ~uint64_t(15);
-    if (bytes > 0xffffffffull) {
+    for (uint32_t b : pl) info.nr_p += emit_block(b);
+    for (uint32_t a : al) info.nr_d += emit_block(dblock[a]);
+    for (uint32_t a : al)
+      if (ublock[a] != 0xffffffffu) info.nr_u += emit_block(ublock[a]);
+    if (pos > 0xfffffff0ull) {
       err = "a CTA stream exceeds 4 GiB; use more CTAs";
       return HBX_ERR_INVALID;
     }
-    info.stream_bytes = (uint32_t)bytes;
+    info.stream_bytes = (uint32_t)pos;  // a multiple of 16 by construction
     plan.ctas[c] = info;
-    off += (bytes + 255) & ~uint64_t(255);
+    off += (pos + 255) & ~uint64_t(255);
   }
   plan.total_bytes = std::max<uint64_t>(off, 256);
   return HBX_OK;
 }
 
 void pack_plan(const stc_HACApK_leafmtxp *st, const Plan &plan, uint8_t *dst) {
-  // zbu offset of each low-rank leaf, to recover a panel's first column
-  std::vector<uint64_t> zoff(plan.nlf, 0);
-  uint64_t z = 0;
-  for (int ip = 0; ip < plan.nlf; ++ip) {
-    const stc_HACApK_leafmtx *s = leaf_at(st, ip);
-    if (s->ltmtx == 1 && s->kt > 0 && s->ndl > 0 && s->ndt > 0) { zoff[ip] = z; z += (uint64_t)s->kt; }
-  }
   const int nc = plan.num_ctas;
 #pragma omp parallel for schedule(dynamic, 1)
   for (int c = 0; c < nc; ++c) {
     const CtaInfo &info = plan.ctas[c];
     uint8_t *base = dst + info.stream_off;
     std::memset(base, 0, info.stream_bytes);
-    const uint32_t nt = info.n_p + info.n_d + info.n_u;
-    for (uint32_t i = 0; i < nt; ++i) {
-      const Term &t = plan.terms[info.term_begin + i];
-      if (t.leaf == 0xffffffffu) continue;
-      const stc_HACApK_leafmtx *s = leaf_at(st, (int)t.leaf);
-      double *d = reinterpret_cast<double *>(base + t.pos);
-      const int kind = t.kind & 0xff;
-      if (kind == kTermP) {
-        const int ndt = s->ndt, kc = (int)t.ncol, hv = (int)t.nrow;
-        const int r0 = (int)t.vec - (s->nstrtt - 1);
-        const int l0 = (int)(t.out - zoff[t.leaf]);
-        const double *V = s->a1;  // V(t, l) = a1[t + l*ndt]
-        for (int l = 0; l < kc; ++l)
-          std::memcpy(d + (size_t)l * hv, V + (size_t)(l0 + l) * ndt + r0, (size_t)hv * 8);
-      } else if (kind == kTermD) {
-        const int h = (int)t.nrow, w = (int)t.ncol, ndt = s->ndt;
-        const int ro = (int)t.out - (s->nstrtl - 1);
-        const int c0 = (int)t.vec - (s->nstrtt - 1);
-        const double *A = s->a1;  // A(il, it) = a1[it + il*ndt]
-        for (int i = 0; i < h; ++i) {
-          const double *row = A + (size_t)(ro + i) * ndt + c0;
-          for (int cc = 0; cc < w; ++cc) d[(size_t)cc * h + i] = row[cc];
+    const uint32_t nr = info.nr_p + info.nr_d + info.nr_u;
+    std::vector<std::pair<uint32_t, uint32_t>> prow;  // P: (leaf, rank) of each slab row
+    for (uint32_t k = 0; k < nr; ++k) {
+      const Run &r = plan.recs[info.rec_begin + k].hdr;
+      const Block &b = plan.blocks[r.block];
+      const uint32_t h = r.nrow, ncol = 2u * r.npair;
+      double *d = reinterpret_cast<double *>(base + r.pos);
+      if (b.kind == kRunP) {
+        // slab rows -> (leaf, rank); V_L(t, k) = a1[t + k*ndt]
+        prow.clear();
+        uint32_t row = 0;
+        for (uint32_t q = plan.group_leaf_begin[b.a]; q < plan.group_leaf_begin[b.a + 1] && prow.size() < h; ++q) {
+          const uint32_t ip = plan.group_leaves[q];
+          const int kt = leaf_at(st, (int)ip)->kt;
+          for (int kk = 0; kk < kt && prow.size() < h; ++kk, ++row)
+            if (row >= b.r0) prow.push_back({ip, (uint32_t)kk});
         }
-      } else {
-        const int h = (int)t.nrow, w = (int)t.ncol, ndl = s->ndl;
-        const int ro = (int)t.out - (s->nstrtl - 1);
-        const int c0 = (int)(t.vec - zoff[t.leaf]);
-        const double *U = a2_of(s);  // U(i, l) = a2[i + l*ndl]
-        for (int l = 0; l < w; ++l) std::memcpy(d + (size_t)l * h, U + (size_t)(c0 + l) * ndl + ro, (size_t)h * 8);
+        for (uint32_t cc = 0; cc < ncol; ++cc) {
+          const uint32_t col = r.col0 + cc;
+          if (col >= b.W) continue;  // zero pad column
+          for (uint32_t i = 0; i < h; ++i) {
+            const stc_HACApK_leafmtx *s = leaf_at(st, (int)prow[i].first);
+            d[((size_t)(cc >> 1) * h + i) * 2 + (cc & 1)] = s->a1[(size_t)col + (size_t)prow[i].second * s->ndt];
+          }
+        }
+        continue;
+      }
+      // D / U: walk the pieces of the run's columns
+      uint32_t piece = 0, piece_c0 = 0;
+      for (uint32_t cc = 0; cc < ncol; ++cc) {
+        const uint32_t col = r.col0 + cc;
+        if (col >= b.W) continue;
+        while (col >= piece_c0 + plan.pieces[b.piece_begin + piece].n) {
+          piece_c0 += plan.pieces[b.piece_begin + piece].n;
+          ++piece;
+        }
+        const Piece &P = plan.pieces[b.piece_begin + piece];
+        const stc_HACApK_leafmtx *s = leaf_at(st, (int)P.leaf);
+        const uint32_t lc = P.c0 + (col - piece_c0);
+        // the block's atom rows, relative to the leaf's first row
+        const uint32_t atom_r0 = r.out;
+        const int ro = (int)atom_r0 - (s->nstrtl - 1);
+        for (uint32_t i = 0; i < h; ++i) {
+          double v;
+          if (b.kind == kRunD) v = s->a1[(size_t)lc + (size_t)(ro + (int)i) * s->ndt];  // A(il, it) = a1[it + il*ndt]
+          else v = a2_of(s)[(size_t)(ro + (int)i) + (size_t)lc * s->ndl];              // U(i, l) = a2[i + l*ndl]
+          d[((size_t)(cc >> 1) * h + i) * 2 + (cc & 1)] = v;
+        }
       }
     }
   }

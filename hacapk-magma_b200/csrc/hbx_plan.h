@@ -1,35 +1,39 @@
 // hbx_plan.h -- device layout of a packed H-matrix and the host planner.
 //
-// The leaf list is re-laid out once, at setup, into one byte stream per
-// persistent CTA.  A CTA's stream is contiguous in HBM, so the kernel moves
-// it into shared memory with plain 1D bulk copies (cp.async.bulk) through a
-// ring of fixed-size chunks, and every byte of H crosses HBM exactly once per
-// matvec.  The stream holds three sections, each a list of terms:
+// Every part of the H-matvec is re-laid out, once at setup, as BLOCKS: a
+// block is h <= 32 output rows times W columns, multiplied by a vector of W
+// entries gathered from x or zbu.  Three kinds of blocks make up a matvec:
 //
-//   P  V-panels: columns [l0, l0+kc) of a low-rank leaf's V (ndt x kt),
-//      stored as row chunks of <= PANEL_ROWS rows, column-major inside a
-//      chunk; one term per chunk (flags mark a panel's first and last
-//      chunk).  Output: zbu[out + l] = sum_t V(t, l0+l) x(nstrtt-1+t).
-//   D  dense terms: the rows of a dense leaf that fall in one row atom,
-//      h x ndt column-major.  Output accumulated into the atom's rows.
-//   U  low-rank terms: the rows of U (ndl x kt) that fall in one row atom,
-//      h x kt column-major, multiplied by the leaf's zbu segment.
+//   P  zbu = V^T x.  Low-rank leaves that share a column range (same nstrtt
+//      and ndt: one column cluster) are stacked, so their V^T form one tall
+//      matrix (sum of kt rows) over the same x segment; it is cut into slabs
+//      of <= 32 rows.  zbu is numbered in this stacking order, so a slab
+//      writes a contiguous zbu range.
+//   D  the rows of the dense leaves that fall in one row atom, side by side
+//      (W = sum of their ndt), times their x segments.
+//   U  the rows of the U factors that fall in one row atom, side by side
+//      (W = sum of their kt), times their zbu segments.
 //
 // Row atoms partition [0, nd) so that every leaf's row range is a union of
-// atoms and no atom is taller than 32 rows.  Each atom belongs to exactly
-// one CTA, which sums all its D and U terms in a fixed order and writes the
-// rows once: no atomics, bit-reproducible results.  The P section of every
-// CTA must complete (grid barrier) before any CTA reads zbu in its U section;
-// the D section sits between the two so the barrier latency is hidden.
+// atoms and no atom is taller than 32 rows.  An atom's D and U blocks belong
+// to one CTA, which sums them in a fixed order and writes each row itself:
+// no atomics, bit-reproducible results.  Every CTA's P blocks must finish
+// (grid barrier) before any CTA reads zbu in its U blocks; the D blocks sit
+// between the two so that the barrier latency is hidden.
 //
-// Every term reads one contiguous vector segment (P: x over its rows, D: x
-// over its columns, U: zbu over its columns).  Consecutive terms of a section
-// are grouped into runs whose segments fit a shared-memory stage buffer; the
-// consumers gather run k+1's segments with cp.async while they compute run k,
-// so no vector load is on the critical path.  A D or U run holds terms of one
-// atom only; their data is back to back in the stream and their segments back
-// to back in the stage, so the kernel treats the whole run as one h x W
-// column-major block times one staged vector.
+// A block is stored as W/2 column-pair panels, each h x 2 row-major: row i
+// of the pair (c, c+1) is the 16 bytes (B(i,c), B(i,c+1)).  One 16-byte
+// shared-memory load then gives a lane one row of two columns, and the 32
+// lanes of a warp read h*16 consecutive bytes, free of bank conflicts.  An
+// odd W gets one zero column.  A block's columns are cut into RUNS of at
+// most kStageCap columns (the vector stage buffer); all CTA data is one
+// contiguous byte stream (P runs, then D runs, then U runs) that the kernel
+// moves into shared memory with 1D bulk copies, so every byte of H crosses
+// HBM once per matvec.
+//
+// Each run has a fixed-size record (header + gather segments) that a
+// descriptor warp copies into shared memory a few runs ahead; consumer warps
+// gather run k+1's vector segments with cp.async while they compute run k.
 #pragma once
 
 #include <cstddef>
@@ -41,32 +45,55 @@
 
 namespace hbx {
 
-constexpr int kAtomMax = 32;       // rows per atom (one lane per row)
-constexpr int kPanelRows = 256;    // rows per V-panel chunk (8 per lane)
+constexpr int kAtomMax = 32;       // rows per block (one lane per row)
 constexpr int kConsumerWarps = 16; // warps that compute (+ a producer and a descriptor warp)
-constexpr int kPanelCols = kConsumerWarps;  // columns per V-panel (one per consumer warp)
-constexpr int kChunkLog = 15;      // ring chunk = 32 KB (bulk copies this size stream at HBM rate)
+#ifndef HBX_CHUNK_LOG
+#define HBX_CHUNK_LOG 15
+#endif
+#ifndef HBX_RING_CHUNKS
+#define HBX_RING_CHUNKS 4
+#endif
+constexpr int kChunkLog = HBX_CHUNK_LOG;      // ring chunk = 32 KB (bulk copies this size stream at HBM rate)
 constexpr int kChunkBytes = 1 << kChunkLog;
-constexpr int kRingChunks = 4;     // 128 KB ring per CTA
-constexpr int kStageCap = 1024;    // doubles per vector stage buffer (x2)
-constexpr int kRunTerms = 64;      // terms per run (descriptor queue slot)
-constexpr int kDescSlots = 4;      // runs staged ahead by the descriptor warp
+constexpr int kRingChunks = HBX_RING_CHUNKS;  // 128 KB ring per CTA (a power of two)
+constexpr int kStageCap = 1024;    // doubles per vector stage buffer (x2); even
+constexpr int kRunSegs = 60;       // gather segments per run record
+constexpr int kSegMax = 64;        // doubles per gather segment (two per lane at most)
+constexpr int kRecBytes = 512;     // one run record: 32-byte header + kRunSegs segments
+constexpr int kDescSlots = 8;      // run records staged ahead by the descriptor warp
 
-enum TermKind : uint16_t { kTermP = 0, kTermD = 1, kTermU = 2 };
-enum TermFlags : uint16_t { kAtomEnd = 0x100, kPanelFirst = 0x200, kPanelLast = 0x400 };
+enum RunKind : uint16_t { kRunP = 0, kRunD = 1, kRunU = 2 };
+enum RunFlags : uint16_t { kFirst = 0x100, kLast = 0x200, kPadCol = 0x400 };
 
-// 32-byte term descriptor.
-struct alignas(16) Term {
-  uint32_t pos;    // byte offset of the term's data inside the CTA stream
-  uint32_t nrow;   // P: chunk rows (<= kPanelRows);  D/U: atom height h
-  uint32_t ncol;   // P: kc;  D: columns (of ndt);  U: columns (of kt)
-  uint32_t vec;    // start of the vector segment: P, D: x index;  U: zbu index
-  uint32_t out;    // P: zbu offset of the panel's column 0;  D/U: first atom row
-  uint16_t kind;   // TermKind | TermFlags
-  uint16_t rot;    // consumer warp that takes column 0 of this term
-  uint32_t leaf;   // leaf index (packing and diagnostics)
-  uint32_t voff;   // offset of the vector segment in the run's stage buffer
+// Gather segment: stage[dst + e] = vec[src + e], e < len (vec = x or zbu).
+struct Seg {
+  uint32_t src;
+  uint16_t len;
+  uint16_t dst;
 };
+static_assert(sizeof(Seg) == 8, "Seg layout");
+
+// 32-byte run header; its segments follow it in the run record.
+struct alignas(16) Run {
+  uint32_t pos;    // byte offset of the run's pair panels in the CTA stream (16-aligned)
+  uint32_t out;    // first output row: zbu index (P) or y row (D, U)
+  uint16_t nrow;   // h, 1..32
+  uint16_t npair;  // column pairs; 2*npair <= kStageCap
+  uint16_t flags;  // RunKind | RunFlags
+  uint16_t rot;    // consumer warp that takes pair 0
+  uint16_t nseg;   // gather segments (<= kRunSegs)
+  uint16_t vlen;   // doubles staged: 2*npair
+  uint32_t block;  // block index (host-side packing and checks)
+  uint32_t col0;   // first block column of the run
+  uint32_t pad;
+};
+static_assert(sizeof(Run) == 32, "Run must stay 32 bytes");
+
+struct alignas(16) RunRec {
+  Run hdr;
+  Seg seg[kRunSegs];
+};
+static_assert(sizeof(RunRec) == kRecBytes, "RunRec must be kRecBytes");
 
 #ifdef __CUDACC__
 #define HBX_HD __host__ __device__
@@ -74,33 +101,16 @@ struct alignas(16) Term {
 #define HBX_HD
 #endif
 
-HBX_HD inline uint32_t term_vlen(const Term &t) {
-  return (t.kind & 0xff) == kTermP ? t.nrow : t.ncol;
-}
-
-struct alignas(16) Run {
-  uint32_t term_first;  // absolute index into the term array
-  uint32_t nterm;
-  uint32_t vlen;        // doubles gathered into the stage buffer
-  uint32_t pos;         // D/U: byte offset of the run's h x W block
-  uint32_t nrow;        // D/U: atom height h
-  uint32_t ncol;        // D/U: W = total columns of the run's terms
-  uint32_t out;         // D/U: first row of the atom
-  uint16_t flags;       // kAtomEnd when the run closes its atom
-  uint16_t rot;         // consumer warp that takes column 0
-};
-static_assert(sizeof(Run) == 32, "Run must stay 32 bytes");
-static_assert(sizeof(Term) == 32, "Term must stay 32 bytes");
+HBX_HD inline uint32_t run_kind(const Run &r) { return r.flags & 0xffu; }
+HBX_HD inline uint32_t run_bytes(const Run &r) { return 16u * r.nrow * r.npair; }
 
 struct CtaInfo {
-  uint64_t stream_off;   // byte offset of the CTA stream in the packed buffer
-  uint32_t stream_bytes; // multiple of 16
-  uint32_t term_begin;
-  uint32_t n_p, n_d, n_u;
-  uint32_t atom_begin, n_atoms;  // owned atoms (rows written by this CTA)
-  uint32_t run_begin;            // runs of the P, D, U sections, in order
+  uint64_t stream_off;    // byte offset of the CTA stream in the packed buffer
+  uint32_t stream_bytes;  // multiple of 16
+  uint32_t rec_begin;     // first run record of the CTA (P, D, U runs in order)
   uint32_t nr_p, nr_d, nr_u;
-  uint32_t pad[3];
+  uint32_t atom_begin, n_atoms;  // owned atoms (rows written by this CTA)
+  uint32_t pad[7];
 };
 static_assert(sizeof(CtaInfo) == 64, "CtaInfo layout");
 
@@ -108,17 +118,35 @@ struct Atom {
   uint32_t r0, h;
 };
 
+// Host-only description of a block, used by the packer and the checks.
+// kind P: `a` = column group, rows [r0, r0+h) of the group's stacked rows.
+// kind D/U: `a` = row atom; columns are the pieces [piece_begin, +npiece).
+struct Block {
+  uint16_t kind, h;
+  uint32_t a, r0, W;
+  uint32_t piece_begin, npiece;
+};
+// A run of block columns taken from one leaf: D -> leaf columns [c0, c0+n)
+// (x index vsrc); U -> ranks [c0, c0+n) of the leaf (zbu index vsrc).
+struct Piece {
+  uint32_t leaf, c0, n, vsrc;
+};
+
 // Host-side plan: everything needed to pack and launch.
 struct Plan {
   int nd = 0, nlf = 0, nlfkt = 0, ktmax = 0;
   int num_ctas = 0;
   std::vector<Atom> atoms;          // in CTA order (atom_begin indexes this)
-  std::vector<Term> terms;          // in CTA order
-  std::vector<Run> runs;            // in CTA order
+  std::vector<RunRec> recs;         // in CTA order
   std::vector<CtaInfo> ctas;
+  std::vector<Block> blocks;
+  std::vector<Piece> pieces;
+  std::vector<uint32_t> group_leaf_begin, group_leaves;  // P column groups (CSR over leaf indices)
+  std::vector<uint64_t> zoff;       // zbu offset of each low-rank leaf
   uint64_t total_bytes = 0;         // packed buffer size
   uint64_t zbu_len = 0;
   uint64_t dense_words = 0, lowrank_words = 0;
+  uint64_t pad_bytes = 0;           // zero columns added for odd widths
   uint64_t alg_bytes = 0, alg_flops = 0;
 };
 

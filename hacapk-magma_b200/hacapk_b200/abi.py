@@ -62,7 +62,7 @@ class Options(C.Structure):
 
 class Info(C.Structure):
     _fields_ = [("nd", C.c_int), ("nlf", C.c_int), ("nlfkt", C.c_int), ("ktmax", C.c_int),
-                ("num_ctas", C.c_int), ("num_atoms", C.c_int), ("num_terms", C.c_int),
+                ("num_ctas", C.c_int), ("num_atoms", C.c_int), ("num_runs", C.c_int),
                 ("precision", C.c_int), ("stream_bytes", C.c_longlong),
                 ("alg_bytes", C.c_longlong), ("alg_flops", C.c_longlong),
                 ("zbu_len", C.c_longlong), ("dense_words", C.c_longlong),

@@ -123,7 +123,7 @@ typedef struct hbx_options {
 
 typedef struct hbx_info {
   int nd, nlf, nlfkt, ktmax;
-  int num_ctas, num_atoms, num_terms, precision;
+  int num_ctas, num_atoms, num_runs, precision;
   long long stream_bytes;  /* packed factor bytes streamed per matvec        */
   long long alg_bytes;     /* algorithmic bytes per single-RHS matvec (B_H)  */
   long long alg_flops;     /* 2*(sum dense ndl*ndt + sum kt*(ndl+ndt))       */
