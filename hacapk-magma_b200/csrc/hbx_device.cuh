@@ -19,10 +19,15 @@
 namespace hbx {
 
 constexpr uint32_t kRingBytes = (uint32_t)kRingChunks * kChunkBytes;
-constexpr uint32_t kRingMask = kRingBytes - 1;
-// consumer warps, then the bulk-copy producer warp, then the descriptor warp
+
+// Shared-memory offset in the ring of stream byte p of absolute chunk c
+// (c = pass base + p / kChunkBytes).  The ring need not be a power of two.
+__device__ __forceinline__ uint32_t ring_off(uint32_t c, uint32_t p) {
+  return (c % (uint32_t)kRingChunks) * (uint32_t)kChunkBytes + (p & (uint32_t)(kChunkBytes - 1));
+}
+// consumer warps, then the bulk-copy producer warp, then the gather warp
 constexpr int kProducerWarp = kConsumerWarps;
-constexpr int kDescWarp = kConsumerWarps + 1;
+constexpr int kGatherWarp = kConsumerWarps + 1;
 constexpr int kThreads = (kConsumerWarps + 2) * 32;
 // Chunks the producer prefetches into L2 beyond the ones in flight into the
 // ring.  The ring alone keeps kRingBytes in flight per SM, about what HBM
@@ -43,12 +48,18 @@ struct SharedLayout {
   static constexpr uint32_t empty = full + 8 * kRingChunks;
   static constexpr uint32_t red = empty + 8 * kRingChunks;            // [2][NW][32] double
   static constexpr uint32_t scal = red + 2 * kConsumerWarps * 32 * 8;  // 64 doubles of scratch
-  static constexpr uint32_t stage = scal + 64 * 8;                     // [2][kStageCap] double
-  static constexpr uint32_t desc = stage + 2 * kStageCap * 8;          // [kDescSlots] run records
-  static constexpr uint32_t dfull = desc + kDescSlots * kRecBytes;
-  static constexpr uint32_t dempty = dfull + 8 * kDescSlots;
-  static constexpr uint32_t bytes = dempty + 8 * kDescSlots;
+  static constexpr uint32_t stage = scal + 64 * 8;                     // [kStages][kStageCap] double
+  static constexpr uint32_t hdr = stage + kStages * kStageCap * 8;     // [kStages] Run
+  static constexpr uint32_t sfull = hdr + kStages * 32;                // stage filled (gather warp)
+  static constexpr uint32_t sempty = sfull + 8 * kStages;              // stage consumed (consumer warps)
+  static constexpr uint32_t xready = sempty + 8 * kStages;             // a pass's x is complete grid-wide
+  static constexpr uint32_t garrive = xready + 8;                      // this CTA arrived on the grid barrier
+  static constexpr uint32_t gen = garrive + 8;                         // grid-barrier generation of that arrival
+  static constexpr uint32_t bytes = gen + 16;
 };
+static_assert(SharedLayout::stage % 16 == 0 && SharedLayout::hdr % 16 == 0 && SharedLayout::sfull % 8 == 0,
+              "shared-memory layout alignment");
+static_assert(SharedLayout::bytes <= 227 * 1024, "shared memory per CTA");
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -80,15 +91,28 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
 // try_wait with a suspend-time hint: a waiting thread is parked (not
 // spinning, so it takes no issue slots) until the phase completes or the
 // hint (ns) elapses.
+#ifndef HBX_SUSPEND_NS
+#define HBX_SUSPEND_NS 1000000
+#endif
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
+#if HBX_SUSPEND_NS > 0
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity), "r"(1000000u)
+      : "r"(smem_u32(bar)), "r"(parity), "r"((uint32_t)HBX_SUSPEND_NS)
       : "memory");
+#else
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+#endif
   return ok != 0;
 }
 
@@ -133,7 +157,12 @@ __device__ __forceinline__ void cp_async16cg(void *dst, const void *src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// The mbarrier receives one arrival once every earlier cp.async of this
+// thread has landed (the barrier's count includes it: .noinc).
+__device__ __forceinline__ void cp_async_arrive(uint64_t *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __device__ __forceinline__ void named_bar(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
@@ -199,7 +228,7 @@ __device__ __forceinline__ void producer_run(const uint8_t *src, uint32_t bytes,
   for (uint32_t g = kRingChunks; g < min(total, (uint32_t)kRingChunks + kL2Ahead); ++g) prefetch(g);
   uint32_t issued = 0;
   for (uint32_t g = 0; g < total; ++g) {
-    const uint32_t s = g & (kRingChunks - 1);
+    const uint32_t s = g % kRingChunks;
     if (g >= (uint32_t)kRingChunks) {
       if (!mbar_wait(&empty[s], ((g / kRingChunks) - 1) & 1, timeout_ns)) {
         atomicOr(err, kErrProducer);
@@ -216,54 +245,8 @@ __device__ __forceinline__ void producer_run(const uint8_t *src, uint32_t bytes,
   }
   // Copies still in flight must land before the CTA exits.
   const uint32_t g0 = issued > (uint32_t)kRingChunks ? issued - kRingChunks : 0;
-  for (uint32_t g = g0; g < issued; ++g) mbar_wait(&full[g & (kRingChunks - 1)], (g / kRingChunks) & 1, timeout_ns);
+  for (uint32_t g = g0; g < issued; ++g) mbar_wait(&full[g % kRingChunks], (g / kRingChunks) & 1, timeout_ns);
 }
-
-// ---- descriptor warp: keeps the descriptor queue kDescSlots run records
-// ahead of the consumers.  Records are fixed-size (kRecBytes) and contiguous
-// per CTA, so each one is a single bulk copy with no dependent load.  Only
-// lane 0 works.
-__device__ __forceinline__ void desc_run(const RunRec *recs, uint32_t nruns, uint32_t npass, uint8_t *dbuf,
-                                         uint64_t *dfull, uint64_t *dempty, int *err, uint64_t timeout_ns) {
-  if ((threadIdx.x & 31) != 0) return;
-  const uint32_t total = nruns * npass;
-  for (uint32_t g = 0; g < total; ++g) {
-    const uint32_t slot = g % kDescSlots;
-    if (g >= (uint32_t)kDescSlots) {
-      if (!mbar_wait(&dempty[slot], ((g / kDescSlots) - 1) & 1, timeout_ns)) {
-        atomicOr(err, kErrProducer);
-        return;
-      }
-    }
-    mbar_arrive_expect_tx(&dfull[slot], (uint32_t)kRecBytes);
-    bulk_g2s(dbuf + slot * kRecBytes, recs + (g % nruns), (uint32_t)kRecBytes, &dfull[slot]);
-  }
-  // the last slots' copies must land before the CTA exits
-  const uint32_t g0 = total > (uint32_t)kDescSlots ? total - kDescSlots : 0;
-  for (uint32_t g = g0; g < total; ++g) mbar_wait(&dfull[g % kDescSlots], (g / kDescSlots) & 1, timeout_ns);
-}
-
-// Consumer view of the descriptor queue; g counts runs across sections and passes.
-struct DescQ {
-  uint8_t *dbuf;
-  uint64_t *dfull, *dempty;
-  uint32_t g;
-  uint64_t timeout_ns;
-  int *err;
-  __device__ __forceinline__ const RunRec *get(uint32_t i, bool &bad) {
-    const uint32_t gi = g + i;
-    const uint32_t slot = gi % kDescSlots;
-    if (!bad && !warp_wait(&dfull[slot], (gi / kDescSlots) & 1, timeout_ns)) {
-      bad = true;
-      if ((threadIdx.x & 31) == 0) atomicOr(err, kErrPipeline);
-    }
-    return reinterpret_cast<const RunRec *>(dbuf + slot * kRecBytes);
-  }
-  __device__ __forceinline__ void release(uint32_t i) {
-    __syncwarp();
-    if ((threadIdx.x & 31) == 0) mbar_arrive(&dempty[(g + i) % kDescSlots]);
-  }
-};
 
 // ---- consumer-side ring state (one per warp) ------------------------------
 struct RingCounters {
@@ -280,18 +263,18 @@ __device__ __noinline__ RingCounters ring_advance(RingCounters rc, uint32_t c0, 
   const int lane = threadIdx.x & 31;
   while (!rc.bad && rc.released < c0) {
     if (rc.waited <= rc.released) {
-      if (!warp_wait(&full[rc.released & (kRingChunks - 1)], (rc.released / kRingChunks) & 1, timeout_ns)) {
+      if (!warp_wait(&full[rc.released % kRingChunks], (rc.released / kRingChunks) & 1, timeout_ns)) {
         rc.bad = 1;
         break;
       }
       rc.waited = rc.released + 1;
     }
     __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[rc.released & (kRingChunks - 1)]);
+    if (lane == 0) mbar_arrive(&empty[rc.released % kRingChunks]);
     ++rc.released;
   }
   while (!rc.bad && rc.waited <= c1) {
-    if (!warp_wait(&full[rc.waited & (kRingChunks - 1)], (rc.waited / kRingChunks) & 1, timeout_ns)) {
+    if (!warp_wait(&full[rc.waited % kRingChunks], (rc.waited / kRingChunks) & 1, timeout_ns)) {
       rc.bad = 1;
       break;
     }
@@ -335,12 +318,6 @@ struct Ring {
   }
   // Release everything below absolute chunk `end` (end of the last pass).
   __device__ __forceinline__ void drain(uint32_t end) { release_below(end); }
-  __device__ __forceinline__ double ld(uint32_t p) const {
-    const uint32_t c = base + (p >> kChunkLog);
-    const double *q = reinterpret_cast<const double *>(buf + (((c & (kRingChunks - 1)) << kChunkLog) |
-                                                              (p & (kChunkBytes - 1))));
-    return *q;
-  }
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -349,74 +326,149 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// ---- vector staging of one run: warp w gathers segments w, w+NW, ... with
-// 8-byte cp.async (segments start anywhere); an odd-width block's zero
-// column is written directly.  The record is in the descriptor queue.
-__device__ __forceinline__ void gather_run(const RunRec &rec, const double *x, const double *zbu, double *stage) {
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const Run &run = rec.hdr;
-  const double *vec = run_kind(run) == kRunU ? zbu : x;
-  for (uint32_t q = w; q < run.nseg; q += kConsumerWarps) {
-    const Seg sg = rec.seg[q];
-    for (uint32_t e = lane; e < sg.len; e += 32) cp_async8(stage + sg.dst + e, vec + sg.src + e);
+// ---- gather warp: for every run of the CTA, in order and for every pass,
+// copies the run header into hdr[slot] and gathers the run's vector segments
+// (x for P and D runs, zbu for U runs) into stage[slot] with 8-byte cp.async
+// (segments start anywhere; each lane copies whole segments of at most
+// kSegMax entries), kStages runs ahead of the consumers.  Lane l
+// holds 16 bytes of the 512-byte record: lanes 0-1 the header, lane l >= 2
+// segments 2(l-2) and 2(l-2)+1.  Before the first run of pass p it waits
+// until that pass's x is complete grid-wide (xready), and before the first U
+// run until every CTA's zbu is (this CTA's grid-barrier arrival, then the
+// barrier).  Every wait is bounded; on a timeout the warp flags the error
+// and stops, and the consumers' own bounded waits end the launch.
+struct GatherCtx {
+  const RunRec *recs;
+  uint32_t nr_p, nr_d, nr_u, npass;
+  const double *x0, *x1;  // x of pass 0 and pass 1
+  const double *zbu;
+  unsigned *gbar;
+  int *err;
+  uint64_t timeout_ns;
+};
+
+__device__ __forceinline__ uint4 ld_rec(const RunRec *recs, uint32_t k, int lane) {
+  return __ldg(reinterpret_cast<const uint4 *>(recs + k) + lane);
+}
+
+template <class SM>
+__device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t nruns = c.nr_p + c.nr_d + c.nr_u, total = nruns * c.npass;
+  if (total == 0) return;
+  uint4 nxt = ld_rec(c.recs, 0, lane);
+  for (uint32_t g = 0; g < total; ++g) {
+    const uint32_t k = g % nruns, pass = g / nruns;
+    const uint4 cur = nxt;
+    if (g + 1 < total) nxt = ld_rec(c.recs, (g + 1) % nruns, lane);
+    bool ok = true;
+    if (k == 0) ok = warp_wait(sm.xready, pass & 1, c.timeout_ns);
+    if (ok && k == c.nr_p + c.nr_d) {  // first U run of the pass: zbu must be complete grid-wide
+      ok = warp_wait(sm.garrive, pass & 1, c.timeout_ns);
+      if (ok) {
+        int gok = 1;
+        if (lane == 0) gok = grid_wait(c.gbar, *sm.gen, c.timeout_ns) ? 1 : 0;
+        ok = __shfl_sync(0xffffffffu, gok, 0) != 0;
+        __syncwarp();
+        __threadfence();
+      }
+    }
+    const uint32_t slot = g % kStages;
+    if (ok && g >= (uint32_t)kStages) ok = warp_wait(&sm.sempty[slot], ((g / kStages) - 1) & 1, c.timeout_ns);
+    if (!ok) {
+      if (lane == 0) atomicOr(c.err, kErrProducer);
+      break;
+    }
+    if (lane < 2) reinterpret_cast<uint4 *>(sm.hdr + slot)[lane] = cur;
+    const uint32_t w2 = __shfl_sync(0xffffffffu, cur.z, 0);  // nrow | npair << 16
+    const uint32_t w3 = __shfl_sync(0xffffffffu, cur.w, 0);  // flags | rot << 16
+    const uint32_t nseg = __shfl_sync(0xffffffffu, cur.x, 1) & 0xffffu;
+    const double *vec = (w3 & 0xffu) == kRunU ? c.zbu : ((pass & 1) ? c.x1 : c.x0);
+    double *st = sm.stage + slot * kStageCap;
+    // lane q copies segment q (and segment 32 + q): segment s sits in lane
+    // 2 + s/2 of the record, fields (x, y) for even s and (z, w) for odd s
+#pragma unroll
+    for (uint32_t round = 0; round < 2; ++round) {
+      const uint32_t q = round * 32u + (uint32_t)lane;
+      const int holder = 2 + (int)(q >> 1);  // > 31 only for q >= 60, which is never a segment
+      const uint32_t sx = __shfl_sync(0xffffffffu, cur.x, holder & 31);
+      const uint32_t sy = __shfl_sync(0xffffffffu, cur.y, holder & 31);
+      const uint32_t sz = __shfl_sync(0xffffffffu, cur.z, holder & 31);
+      const uint32_t sw = __shfl_sync(0xffffffffu, cur.w, holder & 31);
+      if (q < nseg) {
+        const uint32_t src = (q & 1) ? sz : sx, ld = (q & 1) ? sw : sy;
+        const uint32_t len = ld & 0xffffu, dst = ld >> 16;
+        for (uint32_t e = 0; e < len; ++e) cp_async8(st + dst + e, vec + src + e);
+      }
+      if (nseg <= 32) break;
+    }
+    if ((w3 & kPadCol) && lane == 0) st[2u * (w2 >> 16) - 1u] = 0.0;
+    cp_async_arrive(&sm.sfull[slot]);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sm.sfull[slot]);  // releases the header and pad stores
   }
-  if ((run.flags & kPadCol) && w == 0 && lane == 0) stage[2u * run.npair - 1u] = 0.0;
-  cp_async_commit();
+  cp_async_wait_all();
 }
 
 // ---- one run of a block: acc(lane) += sum over the run's column pairs of
 // B(lane, c) v(c).  Pair panel j (16h bytes, row i at 16i) is read by warp
-// (rot + j) mod NW, four panels per iteration; lanes >= h repeat row h-1 and
-// their sums are never used.
+// (rot + j) mod NW, kUnroll panels per iteration, so the 16 warps together
+// hold a window of NW*kUnroll panels of the ring; lanes >= h repeat row h-1
+// and their sums are never used.
+#ifndef HBX_UNROLL
+#define HBX_UNROLL 4
+#endif
+constexpr uint32_t kUnroll = HBX_UNROLL;
+
 __device__ __forceinline__ void run_block(const Run &run, uint32_t stage_s, Ring &R, double &acc) {
-  constexpr uint32_t NW = kConsumerWarps;
+  constexpr uint32_t NW = kConsumerWarps, U = kUnroll;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t h = run.nrow, np = run.npair;
   if (np == 0) return;
   const uint32_t pb = 16u * h;
   const uint32_t lrow = 16u * min((uint32_t)lane, h - 1u);
   const uint32_t ring_s = smem_u32(R.buf);
-  const uint32_t q0 = (R.base << kChunkLog) + run.pos + lrow;
   uint32_t j = (uint32_t)((w - (int)run.rot) & (int)(NW - 1));
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-  for (; j + 3 * NW < np; j += 4 * NW) {
+  double a[2 * U];
+#pragma unroll
+  for (uint32_t u = 0; u < 2 * U; ++u) a[u] = 0.0;
+  for (; j + (U - 1) * NW < np; j += U * NW) {
     const uint32_t p0 = run.pos + j * pb;
-    R.ensure(p0, p0 + 3 * NW * pb + pb);
-    const uint32_t vq = stage_s + 16u * j;
-    const double2 v0 = lds_f64x2(vq), v1 = lds_f64x2(vq + 16 * NW);
-    const double2 v2 = lds_f64x2(vq + 32 * NW), v3 = lds_f64x2(vq + 48 * NW);
-    const uint32_t q = (q0 + j * pb) & kRingMask;
-    double2 m0, m1, m2, m3;
-    if (q + 3 * NW * pb + 16u <= kRingBytes) {  // the four panels do not wrap around the ring end
-      const uint32_t a = ring_s + q;
-      m0 = lds_f64x2(a);
-      m1 = lds_f64x2(a + NW * pb);
-      m2 = lds_f64x2(a + 2 * NW * pb);
-      m3 = lds_f64x2(a + 3 * NW * pb);
+    R.ensure(p0, p0 + (U - 1) * NW * pb + pb);
+    double2 v[U], m[U];
+#pragma unroll
+    for (uint32_t u = 0; u < U; ++u) v[u] = lds_f64x2(stage_s + 16u * (j + u * NW));
+    const uint32_t pl = p0 + lrow;
+    const uint32_t q = ring_off(R.base + (pl >> kChunkLog), pl);
+    if (q + (U - 1) * NW * pb + 16u <= kRingBytes) {  // the panels do not wrap around the ring end
+#pragma unroll
+      for (uint32_t u = 0; u < U; ++u) m[u] = lds_f64x2(ring_s + q + u * NW * pb);
     } else {
-      m0 = lds_f64x2(ring_s + q);
-      m1 = lds_f64x2(ring_s + ((q + NW * pb) & kRingMask));
-      m2 = lds_f64x2(ring_s + ((q + 2 * NW * pb) & kRingMask));
-      m3 = lds_f64x2(ring_s + ((q + 3 * NW * pb) & kRingMask));
+#pragma unroll
+      for (uint32_t u = 0; u < U; ++u) {
+        const uint32_t pu = pl + u * NW * pb;
+        m[u] = lds_f64x2(ring_s + ring_off(R.base + (pu >> kChunkLog), pu));
+      }
     }
-    a0 = fma(m0.x, v0.x, a0);
-    a1 = fma(m0.y, v0.y, a1);
-    a2 = fma(m1.x, v1.x, a2);
-    a3 = fma(m1.y, v1.y, a3);
-    a0 = fma(m2.x, v2.x, a0);
-    a1 = fma(m2.y, v2.y, a1);
-    a2 = fma(m3.x, v3.x, a2);
-    a3 = fma(m3.y, v3.y, a3);
+#pragma unroll
+    for (uint32_t u = 0; u < U; ++u) {
+      a[2 * u] = fma(m[u].x, v[u].x, a[2 * u]);
+      a[2 * u + 1] = fma(m[u].y, v[u].y, a[2 * u + 1]);
+    }
   }
   for (; j < np; j += NW) {
     const uint32_t p0 = run.pos + j * pb;
     R.ensure(p0, p0 + pb);
-    const double2 v = lds_f64x2(stage_s + 16u * j);
-    const double2 m = lds_f64x2(ring_s + ((q0 + j * pb) & kRingMask));
-    a0 = fma(m.x, v.x, a0);
-    a1 = fma(m.y, v.y, a1);
+    const double2 vv = lds_f64x2(stage_s + 16u * j);
+    const uint32_t pl = p0 + lrow;
+    const double2 mm = lds_f64x2(ring_s + ring_off(R.base + (pl >> kChunkLog), pl));
+    a[0] = fma(mm.x, vv.x, a[0]);
+    a[1] = fma(mm.y, vv.y, a[1]);
   }
-  acc += (a0 + a1) + (a2 + a3);
+  double t = 0.0;
+#pragma unroll
+  for (uint32_t u = 0; u < 2 * U; ++u) t += a[u];
+  acc += t;
 }
 
 // ---- compensated (Dot2) accumulation ------------------------------------------

@@ -30,9 +30,11 @@ struct Smem {
   uint64_t *full, *empty;
   double *red;    // [2][NW][32]
   double *scal;   // 64 doubles
-  double *stage;  // [2][kStageCap]
-  uint8_t *desc;  // descriptor queue (run records)
-  uint64_t *dfull, *dempty;
+  double *stage;  // [kStages][kStageCap]
+  Run *hdr;       // [kStages] headers of the staged runs
+  uint64_t *sfull, *sempty;
+  uint64_t *xready, *garrive;
+  unsigned *gen;
 };
 
 __device__ __forceinline__ Smem smem_layout(uint8_t *base) {
@@ -43,9 +45,12 @@ __device__ __forceinline__ Smem smem_layout(uint8_t *base) {
   s.red = reinterpret_cast<double *>(base + SharedLayout::red);
   s.scal = reinterpret_cast<double *>(base + SharedLayout::scal);
   s.stage = reinterpret_cast<double *>(base + SharedLayout::stage);
-  s.desc = base + SharedLayout::desc;
-  s.dfull = reinterpret_cast<uint64_t *>(base + SharedLayout::dfull);
-  s.dempty = reinterpret_cast<uint64_t *>(base + SharedLayout::dempty);
+  s.hdr = reinterpret_cast<Run *>(base + SharedLayout::hdr);
+  s.sfull = reinterpret_cast<uint64_t *>(base + SharedLayout::sfull);
+  s.sempty = reinterpret_cast<uint64_t *>(base + SharedLayout::sempty);
+  s.xready = reinterpret_cast<uint64_t *>(base + SharedLayout::xready);
+  s.garrive = reinterpret_cast<uint64_t *>(base + SharedLayout::garrive);
+  s.gen = reinterpret_cast<unsigned *>(base + SharedLayout::gen);
   return s;
 }
 
@@ -55,10 +60,12 @@ __device__ __forceinline__ void init_barriers(const Smem &s) {
       mbar_init(&s.full[i], 1);
       mbar_init(&s.empty[i], NW);
     }
-    for (int i = 0; i < kDescSlots; ++i) {
-      mbar_init(&s.dfull[i], 1);
-      mbar_init(&s.dempty[i], NW);
+    for (int i = 0; i < kStages; ++i) {
+      mbar_init(&s.sfull[i], 33);  // 32 cp.async arrivals of the gather warp + its lane 0
+      mbar_init(&s.sempty[i], NW);
     }
+    mbar_init(s.xready, 1);
+    mbar_init(s.garrive, 1);
     mbar_fence_init();
   }
   __syncthreads();
@@ -81,7 +88,7 @@ __device__ __forceinline__ void block_end(const Run &run, double &acc, uint32_t 
   double *rb = red + (nae & 1u) * (NW * 32);
   if ((uint32_t)lane < h) rb[w * 32 + lane] = acc;
   named_bar(2, kConsumerThreads);
-  if ((uint32_t)w == (nae & (NW - 1)) && (uint32_t)lane < h) {
+  if (!R.bad && (uint32_t)w == (nae & (NW - 1)) && (uint32_t)lane < h) {
     double s = rb[lane];
 #pragma unroll
     for (int q = 1; q < NW; ++q) s += rb[q * 32 + lane];
@@ -106,33 +113,44 @@ __device__ __forceinline__ void block_end(const Run &run, double &acc, uint32_t 
 // guarantees that nobody still reads the buffer run k+1 is gathered into.
 // Run headers and terms come from the descriptor queue.  process(run, terms,
 // stage) returns the stream position where the run ends.
+// Consumer view of the stage ring: run g (counted over sections and passes)
+// is in slot g % kStages.
+struct StageQ {
+  uint32_t g;
+};
+
+// Runs a section: waits for each run's staged vector, processes it, and
+// gives the slot back.  Before a wait the warp gives back the ring chunks of
+// the previous run, so no warp blocks while holding chunks the others need.
+// process(run, stage) returns the stream position where the run ends.
 template <class F>
-__device__ __forceinline__ void run_section(uint32_t nruns, DescQ &Q, const double *x, const double *zbu,
-                                            const Smem &sm, int &sbuf, Ring &R, F &&process) {
-  if (nruns == 0) return;
-  gather_run(*Q.get(0, R.bad), x, zbu, sm.stage + sbuf * kStageCap);
+__device__ __forceinline__ void run_section(uint32_t nruns, StageQ &Q, const Smem &sm, Ring &R, int *err,
+                                            F &&process) {
   uint32_t rend = 0;
   for (uint32_t k = 0; k < nruns; ++k) {
-    // give back the ring chunks of the previous run before blocking
+    const uint32_t g = Q.g + k, slot = g % kStages;
     if (k > 0) R.release_below(R.base + (rend >> kChunkLog));
-    cp_async_wait_all();
-    named_bar(3, kConsumerThreads);
-    if (k + 1 < nruns) gather_run(*Q.get(k + 1, R.bad), x, zbu, sm.stage + (sbuf ^ 1) * kStageCap);
-    const RunRec *rc = Q.get(k, R.bad);
-    rend = process(rc->hdr, smem_u32(sm.stage + sbuf * kStageCap));
-    Q.release(k);
-    sbuf ^= 1;
+    if (!R.bad && !warp_wait(&sm.sfull[slot], (g / kStages) & 1, R.timeout_ns)) {
+      R.bad = true;
+      if ((threadIdx.x & 31) == 0) atomicOr(err, kErrPipeline);
+    }
+    Run run = sm.hdr[slot];
+    if (R.bad) run.npair = 0;  // after a timed-out wait: touch neither the stage nor the ring
+    rend = process(run, smem_u32(sm.stage + slot * kStageCap));
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) mbar_arrive(&sm.sempty[slot]);
   }
   Q.g += nruns;
 }
 
 // One H-matvec over this CTA's stream (pass starting at absolute chunk R.base,
-// K chunks long).  Contains one grid-barrier instance (arrive after P, wait
-// before U); every warp has released the whole pass when it returns.
-__device__ __forceinline__ void matvec_body(Ring &R, DescQ &Q, uint32_t K, const CtaInfo &ci, const double *x,
-                                            double alpha, double beta,
-                                            const double *yin, double *y, double *zbu, unsigned *gbar, int *err,
-                                            uint64_t timeout_ns, const Smem &sm, uint32_t &nae, int &sbuf,
+// K chunks long).  The CTA arrives on the grid barrier after its P runs; the
+// gather warp waits for the barrier before it stages the first U run, so the
+// D runs hide the barrier latency.  Every warp has released the whole pass
+// when it returns.
+__device__ __forceinline__ void matvec_body(Ring &R, StageQ &Q, uint32_t K, const CtaInfo &ci, double alpha,
+                                            double beta, const double *yin, double *y, double *zbu, unsigned *gbar,
+                                            int *err, const Smem &sm, uint32_t &nae,
                                             unsigned long long *prof = nullptr) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   auto stamp = [&](int k) {
@@ -147,7 +165,7 @@ __device__ __forceinline__ void matvec_body(Ring &R, DescQ &Q, uint32_t K, const
   };
   // ---- P: zbu = V^T x for this CTA's slabs
   uint32_t pend = 0;
-  run_section(ci.nr_p, Q, x, zbu, sm, sbuf, R, [&](const Run &run, uint32_t st) { return pend = block(run, st); });
+  run_section(ci.nr_p, Q, sm, R, err, [&](const Run &run, uint32_t st) { return pend = block(run, st); });
   R.release_below(R.base + (pend >> kChunkLog));
   stamp(1);
   if (lane == 0) __threadfence();
@@ -156,29 +174,23 @@ __device__ __forceinline__ void matvec_body(Ring &R, DescQ &Q, uint32_t K, const
   unsigned gen = 0;
   if (w == 0 && lane == 0) {
     gen = ld_acquire(&gbar[1]);
+    *sm.gen = gen;
     grid_arrive(gbar, gridDim.x);
+    mbar_arrive(sm.garrive);
   }
-  // ---- D: dense rows of the owned atoms (hides the barrier latency)
+  // ---- D: dense rows of the owned atoms
   uint32_t dend = pend;
-  run_section(ci.nr_d, Q, x, zbu, sm, sbuf, R, [&](const Run &run, uint32_t st) { return dend = block(run, st); });
+  run_section(ci.nr_d, Q, sm, R, err, [&](const Run &run, uint32_t st) { return dend = block(run, st); });
   R.release_below(R.base + (dend >> kChunkLog));
   stamp(3);
-  // ---- wait for every CTA's zbu
-  if (w == 0) {
-    int ok = 1;
-    if (lane == 0) {
-      ok = grid_wait(gbar, gen, timeout_ns) ? 1 : 0;
-      if (!ok) atomicOr(err, kErrGridBarrier);
-    }
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    if (lane == 0) sm.scal[63] = ok ? 1.0 : 0.0;
-  }
-  named_bar(1, kConsumerThreads);
   stamp(4);
-  if (sm.scal[63] == 0.0) R.bad = true;
-  // ---- U: U rows of the owned atoms times zbu
-  run_section(ci.nr_u, Q, x, zbu, sm, sbuf, R, [&](const Run &run, uint32_t st) { return block(run, st); });
+  // ---- U: U rows of the owned atoms times zbu (staged after the grid barrier)
+  run_section(ci.nr_u, Q, sm, R, err, [&](const Run &run, uint32_t st) { return block(run, st); });
   R.release_below(R.base + K);
+  // The barrier counts arrivals per instance: this CTA may arrive on the
+  // next instance only once this one is complete (a CTA without U runs has
+  // not waited for it yet).
+  if (w == 0 && lane == 0 && !grid_wait(gbar, gen, R.timeout_ns)) atomicOr(err, kErrGridBarrier);
   stamp(5);
 }
 
@@ -189,23 +201,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   init_barriers(sm);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
-  const uint32_t nruns = ci.nr_p + ci.nr_d + ci.nr_u;
   if (w == kProducerWarp) {
     if (lane == 0 && K > 0)
       producer_run(a.stream + ci.stream_off, ci.stream_bytes, 1, sm.ring, sm.full, sm.empty, a.err, a.timeout_ns);
     return;
   }
-  if (w == kDescWarp) {
-    if (nruns > 0)
-      desc_run(a.recs + ci.rec_begin, nruns, 1, sm.desc, sm.dfull, sm.dempty, a.err, a.timeout_ns);
+  if (w == kGatherWarp) {
+    const GatherCtx c{a.recs + ci.rec_begin, ci.nr_p, ci.nr_d, ci.nr_u, 1, a.x, a.x, a.zbu, a.gbar, a.err,
+                      a.timeout_ns};
+    gather_warp(c, sm);
     return;
   }
+  if (threadIdx.x == 0) mbar_arrive(sm.xready);  // x is an input: ready from the start
   Ring R{sm.ring, sm.full, sm.empty, 0, 0, 0, a.timeout_ns, a.err, false};
-  DescQ Q{sm.desc, sm.dfull, sm.dempty, 0, a.timeout_ns, a.err};
+  StageQ Q{0};
   uint32_t nae = 0;
-  int sbuf = 0;
-  matvec_body(R, Q, K, ci, a.x, a.alpha, a.beta, a.yin, a.y, a.zbu, a.gbar, a.err, a.timeout_ns, sm, nae, sbuf,
-              a.prof);
+  matvec_body(R, Q, K, ci, a.alpha, a.beta, a.yin, a.y, a.zbu, a.gbar, a.err, sm, nae, a.prof);
   R.drain(K);
 }
 
@@ -363,21 +374,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   const int iter = (int)sm.scal[6];
 
   const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
-  const uint32_t nruns = ci.nr_p + ci.nr_d + ci.nr_u;
   if (w == kProducerWarp) {
     if (lane == 0 && K > 0)
       producer_run(a.stream + ci.stream_off, ci.stream_bytes, 2, sm.ring, sm.full, sm.empty, a.err, a.timeout_ns);
     return;
   }
-  if (w == kDescWarp) {
-    if (nruns > 0)
-      desc_run(a.recs + ci.rec_begin, nruns, 2, sm.desc, sm.dfull, sm.dempty, a.err, a.timeout_ns);
+  if (w == kGatherWarp) {
+    const GatherCtx c{a.recs + ci.rec_begin, ci.nr_p, ci.nr_d, ci.nr_u, 2, a.p, a.t, a.zbu, a.gbar, a.err,
+                      a.timeout_ns};
+    gather_warp(c, sm);
     return;
   }
   Ring R{sm.ring, sm.full, sm.empty, 0, 0, 0, a.timeout_ns, a.err, false};
-  DescQ Q{sm.desc, sm.dfull, sm.dempty, 0, a.timeout_ns, a.err};
+  StageQ Q{0};
   uint32_t nae = 0;
-  int sbuf = 0;
 
   // ---- S1: p = r + beta*(p - zeta*Ap)  (p = r on the first step)
   if (beta == 0.0) {
@@ -390,6 +400,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
   __threadfence();
   grid_sync(a.gbar, a.err, a.timeout_ns, sm);
+  if (threadIdx.x == 0) mbar_arrive(sm.xready);  // p complete grid-wide: pass 1 may be staged
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.state->iter = iter + 1;
     a.state->beta = beta;
@@ -400,7 +411,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
 
   // ---- S2: Ap = H p;  rh . Ap
-  matvec_body(R, Q, K, ci, a.p, 1.0, 0.0, nullptr, a.ap, a.zbu, a.gbar, a.err, a.timeout_ns, sm, nae, sbuf);
+  matvec_body(R, Q, K, ci, 1.0, 0.0, nullptr, a.ap, a.zbu, a.gbar, a.err, sm, nae);
   {
     Acc2 acc[1] = {{0, 0}};
     named_bar(1, kConsumerThreads);
@@ -419,10 +430,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   for_own_rows(a.atoms, ci, [&](uint32_t r) { a.t[r] = fma(-alpha, a.ap[r], a.r[r]); });
   __threadfence();
   grid_sync(a.gbar, a.err, a.timeout_ns, sm);
+  if (threadIdx.x == 0) mbar_arrive(sm.xready);  // t complete grid-wide: pass 2 may be staged
 
   // ---- S4: At = H t;  At . t,  At . At
   R.base = K;
-  matvec_body(R, Q, K, ci, a.t, 1.0, 0.0, nullptr, a.at, a.zbu, a.gbar, a.err, a.timeout_ns, sm, nae, sbuf);
+  matvec_body(R, Q, K, ci, 1.0, 0.0, nullptr, a.at, a.zbu, a.gbar, a.err, sm, nae);
   {
     Acc2 acc[2] = {{0, 0}, {0, 0}};
     named_bar(1, kConsumerThreads);

@@ -31,9 +31,10 @@
 // moves into shared memory with 1D bulk copies, so every byte of H crosses
 // HBM once per matvec.
 //
-// Each run has a fixed-size record (header + gather segments) that a
-// descriptor warp copies into shared memory a few runs ahead; consumer warps
-// gather run k+1's vector segments with cp.async while they compute run k.
+// Each run has a fixed-size record (header + gather segments).  A gather
+// warp reads the records and fills a ring of kStages vector stage buffers
+// with cp.async, several runs ahead of the consumer warps, so no gather
+// latency and no CTA-wide barrier sits between two runs.
 #pragma once
 
 #include <cstddef>
@@ -55,12 +56,15 @@ constexpr int kConsumerWarps = 16; // warps that compute (+ a producer and a des
 #endif
 constexpr int kChunkLog = HBX_CHUNK_LOG;      // ring chunk = 32 KB (bulk copies this size stream at HBM rate)
 constexpr int kChunkBytes = 1 << kChunkLog;
-constexpr int kRingChunks = HBX_RING_CHUNKS;  // 128 KB ring per CTA (a power of two)
+constexpr int kRingChunks = HBX_RING_CHUNKS;  // 128 KB ring per CTA
 constexpr int kStageCap = 1024;    // doubles per vector stage buffer (x2); even
 constexpr int kRunSegs = 60;       // gather segments per run record
-constexpr int kSegMax = 64;        // doubles per gather segment (two per lane at most)
-constexpr int kRecBytes = 512;     // one run record: 32-byte header + kRunSegs segments
-constexpr int kDescSlots = 8;      // run records staged ahead by the descriptor warp
+constexpr int kSegMax = 32;        // doubles per gather segment (one gather lane copies one segment)
+constexpr int kRecBytes = 512;     // one run record: 32-byte header + kRunSegs segments (16 B per lane)
+#ifndef HBX_STAGES
+#define HBX_STAGES 4
+#endif
+constexpr int kStages = HBX_STAGES;  // vector stage buffers: runs gathered ahead of the consumers
 
 enum RunKind : uint16_t { kRunP = 0, kRunD = 1, kRunU = 2 };
 enum RunFlags : uint16_t { kFirst = 0x100, kLast = 0x200, kPadCol = 0x400 };
