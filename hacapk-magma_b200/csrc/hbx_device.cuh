@@ -19,6 +19,16 @@
 namespace hbx {
 
 constexpr uint32_t kRingBytes = (uint32_t)kRingChunks * kChunkBytes;
+// Run records in flight: the gather warp bulk-copies the records it will
+// need this many runs ahead (they come from HBM: the matrix stream evicts
+// them from L2 between two matvecs).
+constexpr uint32_t kRecSlots = 8;
+// Block ends are summed kGroup at a time, after one CTA barrier for the
+// group; the partials of two groups fit in shared memory.
+#ifndef HBX_GROUP
+#define HBX_GROUP 4
+#endif
+constexpr uint32_t kGroup = HBX_GROUP;
 
 // Shared-memory offset in the ring of stream byte p of absolute chunk c
 // (c = pass base + p / kChunkBytes).  The ring need not be a power of two.
@@ -46,18 +56,22 @@ struct SharedLayout {
   static constexpr uint32_t ring = 0;
   static constexpr uint32_t full = kRingBytes;
   static constexpr uint32_t empty = full + 8 * kRingChunks;
-  static constexpr uint32_t red = empty + 8 * kRingChunks;            // [2][NW][32] double
-  static constexpr uint32_t scal = red + 2 * kConsumerWarps * 32 * 8;  // 64 doubles of scratch
+  static constexpr uint32_t red = empty + 8 * kRingChunks;            // [2*kGroup][NW][32] double
+  static constexpr uint32_t scal = red + 2 * kGroup * kConsumerWarps * 32 * 8;  // 64 doubles of scratch
   static constexpr uint32_t stage = scal + 64 * 8;                     // [kStages][kStageCap] double
-  static constexpr uint32_t hdr = stage + kStages * kStageCap * 8;     // [kStages] Run
+  static constexpr uint32_t rec = stage + kStages * kStageCap * 8;     // [kRecSlots] run records
+  static constexpr uint32_t rfull = rec + kRecSlots * kRecBytes;       // [kRecSlots] record landed
+  static constexpr uint32_t hdr = rfull + 8 * kRecSlots;               // [kStages] Run
   static constexpr uint32_t sfull = hdr + kStages * 32;                // stage filled (gather warp)
   static constexpr uint32_t sempty = sfull + 8 * kStages;              // stage consumed (consumer warps)
   static constexpr uint32_t xready = sempty + 8 * kStages;             // a pass's x is complete grid-wide
   static constexpr uint32_t garrive = xready + 8;                      // this CTA arrived on the grid barrier
   static constexpr uint32_t gen = garrive + 8;                         // grid-barrier generation of that arrival
-  static constexpr uint32_t bytes = gen + 16;
+  static constexpr uint32_t binfo = gen + 16;                          // [2*kGroup] pending block ends
+  static constexpr uint32_t bytes = binfo + 2 * kGroup * 8;
 };
-static_assert(SharedLayout::stage % 16 == 0 && SharedLayout::hdr % 16 == 0 && SharedLayout::sfull % 8 == 0,
+static_assert(SharedLayout::stage % 16 == 0 && SharedLayout::hdr % 16 == 0 && SharedLayout::sfull % 8 == 0 &&
+                  SharedLayout::rec % 16 == 0,
               "shared-memory layout alignment");
 static_assert(SharedLayout::bytes <= 227 * 1024, "shared memory per CTA");
 
@@ -347,20 +361,35 @@ struct GatherCtx {
   uint64_t timeout_ns;
 };
 
-__device__ __forceinline__ uint4 ld_rec(const RunRec *recs, uint32_t k, int lane) {
-  return __ldg(reinterpret_cast<const uint4 *>(recs + k) + lane);
-}
-
 template <class SM>
 __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm) {
   const int lane = threadIdx.x & 31;
   const uint32_t nruns = c.nr_p + c.nr_d + c.nr_u, total = nruns * c.npass;
   if (total == 0) return;
-  uint4 nxt = ld_rec(c.recs, 0, lane);
-  for (uint32_t g = 0; g < total; ++g) {
+  // records g .. g + kRecSlots - 1 are in flight into slots g % kRecSlots
+  uint32_t issued = 0;
+  auto issue = [&](uint32_t gg) {
+    const uint32_t rs = gg % kRecSlots;
+    mbar_arrive_expect_tx(&sm.rfull[rs], (uint32_t)kRecBytes);
+    bulk_g2s(sm.rec + rs * kRecBytes, c.recs + (gg % nruns), (uint32_t)kRecBytes, &sm.rfull[rs]);
+  };
+  if (lane == 0)
+    for (uint32_t gg = 0; gg < min(total, kRecSlots); ++gg) issue(gg);
+  issued = min(total, kRecSlots);
+  uint32_t g = 0;
+  for (; g < total; ++g) {
     const uint32_t k = g % nruns, pass = g / nruns;
-    const uint4 cur = nxt;
-    if (g + 1 < total) nxt = ld_rec(c.recs, (g + 1) % nruns, lane);
+    const uint32_t rs = g % kRecSlots;
+    if (!warp_wait(&sm.rfull[rs], (g / kRecSlots) & 1, c.timeout_ns)) {
+      if (lane == 0) atomicOr(c.err, kErrProducer);
+      break;
+    }
+    const uint4 cur = reinterpret_cast<const uint4 *>(sm.rec + rs * kRecBytes)[lane];
+    __syncwarp();  // every lane has read the slot before it is refilled
+    if (g + kRecSlots < total) {
+      if (lane == 0) issue(g + kRecSlots);
+      issued = g + kRecSlots + 1;
+    }
     bool ok = true;
     if (k == 0) ok = warp_wait(sm.xready, pass & 1, c.timeout_ns);
     if (ok && k == c.nr_p + c.nr_d) {  // first U run of the pass: zbu must be complete grid-wide
@@ -377,6 +406,7 @@ __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm) {
     if (ok && g >= (uint32_t)kStages) ok = warp_wait(&sm.sempty[slot], ((g / kStages) - 1) & 1, c.timeout_ns);
     if (!ok) {
       if (lane == 0) atomicOr(c.err, kErrProducer);
+      ++g;  // this record was consumed
       break;
     }
     if (lane < 2) reinterpret_cast<uint4 *>(sm.hdr + slot)[lane] = cur;
@@ -407,6 +437,9 @@ __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm) {
     __syncwarp();
     if (lane == 0) mbar_arrive(&sm.sfull[slot]);  // releases the header and pad stores
   }
+  // record copies still in flight (only after an error) must land before exit
+  if (lane == 0)
+    for (uint32_t gg = g; gg < issued; ++gg) mbar_wait(&sm.rfull[gg % kRecSlots], (gg / kRecSlots) & 1, c.timeout_ns);
   cp_async_wait_all();
 }
 

@@ -28,9 +28,12 @@ constexpr int kConsumerThreads = NW * 32;
 struct Smem {
   uint8_t *ring;
   uint64_t *full, *empty;
-  double *red;    // [2][NW][32]
+  double *red;    // [2*kGroup][NW][32]
+  uint2 *binfo;   // [2*kGroup] (out, h | kind << 16) of the pending block ends
   double *scal;   // 64 doubles
   double *stage;  // [kStages][kStageCap]
+  uint8_t *rec;   // [kRecSlots] run records
+  uint64_t *rfull;
   Run *hdr;       // [kStages] headers of the staged runs
   uint64_t *sfull, *sempty;
   uint64_t *xready, *garrive;
@@ -45,12 +48,15 @@ __device__ __forceinline__ Smem smem_layout(uint8_t *base) {
   s.red = reinterpret_cast<double *>(base + SharedLayout::red);
   s.scal = reinterpret_cast<double *>(base + SharedLayout::scal);
   s.stage = reinterpret_cast<double *>(base + SharedLayout::stage);
+  s.rec = base + SharedLayout::rec;
+  s.rfull = reinterpret_cast<uint64_t *>(base + SharedLayout::rfull);
   s.hdr = reinterpret_cast<Run *>(base + SharedLayout::hdr);
   s.sfull = reinterpret_cast<uint64_t *>(base + SharedLayout::sfull);
   s.sempty = reinterpret_cast<uint64_t *>(base + SharedLayout::sempty);
   s.xready = reinterpret_cast<uint64_t *>(base + SharedLayout::xready);
   s.garrive = reinterpret_cast<uint64_t *>(base + SharedLayout::garrive);
   s.gen = reinterpret_cast<unsigned *>(base + SharedLayout::gen);
+  s.binfo = reinterpret_cast<uint2 *>(base + SharedLayout::binfo);
   return s;
 }
 
@@ -64,6 +70,7 @@ __device__ __forceinline__ void init_barriers(const Smem &s) {
       mbar_init(&s.sfull[i], 33);  // 32 cp.async arrivals of the gather warp + its lane 0
       mbar_init(&s.sempty[i], NW);
     }
+    for (uint32_t i = 0; i < kRecSlots; ++i) mbar_init(&s.rfull[i], 1);
     mbar_init(s.xready, 1);
     mbar_init(s.garrive, 1);
     mbar_fence_init();
@@ -73,27 +80,34 @@ __device__ __forceinline__ void init_barriers(const Smem &s) {
 
 __device__ __forceinline__ uint32_t run_end(const Run &r) { return r.pos + run_bytes(r); }
 
-// End of a block (rows out..out+h-1): the NW warp partials are summed in warp
-// order by warp (nae mod NW), so the summing work rotates over the warps.
-// kind P: zbu[out+i] = s;  D: y = alpha*s + beta*yin;  U: y += alpha*s.
-// Before the named barrier a warp gives back every ring chunk it will not
-// read again, so that warps still working on the block can get the chunks
-// they need from the producer (no warp waits at a barrier while holding
-// chunks the others depend on).
-__device__ __forceinline__ void block_end(const Run &run, double &acc, uint32_t &nae, double *red, double alpha,
-                                          double beta, const double *yin, double *y, double *zbu, Ring &R) {
+// Cross-warp sums of the finished blocks.  A warp that finishes its part of
+// a block writes its 32 partial sums to red buffer nae % (2 kGroup); after
+// every kGroup blocks (and at the end of a section) one CTA barrier makes
+// them visible and warp (block mod NW) sums each pending block in warp order
+// and writes its rows:  kind P: zbu[out+i] = s;  D: y = alpha*s + beta*yin;
+// U: y += alpha*s.  A group's buffers are refilled only after the next
+// group's barrier, which its summing warps pass after they have summed.
+struct BlockEnds {
+  uint32_t nae = 0;   // blocks finished so far (the same in every warp)
+  uint32_t pend = 0;  // finished but not yet summed
+};
+
+__device__ __forceinline__ void flush_block_ends(BlockEnds &B, const Smem &sm, double alpha, double beta,
+                                                 const double *yin, double *y, double *zbu, const Ring &R) {
+  if (B.pend == 0) return;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t h = run.nrow;
-  R.release_below(R.base + (run_end(run) >> kChunkLog));
-  double *rb = red + (nae & 1u) * (NW * 32);
-  if ((uint32_t)lane < h) rb[w * 32 + lane] = acc;
   named_bar(2, kConsumerThreads);
-  if (!R.bad && (uint32_t)w == (nae & (NW - 1)) && (uint32_t)lane < h) {
+  for (uint32_t q = B.nae - B.pend; q < B.nae; ++q) {
+    if ((uint32_t)w != q % NW || R.bad) continue;
+    const uint32_t b = q % (2 * kGroup);
+    const uint2 bi = sm.binfo[b];
+    const uint32_t h = bi.y & 0xffffu, kind = bi.y >> 16;
+    if ((uint32_t)lane >= h) continue;
+    const double *rb = sm.red + b * (NW * 32);
     double s = rb[lane];
 #pragma unroll
-    for (int q = 1; q < NW; ++q) s += rb[q * 32 + lane];
-    const uint32_t r = run.out + lane;
-    const uint32_t kind = run_kind(run);
+    for (int k = 1; k < NW; ++k) s += rb[k * 32 + lane];
+    const uint32_t r = bi.x + lane;
     if (kind == kRunP) {
       zbu[r] = s;
     } else if (kind == kRunD) {
@@ -104,15 +118,24 @@ __device__ __forceinline__ void block_end(const Run &run, double &acc, uint32_t 
       y[r] = fma(alpha, s, y[r]);
     }
   }
-  acc = 0.0;
-  ++nae;
+  B.pend = 0;
 }
 
-// Runs a section: gathers run k+1's vector segments while computing run k.
-// One named barrier per run makes run k's gathers visible to every warp and
-// guarantees that nobody still reads the buffer run k+1 is gathered into.
-// Run headers and terms come from the descriptor queue.  process(run, terms,
-// stage) returns the stream position where the run ends.
+// End of a block: park this warp's partials; sum the group when it is full.
+// Before the barrier a warp gives back every ring chunk it will not read
+// again, so no warp waits at a barrier while holding chunks others need.
+__device__ __forceinline__ void block_end(const Run &run, double &acc, BlockEnds &B, const Smem &sm, double alpha,
+                                          double beta, const double *yin, double *y, double *zbu, Ring &R) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  R.release_below(R.base + (run_end(run) >> kChunkLog));
+  const uint32_t b = B.nae % (2 * kGroup);
+  sm.red[b * (NW * 32) + w * 32 + lane] = acc;
+  if (w == 0 && lane == 0) sm.binfo[b] = make_uint2(run.out, (uint32_t)run.nrow | (run_kind(run) << 16));
+  acc = 0.0;
+  ++B.nae;
+  if (++B.pend == kGroup) flush_block_ends(B, sm, alpha, beta, yin, y, zbu, R);
+}
+
 // Consumer view of the stage ring: run g (counted over sections and passes)
 // is in slot g % kStages.
 struct StageQ {
@@ -150,7 +173,7 @@ __device__ __forceinline__ void run_section(uint32_t nruns, StageQ &Q, const Sme
 // when it returns.
 __device__ __forceinline__ void matvec_body(Ring &R, StageQ &Q, uint32_t K, const CtaInfo &ci, double alpha,
                                             double beta, const double *yin, double *y, double *zbu, unsigned *gbar,
-                                            int *err, const Smem &sm, uint32_t &nae,
+                                            int *err, const Smem &sm, BlockEnds &B,
                                             unsigned long long *prof = nullptr) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   auto stamp = [&](int k) {
@@ -160,13 +183,14 @@ __device__ __forceinline__ void matvec_body(Ring &R, StageQ &Q, uint32_t K, cons
   double acc = 0.0;
   auto block = [&](const Run &run, uint32_t stage_s) {
     run_block(run, stage_s, R, acc);
-    if (run.flags & kLast) block_end(run, acc, nae, sm.red, alpha, beta, yin, y, zbu, R);
+    if (run.flags & kLast) block_end(run, acc, B, sm, alpha, beta, yin, y, zbu, R);
     return run_end(run);
   };
   // ---- P: zbu = V^T x for this CTA's slabs
   uint32_t pend = 0;
   run_section(ci.nr_p, Q, sm, R, err, [&](const Run &run, uint32_t st) { return pend = block(run, st); });
   R.release_below(R.base + (pend >> kChunkLog));
+  flush_block_ends(B, sm, alpha, beta, yin, y, zbu, R);
   stamp(1);
   if (lane == 0) __threadfence();
   named_bar(1, kConsumerThreads);
@@ -182,11 +206,13 @@ __device__ __forceinline__ void matvec_body(Ring &R, StageQ &Q, uint32_t K, cons
   uint32_t dend = pend;
   run_section(ci.nr_d, Q, sm, R, err, [&](const Run &run, uint32_t st) { return dend = block(run, st); });
   R.release_below(R.base + (dend >> kChunkLog));
+  flush_block_ends(B, sm, alpha, beta, yin, y, zbu, R);
   stamp(3);
   stamp(4);
   // ---- U: U rows of the owned atoms times zbu (staged after the grid barrier)
   run_section(ci.nr_u, Q, sm, R, err, [&](const Run &run, uint32_t st) { return block(run, st); });
   R.release_below(R.base + K);
+  flush_block_ends(B, sm, alpha, beta, yin, y, zbu, R);
   // The barrier counts arrivals per instance: this CTA may arrive on the
   // next instance only once this one is complete (a CTA without U runs has
   // not waited for it yet).
@@ -215,8 +241,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   if (threadIdx.x == 0) mbar_arrive(sm.xready);  // x is an input: ready from the start
   Ring R{sm.ring, sm.full, sm.empty, 0, 0, 0, a.timeout_ns, a.err, false};
   StageQ Q{0};
-  uint32_t nae = 0;
-  matvec_body(R, Q, K, ci, a.alpha, a.beta, a.yin, a.y, a.zbu, a.gbar, a.err, sm, nae, a.prof);
+  BlockEnds B;
+  matvec_body(R, Q, K, ci, a.alpha, a.beta, a.yin, a.y, a.zbu, a.gbar, a.err, sm, B, a.prof);
   R.drain(K);
 }
 
@@ -387,7 +413,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
   Ring R{sm.ring, sm.full, sm.empty, 0, 0, 0, a.timeout_ns, a.err, false};
   StageQ Q{0};
-  uint32_t nae = 0;
+  BlockEnds B;
 
   // ---- S1: p = r + beta*(p - zeta*Ap)  (p = r on the first step)
   if (beta == 0.0) {
@@ -411,7 +437,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
 
   // ---- S2: Ap = H p;  rh . Ap
-  matvec_body(R, Q, K, ci, 1.0, 0.0, nullptr, a.ap, a.zbu, a.gbar, a.err, sm, nae);
+  matvec_body(R, Q, K, ci, 1.0, 0.0, nullptr, a.ap, a.zbu, a.gbar, a.err, sm, B);
   {
     Acc2 acc[1] = {{0, 0}};
     named_bar(1, kConsumerThreads);
@@ -434,7 +460,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
 
   // ---- S4: At = H t;  At . t,  At . At
   R.base = K;
-  matvec_body(R, Q, K, ci, 1.0, 0.0, nullptr, a.at, a.zbu, a.gbar, a.err, sm, nae);
+  matvec_body(R, Q, K, ci, 1.0, 0.0, nullptr, a.at, a.zbu, a.gbar, a.err, sm, B);
   {
     Acc2 acc[2] = {{0, 0}, {0, 0}};
     named_bar(1, kConsumerThreads);

@@ -34,7 +34,17 @@ const double *a2_of(const stc_HACApK_leafmtx *s) {
 bool lowrank_active(const stc_HACApK_leafmtx *s) { return s->ltmtx == 1 && s->kt > 0 && s->ndl > 0 && s->ndt > 0; }
 bool dense_active(const stc_HACApK_leafmtx *s) { return s->ltmtx == 2 && s->ndl > 0 && s->ndt > 0; }
 
-constexpr uint64_t kRunOverhead = 2048;  // bytes-equivalent fixed cost of a run (balancing only)
+// Bytes-equivalent fixed costs of a block and of a run, for balancing only
+// (the latency of a block end or a run switch, at the per-SM share of HBM
+// bandwidth).
+#ifndef HBX_BLOCK_COST
+#define HBX_BLOCK_COST 8192
+#endif
+#ifndef HBX_RUN_COST
+#define HBX_RUN_COST 4096
+#endif
+constexpr uint64_t kBlockOverhead = HBX_BLOCK_COST;
+constexpr uint64_t kRunOverhead = HBX_RUN_COST;
 
 // Min-heap load balancer (longest processing time first).
 struct Bins {
@@ -55,7 +65,7 @@ struct Bins {
 
 uint64_t block_cost(uint32_t h, uint32_t W) {
   const uint64_t wp = W + (W & 1u);
-  return 8ull * h * wp + kRunOverhead * (1 + wp / kStageCap);
+  return 8ull * h * wp + kBlockOverhead + kRunOverhead * (1 + wp / kStageCap);
 }
 
 // Vector index of block column c (c < W): P -> x index, D -> x index, U -> zbu index.
