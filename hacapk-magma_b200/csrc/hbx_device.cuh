@@ -270,9 +270,8 @@ struct RingCounters {
 
 // Releases every chunk below c0 (each only after it was observed full, so
 // every release lands in the right barrier phase), then waits until chunk c1
-// is full.  Out of line and by value, so the per-warp ring state stays in
-// registers on the fast path.
-__device__ __noinline__ RingCounters ring_advance(RingCounters rc, uint32_t c0, uint32_t c1, uint64_t *full,
+// is full.  Inlined: a chunk switch is frequent enough that a call costs.
+__device__ __forceinline__ RingCounters ring_advance(RingCounters rc, uint32_t c0, uint32_t c1, uint64_t *full,
                                                   uint64_t *empty, uint64_t timeout_ns, int *err) {
   const int lane = threadIdx.x & 31;
   while (!rc.bad && rc.released < c0) {
