@@ -182,9 +182,9 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hb
   if (tmo) h->timeout_ns = (unsigned long long)(std::atof(tmo) * 1e6);
   const char *prof = std::getenv("HBX_PROFILE");
   if (prof && std::atoi(prof) > 0) {
-    if ((e = cudaMalloc(&h->d_prof, (size_t)nc * 8 * sizeof(unsigned long long))) != cudaSuccess)
+    if ((e = cudaMalloc(&h->d_prof, (size_t)nc * 16 * sizeof(unsigned long long))) != cudaSuccess)
       return bail(cuda_fail(e, "cudaMalloc(prof)"));
-    cudaMemset(h->d_prof, 0, (size_t)nc * 8 * sizeof(unsigned long long));
+    cudaMemset(h->d_prof, 0, (size_t)nc * 16 * sizeof(unsigned long long));
   }
 
   std::string err;
@@ -253,7 +253,7 @@ int hbx_destroy(hbx_hmat *h) {
 // (HBX_PROFILE=1 at create time) into out[num_ctas*8]; returns the count.
 int hbx_debug_phase_stamps(hbx_hmat *h, unsigned long long *out, int cap) {
   if (!h || !out || !h->d_prof) return 0;
-  const int n = std::min(cap, h->num_ctas * 8);
+  const int n = std::min(cap, h->num_ctas * 16);
   cudaDeviceSynchronize();
   cudaMemcpy(out, h->d_prof, (size_t)n * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
   return n;
@@ -391,6 +391,7 @@ static hbx::BicgArgs bicg_args(hbx_hmat *h, const double *b, double *u, double t
   a.part = h->d_part;
   a.state = h->d_state;
   a.hist = h->d_hist;
+  a.prof = h->d_prof;
   a.tol = tol;
   a.max_iter = max_iter;
   return a;

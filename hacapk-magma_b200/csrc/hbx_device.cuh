@@ -342,8 +342,8 @@ __device__ __forceinline__ double warp_sum(double v) {
 // ---- gather warp: for every run of the CTA, in order and for every pass,
 // copies the run header into hdr[slot] and gathers the run's vector segments
 // (x for P and D runs, zbu for U runs) into stage[slot] with 8-byte cp.async
-// (segments start anywhere; each lane copies whole segments of at most
-// kSegMax entries), kStages runs ahead of the consumers.  Lane l
+// (segments start anywhere; the warp copies long segments together and
+// short ones one per lane), kStages runs ahead of the consumers.  Lane l
 // holds 16 bytes of the 512-byte record: lanes 0-1 the header, lane l >= 2
 // segments 2(l-2) and 2(l-2)+1.  Before the first run of pass p it waits
 // until that pass's x is complete grid-wide (xready), and before the first U
@@ -414,22 +414,29 @@ __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm) {
     const uint32_t nseg = __shfl_sync(0xffffffffu, cur.x, 1) & 0xffffu;
     const double *vec = (w3 & 0xffu) == kRunU ? c.zbu : ((pass & 1) ? c.x1 : c.x0);
     double *st = sm.stage + slot * kStageCap;
-    // lane q copies segment q (and segment 32 + q): segment s sits in lane
-    // 2 + s/2 of the record, fields (x, y) for even s and (z, w) for odd s
-#pragma unroll
-    for (uint32_t round = 0; round < 2; ++round) {
-      const uint32_t q = round * 32u + (uint32_t)lane;
-      const int holder = 2 + (int)(q >> 1);  // > 31 only for q >= 60, which is never a segment
-      const uint32_t sx = __shfl_sync(0xffffffffu, cur.x, holder & 31);
-      const uint32_t sy = __shfl_sync(0xffffffffu, cur.y, holder & 31);
-      const uint32_t sz = __shfl_sync(0xffffffffu, cur.z, holder & 31);
-      const uint32_t sw = __shfl_sync(0xffffffffu, cur.w, holder & 31);
+    const uint32_t nlong = __shfl_sync(0xffffffffu, cur.w, 1);
+    // long segments: the whole warp copies each one (segment s sits in lane
+    // 2 + s/2 of the record, fields (x, y) for even s and (z, w) for odd s)
+    for (uint32_t q = 0; q < nlong; ++q) {
+      const int holder = 2 + (int)(q >> 1);
+      const uint32_t src = __shfl_sync(0xffffffffu, (q & 1) ? cur.z : cur.x, holder);
+      const uint32_t ld = __shfl_sync(0xffffffffu, (q & 1) ? cur.w : cur.y, holder);
+      const uint32_t len = ld & 0xffffu, dst = ld >> 16;
+      for (uint32_t e = lane; e < len; e += 32) cp_async8(st + dst + e, vec + src + e);
+    }
+    // short segments: lane i copies segment nlong + i (and nlong + 32 + i)
+    for (uint32_t base = nlong; base < nseg; base += 32) {
+      const uint32_t q = base + (uint32_t)lane;
+      const int holder = 2 + (int)((q >> 1) & 31u);  // only q < nseg <= 60 is used
+      const uint32_t sx = __shfl_sync(0xffffffffu, cur.x, holder);
+      const uint32_t sy = __shfl_sync(0xffffffffu, cur.y, holder);
+      const uint32_t sz = __shfl_sync(0xffffffffu, cur.z, holder);
+      const uint32_t sw = __shfl_sync(0xffffffffu, cur.w, holder);
       if (q < nseg) {
         const uint32_t src = (q & 1) ? sz : sx, ld = (q & 1) ? sw : sy;
         const uint32_t len = ld & 0xffffu, dst = ld >> 16;
         for (uint32_t e = 0; e < len; ++e) cp_async8(st + dst + e, vec + src + e);
       }
-      if (nseg <= 32) break;
     }
     if ((w3 & kPadCol) && lane == 0) st[2u * (w2 >> 16) - 1u] = 0.0;
     cp_async_arrive(&sm.sfull[slot]);

@@ -42,7 +42,7 @@ struct MatvecArgs {
   unsigned *gbar;
   int *err;
   unsigned long long timeout_ns;
-  unsigned long long *prof;  // optional: per-CTA %globaltimer stamps [num_ctas][8]
+  unsigned long long *prof;  // optional: per-CTA %globaltimer stamps [num_ctas][16], slots 0-5
 };
 
 struct BicgArgs {
@@ -59,6 +59,7 @@ struct BicgArgs {
   double *part;   // [num_ctas][kSlots][2]
   BicgState *state;
   double *hist;   // relres per iteration (max_iter + 1 entries)
+  unsigned long long *prof;  // optional: per-CTA %globaltimer stamps [num_ctas][16], slots 8-15
   double tol;
   int max_iter;
 };

@@ -177,7 +177,7 @@ __device__ __forceinline__ void matvec_body(Ring &R, StageQ &Q, uint32_t K, cons
                                             unsigned long long *prof = nullptr) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   auto stamp = [&](int k) {
-    if (prof && w == 0 && lane == 0) prof[blockIdx.x * 8 + k] = gtimer();
+    if (prof && w == 0 && lane == 0) prof[blockIdx.x * 16 + k] = gtimer();
   };
   stamp(0);
   double acc = 0.0;
@@ -344,6 +344,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   const CtaInfo ci = a.ctas[blockIdx.x];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ncta = gridDim.x;
+  auto stamp = [&](int k) {
+    if (a.prof && threadIdx.x == 0) a.prof[blockIdx.x * 16 + 8 + k] = gtimer();
+  };
+  const uint64_t t_start = a.prof ? gtimer() : 0;
   init_barriers(sm);
 
   // ---- S0: scalars of the previous step; stop test at the top of the loop
@@ -395,6 +399,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
   __syncthreads();
   if (sm.scal[0] != 0.0) return;
+  if (a.prof && threadIdx.x == 0) a.prof[blockIdx.x * 16 + 8] = t_start;  // stamps of working steps only
   const double beta = sm.scal[2], zeta_prev = sm.scal[3], rho = sm.scal[4];
   const double relres = sm.scal[5], bnorm = sm.scal[7];
   const int iter = (int)sm.scal[6];
@@ -427,6 +432,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   __threadfence();
   grid_sync(a.gbar, a.err, a.timeout_ns, sm);
   if (threadIdx.x == 0) mbar_arrive(sm.xready);  // p complete grid-wide: pass 1 may be staged
+  stamp(1);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.state->iter = iter + 1;
     a.state->beta = beta;
@@ -438,6 +444,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
 
   // ---- S2: Ap = H p;  rh . Ap
   matvec_body(R, Q, K, ci, 1.0, 0.0, nullptr, a.ap, a.zbu, a.gbar, a.err, sm, B);
+  stamp(2);
   {
     Acc2 acc[1] = {{0, 0}};
     named_bar(1, kConsumerThreads);
@@ -451,16 +458,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
   named_bar(1, kConsumerThreads);
   const double alpha = sm.scal[8];
+  stamp(3);
 
   // ---- S3: t = r - alpha*Ap
   for_own_rows(a.atoms, ci, [&](uint32_t r) { a.t[r] = fma(-alpha, a.ap[r], a.r[r]); });
   __threadfence();
   grid_sync(a.gbar, a.err, a.timeout_ns, sm);
   if (threadIdx.x == 0) mbar_arrive(sm.xready);  // t complete grid-wide: pass 2 may be staged
+  stamp(4);
 
   // ---- S4: At = H t;  At . t,  At . At
   R.base = K;
   matvec_body(R, Q, K, ci, 1.0, 0.0, nullptr, a.at, a.zbu, a.gbar, a.err, sm, B);
+  stamp(5);
   {
     Acc2 acc[2] = {{0, 0}, {0, 0}};
     named_bar(1, kConsumerThreads);
@@ -488,6 +498,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
   named_bar(1, kConsumerThreads);
   const double zeta = sm.scal[9];
+  stamp(6);
 
   // ---- S5: u += alpha*p + zeta*t;  r = t - zeta*At;  rh . r,  r . r
   {
@@ -503,6 +514,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     cta_partials<2>(acc, a.part, kSlotRhoR, sm);
   }
   R.drain(2 * K);
+  stamp(7);
 }
 
 // part[cta][slot] over own rows, then (block 0 of a second launch) the total.

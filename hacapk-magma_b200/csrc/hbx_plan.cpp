@@ -87,7 +87,7 @@ struct ColumnMap {
 };
 
 // Gather segments of block columns [c0, c1) (c1 <= W): contiguous vector
-// ranges merged, each at most kSegMax long.
+// ranges merged; the ones longer than kSegShort are moved to the front.
 void segments(const ColumnMap &M, uint32_t c0, uint32_t c1, std::vector<Seg> &out) {
   out.clear();
   uint32_t piece = 0, piece_c0 = 0;
@@ -97,17 +97,22 @@ void segments(const ColumnMap &M, uint32_t c0, uint32_t c1, std::vector<Seg> &ou
     uint32_t n = std::min(avail, c1 - c);
     if (!out.empty()) {
       Seg &L = out.back();
-      if (L.src + L.len == src && L.len < (uint32_t)kSegMax) {
-        const uint32_t take = std::min<uint32_t>(n, kSegMax - L.len);
-        L.len = (uint16_t)(L.len + take);
-        c += take;
+      if (L.src + L.len == src) {
+        L.len = (uint16_t)(L.len + n);
+        c += n;
         continue;
       }
     }
-    const uint32_t take = std::min<uint32_t>(n, kSegMax);
-    out.push_back(Seg{src, (uint16_t)take, (uint16_t)(c - c0)});
-    c += take;
+    out.push_back(Seg{src, (uint16_t)n, (uint16_t)(c - c0)});
+    c += n;
   }
+  std::stable_partition(out.begin(), out.end(), [](const Seg &s) { return s.len > (uint32_t)kSegShort; });
+}
+
+uint32_t count_long(const std::vector<Seg> &segs) {
+  uint32_t n = 0;
+  for (const Seg &s : segs) n += s.len > (uint32_t)kSegShort ? 1u : 0u;
+  return n;
 }
 
 }  // namespace
@@ -336,8 +341,8 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
       do {
         uint32_t nc = std::min<uint32_t>(kStageCap, Wp - col);
         segments(M, col, std::min(col + nc, b.W), segs);
-        if (segs.size() > (size_t)kRunSegs) {
-          nc = (segs[kRunSegs - 1].dst + segs[kRunSegs - 1].len) & ~1u;
+        while (segs.size() > (size_t)kRunSegs) {  // too many pieces: take fewer columns
+          nc = std::max<uint32_t>(2, (nc / 2) & ~1u);
           segments(M, col, std::min(col + nc, b.W), segs);
         }
         RunRec rec{};
@@ -351,6 +356,7 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
                              (last && (b.W & 1u) ? kPadCol : 0));
         r.rot = (uint16_t)rot;
         r.nseg = (uint16_t)segs.size();
+        r.nlong = count_long(segs);
         r.vlen = (uint16_t)nc;
         r.block = bi;
         r.col0 = col;

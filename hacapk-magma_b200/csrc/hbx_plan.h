@@ -59,7 +59,8 @@ constexpr int kChunkBytes = 1 << kChunkLog;
 constexpr int kRingChunks = HBX_RING_CHUNKS;  // 128 KB ring per CTA
 constexpr int kStageCap = 1024;    // doubles per vector stage buffer (x2); even
 constexpr int kRunSegs = 60;       // gather segments per run record
-constexpr int kSegMax = 32;        // doubles per gather segment (one gather lane copies one segment)
+constexpr int kSegShort = 32;      // a segment this long or shorter is copied by one gather lane;
+                                   // a longer one by the whole gather warp
 constexpr int kRecBytes = 512;     // one run record: 32-byte header + kRunSegs segments (16 B per lane)
 #ifndef HBX_STAGES
 #define HBX_STAGES 4
@@ -89,7 +90,7 @@ struct alignas(16) Run {
   uint16_t vlen;   // doubles staged: 2*npair
   uint32_t block;  // block index (host-side packing and checks)
   uint32_t col0;   // first block column of the run
-  uint32_t pad;
+  uint32_t nlong;  // the first nlong segments are longer than kSegShort
 };
 static_assert(sizeof(Run) == 32, "Run must stay 32 bytes");
 

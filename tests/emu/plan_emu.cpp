@@ -54,12 +54,19 @@ extern "C" int emu_matvec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, c
       pos += run_bytes(r);
       if ((r.flags & kPadCol) && (!(r.flags & kLast) || r.npair == 0)) return "pad column outside a last run";
       const uint32_t real = 2u * r.npair - ((r.flags & kPadCol) ? 1u : 0u);
-      uint32_t d = 0;
       const uint64_t vmax = want == kRunU ? plan.zbu_len : (uint64_t)nd;
+      std::vector<char> cov(real, 0);
+      uint32_t d = 0;
+      if (r.nlong > r.nseg) return "nlong > nseg";
       for (uint32_t q = 0; q < r.nseg; ++q) {
         const Seg &s = plan.recs[ci.rec_begin + k].seg[q];
-        if (s.dst != d || s.len == 0 || s.len > kSegMax) return "segments do not tile the stage";
+        if (s.len == 0 || (uint32_t)s.dst + s.len > real) return "segment outside the stage";
+        if ((q < r.nlong) != (s.len > (uint32_t)kSegShort)) return "long segments not first";
         if ((uint64_t)s.src + s.len > vmax) return "segment source out of range";
+        for (uint32_t e = 0; e < s.len; ++e) {
+          if (cov[s.dst + e]) return "segments overlap";
+          cov[s.dst + e] = 1;
+        }
         d += s.len;
       }
       if (d != real) return "segments cover " + std::to_string(d) + " of " + std::to_string(real) + " columns";
