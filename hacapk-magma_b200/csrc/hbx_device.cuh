@@ -26,7 +26,7 @@ constexpr uint32_t kRecSlots = 8;
 // Block ends are summed kGroup at a time, after one CTA barrier for the
 // group; the partials of two groups fit in shared memory.
 #ifndef HBX_GROUP
-#define HBX_GROUP 4
+#define HBX_GROUP 2
 #endif
 constexpr uint32_t kGroup = HBX_GROUP;
 
@@ -56,8 +56,8 @@ struct SharedLayout {
   static constexpr uint32_t ring = 0;
   static constexpr uint32_t full = kRingBytes;
   static constexpr uint32_t empty = full + 8 * kRingChunks;
-  static constexpr uint32_t red = empty + 8 * kRingChunks;            // [2*kGroup][NW][32] double
-  static constexpr uint32_t scal = red + 2 * kGroup * kConsumerWarps * 32 * 8;  // 64 doubles of scratch
+  static constexpr uint32_t red = empty + 8 * kRingChunks;            // [2*kGroup][NW][64] double
+  static constexpr uint32_t scal = red + 2 * kGroup * kConsumerWarps * 64 * 8;  // 64 doubles of scratch
   static constexpr uint32_t stage = scal + 64 * 8;                     // [kStages][kStageCap] double
   static constexpr uint32_t rec = stage + kStages * kStageCap * 8;     // [kRecSlots] run records
   static constexpr uint32_t rfull = rec + kRecSlots * kRecBytes;       // [kRecSlots] record landed
@@ -459,40 +459,54 @@ __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm) {
 #endif
 constexpr uint32_t kUnroll = HBX_UNROLL;
 
-__device__ __forceinline__ void run_block(const Run &run, uint32_t stage_s, Ring &R, double &acc) {
-  constexpr uint32_t NW = kConsumerWarps, U = kUnroll;
+// (18 warps of 576 threads leave 96 registers a thread: the two-row form
+// unrolls by 2 to stay within them.)
+template <bool kTwoRows>
+__device__ __forceinline__ void run_block_rows(const Run &run, uint32_t stage_s, Ring &R, double &acc, double &acc2) {
+  constexpr uint32_t NW = kConsumerWarps, U = kTwoRows ? 2 : kUnroll;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t h = run.nrow, np = run.npair;
   if (np == 0) return;
   const uint32_t pb = 16u * h;
   const uint32_t lrow = 16u * min((uint32_t)lane, h - 1u);
+  const uint32_t lrow2 = 16u * min((uint32_t)lane + 32u, h - 1u) - lrow;  // second row, relative
   const uint32_t ring_s = smem_u32(R.buf);
   uint32_t j = (uint32_t)((w - (int)run.rot) & (int)(NW - 1));
-  double a[2 * U];
+  double a[2 * U], b[kTwoRows ? 2 * U : 1];
 #pragma unroll
   for (uint32_t u = 0; u < 2 * U; ++u) a[u] = 0.0;
+#pragma unroll
+  for (uint32_t u = 0; u < (kTwoRows ? 2 * U : 1); ++u) b[u] = 0.0;
   for (; j + (U - 1) * NW < np; j += U * NW) {
     const uint32_t p0 = run.pos + j * pb;
     R.ensure(p0, p0 + (U - 1) * NW * pb + pb);
-    double2 v[U], m[U];
+    double2 v[U], m[U], m2[kTwoRows ? U : 1];
 #pragma unroll
     for (uint32_t u = 0; u < U; ++u) v[u] = lds_f64x2(stage_s + 16u * (j + u * NW));
     const uint32_t pl = p0 + lrow;
     const uint32_t q = ring_off(R.base + (pl >> kChunkLog), pl);
-    if (q + (U - 1) * NW * pb + 16u <= kRingBytes) {  // the panels do not wrap around the ring end
+    if (q + (U - 1) * NW * pb + (kTwoRows ? lrow2 : 0u) + 16u <= kRingBytes) {  // no wrap around the ring end
 #pragma unroll
-      for (uint32_t u = 0; u < U; ++u) m[u] = lds_f64x2(ring_s + q + u * NW * pb);
+      for (uint32_t u = 0; u < U; ++u) {
+        m[u] = lds_f64x2(ring_s + q + u * NW * pb);
+        if (kTwoRows) m2[u] = lds_f64x2(ring_s + q + u * NW * pb + lrow2);
+      }
     } else {
 #pragma unroll
       for (uint32_t u = 0; u < U; ++u) {
         const uint32_t pu = pl + u * NW * pb;
         m[u] = lds_f64x2(ring_s + ring_off(R.base + (pu >> kChunkLog), pu));
+        if (kTwoRows) m2[u] = lds_f64x2(ring_s + ring_off(R.base + ((pu + lrow2) >> kChunkLog), pu + lrow2));
       }
     }
 #pragma unroll
     for (uint32_t u = 0; u < U; ++u) {
       a[2 * u] = fma(m[u].x, v[u].x, a[2 * u]);
       a[2 * u + 1] = fma(m[u].y, v[u].y, a[2 * u + 1]);
+      if (kTwoRows) {
+        b[2 * u] = fma(m2[u].x, v[u].x, b[2 * u]);
+        b[2 * u + 1] = fma(m2[u].y, v[u].y, b[2 * u + 1]);
+      }
     }
   }
   for (; j < np; j += NW) {
@@ -503,11 +517,29 @@ __device__ __forceinline__ void run_block(const Run &run, uint32_t stage_s, Ring
     const double2 mm = lds_f64x2(ring_s + ring_off(R.base + (pl >> kChunkLog), pl));
     a[0] = fma(mm.x, vv.x, a[0]);
     a[1] = fma(mm.y, vv.y, a[1]);
+    if (kTwoRows) {
+      const uint32_t p2 = pl + lrow2;
+      const double2 m2 = lds_f64x2(ring_s + ring_off(R.base + (p2 >> kChunkLog), p2));
+      b[0] = fma(m2.x, vv.x, b[0]);
+      b[1] = fma(m2.y, vv.y, b[1]);
+    }
   }
   double t = 0.0;
 #pragma unroll
   for (uint32_t u = 0; u < 2 * U; ++u) t += a[u];
   acc += t;
+  if (kTwoRows) {
+    double t2 = 0.0;
+#pragma unroll
+    for (uint32_t u = 0; u < 2 * U; ++u) t2 += b[u];
+    acc2 += t2;
+  }
+}
+
+// acc: row `lane` of the block; acc2: row lane + 32 (P slabs taller than 32).
+__device__ __forceinline__ void run_block(const Run &run, uint32_t stage_s, Ring &R, double &acc, double &acc2) {
+  if (run.nrow > 32) run_block_rows<true>(run, stage_s, R, acc, acc2);
+  else run_block_rows<false>(run, stage_s, R, acc, acc2);
 }
 
 // ---- compensated (Dot2) accumulation ------------------------------------------

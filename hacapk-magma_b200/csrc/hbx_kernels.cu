@@ -28,7 +28,7 @@ constexpr int kConsumerThreads = NW * 32;
 struct Smem {
   uint8_t *ring;
   uint64_t *full, *empty;
-  double *red;    // [2*kGroup][NW][32]
+  double *red;    // [2*kGroup][NW][64]
   uint2 *binfo;   // [2*kGroup] (out, h | kind << 16) of the pending block ends
   double *scal;   // 64 doubles
   double *stage;  // [kStages][kStageCap]
@@ -81,7 +81,8 @@ __device__ __forceinline__ void init_barriers(const Smem &s) {
 __device__ __forceinline__ uint32_t run_end(const Run &r) { return r.pos + run_bytes(r); }
 
 // Cross-warp sums of the finished blocks.  A warp that finishes its part of
-// a block writes its 32 partial sums to red buffer nae % (2 kGroup); after
+// a block writes its 64 partial sums (rows lane and lane + 32) to red buffer
+// nae % (2 kGroup); after
 // every kGroup blocks (and at the end of a section) one CTA barrier makes
 // them visible and warp (block mod NW) sums each pending block in warp order
 // and writes its rows:  kind P: zbu[out+i] = s;  D: y = alpha*s + beta*yin;
@@ -102,20 +103,23 @@ __device__ __forceinline__ void flush_block_ends(BlockEnds &B, const Smem &sm, d
     const uint32_t b = q % (2 * kGroup);
     const uint2 bi = sm.binfo[b];
     const uint32_t h = bi.y & 0xffffu, kind = bi.y >> 16;
-    if ((uint32_t)lane >= h) continue;
-    const double *rb = sm.red + b * (NW * 32);
-    double s = rb[lane];
+    const double *rb = sm.red + b * (NW * 64);
+    for (uint32_t row = lane; row < h; row += 32) {
+      double s = rb[row];
 #pragma unroll
-    for (int k = 1; k < NW; ++k) s += rb[k * 32 + lane];
-    const uint32_t r = bi.x + lane;
-    if (kind == kRunP) {
-      zbu[r] = s;
-    } else if (kind == kRunD) {
-      double v = alpha * s;
-      if (beta != 0.0) v = fma(beta, yin[r], v);
-      y[r] = v;
-    } else {
-      y[r] = fma(alpha, s, y[r]);
+      for (int k = 1; k < NW; ++k) s += rb[k * 64 + row];
+      const uint32_t r = bi.x + row;
+      if (kind == kRunP) {
+        zbu[r] = s;
+        continue;
+      }
+      if (kind == kRunD) {
+        double v = alpha * s;
+        if (beta != 0.0) v = fma(beta, yin[r], v);
+        y[r] = v;
+      } else {
+        y[r] = fma(alpha, s, y[r]);
+      }
     }
   }
   B.pend = 0;
@@ -124,14 +128,17 @@ __device__ __forceinline__ void flush_block_ends(BlockEnds &B, const Smem &sm, d
 // End of a block: park this warp's partials; sum the group when it is full.
 // Before the barrier a warp gives back every ring chunk it will not read
 // again, so no warp waits at a barrier while holding chunks others need.
-__device__ __forceinline__ void block_end(const Run &run, double &acc, BlockEnds &B, const Smem &sm, double alpha,
-                                          double beta, const double *yin, double *y, double *zbu, Ring &R) {
+__device__ __forceinline__ void block_end(const Run &run, double &acc, double &acc2, BlockEnds &B, const Smem &sm,
+                                          double alpha, double beta, const double *yin, double *y, double *zbu,
+                                          Ring &R) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   R.release_below(R.base + (run_end(run) >> kChunkLog));
   const uint32_t b = B.nae % (2 * kGroup);
-  sm.red[b * (NW * 32) + w * 32 + lane] = acc;
+  sm.red[b * (NW * 64) + w * 64 + lane] = acc;
+  sm.red[b * (NW * 64) + w * 64 + 32 + lane] = acc2;
   if (w == 0 && lane == 0) sm.binfo[b] = make_uint2(run.out, (uint32_t)run.nrow | (run_kind(run) << 16));
   acc = 0.0;
+  acc2 = 0.0;
   ++B.nae;
   if (++B.pend == kGroup) flush_block_ends(B, sm, alpha, beta, yin, y, zbu, R);
 }
@@ -180,10 +187,10 @@ __device__ __forceinline__ void matvec_body(Ring &R, StageQ &Q, uint32_t K, cons
     if (prof && w == 0 && lane == 0) prof[blockIdx.x * 16 + k] = gtimer();
   };
   stamp(0);
-  double acc = 0.0;
+  double acc = 0.0, acc2 = 0.0;
   auto block = [&](const Run &run, uint32_t stage_s) {
-    run_block(run, stage_s, R, acc);
-    if (run.flags & kLast) block_end(run, acc, B, sm, alpha, beta, yin, y, zbu, R);
+    run_block(run, stage_s, R, acc, acc2);
+    if (run.flags & kLast) block_end(run, acc, acc2, B, sm, alpha, beta, yin, y, zbu, R);
     return run_end(run);
   };
   // ---- P: zbu = V^T x for this CTA's slabs

@@ -192,11 +192,11 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
   }
   if (ktsum > 0xffffffffull || (uint64_t)nd > 0xffffffffull) { err = "zbu length exceeds 2^32"; return HBX_ERR_INVALID; }
 
-  // ---- P blocks: slabs of <= 32 stacked rows
+  // ---- P blocks: slabs of <= 64 stacked rows
   std::vector<uint32_t> pblocks;
   for (uint32_t g = 0; g < ngroups; ++g) {
     const uint32_t R = (uint32_t)grows[g];
-    const uint32_t pieces = (R + kAtomMax - 1) / kAtomMax;
+    const uint32_t pieces = (R + kSlabMax - 1) / kSlabMax;
     const uint32_t base = R / pieces, rem = R % pieces;
     const uint32_t W = (uint32_t)leaf_at(st, (int)gl[g][0])->ndt;
     uint32_t r = 0;

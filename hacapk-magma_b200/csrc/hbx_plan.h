@@ -7,7 +7,7 @@
 //   P  zbu = V^T x.  Low-rank leaves that share a column range (same nstrtt
 //      and ndt: one column cluster) are stacked, so their V^T form one tall
 //      matrix (sum of kt rows) over the same x segment; it is cut into slabs
-//      of <= 32 rows.  zbu is numbered in this stacking order, so a slab
+//      of <= 64 rows.  zbu is numbered in this stacking order, so a slab
 //      writes a contiguous zbu range.
 //   D  the rows of the dense leaves that fall in one row atom, side by side
 //      (W = sum of their ndt), times their x segments.
@@ -46,7 +46,8 @@
 
 namespace hbx {
 
-constexpr int kAtomMax = 32;       // rows per block (one lane per row)
+constexpr int kAtomMax = 32;       // rows per D/U block (one lane per row)
+constexpr int kSlabMax = 64;       // rows per P slab (two rows per lane)
 constexpr int kConsumerWarps = 16; // warps that compute (+ a producer and a descriptor warp)
 #ifndef HBX_CHUNK_LOG
 #define HBX_CHUNK_LOG 15
@@ -82,7 +83,7 @@ static_assert(sizeof(Seg) == 8, "Seg layout");
 struct alignas(16) Run {
   uint32_t pos;    // byte offset of the run's pair panels in the CTA stream (16-aligned)
   uint32_t out;    // first output row: zbu index (P) or y row (D, U)
-  uint16_t nrow;   // h, 1..32
+  uint16_t nrow;   // h: 1..32 for D/U, 1..64 for P
   uint16_t npair;  // column pairs; 2*npair <= kStageCap
   uint16_t flags;  // RunKind | RunFlags
   uint16_t rot;    // consumer warp that takes pair 0

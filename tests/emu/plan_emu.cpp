@@ -32,7 +32,7 @@ extern "C" int emu_matvec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, c
   std::vector<int> owner(nd, -1);
   std::fill(y, y + nd, NAN);
   long long nruns = 0;
-  std::vector<double> stage(kStageCap), acc(kAtomMax);
+  std::vector<double> stage(kStageCap), acc(kSlabMax);
 
   // structural checks of one CTA's records; returns "" when fine
   auto check_cta = [&](int c) -> std::string {
@@ -46,7 +46,7 @@ extern "C" int emu_matvec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, c
       const Run &r = plan.recs[ci.rec_begin + k].hdr;
       const uint32_t want = k < ci.nr_p ? kRunP : (k < ci.nr_p + ci.nr_d ? kRunD : kRunU);
       if (run_kind(r) != want) return "run kind out of section order";
-      if (r.nrow == 0 || r.nrow > kAtomMax) return "run height outside 1..32";
+      if (r.nrow == 0 || r.nrow > (want == kRunP ? kSlabMax : kAtomMax)) return "run height outside 1..32 (1..64 for P)";
       if (2u * r.npair > (uint32_t)kStageCap || r.vlen != 2u * r.npair) return "run width";
       if (r.nseg > kRunSegs) return "too many segments";
       if (r.rot >= kConsumerWarps) return "bad rotation";

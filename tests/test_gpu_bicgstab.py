@@ -1,6 +1,7 @@
 """GPU BiCGSTAB through the C ABI against the CPU restatement of
 HACApK_SOLVER.c:254-417 using the reference matvec.  Bar: the same iteration
-count within +-1, and a true residual ||b - H u||/||b|| below the tolerance."""
+count within +-1 where the problem's rounding sensitivity allows it (BANDS
+below), and a true residual ||b - H u||/||b|| below the tolerance."""
 import ctypes as C
 
 import numpy as np
@@ -9,6 +10,16 @@ import pytest
 from conftest import sphere
 
 pytestmark = pytest.mark.gpu
+
+
+# Iteration-count band against the oracle.  BiCGSTAB's count follows the
+# last bits of every product on these problems: the oracle loop itself, fed
+# the oracle matvec plus 1e-15*max|y| of random noise, takes 14 iterations on
+# the level-3 sphere whatever the noise, 20-25 on level 4 (20 without noise)
+# and 28-33 on level 5 (24 draws: 28 x1, 29 x1, 30 x4, 31 x2, 32 x10, 33 x6;
+# 32 without noise).  Level 3 and 4 are held to +-1; level 5 to the oracle's
+# own spread, with the true residual below the tolerance in every case.
+BANDS = {3: (1, 1), 4: (1, 1), 5: (4, 1)}
 
 
 @pytest.mark.parametrize("level", [3, 4, 5])
@@ -22,7 +33,8 @@ def test_iterations_and_residual_match_oracle(gpu, build_libs, level):
     u_ref, n_ref, hist, _ = oracle.bicgstab(H.st, b, tol=1e-8, max_iter=1000,
                                             kind="ref" if oracle.have_ref() else "restated")
     assert info["status"] == 0
-    assert abs(info["iterations"] - n_ref) <= 1
+    lo, hi = BANDS[level]
+    assert n_ref - lo <= info["iterations"] <= n_ref + hi
     r = b - oracle.matvec(H.st, u)
     assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-8 * 1.01
     assert info["true_relres"] == pytest.approx(np.linalg.norm(r) / np.linalg.norm(b), rel=1e-3)
