@@ -358,50 +358,60 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   init_barriers(sm);
 
   // ---- S0: scalars of the previous step; stop test at the top of the loop
-  // (HACApK_SOLVER.c:602-603).  Every CTA computes identical values.
-  if (w == 0) {
-    const double rho_new = reduce_slot(a.part, ncta, kSlotRhoR);
-    const double rr = reduce_slot(a.part, ncta, kSlotRR);
-    const double bb = reduce_slot(a.part, ncta, kSlotBB);
-    if (lane == 0) {
-      BicgState st;
-      st.alpha = __ldcg(&a.state->alpha);
-      st.zeta = __ldcg(&a.state->zeta);
-      st.rho = __ldcg(&a.state->rho);
-      st.iter = __ldcg(&a.state->iter);
-      st.done = __ldcg(&a.state->done);
-      st.status = __ldcg(&a.state->status);
-      st.breakdown = __ldcg(&a.state->breakdown);
-      const double bnorm = sqrt(bb);
-      const double relres = (bnorm > 0.0) ? sqrt(rr) / bnorm : 0.0;
-      int done = st.done, status = st.status;
-      double beta = 0.0;
-      if (!done) {
-        if (st.breakdown) { done = 1; status = HBX_ERR_BREAKDOWN; }
-        else if (relres < a.tol) { done = 1; status = HBX_OK; }
-        else if (!isfinite(relres)) { done = 1; status = HBX_ERR_BREAKDOWN; }
-        else if (st.iter >= a.max_iter) { done = 1; status = HBX_ERR_NOT_CONVERGED; }
-        else if (st.iter > 0) {
-          // beta = -alpha/zeta * (rh.r_new)/znormold with the reference's sign
-          // flips (HACApK_SOLVER.c:650-655, :699, :724) = (alpha/zeta) rho_new/rho_old
-          beta = (st.alpha / st.zeta) * (rho_new / st.rho);
-          if (!isfinite(beta)) { done = 1; status = HBX_ERR_BREAKDOWN; }
-        }
+  // (HACApK_SOLVER.c:602-603).  Every CTA computes identical values: warps
+  // 0-2 reduce the three dot products side by side, warp 3 reads the state.
+  if (w < 3) {
+    const double v = reduce_slot(a.part, ncta, w == 0 ? kSlotRhoR : (w == 1 ? kSlotRR : kSlotBB));
+    if (lane == 0) sm.scal[10 + w] = v;
+  } else if (w == 3 && lane == 0) {
+    sm.scal[13] = __ldcg(&a.state->alpha);
+    sm.scal[14] = __ldcg(&a.state->zeta);
+    sm.scal[15] = __ldcg(&a.state->rho);
+    sm.scal[16] = (double)__ldcg(&a.state->iter);
+    sm.scal[17] = (double)__ldcg(&a.state->done);
+    sm.scal[18] = (double)__ldcg(&a.state->status);
+    sm.scal[19] = (double)__ldcg(&a.state->breakdown);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double rho_new = sm.scal[10], rr = sm.scal[11], bb = sm.scal[12];
+    BicgState st;
+    st.alpha = sm.scal[13];
+    st.zeta = sm.scal[14];
+    st.rho = sm.scal[15];
+    st.iter = (int)sm.scal[16];
+    st.done = (int)sm.scal[17];
+    st.status = (int)sm.scal[18];
+    st.breakdown = (int)sm.scal[19];
+    const double bnorm = sqrt(bb);
+    const double relres = (bnorm > 0.0) ? sqrt(rr) / bnorm : 0.0;
+    int done = st.done, status = st.status;
+    double beta = 0.0;
+    if (!done) {
+      if (st.breakdown) { done = 1; status = HBX_ERR_BREAKDOWN; }
+      else if (relres < a.tol) { done = 1; status = HBX_OK; }
+      else if (!isfinite(relres)) { done = 1; status = HBX_ERR_BREAKDOWN; }
+      else if (st.iter >= a.max_iter) { done = 1; status = HBX_ERR_NOT_CONVERGED; }
+      else if (st.iter > 0) {
+        // beta = -alpha/zeta * (rh.r_new)/znormold with the reference's sign
+        // flips (HACApK_SOLVER.c:650-655, :699, :724) = (alpha/zeta) rho_new/rho_old
+        beta = (st.alpha / st.zeta) * (rho_new / st.rho);
+        if (!isfinite(beta)) { done = 1; status = HBX_ERR_BREAKDOWN; }
       }
-      sm.scal[0] = done;
-      sm.scal[1] = status;
-      sm.scal[2] = beta;
-      sm.scal[3] = st.zeta;
-      sm.scal[4] = rho_new;
-      sm.scal[5] = relres;
-      sm.scal[6] = st.iter;
-      sm.scal[7] = bnorm;
-      if (done && blockIdx.x == 0) {
-        a.state->done = 1;
-        a.state->status = status;
-        a.state->relres = relres;
-        a.state->bnorm = bnorm;
-      }
+    }
+    sm.scal[0] = done;
+    sm.scal[1] = status;
+    sm.scal[2] = beta;
+    sm.scal[3] = st.zeta;
+    sm.scal[4] = rho_new;
+    sm.scal[5] = relres;
+    sm.scal[6] = st.iter;
+    sm.scal[7] = bnorm;
+    if (done && blockIdx.x == 0) {
+      a.state->done = 1;
+      a.state->status = status;
+      a.state->relres = relres;
+      a.state->bnorm = bnorm;
     }
   }
   __syncthreads();
@@ -489,9 +499,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     cta_partials<2>(acc, a.part, kSlotAtT, sm);
   }
   grid_sync(a.gbar, a.err, a.timeout_ns, sm);
+  if (w < 2) {  // the two sums side by side
+    const double v = reduce_slot(a.part, ncta, w == 0 ? kSlotAtT : kSlotAtAt);
+    if (lane == 0) sm.scal[10 + w] = v;
+  }
+  named_bar(1, kConsumerThreads);
   if (w == 0) {
-    const double s3 = reduce_slot(a.part, ncta, kSlotAtT);
-    const double s4 = reduce_slot(a.part, ncta, kSlotAtAt);
+    const double s3 = sm.scal[10], s4 = sm.scal[11];
     if (lane == 0) {
       const double zeta = (s4 != 0.0) ? s3 / s4 : 0.0;
       sm.scal[9] = zeta;
