@@ -188,6 +188,13 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hb
   }
 
   std::string err;
+  hbx::TransposedLeaves tleaves;  // H^T (host memory until the stream is packed)
+  if (opt && opt->transpose) {
+    int rc = hbx::transpose_leaves(st, nd, tleaves, err);
+    if (rc != HBX_OK) return bail(fail(rc, "hbx_create: " + err));
+    st = &tleaves.container;
+    h->transposed = 1;
+  }
   int st_plan = hbx::make_plan(st, nd, nc, h->plan, err);
   if (st_plan != HBX_OK) return bail(fail(st_plan, "hbx_create: " + err));
   const hbx::Plan &P = h->plan;
@@ -280,6 +287,7 @@ int hbx_get_info(const hbx_hmat *h, hbx_info *info) {
   info->dense_words = (long long)P.dense_words;
   info->lowrank_words = (long long)P.lowrank_words;
   info->setup_seconds = h->setup_seconds;
+  info->transposed = h->transposed;
   return HBX_OK;
 }
 
@@ -533,6 +541,30 @@ int hbx_bicgstab_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_o
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "hbx_bicgstab_host copy-out");
   return st;
+}
+
+// dJ/dg for J = 0.5 ||sigma - sigma_t||^2, H sigma = g: the forward solve,
+// then the adjoint solve H^T lambda = sigma - sigma_t on the transposed engine.
+int hbx_gradient_host(hbx_hmat *h, hbx_hmat *ht, const double *g, const double *sigma_t, double *sigma,
+                      double *grad, double *J, const hbx_solve_opts *opts, hbx_solve_info *fwd,
+                      hbx_solve_info *adj) {
+  if (!h || !ht || !g || !sigma_t || !sigma || !grad) return fail(HBX_ERR_INVALID, "hbx_gradient_host: NULL argument");
+  if (h->transposed || !ht->transposed)
+    return fail(HBX_ERR_INVALID, "hbx_gradient_host: h must hold H and ht must hold H^T (hbx_options.transpose)");
+  if (h->plan.nd != ht->plan.nd) return fail(HBX_ERR_INVALID, "hbx_gradient_host: h and ht differ in size");
+  const size_t n = (size_t)h->plan.nd;
+  std::fill(sigma, sigma + n, 0.0);
+  int st = hbx_bicgstab_host(h, g, sigma, opts, fwd);
+  if (st != HBX_OK) return st;
+  std::vector<double> d(n);
+  double j = 0.0;
+  for (size_t i = 0; i < n; ++i) {
+    d[i] = sigma[i] - sigma_t[i];
+    j += d[i] * d[i];
+  }
+  if (J) *J = 0.5 * j;
+  std::fill(grad, grad + n, 0.0);
+  return hbx_bicgstab_host(ht, d.data(), grad, opts, adj);
 }
 
 // ------------------------------------------------------------------------

@@ -86,6 +86,7 @@ cudaError_t launch_dot(const BicgArgs &a, const double *x, const double *y, int 
 struct hbx_hmat {
   int device = 0;
   int num_ctas = 0;
+  int transposed = 0;  // the packed stream holds H^T
   hbx::Plan plan;
   uint8_t *d_stream = nullptr;
   hbx::RunRec *d_recs = nullptr;

@@ -446,4 +446,61 @@ void pack_plan(const stc_HACApK_leafmtxp *st, const Plan &plan, uint8_t *dst) {
   }
 }
 
+int transpose_leaves(const stc_HACApK_leafmtxp *st, int nd, TransposedLeaves &out, std::string &err) {
+  out = TransposedLeaves();
+  if (!st || nd <= 0) { err = "null container or nd <= 0"; return HBX_ERR_INVALID; }
+  const int nlf = st->nlf;
+  if (nlf < 0 || (nlf > 0 && (!st->st_lf || st->st_lf_stride < (int)sizeof(stc_HACApK_leafmtx)))) {
+    err = "bad leaf array (nlf, st_lf or st_lf_stride)";
+    return HBX_ERR_INVALID;
+  }
+  // sizes first (one allocation), then the copies
+  std::vector<size_t> off(nlf + 1, 0);
+  for (int ip = 0; ip < nlf; ++ip) {
+    const stc_HACApK_leafmtx *s = leaf_at(st, ip);
+    size_t words = 0;
+    if (s->ndl > 0 && s->ndt > 0 && s->a1) {
+      if (s->ltmtx == 2) words = (size_t)s->ndl * s->ndt;
+      else if (s->ltmtx == 1 && s->kt > 0) words = (size_t)s->kt * (s->ndl + s->ndt);
+    }
+    off[ip + 1] = off[ip] + words;
+  }
+  out.data.resize(std::max<size_t>(1, off[nlf]));
+  out.leaves.resize(std::max(1, nlf));
+  for (int ip = 0; ip < nlf; ++ip) {
+    const stc_HACApK_leafmtx *s = leaf_at(st, ip);
+    stc_HACApK_leafmtx t = *s;
+    t.nstrtl = s->nstrtt;
+    t.ndl = s->ndt;
+    t.nstrtt = s->nstrtl;
+    t.ndt = s->ndl;
+    t.a1 = nullptr;
+    t.a2 = nullptr;
+    t.a1size = 0;
+    double *d = out.data.data() + off[ip];
+    if (off[ip + 1] > off[ip]) {
+      if (s->ltmtx == 2) {
+        // A(il, it) = a1[it + il*ndt];  A^T(it, il) = a1'[il + it*ndl]
+        for (int il = 0; il < s->ndl; ++il)
+          for (int it = 0; it < s->ndt; ++it) d[(size_t)il + (size_t)it * s->ndl] = s->a1[(size_t)it + (size_t)il * s->ndt];
+        t.a1 = d;
+        t.a1size = (long long)s->ndl * s->ndt * 8;
+      } else {
+        // new V (ndt' x kt = ndl x kt) is the old U, new U is the old V
+        const size_t nu = (size_t)s->ndl * s->kt, nv = (size_t)s->ndt * s->kt;
+        std::memcpy(d, a2_of(s), nu * 8);
+        std::memcpy(d + nu, s->a1, nv * 8);
+        t.a1 = d;
+        t.a1size = (long long)nu * 8;
+        t.a2 = d + nu;
+      }
+    }
+    out.leaves[ip] = t;
+  }
+  out.container = *st;
+  out.container.st_lf = out.leaves.data();
+  out.container.st_lf_stride = (int)sizeof(stc_HACApK_leafmtx);
+  return HBX_OK;
+}
+
 }  // namespace hbx

@@ -163,4 +163,16 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
 // Writes the packed stream of every CTA into `dst` (plan.total_bytes bytes).
 void pack_plan(const stc_HACApK_leafmtxp *st, const Plan &plan, uint8_t *dst);
 
+// The leaf list of H^T, in host memory owned by the object: a dense leaf
+// (ndl x ndt) becomes its transpose (ndt x ndl); a low-rank leaf U V^T becomes
+// V U^T (the factors swap places, no arithmetic), so the packed H^T streams
+// exactly the bytes of H.  The reference has no transposed product
+// (HACApK_BATCH_SORT.c:123 only changes the storage orientation of A*x).
+struct TransposedLeaves {
+  std::vector<stc_HACApK_leafmtx> leaves;
+  std::vector<double> data;
+  stc_HACApK_leafmtxp container{};
+};
+int transpose_leaves(const stc_HACApK_leafmtxp *st, int nd, TransposedLeaves &out, std::string &err);
+
 }  // namespace hbx

@@ -57,7 +57,7 @@ class LControl(C.Structure):
 
 
 class Options(C.Structure):
-    _fields_ = [("precision", C.c_int), ("num_ctas", C.c_int), ("reserved", C.c_int * 14)]
+    _fields_ = [("precision", C.c_int), ("num_ctas", C.c_int), ("transpose", C.c_int), ("reserved", C.c_int * 13)]
 
 
 class Info(C.Structure):
@@ -67,7 +67,7 @@ class Info(C.Structure):
                 ("alg_bytes", C.c_longlong), ("alg_flops", C.c_longlong),
                 ("zbu_len", C.c_longlong), ("dense_words", C.c_longlong),
                 ("lowrank_words", C.c_longlong), ("setup_seconds", C.c_double),
-                ("reserved", C.c_int * 8)]
+                ("transposed", C.c_int), ("reserved", C.c_int * 7)]
 
 
 class SolveOpts(C.Structure):
@@ -118,6 +118,8 @@ ENGINE_SYMBOLS = [
     ("hbx_matvec_host", C.c_int, [_VP, _DP, _DP, C.c_int, _DP, _DP]),
     ("hbx_bicgstab", C.c_int, [_VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
     ("hbx_bicgstab_host", C.c_int, [_VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
+    ("hbx_gradient_host", C.c_int, [_VP, _VP, _DP, _DP, _DP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo),
+                                    C.POINTER(SolveInfo)]),
     ("hbx_debug_phase_stamps", C.c_int, [_VP, C.POINTER(C.c_ulonglong), C.c_int]),
     ("hbx_status_string", C.c_char_p, [C.c_int]),
     ("hbx_last_error", C.c_char_p, []),

@@ -29,11 +29,13 @@ def _check(status: int, where: str):
 class Engine:
     """Packed H-matrix resident on the current CUDA device."""
 
-    def __init__(self, st, nd: int, num_ctas: int = 0):
+    def __init__(self, st, nd: int, num_ctas: int = 0, transpose: bool = False):
+        """transpose=True packs H^T: products and solves with the adjoint."""
         self.lib = abi.engine_lib()
         opt = abi.Options()
         opt.precision = 0
         opt.num_ctas = num_ctas
+        opt.transpose = 1 if transpose else 0
         h = C.c_void_p()
         _check(self.lib.hbx_create(st, nd, C.byref(opt), C.byref(h)), "hbx_create")
         self._h = h
@@ -114,3 +116,19 @@ class Engine:
         if check:
             _check(st, "hbx_bicgstab")
         return self._info(si)
+
+    def gradient_host(self, adjoint: "Engine", g: np.ndarray, sigma_t: np.ndarray, tol: float = 1e-8,
+                      max_iter: int = 1000):
+        """dJ/dg for J = 0.5||sigma - sigma_t||^2 with H sigma = g (self holds H,
+        `adjoint` holds H^T).  Returns (J, grad, sigma, forward info, adjoint info)."""
+        g = np.ascontiguousarray(g, np.float64)
+        sigma_t = np.ascontiguousarray(sigma_t, np.float64)
+        sigma = np.zeros(self.nd)
+        grad = np.zeros(self.nd)
+        J = C.c_double(0.0)
+        o = self._opts(tol, max_iter, 0, 8)
+        fi, ai = abi.SolveInfo(), abi.SolveInfo()
+        _check(self.lib.hbx_gradient_host(self._h, adjoint._h, abi.dptr(g), abi.dptr(sigma_t), abi.dptr(sigma),
+                                          abi.dptr(grad), C.byref(J), C.byref(o), C.byref(fi), C.byref(ai)),
+               "hbx_gradient_host")
+        return J.value, grad, sigma, self._info(fi), self._info(ai)

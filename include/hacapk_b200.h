@@ -118,7 +118,9 @@ typedef struct hbx_hmat hbx_hmat;
 typedef struct hbx_options {
   int precision;   /* HBX_FP64 (only value accepted by this ABI version) */
   int num_ctas;    /* persistent CTAs; 0 = one per SM                     */
-  int reserved[14];
+  int transpose;   /* 1: the engine holds H^T (adjoint products and solves;
+                      no counterpart in the reference)                    */
+  int reserved[13];
 } hbx_options;
 
 typedef struct hbx_info {
@@ -130,7 +132,8 @@ typedef struct hbx_info {
   long long zbu_len;       /* sum of kt over low-rank leaves                  */
   long long dense_words, lowrank_words;
   double setup_seconds;
-  int reserved[8];
+  int transposed;          /* 1 when the engine holds H^T                    */
+  int reserved[7];
 } hbx_info;
 
 typedef struct hbx_solve_opts {
@@ -188,6 +191,17 @@ int hbx_matvec(hbx_hmat *h, double alpha, const double *x, double beta,
  * word (hbx_sync). */
 int hbx_matvec_noalloc(hbx_hmat *h, double alpha, const double *x, double beta,
                        const double *yin, double *y, void *stream);
+
+/* Adjoint sensitivity of J(g) = 0.5 ||sigma - sigma_t||^2 where H sigma = g
+ * (no counterpart in the reference): solves H sigma = g with `h`, then
+ * H^T lambda = sigma - sigma_t with `ht` (an engine created with
+ * hbx_options.transpose = 1 on the same leaf list), and returns
+ * grad = dJ/dg = lambda.  Host vectors of nd doubles; sigma and grad are
+ * written (their contents on entry are ignored: both solves start from 0).
+ * `fwd` / `adj` (optional) receive the two solves' statistics. */
+int hbx_gradient_host(hbx_hmat *h, hbx_hmat *ht, const double *g, const double *sigma_t, double *sigma,
+                      double *grad, double *J, const hbx_solve_opts *opts, hbx_solve_info *fwd,
+                      hbx_solve_info *adj);
 
 /* Waits for `stream` and returns the device error latched by earlier async
  * calls on this engine (HBX_ERR_TIMEOUT when a bounded device wait expired),

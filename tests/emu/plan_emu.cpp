@@ -156,3 +156,15 @@ extern "C" int emu_matvec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, c
   }
   return 0;
 }
+
+// The same walk over the packed layout of H^T (hbx_plan.cpp:transpose_leaves).
+extern "C" int emu_matvec_transposed(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, const double *x, double *y,
+                                     long long *stats, char *msg, int msglen) {
+  TransposedLeaves tl;
+  std::string err;
+  if (transpose_leaves(st, nd, tl, err) != 0) {
+    std::snprintf(msg, msglen, "transpose_leaves: %s", err.c_str());
+    return 1;
+  }
+  return emu_matvec(&tl.container, nd, num_ctas, x, y, stats, msg, msglen);
+}

@@ -23,15 +23,17 @@ def emu(build_libs):
     lib = C.CDLL(EMU_LIB)
     lib.emu_matvec.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                C.POINTER(C.c_longlong), C.c_char_p, C.c_int]
+    lib.emu_matvec_transposed.argtypes = lib.emu_matvec.argtypes
     return lib
 
 
-def run_emu(lib, st_ptr, nd, nc, x):
+def run_emu(lib, st_ptr, nd, nc, x, transposed=False):
     y = np.zeros(nd)
     stats = (C.c_longlong * 8)()
     msg = C.create_string_buffer(512)
-    rc = lib.emu_matvec(st_ptr, nd, nc, x.ctypes.data_as(C.POINTER(C.c_double)),
-                        y.ctypes.data_as(C.POINTER(C.c_double)), stats, msg, 512)
+    fn = lib.emu_matvec_transposed if transposed else lib.emu_matvec
+    rc = fn(st_ptr, nd, nc, x.ctypes.data_as(C.POINTER(C.c_double)), y.ctypes.data_as(C.POINTER(C.c_double)),
+            stats, msg, 512)
     return rc, msg.value.decode(), y, list(stats)
 
 
@@ -148,3 +150,36 @@ def test_malformed_leaves_are_rejected(emu):
         P, keep = _custom(leaves, 100)
         rc, msg, _, _ = run_emu(emu, C.cast(C.pointer(P), C.c_void_p), 100, 4, np.ones(100))
         assert rc != 0 and "make_plan" in msg
+
+
+@pytest.mark.parametrize("level,nc", [(3, 148), (4, 148), (3, 5)])
+def test_transposed_layout_reproduces_oracle_transpose(emu, level, nc):
+    """H^T packed from the transposed leaf list (hbx_plan.cpp:transpose_leaves)
+    against the oracle's transposed product; same bytes as H."""
+    import oracle
+    H = sphere(level)
+    x = np.random.default_rng(level + 40).standard_normal(H.nd)
+    rc, msg, y, stats = run_emu(emu, C.cast(H.st, C.c_void_p), H.nd, nc, x, transposed=True)
+    assert rc == 0, msg
+    ref = oracle.matvec_t(H.st, x)
+    assert np.abs(y - ref).max() <= 1e-14 * np.abs(ref).max()
+    d, lr = H.storage_words()
+    assert stats[6] == 8 * (d + lr) + stats[7]
+
+
+def test_transposed_edge_cases(emu):
+    rng = np.random.default_rng(19)
+    nd = 100
+    leaves = [
+        (2, 0, 1, 40, 1, 100, rng.standard_normal(40 * 100)),
+        (1, 0, 41, 30, 1, 50, np.zeros(0)),
+        (1, 3, 41, 30, 51, 50, rng.standard_normal(3 * (30 + 50))),
+        (1, 70, 71, 30, 1, 100, rng.standard_normal(70 * 130)),
+        (2, 0, 41, 30, 1, 50, rng.standard_normal(30 * 50)),
+    ]
+    P, keep = _custom(leaves, nd)
+    x = rng.standard_normal(nd)
+    rc, msg, y, _ = run_emu(emu, C.cast(C.pointer(P), C.c_void_p), nd, 7, x, transposed=True)
+    assert rc == 0, msg
+    ref = _dense_of(leaves, nd).T @ x
+    assert np.abs(y - ref).max() <= 1e-13 * np.abs(ref).max()
