@@ -61,6 +61,8 @@ void free_engine(hbx_hmat *h) {
   cudaFree(h->d_dot);
   cudaFree(h->d_state);
   cudaFree(h->d_hist);
+  cudaFree(h->d_refine);
+  cudaFree(h->d_f32);
   if (h->h_pin) cudaFreeHost(h->h_pin);
   if (h->h_state) cudaFreeHost(h->h_state);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -98,6 +100,10 @@ hbx::MatvecArgs matvec_args(hbx_hmat *h, double alpha, const double *x, double b
   a.yin = yin;
   a.y = y;
   a.zbu = h->d_zbu;
+  if (h->d_f32) {
+    a.x32 = h->d_f32;
+    a.zbu32 = h->d_f32 + 3 * (size_t)h->plan.nd;
+  }
   a.alpha = alpha;
   a.beta = beta;
   a.gbar = h->d_gbar;
@@ -105,6 +111,15 @@ hbx::MatvecArgs matvec_args(hbx_hmat *h, double alpha, const double *x, double b
   a.timeout_ns = h->timeout_ns;
   a.prof = h->d_prof;
   return a;
+}
+
+// One H-matvec launch; an FP32 engine first rounds x into its float copy.
+cudaError_t mv_launch(hbx_hmat *h, const hbx::MatvecArgs &a, cudaStream_t s) {
+  if (h->plan.precision == hbx::kFP32) {
+    cudaError_t e = hbx::launch_to_float(a.x, h->d_f32, (size_t)h->plan.nd, s);
+    if (e != cudaSuccess) return e;
+  }
+  return hbx::launch_matvec(a, h->num_ctas, s, h->plan.precision);
 }
 
 int ensure_host_staging(hbx_hmat *h) {
@@ -160,7 +175,8 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hb
   *out = nullptr;
   if (!st) return fail(HBX_ERR_INVALID, "hbx_create: container is NULL");
   if (nd <= 0) return fail(HBX_ERR_INVALID, "hbx_create: nd <= 0");
-  if (opt && opt->precision != HBX_FP64) return fail(HBX_ERR_UNSUPPORTED, "hbx_create: only HBX_FP64 is supported");
+  if (opt && opt->precision != HBX_FP64 && opt->precision != HBX_FP32)
+    return fail(HBX_ERR_UNSUPPORTED, "hbx_create: precision must be HBX_FP64 or HBX_FP32");
   const double t0 = now_s();
   hbx_hmat *h = new (std::nothrow) hbx_hmat();
   if (!h) return fail(HBX_ERR_NOMEM, "hbx_create: host allocation");
@@ -195,7 +211,7 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hb
     st = &tleaves.container;
     h->transposed = 1;
   }
-  int st_plan = hbx::make_plan(st, nd, nc, h->plan, err);
+  int st_plan = hbx::make_plan(st, nd, nc, h->plan, err, (opt && opt->precision == HBX_FP32) ? hbx::kFP32 : hbx::kFP64);
   if (st_plan != HBX_OK) return bail(fail(st_plan, "hbx_create: " + err));
   const hbx::Plan &P = h->plan;
 
@@ -221,6 +237,9 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hb
     return bail(cuda_fail(e, "cudaMalloc(atoms)"));
   if ((e = cudaMalloc(&h->d_zbu, std::max<uint64_t>(1, P.zbu_len) * sizeof(double))) != cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(zbu)"));
+  if (P.precision == hbx::kFP32 &&
+      (e = cudaMalloc(&h->d_f32, (3 * (size_t)nd + std::max<uint64_t>(1, P.zbu_len)) * sizeof(float))) != cudaSuccess)
+    return bail(cuda_fail(e, "cudaMalloc(float copies)"));
   if ((e = cudaMalloc(&h->d_gbar, 4 * sizeof(unsigned))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(gbar)"));
   if ((e = cudaMalloc(&h->d_err, sizeof(int))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(err)"));
   if ((e = cudaMemcpy(h->d_stream, host.data(), P.total_bytes, cudaMemcpyHostToDevice)) != cudaSuccess)
@@ -277,7 +296,7 @@ int hbx_get_info(const hbx_hmat *h, hbx_info *info) {
   info->num_ctas = h->num_ctas;
   info->num_atoms = (int)P.atoms.size();
   info->num_runs = (int)h->num_runs;
-  info->precision = HBX_FP64;
+  info->precision = P.precision == hbx::kFP32 ? HBX_FP32 : HBX_FP64;
   uint64_t sb = 0;
   for (const auto &c : P.ctas) sb += c.stream_bytes;
   info->stream_bytes = (long long)sb;
@@ -294,7 +313,7 @@ int hbx_get_info(const hbx_hmat *h, hbx_info *info) {
 int hbx_matvec(hbx_hmat *h, double alpha, const double *x, double beta, const double *yin, double *y, void *stream) {
   if (!h || !x || !y) return fail(HBX_ERR_INVALID, "hbx_matvec: NULL argument");
   if (beta != 0.0 && !yin) return fail(HBX_ERR_INVALID, "hbx_matvec: beta != 0 needs yin");
-  cudaError_t e = hbx::launch_matvec(matvec_args(h, alpha, x, beta, yin, y), h->num_ctas, (cudaStream_t)stream);
+  cudaError_t e = mv_launch(h, matvec_args(h, alpha, x, beta, yin, y), (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(e, "hbx_matvec launch");
   return HBX_OK;
 }
@@ -315,6 +334,8 @@ int hbx_matvec_noalloc(hbx_hmat *h, double alpha, const double *x, double beta, 
                        void *stream) {
   if (!h || !x || !y) return fail(HBX_ERR_INVALID, "hbx_matvec_noalloc: NULL argument");
   if (beta != 0.0 && !yin) return fail(HBX_ERR_INVALID, "hbx_matvec_noalloc: beta != 0 needs yin");
+  if (h->plan.precision != hbx::kFP64)
+    return fail(HBX_ERR_UNSUPPORTED, "hbx_matvec_noalloc: FP64 engines only (use hbx_matvec)");
   if (h->plan.zbu_len > hbx::kNoallocZbuMax)
     return fail(HBX_ERR_INVALID, "hbx_matvec_noalloc: the matrix needs " + std::to_string(h->plan.zbu_len) +
                                      " zbu doubles; the static scratch holds " +
@@ -342,7 +363,7 @@ int hbx_matvec_noalloc(hbx_hmat *h, double alpha, const double *x, double beta, 
   a.gbar = reinterpret_cast<unsigned *>(base);
   a.zbu = reinterpret_cast<double *>(reinterpret_cast<char *>(base) + hbx::kNoallocCtlBytes);
   a.prof = nullptr;
-  e = hbx::launch_matvec(a, h->num_ctas, s);
+  e = hbx::launch_matvec(a, h->num_ctas, s, h->plan.precision);
   if (e != cudaSuccess) return cuda_fail(e, "hbx_matvec_noalloc launch");
   return HBX_OK;
 }
@@ -365,7 +386,7 @@ int hbx_matvec_host(hbx_hmat *h, const double *zu, double *zau, int accumulate, 
   HBX_CUDA(cudaMemcpyAsync(h->d_x, zu, bytes, cudaMemcpyHostToDevice, s));
   if (accumulate) HBX_CUDA(cudaMemcpyAsync(h->d_y, zau, bytes, cudaMemcpyHostToDevice, s));
   HBX_CUDA(cudaEventRecord(h->ev0, s));
-  HBX_CUDA(hbx::launch_matvec(matvec_args(h, 1.0, h->d_x, accumulate ? 1.0 : 0.0, h->d_y, h->d_y), h->num_ctas, s));
+  HBX_CUDA(mv_launch(h, matvec_args(h, 1.0, h->d_x, accumulate ? 1.0 : 0.0, h->d_y, h->d_y), s));
   HBX_CUDA(cudaEventRecord(h->ev1, s));
   HBX_CUDA(cudaMemcpyAsync(zau, h->d_y, bytes, cudaMemcpyDeviceToHost, s));
   HBX_CUDA(cudaStreamSynchronize(s));
@@ -396,6 +417,11 @@ static hbx::BicgArgs bicg_args(hbx_hmat *h, const double *b, double *u, double t
   a.ap = h->d_work + 3 * n;
   a.t = h->d_work + 4 * n;
   a.at = h->d_work + 5 * n;
+  if (h->d_f32) {
+    a.p32 = h->d_f32 + n;
+    a.t32 = h->d_f32 + 2 * n;
+    a.zbu32 = h->d_f32 + 3 * n;
+  }
   a.part = h->d_part;
   a.state = h->d_state;
   a.hist = h->d_hist;
@@ -419,7 +445,7 @@ static int get_graph(hbx_hmat *h, const hbx::BicgArgs &a, int batch) {
   cudaGraph_t g = nullptr;
   cudaStream_t s = h->stream;
   if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return HBX_ERR_CUDA;
-  for (int i = 0; i < batch; ++i) hbx::launch_bicg_iter(a, h->num_ctas, s);
+  for (int i = 0; i < batch; ++i) hbx::launch_bicg_iter(a, h->num_ctas, s, h->plan.precision);
   cudaError_t e = cudaStreamEndCapture(s, &g);
   if (e != cudaSuccess || !g) {
     cudaGetLastError();
@@ -450,7 +476,7 @@ static int bicgstab_dev(hbx_hmat *h, const double *b, double *u, const hbx_solve
   const hbx::BicgArgs a = bicg_args(h, b, u, tol, max_iter);
   HBX_CUDA(cudaEventRecord(h->ev0, s));
   // r = b - H u  (HACApK_SOLVER.c:562-573)
-  HBX_CUDA(hbx::launch_matvec(matvec_args(h, -1.0, u, 1.0, b, a.r), h->num_ctas, s));
+  HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, a.r), s));
   HBX_CUDA(hbx::launch_bicg_setup(a, h->num_ctas, s));
   const bool use_graph = get_graph(h, a, batch) == HBX_OK;
   int launched = 0;
@@ -460,7 +486,7 @@ static int bicgstab_dev(hbx_hmat *h, const double *b, double *u, const hbx_solve
     if (use_graph) {
       HBX_CUDA(cudaGraphLaunch(h->graph, s));
     } else {
-      for (int i = 0; i < batch; ++i) HBX_CUDA(hbx::launch_bicg_iter(a, h->num_ctas, s));
+      for (int i = 0; i < batch; ++i) HBX_CUDA(hbx::launch_bicg_iter(a, h->num_ctas, s, h->plan.precision));
     }
     HBX_CUDA(cudaEventRecord(h->ev4, s));
     launched += batch;
@@ -477,7 +503,7 @@ static int bicgstab_dev(hbx_hmat *h, const double *b, double *u, const hbx_solve
   HBX_CUDA(cudaEventRecord(h->ev1, s));
   const hbx::BicgState S = *h->h_state;
   // true residual ||b - H u|| (HACApK_SOLVER.c:737-746)
-  HBX_CUDA(hbx::launch_matvec(matvec_args(h, -1.0, u, 1.0, b, a.t), h->num_ctas, s));
+  HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, a.t), s));
   HBX_CUDA(hbx::launch_dot(a, a.t, a.t, hbx::kSlotAux, h->d_dot, h->num_ctas, s));
   double tr2 = 0.0;
   HBX_CUDA(cudaMemcpyAsync(&tr2, h->d_dot, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -540,6 +566,114 @@ int hbx_bicgstab_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_o
   cudaError_t e = cudaMemcpyAsync(u, du, bytes, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "hbx_bicgstab_host copy-out");
+  return st;
+}
+
+// Mixed-precision solve: FP64 residuals on `h`, inner BiCGSTAB on `hl`, all
+// on hl's stream.  The inner solve's target is relative to the current
+// residual; the last one is asked for no more than the outer tolerance needs.
+static int refined_dev(hbx_hmat *h, hbx_hmat *hl, const double *b, double *u, const hbx_solve_opts *opts,
+                       hbx_solve_info *info) {
+  const double tol = opts ? opts->tol : 1e-8;
+  const int max_iter = opts ? opts->max_iter : 1000;
+  const double floor_tol = (opts && opts->inner_tol > 0.0) ? opts->inner_tol : 1e-6;
+  if (max_iter < 0 || !(tol >= 0.0)) return fail(HBX_ERR_INVALID, "hbx_bicgstab_refined: bad tol or max_iter");
+  int st = ensure_solver(hl, max_iter);
+  if (st != HBX_OK) return st;
+  const size_t n = (size_t)h->plan.nd;
+  if (!hl->d_refine) HBX_CUDA(cudaMalloc(&hl->d_refine, 2 * n * sizeof(double)));
+  double *r = hl->d_refine, *d = hl->d_refine + n;
+  cudaStream_t s = hl->stream;
+  const hbx::BicgArgs a = bicg_args(hl, b, u, tol, max_iter);
+  auto dot = [&](const double *x, const double *y, double &out) -> int {
+    HBX_CUDA(hbx::launch_dot(a, x, y, hbx::kSlotAux, hl->d_dot, hl->num_ctas, s));
+    HBX_CUDA(cudaMemcpyAsync(&out, hl->d_dot, sizeof(double), cudaMemcpyDeviceToHost, s));
+    HBX_CUDA(cudaStreamSynchronize(s));
+    return HBX_OK;
+  };
+  cudaEvent_t e0 = h->ev0, e1 = h->ev1;
+  HBX_CUDA(cudaEventRecord(e0, s));
+  double bb = 0.0;
+  if ((st = dot(b, b, bb)) != HBX_OK) return st;
+  const double bnorm = std::sqrt(bb);
+  int inner_total = 0, outer = 0, launches = 1, status = HBX_ERR_NOT_CONVERGED;
+  double relres = 1.0, iter_s = 0.0;
+  for (;;) {
+    HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, r), s));
+    double rr = 0.0;
+    if ((st = dot(r, r, rr)) != HBX_OK) return st;
+    launches += 3;
+    relres = bnorm > 0.0 ? std::sqrt(rr) / bnorm : std::sqrt(rr);
+    if (!std::isfinite(relres)) { status = HBX_ERR_BREAKDOWN; break; }
+    if (relres < tol) { status = HBX_OK; break; }
+    if (inner_total >= max_iter || outer >= 64) break;
+    HBX_CUDA(cudaMemsetAsync(d, 0, n * sizeof(double), s));
+    hbx_solve_opts io{};
+    io.tol = std::max(floor_tol, 0.5 * tol / relres);
+    io.max_iter = max_iter - inner_total;
+    io.batch = opts ? opts->batch : 0;
+    hbx_solve_info ii{};
+    int ist = bicgstab_dev(hl, r, d, &io, &ii);
+    inner_total += ii.iterations;
+    iter_s += ii.iter_kernel_seconds;
+    launches += ii.launches;
+    ++outer;
+    if (ist != HBX_OK && ist != HBX_ERR_NOT_CONVERGED && ist != HBX_ERR_BREAKDOWN) return ist;
+    if (ii.iterations == 0 && ist != HBX_OK) { status = ist; break; }
+    HBX_CUDA(hbx::launch_axpy(1.0, d, u, n, s));
+    ++launches;
+  }
+  HBX_CUDA(cudaEventRecord(e1, s));
+  HBX_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  if (info) {
+    std::memset(info, 0, sizeof(*info));
+    info->iterations = inner_total;
+    info->outer = outer;
+    info->status = status;
+    info->bnorm = bnorm;
+    info->relres = relres;
+    info->true_relres = relres;
+    info->seconds = ms * 1e-3;
+    info->iter_kernel_seconds = iter_s;
+    info->launches = launches;
+  }
+  if (status != HBX_OK) return fail(status, std::string("hbx_bicgstab_refined: ") + hbx_status_string(status));
+  return check_device_error(hl, s);
+}
+
+int hbx_bicgstab_refined(hbx_hmat *h, hbx_hmat *hl, const double *b, double *u, const hbx_solve_opts *opts,
+                         hbx_solve_info *info, void *stream) {
+  if (!h || !hl || !b || !u) return fail(HBX_ERR_INVALID, "hbx_bicgstab_refined: NULL argument");
+  if (h->plan.nd != hl->plan.nd || h->transposed != hl->transposed || h->device != hl->device)
+    return fail(HBX_ERR_INVALID, "hbx_bicgstab_refined: h and hl must hold the same operator on one device");
+  cudaStream_t us = (cudaStream_t)stream;
+  HBX_CUDA(cudaEventRecord(hl->ev2, us));
+  HBX_CUDA(cudaStreamWaitEvent(hl->stream, hl->ev2, 0));
+  int st = refined_dev(h, hl, b, u, opts, info);
+  cudaEventRecord(hl->ev2, hl->stream);
+  cudaStreamWaitEvent(us, hl->ev2, 0);
+  return st;
+}
+
+int hbx_bicgstab_refined_host(hbx_hmat *h, hbx_hmat *hl, const double *b, double *u, const hbx_solve_opts *opts,
+                              hbx_solve_info *info) {
+  if (!h || !hl || !b || !u) return fail(HBX_ERR_INVALID, "hbx_bicgstab_refined_host: NULL argument");
+  if (h->plan.nd != hl->plan.nd || h->transposed != hl->transposed || h->device != hl->device)
+    return fail(HBX_ERR_INVALID, "hbx_bicgstab_refined: h and hl must hold the same operator on one device");
+  const int max_iter = opts ? opts->max_iter : 1000;
+  int st = ensure_solver(hl, max_iter < 0 ? 0 : max_iter);
+  if (st != HBX_OK) return st;
+  const size_t n = (size_t)hl->plan.nd, bytes = n * sizeof(double);
+  double *db = hl->d_work + 6 * n, *du = hl->d_work + 7 * n;
+  cudaStream_t s = hl->stream;
+  HBX_CUDA(cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, s));
+  HBX_CUDA(cudaMemcpyAsync(du, u, bytes, cudaMemcpyHostToDevice, s));
+  st = refined_dev(h, hl, db, du, opts, info);
+  cudaError_t e = cudaMemcpyAsync(u, du, bytes, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "hbx_bicgstab_refined_host copy-out");
   return st;
 }
 

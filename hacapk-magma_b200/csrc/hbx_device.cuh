@@ -58,8 +58,8 @@ struct SharedLayout {
   static constexpr uint32_t empty = full + 8 * kRingChunks;
   static constexpr uint32_t red = empty + 8 * kRingChunks;            // [2*kGroup][NW][64] double
   static constexpr uint32_t scal = red + 2 * kGroup * kConsumerWarps * 64 * 8;  // 64 doubles of scratch
-  static constexpr uint32_t stage = scal + 64 * 8;                     // [kStages][kStageCap] double
-  static constexpr uint32_t rec = stage + kStages * kStageCap * 8;     // [kRecSlots] run records
+  static constexpr uint32_t stage = scal + 64 * 8;                     // [kStages][kStageBytes]
+  static constexpr uint32_t rec = stage + kStages * kStageBytes;       // [kRecSlots] run records
   static constexpr uint32_t rfull = rec + kRecSlots * kRecBytes;       // [kRecSlots] record landed
   static constexpr uint32_t hdr = rfull + 8 * kRecSlots;               // [kStages] Run
   static constexpr uint32_t sfull = hdr + kStages * 32;                // stage filled (gather warp)
@@ -164,6 +164,9 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes
 
 // Ampere-style asynchronous gathers into shared memory (vector staging).
 // 8-byte copies go through L1 (.ca); 16-byte copies bypass it (.cg).
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async8(void *dst, const void *src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
@@ -353,14 +356,30 @@ __device__ __forceinline__ double warp_sum(double v) {
 struct GatherCtx {
   const RunRec *recs;
   uint32_t nr_p, nr_d, nr_u, npass;
-  const double *x0, *x1;  // x of pass 0 and pass 1
-  const double *zbu;
+  const void *x0, *x1;  // x of pass 0 and pass 1 (float copies for FP32 engines)
+  const void *zbu;       // zbu (float copy for FP32 engines)
   unsigned *gbar;
   int *err;
   uint64_t timeout_ns;
 };
 
-template <class SM>
+// Staging copies with cp.async: doubles for FP64 engines, the float copies
+// of the vectors for FP32 engines.
+template <bool kF32>
+__device__ __forceinline__ void stage_elems(uint8_t *st, uint32_t dst, const void *src, uint32_t e0, uint32_t len,
+                                            uint32_t step) {
+  if (kF32) {
+    float *sf = reinterpret_cast<float *>(st) + dst;
+    const float *s = reinterpret_cast<const float *>(src);
+    for (uint32_t e = e0; e < len; e += step) cp_async4(sf + e, s + e);
+  } else {
+    double *sd = reinterpret_cast<double *>(st) + dst;
+    const double *s = reinterpret_cast<const double *>(src);
+    for (uint32_t e = e0; e < len; e += step) cp_async8(sd + e, s + e);
+  }
+}
+
+template <bool kF32, class SM>
 __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm) {
   const int lane = threadIdx.x & 31;
   const uint32_t nruns = c.nr_p + c.nr_d + c.nr_u, total = nruns * c.npass;
@@ -409,11 +428,13 @@ __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm) {
       break;
     }
     if (lane < 2) reinterpret_cast<uint4 *>(sm.hdr + slot)[lane] = cur;
-    const uint32_t w2 = __shfl_sync(0xffffffffu, cur.z, 0);  // nrow | npair << 16
+    const uint32_t w2 = __shfl_sync(0xffffffffu, cur.z, 0);  // nrow | npanel << 16
     const uint32_t w3 = __shfl_sync(0xffffffffu, cur.w, 0);  // flags | rot << 16
-    const uint32_t nseg = __shfl_sync(0xffffffffu, cur.x, 1) & 0xffffu;
-    const double *vec = (w3 & 0xffu) == kRunU ? c.zbu : ((pass & 1) ? c.x1 : c.x0);
-    double *st = sm.stage + slot * kStageCap;
+    const uint32_t w4 = __shfl_sync(0xffffffffu, cur.x, 1);  // nseg | vlen << 16
+    const uint32_t nseg = w4 & 0xffffu, vlen = w4 >> 16;
+    const void *vec = (w3 & 0xffu) == kRunU ? c.zbu : ((pass & 1) ? c.x1 : c.x0);
+    const uint32_t esz = kF32 ? 4u : 8u;
+    uint8_t *st = sm.stage + slot * kStageBytes;
     const uint32_t nlong = __shfl_sync(0xffffffffu, cur.w, 1);
     // long segments: the whole warp copies each one (segment s sits in lane
     // 2 + s/2 of the record, fields (x, y) for even s and (z, w) for odd s)
@@ -422,7 +443,7 @@ __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm) {
       const uint32_t src = __shfl_sync(0xffffffffu, (q & 1) ? cur.z : cur.x, holder);
       const uint32_t ld = __shfl_sync(0xffffffffu, (q & 1) ? cur.w : cur.y, holder);
       const uint32_t len = ld & 0xffffu, dst = ld >> 16;
-      for (uint32_t e = lane; e < len; e += 32) cp_async8(st + dst + e, vec + src + e);
+      stage_elems<kF32>(st, dst, static_cast<const uint8_t *>(vec) + (size_t)src * esz, (uint32_t)lane, len, 32);
     }
     // short segments: lane i copies segment nlong + i (and nlong + 32 + i)
     for (uint32_t base = nlong; base < nseg; base += 32) {
@@ -435,13 +456,18 @@ __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm) {
       if (q < nseg) {
         const uint32_t src = (q & 1) ? sz : sx, ld = (q & 1) ? sw : sy;
         const uint32_t len = ld & 0xffffu, dst = ld >> 16;
-        for (uint32_t e = 0; e < len; ++e) cp_async8(st + dst + e, vec + src + e);
+        stage_elems<kF32>(st, dst, static_cast<const uint8_t *>(vec) + (size_t)src * esz, 0, len, 1);
       }
     }
-    if ((w3 & kPadCol) && lane == 0) st[2u * (w2 >> 16) - 1u] = 0.0;
+    // the zero columns that fill the last panel
+    const uint32_t vend = (w2 >> 16) * (kF32 ? 4u : 2u);
+    for (uint32_t e = vlen + (uint32_t)lane; e < vend; e += 32) {
+      if (kF32) reinterpret_cast<float *>(st)[e] = 0.0f;
+      else reinterpret_cast<double *>(st)[e] = 0.0;
+    }
     cp_async_arrive(&sm.sfull[slot]);
     __syncwarp();
-    if (lane == 0) mbar_arrive(&sm.sfull[slot]);  // releases the header and pad stores
+    if (lane == 0) mbar_arrive(&sm.sfull[slot]);  // releases the header and the plain stores
   }
   // record copies still in flight (only after an error) must land before exit
   if (lane == 0)
@@ -449,97 +475,129 @@ __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm) {
   cp_async_wait_all();
 }
 
-// ---- one run of a block: acc(lane) += sum over the run's column pairs of
-// B(lane, c) v(c).  Pair panel j (16h bytes, row i at 16i) is read by warp
-// (rot + j) mod NW, kUnroll panels per iteration, so the 16 warps together
-// hold a window of NW*kUnroll panels of the ring; lanes >= h repeat row h-1
-// and their sums are never used.
+// ---- one run of a block: acc(lane) += sum over the run's panels of
+// B(lane, c) v(c).  Panel j (16h bytes, row i at 16i: two double columns or
+// four float columns) is read by warp (rot + j) mod NW, kUnroll panels per
+// iteration, so the 16 warps together hold a window of NW*kUnroll panels of
+// the ring; lanes >= h repeat row h-1 and their sums are never used.  FP32
+// panels are multiplied in float (four accumulators per row) and added to the
+// row's double accumulator at the end of the run.
 #ifndef HBX_UNROLL
 #define HBX_UNROLL 4
 #endif
 constexpr uint32_t kUnroll = HBX_UNROLL;
 
+__device__ __forceinline__ float4 lds_f32x4(uint32_t addr) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(addr));
+  return v;
+}
+
+// Per-precision panel arithmetic: load a 16-byte stage group / panel row and
+// multiply-accumulate it.
+template <bool kF32>
+struct PanelMath;
+template <>
+struct PanelMath<false> {
+  using V = double2;
+  struct Acc {
+    double a0 = 0.0, a1 = 0.0;
+    __device__ __forceinline__ double sum() const { return a0 + a1; }
+  };
+  static __device__ __forceinline__ V ld(uint32_t addr) { return lds_f64x2(addr); }
+  static __device__ __forceinline__ void fma(Acc &a, const V &m, const V &v) {
+    a.a0 = ::fma(m.x, v.x, a.a0);
+    a.a1 = ::fma(m.y, v.y, a.a1);
+  }
+};
+template <>
+struct PanelMath<true> {
+  using V = float4;
+  struct Acc {
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    __device__ __forceinline__ double sum() const { return ((double)a0 + (double)a1) + ((double)a2 + (double)a3); }
+  };
+  static __device__ __forceinline__ V ld(uint32_t addr) { return lds_f32x4(addr); }
+  static __device__ __forceinline__ void fma(Acc &a, const V &m, const V &v) {
+    a.a0 = fmaf(m.x, v.x, a.a0);
+    a.a1 = fmaf(m.y, v.y, a.a1);
+    a.a2 = fmaf(m.z, v.z, a.a2);
+    a.a3 = fmaf(m.w, v.w, a.a3);
+  }
+};
+
 // (18 warps of 576 threads leave 96 registers a thread: the two-row form
 // unrolls by 2 to stay within them.)
-template <bool kTwoRows>
+template <bool kTwoRows, bool kF32>
 __device__ __forceinline__ void run_block_rows(const Run &run, uint32_t stage_s, Ring &R, double &acc, double &acc2) {
+  using PM = PanelMath<kF32>;
+  using V = typename PM::V;
   constexpr uint32_t NW = kConsumerWarps, U = kTwoRows ? 2 : kUnroll;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t h = run.nrow, np = run.npair;
+  const uint32_t h = run.nrow, np = run.npanel;
   if (np == 0) return;
   const uint32_t pb = 16u * h;
   const uint32_t lrow = 16u * min((uint32_t)lane, h - 1u);
   const uint32_t lrow2 = 16u * min((uint32_t)lane + 32u, h - 1u) - lrow;  // second row, relative
   const uint32_t ring_s = smem_u32(R.buf);
   uint32_t j = (uint32_t)((w - (int)run.rot) & (int)(NW - 1));
-  double a[2 * U], b[kTwoRows ? 2 * U : 1];
-#pragma unroll
-  for (uint32_t u = 0; u < 2 * U; ++u) a[u] = 0.0;
-#pragma unroll
-  for (uint32_t u = 0; u < (kTwoRows ? 2 * U : 1); ++u) b[u] = 0.0;
+  typename PM::Acc a[U], b[kTwoRows ? U : 1];
   for (; j + (U - 1) * NW < np; j += U * NW) {
     const uint32_t p0 = run.pos + j * pb;
     R.ensure(p0, p0 + (U - 1) * NW * pb + pb);
-    double2 v[U], m[U], m2[kTwoRows ? U : 1];
+    V v[U], m[U], m2[kTwoRows ? U : 1];
 #pragma unroll
-    for (uint32_t u = 0; u < U; ++u) v[u] = lds_f64x2(stage_s + 16u * (j + u * NW));
+    for (uint32_t u = 0; u < U; ++u) v[u] = PM::ld(stage_s + 16u * (j + u * NW));
     const uint32_t pl = p0 + lrow;
     const uint32_t q = ring_off(R.base + (pl >> kChunkLog), pl);
     if (q + (U - 1) * NW * pb + (kTwoRows ? lrow2 : 0u) + 16u <= kRingBytes) {  // no wrap around the ring end
 #pragma unroll
       for (uint32_t u = 0; u < U; ++u) {
-        m[u] = lds_f64x2(ring_s + q + u * NW * pb);
-        if (kTwoRows) m2[u] = lds_f64x2(ring_s + q + u * NW * pb + lrow2);
+        m[u] = PM::ld(ring_s + q + u * NW * pb);
+        if (kTwoRows) m2[u] = PM::ld(ring_s + q + u * NW * pb + lrow2);
       }
     } else {
 #pragma unroll
       for (uint32_t u = 0; u < U; ++u) {
         const uint32_t pu = pl + u * NW * pb;
-        m[u] = lds_f64x2(ring_s + ring_off(R.base + (pu >> kChunkLog), pu));
-        if (kTwoRows) m2[u] = lds_f64x2(ring_s + ring_off(R.base + ((pu + lrow2) >> kChunkLog), pu + lrow2));
+        m[u] = PM::ld(ring_s + ring_off(R.base + (pu >> kChunkLog), pu));
+        if (kTwoRows) m2[u] = PM::ld(ring_s + ring_off(R.base + ((pu + lrow2) >> kChunkLog), pu + lrow2));
       }
     }
 #pragma unroll
     for (uint32_t u = 0; u < U; ++u) {
-      a[2 * u] = fma(m[u].x, v[u].x, a[2 * u]);
-      a[2 * u + 1] = fma(m[u].y, v[u].y, a[2 * u + 1]);
-      if (kTwoRows) {
-        b[2 * u] = fma(m2[u].x, v[u].x, b[2 * u]);
-        b[2 * u + 1] = fma(m2[u].y, v[u].y, b[2 * u + 1]);
-      }
+      PM::fma(a[u], m[u], v[u]);
+      if (kTwoRows) PM::fma(b[u], m2[u], v[u]);
     }
   }
   for (; j < np; j += NW) {
     const uint32_t p0 = run.pos + j * pb;
     R.ensure(p0, p0 + pb);
-    const double2 vv = lds_f64x2(stage_s + 16u * j);
+    const V vv = PM::ld(stage_s + 16u * j);
     const uint32_t pl = p0 + lrow;
-    const double2 mm = lds_f64x2(ring_s + ring_off(R.base + (pl >> kChunkLog), pl));
-    a[0] = fma(mm.x, vv.x, a[0]);
-    a[1] = fma(mm.y, vv.y, a[1]);
+    PM::fma(a[0], PM::ld(ring_s + ring_off(R.base + (pl >> kChunkLog), pl)), vv);
     if (kTwoRows) {
       const uint32_t p2 = pl + lrow2;
-      const double2 m2 = lds_f64x2(ring_s + ring_off(R.base + (p2 >> kChunkLog), p2));
-      b[0] = fma(m2.x, vv.x, b[0]);
-      b[1] = fma(m2.y, vv.y, b[1]);
+      PM::fma(b[0], PM::ld(ring_s + ring_off(R.base + (p2 >> kChunkLog), p2)), vv);
     }
   }
   double t = 0.0;
 #pragma unroll
-  for (uint32_t u = 0; u < 2 * U; ++u) t += a[u];
+  for (uint32_t u = 0; u < U; ++u) t += a[u].sum();
   acc += t;
   if (kTwoRows) {
     double t2 = 0.0;
 #pragma unroll
-    for (uint32_t u = 0; u < 2 * U; ++u) t2 += b[u];
+    for (uint32_t u = 0; u < U; ++u) t2 += b[u].sum();
     acc2 += t2;
   }
 }
 
 // acc: row `lane` of the block; acc2: row lane + 32 (P slabs taller than 32).
+template <bool kF32>
 __device__ __forceinline__ void run_block(const Run &run, uint32_t stage_s, Ring &R, double &acc, double &acc2) {
-  if (run.nrow > 32) run_block_rows<true>(run, stage_s, R, acc, acc2);
-  else run_block_rows<false>(run, stage_s, R, acc, acc2);
+  if (run.nrow > 32) run_block_rows<true, kF32>(run, stage_s, R, acc, acc2);
+  else run_block_rows<false, kF32>(run, stage_s, R, acc, acc2);
 }
 
 // ---- compensated (Dot2) accumulation ------------------------------------------

@@ -38,6 +38,8 @@ struct MatvecArgs {
   const double *yin;
   double *y;
   double *zbu;
+  const float *x32;  // FP32 engines: x rounded to float (gathered instead of x)
+  float *zbu32;      // FP32 engines: zbu rounded to float (gathered by the U runs)
   double alpha, beta;
   unsigned *gbar;
   int *err;
@@ -56,6 +58,7 @@ struct BicgArgs {
   unsigned long long timeout_ns;
   const double *b;
   double *u, *r, *rh, *p, *ap, *t, *at;
+  float *p32, *t32, *zbu32;  // FP32 engines: float copies of the matvec inputs
   double *part;   // [num_ctas][kSlots][2]
   BicgState *state;
   double *hist;   // relres per iteration (max_iter + 1 entries)
@@ -74,10 +77,12 @@ cudaError_t noalloc_scratch_address(void **ptr);
 // Kernel launchers (hbx_kernels.cu).
 size_t kernel_smem_bytes();
 cudaError_t configure_kernels();
-cudaError_t launch_matvec(const MatvecArgs &a, int num_ctas, cudaStream_t s);
+cudaError_t launch_matvec(const MatvecArgs &a, int num_ctas, cudaStream_t s, int precision);
 cudaError_t launch_bicg_setup(const BicgArgs &a, int num_ctas, cudaStream_t s);
-cudaError_t launch_bicg_iter(const BicgArgs &a, int num_ctas, cudaStream_t s);
+cudaError_t launch_bicg_iter(const BicgArgs &a, int num_ctas, cudaStream_t s, int precision);
 // part[.][slot] = sum over own rows of x.y; then out[0] = the total (one block).
+cudaError_t launch_axpy(double alpha, const double *x, double *y, size_t n, cudaStream_t s);
+cudaError_t launch_to_float(const double *x, float *y, size_t n, cudaStream_t s);
 cudaError_t launch_dot(const BicgArgs &a, const double *x, const double *y, int slot, double *out,
                        int num_ctas, cudaStream_t s);
 
@@ -111,6 +116,8 @@ struct hbx_hmat {
   hbx::BicgState *d_state = nullptr;
   hbx::BicgState *h_state = nullptr;  // pinned
   double *d_hist = nullptr;
+  double *d_refine = nullptr;     // mixed-precision solve: outer residual and correction (2*nd)
+  float *d_f32 = nullptr;         // FP32 engines: x, p, t (3*nd) and zbu (zbu_len) rounded to float
   int hist_cap = 0;
   // captured iteration batch
   cudaGraphExec_t graph = nullptr;

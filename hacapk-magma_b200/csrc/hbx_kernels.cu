@@ -31,7 +31,7 @@ struct Smem {
   double *red;    // [2*kGroup][NW][64]
   uint2 *binfo;   // [2*kGroup] (out, h | kind << 16) of the pending block ends
   double *scal;   // 64 doubles
-  double *stage;  // [kStages][kStageCap]
+  uint8_t *stage; // [kStages][kStageBytes]
   uint8_t *rec;   // [kRecSlots] run records
   uint64_t *rfull;
   Run *hdr;       // [kStages] headers of the staged runs
@@ -47,7 +47,7 @@ __device__ __forceinline__ Smem smem_layout(uint8_t *base) {
   s.empty = reinterpret_cast<uint64_t *>(base + SharedLayout::empty);
   s.red = reinterpret_cast<double *>(base + SharedLayout::red);
   s.scal = reinterpret_cast<double *>(base + SharedLayout::scal);
-  s.stage = reinterpret_cast<double *>(base + SharedLayout::stage);
+  s.stage = base + SharedLayout::stage;
   s.rec = base + SharedLayout::rec;
   s.rfull = reinterpret_cast<uint64_t *>(base + SharedLayout::rfull);
   s.hdr = reinterpret_cast<Run *>(base + SharedLayout::hdr);
@@ -94,7 +94,8 @@ struct BlockEnds {
 };
 
 __device__ __forceinline__ void flush_block_ends(BlockEnds &B, const Smem &sm, double alpha, double beta,
-                                                 const double *yin, double *y, double *zbu, const Ring &R) {
+                                                 const double *yin, double *y, double *zbu, float *zbu32,
+                                                 const Ring &R) {
   if (B.pend == 0) return;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   named_bar(2, kConsumerThreads);
@@ -111,6 +112,7 @@ __device__ __forceinline__ void flush_block_ends(BlockEnds &B, const Smem &sm, d
       const uint32_t r = bi.x + row;
       if (kind == kRunP) {
         zbu[r] = s;
+        if (zbu32) zbu32[r] = (float)s;
         continue;
       }
       if (kind == kRunD) {
@@ -130,7 +132,7 @@ __device__ __forceinline__ void flush_block_ends(BlockEnds &B, const Smem &sm, d
 // again, so no warp waits at a barrier while holding chunks others need.
 __device__ __forceinline__ void block_end(const Run &run, double &acc, double &acc2, BlockEnds &B, const Smem &sm,
                                           double alpha, double beta, const double *yin, double *y, double *zbu,
-                                          Ring &R) {
+                                          float *zbu32, Ring &R) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   R.release_below(R.base + (run_end(run) >> kChunkLog));
   const uint32_t b = B.nae % (2 * kGroup);
@@ -140,7 +142,7 @@ __device__ __forceinline__ void block_end(const Run &run, double &acc, double &a
   acc = 0.0;
   acc2 = 0.0;
   ++B.nae;
-  if (++B.pend == kGroup) flush_block_ends(B, sm, alpha, beta, yin, y, zbu, R);
+  if (++B.pend == kGroup) flush_block_ends(B, sm, alpha, beta, yin, y, zbu, zbu32, R);
 }
 
 // Consumer view of the stage ring: run g (counted over sections and passes)
@@ -165,8 +167,8 @@ __device__ __forceinline__ void run_section(uint32_t nruns, StageQ &Q, const Sme
       if ((threadIdx.x & 31) == 0) atomicOr(err, kErrPipeline);
     }
     Run run = sm.hdr[slot];
-    if (R.bad) run.npair = 0;  // after a timed-out wait: touch neither the stage nor the ring
-    rend = process(run, smem_u32(sm.stage + slot * kStageCap));
+    if (R.bad) run.npanel = 0;  // after a timed-out wait: touch neither the stage nor the ring
+    rend = process(run, smem_u32(sm.stage + slot * kStageBytes));
     __syncwarp();
     if ((threadIdx.x & 31) == 0) mbar_arrive(&sm.sempty[slot]);
   }
@@ -178,9 +180,10 @@ __device__ __forceinline__ void run_section(uint32_t nruns, StageQ &Q, const Sme
 // gather warp waits for the barrier before it stages the first U run, so the
 // D runs hide the barrier latency.  Every warp has released the whole pass
 // when it returns.
+template <bool kF32>
 __device__ __forceinline__ void matvec_body(Ring &R, StageQ &Q, uint32_t K, const CtaInfo &ci, double alpha,
-                                            double beta, const double *yin, double *y, double *zbu, unsigned *gbar,
-                                            int *err, const Smem &sm, BlockEnds &B,
+                                            double beta, const double *yin, double *y, double *zbu, float *zbu32,
+                                            unsigned *gbar, int *err, const Smem &sm, BlockEnds &B,
                                             unsigned long long *prof = nullptr) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   auto stamp = [&](int k) {
@@ -189,15 +192,15 @@ __device__ __forceinline__ void matvec_body(Ring &R, StageQ &Q, uint32_t K, cons
   stamp(0);
   double acc = 0.0, acc2 = 0.0;
   auto block = [&](const Run &run, uint32_t stage_s) {
-    run_block(run, stage_s, R, acc, acc2);
-    if (run.flags & kLast) block_end(run, acc, acc2, B, sm, alpha, beta, yin, y, zbu, R);
+    run_block<kF32>(run, stage_s, R, acc, acc2);
+    if (run.flags & kLast) block_end(run, acc, acc2, B, sm, alpha, beta, yin, y, zbu, zbu32, R);
     return run_end(run);
   };
   // ---- P: zbu = V^T x for this CTA's slabs
   uint32_t pend = 0;
   run_section(ci.nr_p, Q, sm, R, err, [&](const Run &run, uint32_t st) { return pend = block(run, st); });
   R.release_below(R.base + (pend >> kChunkLog));
-  flush_block_ends(B, sm, alpha, beta, yin, y, zbu, R);
+  flush_block_ends(B, sm, alpha, beta, yin, y, zbu, zbu32, R);
   stamp(1);
   if (lane == 0) __threadfence();
   named_bar(1, kConsumerThreads);
@@ -213,13 +216,13 @@ __device__ __forceinline__ void matvec_body(Ring &R, StageQ &Q, uint32_t K, cons
   uint32_t dend = pend;
   run_section(ci.nr_d, Q, sm, R, err, [&](const Run &run, uint32_t st) { return dend = block(run, st); });
   R.release_below(R.base + (dend >> kChunkLog));
-  flush_block_ends(B, sm, alpha, beta, yin, y, zbu, R);
+  flush_block_ends(B, sm, alpha, beta, yin, y, zbu, zbu32, R);
   stamp(3);
   stamp(4);
   // ---- U: U rows of the owned atoms times zbu (staged after the grid barrier)
   run_section(ci.nr_u, Q, sm, R, err, [&](const Run &run, uint32_t st) { return block(run, st); });
   R.release_below(R.base + K);
-  flush_block_ends(B, sm, alpha, beta, yin, y, zbu, R);
+  flush_block_ends(B, sm, alpha, beta, yin, y, zbu, zbu32, R);
   // The barrier counts arrivals per instance: this CTA may arrive on the
   // next instance only once this one is complete (a CTA without U runs has
   // not waited for it yet).
@@ -227,6 +230,7 @@ __device__ __forceinline__ void matvec_body(Ring &R, StageQ &Q, uint32_t K, cons
   stamp(5);
 }
 
+template <bool kF32>
 __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const Smem sm = smem_layout(smem_raw);
@@ -240,16 +244,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
     return;
   }
   if (w == kGatherWarp) {
-    const GatherCtx c{a.recs + ci.rec_begin, ci.nr_p, ci.nr_d, ci.nr_u, 1, a.x, a.x, a.zbu, a.gbar, a.err,
+    const void *xs = kF32 ? static_cast<const void *>(a.x32) : static_cast<const void *>(a.x);
+    const void *zs = kF32 ? static_cast<const void *>(a.zbu32) : static_cast<const void *>(a.zbu);
+    const GatherCtx c{a.recs + ci.rec_begin, ci.nr_p, ci.nr_d, ci.nr_u, 1, xs, xs, zs, a.gbar, a.err,
                       a.timeout_ns};
-    gather_warp(c, sm);
+    gather_warp<kF32>(c, sm);
     return;
   }
   if (threadIdx.x == 0) mbar_arrive(sm.xready);  // x is an input: ready from the start
   Ring R{sm.ring, sm.full, sm.empty, 0, 0, 0, a.timeout_ns, a.err, false};
   StageQ Q{0};
   BlockEnds B;
-  matvec_body(R, Q, K, ci, a.alpha, a.beta, a.yin, a.y, a.zbu, a.gbar, a.err, sm, B, a.prof);
+  matvec_body<kF32>(R, Q, K, ci, a.alpha, a.beta, a.yin, a.y, a.zbu, kF32 ? a.zbu32 : nullptr, a.gbar, a.err, sm, B,
+                    a.prof);
   R.drain(K);
 }
 
@@ -345,6 +352,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_setup(BicgArgs a) {
   }
 }
 
+template <bool kF32>
 __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const Smem sm = smem_layout(smem_raw);
@@ -428,9 +436,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     return;
   }
   if (w == kGatherWarp) {
-    const GatherCtx c{a.recs + ci.rec_begin, ci.nr_p, ci.nr_d, ci.nr_u, 2, a.p, a.t, a.zbu, a.gbar, a.err,
+    const void *x0 = kF32 ? static_cast<const void *>(a.p32) : static_cast<const void *>(a.p);
+    const void *x1 = kF32 ? static_cast<const void *>(a.t32) : static_cast<const void *>(a.t);
+    const void *zs = kF32 ? static_cast<const void *>(a.zbu32) : static_cast<const void *>(a.zbu);
+    const GatherCtx c{a.recs + ci.rec_begin, ci.nr_p, ci.nr_d, ci.nr_u, 2, x0, x1, zs, a.gbar, a.err,
                       a.timeout_ns};
-    gather_warp(c, sm);
+    gather_warp<kF32>(c, sm);
     return;
   }
   Ring R{sm.ring, sm.full, sm.empty, 0, 0, 0, a.timeout_ns, a.err, false};
@@ -439,11 +450,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
 
   // ---- S1: p = r + beta*(p - zeta*Ap)  (p = r on the first step)
   if (beta == 0.0) {
-    for_own_rows(a.atoms, ci, [&](uint32_t r) { a.p[r] = a.r[r]; });
+    for_own_rows(a.atoms, ci, [&](uint32_t r) {
+      const double v = a.r[r];
+      a.p[r] = v;
+      if (kF32) a.p32[r] = (float)v;
+    });
   } else {
     for_own_rows(a.atoms, ci, [&](uint32_t r) {
       const double v = fma(-zeta_prev, a.ap[r], a.p[r]) * beta;
-      a.p[r] = v + a.r[r];
+      const double pv = v + a.r[r];
+      a.p[r] = pv;
+      if (kF32) a.p32[r] = (float)pv;
     });
   }
   __threadfence();
@@ -460,7 +477,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
 
   // ---- S2: Ap = H p;  rh . Ap
-  matvec_body(R, Q, K, ci, 1.0, 0.0, nullptr, a.ap, a.zbu, a.gbar, a.err, sm, B);
+  matvec_body<kF32>(R, Q, K, ci, 1.0, 0.0, nullptr, a.ap, a.zbu, kF32 ? a.zbu32 : nullptr, a.gbar, a.err, sm, B);
   stamp(2);
   {
     Acc2 acc[1] = {{0, 0}};
@@ -478,7 +495,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   stamp(3);
 
   // ---- S3: t = r - alpha*Ap
-  for_own_rows(a.atoms, ci, [&](uint32_t r) { a.t[r] = fma(-alpha, a.ap[r], a.r[r]); });
+  for_own_rows(a.atoms, ci, [&](uint32_t r) {
+    const double v = fma(-alpha, a.ap[r], a.r[r]);
+    a.t[r] = v;
+    if (kF32) a.t32[r] = (float)v;
+  });
   __threadfence();
   grid_sync(a.gbar, a.err, a.timeout_ns, sm);
   if (threadIdx.x == 0) mbar_arrive(sm.xready);  // t complete grid-wide: pass 2 may be staged
@@ -486,7 +507,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
 
   // ---- S4: At = H t;  At . t,  At . At
   R.base = K;
-  matvec_body(R, Q, K, ci, 1.0, 0.0, nullptr, a.at, a.zbu, a.gbar, a.err, sm, B);
+  matvec_body<kF32>(R, Q, K, ci, 1.0, 0.0, nullptr, a.at, a.zbu, kF32 ? a.zbu32 : nullptr, a.gbar, a.err, sm, B);
   stamp(5);
   {
     Acc2 acc[2] = {{0, 0}, {0, 0}};
@@ -549,6 +570,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_dot_partial(BicgArgs a, const d
   cta_partials<1>(acc, a.part, slot, sm);
 }
 
+// y = (float)x: the input of an FP32 engine's matvec.
+__global__ void k_to_float(const double *x, float *y, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    y[i] = (float)x[i];
+}
+
+// y += a * x (the refinement update of the mixed-precision solve).
+__global__ void k_axpy(double a, const double *x, double *y, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    y[i] = fma(a, x[i], y[i]);
+}
+
 __global__ void k_dot_total(const double *part, int ncta, int slot, double *out) {
   const double v = reduce_slot(part, ncta, slot);
   if (threadIdx.x == 0) *out = v;
@@ -569,9 +602,11 @@ size_t kernel_smem_bytes() { return SharedLayout::bytes; }
 cudaError_t configure_kernels() {
   const int smem = (int)SharedLayout::bytes;
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_matvec, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_matvec<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_matvec<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_bicg_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(k_bicg_iter, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_bicg_iter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_bicg_iter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_dot_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
   return cudaSuccess;
 }
@@ -591,8 +626,8 @@ static cudaError_t launch_coop(void (*kern)(Args), const Args &a, int num_ctas, 
   return cudaLaunchKernelEx(&cfg, kern, a);
 }
 
-cudaError_t launch_matvec(const MatvecArgs &a, int num_ctas, cudaStream_t s) {
-  return launch_coop(k_matvec, a, num_ctas, s);
+cudaError_t launch_matvec(const MatvecArgs &a, int num_ctas, cudaStream_t s, int precision) {
+  return precision == kFP32 ? launch_coop(k_matvec<true>, a, num_ctas, s) : launch_coop(k_matvec<false>, a, num_ctas, s);
 }
 
 cudaError_t launch_bicg_setup(const BicgArgs &a, int num_ctas, cudaStream_t s) {
@@ -600,8 +635,19 @@ cudaError_t launch_bicg_setup(const BicgArgs &a, int num_ctas, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_bicg_iter(const BicgArgs &a, int num_ctas, cudaStream_t s) {
-  return launch_coop(k_bicg_iter, a, num_ctas, s);
+cudaError_t launch_bicg_iter(const BicgArgs &a, int num_ctas, cudaStream_t s, int precision) {
+  return precision == kFP32 ? launch_coop(k_bicg_iter<true>, a, num_ctas, s)
+                            : launch_coop(k_bicg_iter<false>, a, num_ctas, s);
+}
+
+cudaError_t launch_to_float(const double *x, float *y, size_t n, cudaStream_t s) {
+  k_to_float<<<296, 256, 0, s>>>(x, y, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_axpy(double alpha, const double *x, double *y, size_t n, cudaStream_t s) {
+  k_axpy<<<296, 256, 0, s>>>(alpha, x, y, n);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_dot(const BicgArgs &a, const double *x, const double *y, int slot, double *out, int num_ctas,

@@ -6,8 +6,9 @@
 // lda=roundup(M,32) (:541-811), this planner stacks the V factors of every
 // column cluster into P slabs, cuts the dense and U factors into row-atom
 // blocks, balances the blocks over the persistent CTAs by bytes (longest
-// processing time first), and packs every CTA's runs back to back as
-// column-pair panels (one zero column per odd-width block, nothing else).
+// processing time first), and packs every CTA's runs back to back as panels
+// of 16-byte rows (two double or four float columns; zero columns fill a
+// block's last panel, nothing else).
 #include "hbx_plan.h"
 
 #include <algorithm>
@@ -63,9 +64,9 @@ struct Bins {
   }
 };
 
-uint64_t block_cost(uint32_t h, uint32_t W) {
-  const uint64_t wp = W + (W & 1u);
-  return 8ull * h * wp + kBlockOverhead + kRunOverhead * (1 + wp / kStageCap);
+uint64_t block_cost(uint32_t h, uint32_t W, int prec) {
+  const uint64_t g = group_cols(prec), wp = (W + g - 1) / g * g;
+  return (uint64_t)elem_bytes(prec) * h * wp + kBlockOverhead + kRunOverhead * (1 + wp * elem_bytes(prec) / kStageBytes);
 }
 
 // Vector index of block column c (c < W): P -> x index, D -> x index, U -> zbu index.
@@ -117,8 +118,12 @@ uint32_t count_long(const std::vector<Seg> &segs) {
 
 }  // namespace
 
-int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, std::string &err) {
+int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, std::string &err, int precision) {
   plan = Plan();
+  if (precision != kFP64 && precision != kFP32) { err = "unknown storage precision"; return HBX_ERR_INVALID; }
+  plan.precision = precision;
+  const uint32_t G = group_cols(precision);
+  const uint32_t stage_cols = kStageBytes / elem_bytes(precision);
   if (!st || nd <= 0 || num_ctas <= 0) { err = "null container, nd <= 0 or no CTAs"; return HBX_ERR_INVALID; }
   const int nlf = st->nlf;
   if (nlf < 0 || (nlf > 0 && (!st->st_lf || st->st_lf_stride < (int)sizeof(stc_HACApK_leafmtx)))) {
@@ -275,7 +280,7 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
     }
     dblock[a] = (uint32_t)plan.blocks.size();
     plan.blocks.push_back(b);
-    acost[a] = block_cost(b.h, b.W);
+    acost[a] = block_cost(b.h, b.W, precision);
     if (ucnt[a + 1] > ucnt[a]) {
       // zbu order, so that the segments of one column group merge
       std::sort(uleaf.begin() + ucnt[a], uleaf.begin() + ucnt[a + 1],
@@ -289,7 +294,7 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
       }
       ublock[a] = (uint32_t)plan.blocks.size();
       plan.blocks.push_back(u);
-      acost[a] += block_cost(u.h, u.W);
+      acost[a] += block_cost(u.h, u.W, precision);
     }
   }
 
@@ -299,9 +304,10 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
   {
     std::vector<uint32_t> order(pblocks);
     std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
-      return block_cost(plan.blocks[x].h, plan.blocks[x].W) > block_cost(plan.blocks[y].h, plan.blocks[y].W);
+      return block_cost(plan.blocks[x].h, plan.blocks[x].W, precision) >
+             block_cost(plan.blocks[y].h, plan.blocks[y].W, precision);
     });
-    for (uint32_t b : order) cta_p[bins.take(block_cost(plan.blocks[b].h, plan.blocks[b].W))].push_back(b);
+    for (uint32_t b : order) cta_p[bins.take(block_cost(plan.blocks[b].h, plan.blocks[b].W, precision))].push_back(b);
     std::vector<int> aorder(natoms);
     std::iota(aorder.begin(), aorder.end(), 0);
     std::stable_sort(aorder.begin(), aorder.end(), [&](int x, int y) { return acost[x] > acost[y]; });
@@ -327,7 +333,7 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
     uint32_t rot = 0;
     auto emit_block = [&](uint32_t bi) -> uint32_t {
       const Block &b = plan.blocks[bi];
-      const uint32_t Wp = b.W + (b.W & 1u);
+      const uint32_t Wp = (b.W + G - 1) / G * G;
       ColumnMap M{plan, b, 0};
       uint32_t out = 0;
       if (b.kind == kRunP) {
@@ -339,10 +345,10 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
       }
       uint32_t nr = 0, col = 0;
       do {
-        uint32_t nc = std::min<uint32_t>(kStageCap, Wp - col);
+        uint32_t nc = std::min<uint32_t>(stage_cols, Wp - col);
         segments(M, col, std::min(col + nc, b.W), segs);
         while (segs.size() > (size_t)kRunSegs) {  // too many pieces: take fewer columns
-          nc = std::max<uint32_t>(2, (nc / 2) & ~1u);
+          nc = std::max<uint32_t>(G, (nc / 2) / G * G);
           segments(M, col, std::min(col + nc, b.W), segs);
         }
         RunRec rec{};
@@ -350,21 +356,20 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
         r.pos = (uint32_t)pos;
         r.out = out;
         r.nrow = b.h;
-        r.npair = (uint16_t)(nc / 2);
+        r.npanel = (uint16_t)(nc / G);
         const bool last = (col + nc == Wp);
-        r.flags = (uint16_t)(b.kind | (col == 0 ? kFirst : 0) | (last ? kLast : 0) |
-                             (last && (b.W & 1u) ? kPadCol : 0));
+        r.flags = (uint16_t)(b.kind | (col == 0 ? kFirst : 0) | (last ? kLast : 0));
         r.rot = (uint16_t)rot;
         r.nseg = (uint16_t)segs.size();
         r.nlong = count_long(segs);
-        r.vlen = (uint16_t)nc;
+        r.vlen = (uint16_t)(std::min(col + nc, b.W) - col);
         r.block = bi;
         r.col0 = col;
         std::copy(segs.begin(), segs.end(), rec.seg);
         plan.recs.push_back(rec);
-        if (r.flags & kPadCol) plan.pad_bytes += 8ull * b.h;
-        pos += 16ull * b.h * r.npair;
-        rot = (rot + r.npair) % kConsumerWarps;
+        plan.pad_bytes += (uint64_t)elem_bytes(precision) * b.h * (nc - r.vlen);
+        pos += 16ull * b.h * r.npanel;
+        rot = (rot + r.npanel) % kConsumerWarps;
         col += nc;
         ++nr;
       } while (col < Wp);
@@ -398,8 +403,16 @@ void pack_plan(const stc_HACApK_leafmtxp *st, const Plan &plan, uint8_t *dst) {
     for (uint32_t k = 0; k < nr; ++k) {
       const Run &r = plan.recs[info.rec_begin + k].hdr;
       const Block &b = plan.blocks[r.block];
-      const uint32_t h = r.nrow, ncol = 2u * r.npair;
+      const uint32_t h = r.nrow, G = group_cols(plan.precision), ncol = G * r.npanel;
+      const bool f32 = plan.precision == kFP32;
       double *d = reinterpret_cast<double *>(base + r.pos);
+      float *f = reinterpret_cast<float *>(base + r.pos);
+      // element (row i, run column cc): panel cc/G, row i, slot cc%G (16-byte rows)
+      auto put = [&](uint32_t i, uint32_t cc, double v) {
+        const size_t k = ((size_t)(cc / G) * h + i) * G + cc % G;
+        if (f32) f[k] = (float)v;
+        else d[k] = v;
+      };
       if (b.kind == kRunP) {
         // slab rows -> (leaf, rank); V_L(t, k) = a1[t + k*ndt]
         prow.clear();
@@ -415,7 +428,7 @@ void pack_plan(const stc_HACApK_leafmtxp *st, const Plan &plan, uint8_t *dst) {
           if (col >= b.W) continue;  // zero pad column
           for (uint32_t i = 0; i < h; ++i) {
             const stc_HACApK_leafmtx *s = leaf_at(st, (int)prow[i].first);
-            d[((size_t)(cc >> 1) * h + i) * 2 + (cc & 1)] = s->a1[(size_t)col + (size_t)prow[i].second * s->ndt];
+            put(i, cc, s->a1[(size_t)col + (size_t)prow[i].second * s->ndt]);
           }
         }
         continue;
@@ -439,7 +452,7 @@ void pack_plan(const stc_HACApK_leafmtxp *st, const Plan &plan, uint8_t *dst) {
           double v;
           if (b.kind == kRunD) v = s->a1[(size_t)lc + (size_t)(ro + (int)i) * s->ndt];  // A(il, it) = a1[it + il*ndt]
           else v = a2_of(s)[(size_t)(ro + (int)i) + (size_t)lc * s->ndl];              // U(i, l) = a2[i + l*ndl]
-          d[((size_t)(cc >> 1) * h + i) * 2 + (cc & 1)] = v;
+          put(i, cc, v);
         }
       }
     }

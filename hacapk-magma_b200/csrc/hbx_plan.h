@@ -21,12 +21,13 @@
 // (grid barrier) before any CTA reads zbu in its U blocks; the D blocks sit
 // between the two so that the barrier latency is hidden.
 //
-// A block is stored as W/2 column-pair panels, each h x 2 row-major: row i
-// of the pair (c, c+1) is the 16 bytes (B(i,c), B(i,c+1)).  One 16-byte
-// shared-memory load then gives a lane one row of two columns, and the 32
-// lanes of a warp read h*16 consecutive bytes, free of bank conflicts.  An
-// odd W gets one zero column.  A block's columns are cut into RUNS of at
-// most kStageCap columns (the vector stage buffer); all CTA data is one
+// A block is stored as panels of column groups, each h x G row-major with
+// 16-byte rows: G = 2 double columns (FP64 storage) or G = 4 float columns
+// (FP32 storage).  One 16-byte shared-memory load then gives a lane one row
+// of G columns, and the 32 lanes of a warp read h*16 consecutive bytes, free
+// of bank conflicts.  A block's last panel is filled with zero columns.  A
+// block's columns are cut into RUNS that fit the 8 KB vector stage buffer
+// (1024 doubles or 2048 floats); all CTA data is one
 // contiguous byte stream (P runs, then D runs, then U runs) that the kernel
 // moves into shared memory with 1D bulk copies, so every byte of H crosses
 // HBM once per matvec.
@@ -46,6 +47,12 @@
 
 namespace hbx {
 
+#ifdef __CUDACC__
+#define HBX_HD __host__ __device__
+#else
+#define HBX_HD
+#endif
+
 constexpr int kAtomMax = 32;       // rows per D/U block (one lane per row)
 constexpr int kSlabMax = 64;       // rows per P slab (two rows per lane)
 constexpr int kConsumerWarps = 16; // warps that compute (+ a producer and a descriptor warp)
@@ -58,7 +65,8 @@ constexpr int kConsumerWarps = 16; // warps that compute (+ a producer and a des
 constexpr int kChunkLog = HBX_CHUNK_LOG;      // ring chunk = 32 KB (bulk copies this size stream at HBM rate)
 constexpr int kChunkBytes = 1 << kChunkLog;
 constexpr int kRingChunks = HBX_RING_CHUNKS;  // 128 KB ring per CTA
-constexpr int kStageCap = 1024;    // doubles per vector stage buffer (x2); even
+constexpr int kStageBytes = 8192;  // one vector stage buffer: 1024 doubles or 2048 floats
+constexpr int kStageCap = kStageBytes / 8;  // doubles per stage buffer
 constexpr int kRunSegs = 60;       // gather segments per run record
 constexpr int kSegShort = 32;      // a segment this long or shorter is copied by one gather lane;
                                    // a longer one by the whole gather warp
@@ -69,7 +77,13 @@ constexpr int kRecBytes = 512;     // one run record: 32-byte header + kRunSegs 
 constexpr int kStages = HBX_STAGES;  // vector stage buffers: runs gathered ahead of the consumers
 
 enum RunKind : uint16_t { kRunP = 0, kRunD = 1, kRunU = 2 };
-enum RunFlags : uint16_t { kFirst = 0x100, kLast = 0x200, kPadCol = 0x400 };
+enum RunFlags : uint16_t { kFirst = 0x100, kLast = 0x200 };
+
+// Storage precision of the packed factors.  A panel row is always 16 bytes:
+// two double columns or four float columns.
+enum Precision : int { kFP64 = 0, kFP32 = 1 };
+HBX_HD inline uint32_t group_cols(int prec) { return prec == kFP32 ? 4u : 2u; }
+HBX_HD inline uint32_t elem_bytes(int prec) { return prec == kFP32 ? 4u : 8u; }
 
 // Gather segment: stage[dst + e] = vec[src + e], e < len (vec = x or zbu).
 struct Seg {
@@ -84,11 +98,11 @@ struct alignas(16) Run {
   uint32_t pos;    // byte offset of the run's pair panels in the CTA stream (16-aligned)
   uint32_t out;    // first output row: zbu index (P) or y row (D, U)
   uint16_t nrow;   // h: 1..32 for D/U, 1..64 for P
-  uint16_t npair;  // column pairs; 2*npair <= kStageCap
+  uint16_t npanel; // column-group panels (2 columns each for FP64, 4 for FP32)
   uint16_t flags;  // RunKind | RunFlags
-  uint16_t rot;    // consumer warp that takes pair 0
+  uint16_t rot;    // consumer warp that takes panel 0
   uint16_t nseg;   // gather segments (<= kRunSegs)
-  uint16_t vlen;   // doubles staged: 2*npair
+  uint16_t vlen;   // real columns; the stage is zero from vlen to the end of the last panel
   uint32_t block;  // block index (host-side packing and checks)
   uint32_t col0;   // first block column of the run
   uint32_t nlong;  // the first nlong segments are longer than kSegShort
@@ -101,14 +115,8 @@ struct alignas(16) RunRec {
 };
 static_assert(sizeof(RunRec) == kRecBytes, "RunRec must be kRecBytes");
 
-#ifdef __CUDACC__
-#define HBX_HD __host__ __device__
-#else
-#define HBX_HD
-#endif
-
 HBX_HD inline uint32_t run_kind(const Run &r) { return r.flags & 0xffu; }
-HBX_HD inline uint32_t run_bytes(const Run &r) { return 16u * r.nrow * r.npair; }
+HBX_HD inline uint32_t run_bytes(const Run &r) { return 16u * r.nrow * r.npanel; }
 
 struct CtaInfo {
   uint64_t stream_off;    // byte offset of the CTA stream in the packed buffer
@@ -142,6 +150,7 @@ struct Piece {
 struct Plan {
   int nd = 0, nlf = 0, nlfkt = 0, ktmax = 0;
   int num_ctas = 0;
+  int precision = kFP64;
   std::vector<Atom> atoms;          // in CTA order (atom_begin indexes this)
   std::vector<RunRec> recs;         // in CTA order
   std::vector<CtaInfo> ctas;
@@ -152,13 +161,14 @@ struct Plan {
   uint64_t total_bytes = 0;         // packed buffer size
   uint64_t zbu_len = 0;
   uint64_t dense_words = 0, lowrank_words = 0;
-  uint64_t pad_bytes = 0;           // zero columns added for odd widths
+  uint64_t pad_bytes = 0;           // zero columns that fill a block's last panel
   uint64_t alg_bytes = 0, alg_flops = 0;
 };
 
 // Validates the leaf list and builds the plan.  Returns HBX_OK or an error
 // (message in `err`).
-int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, std::string &err);
+int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, std::string &err,
+              int precision = kFP64);
 
 // Writes the packed stream of every CTA into `dst` (plan.total_bytes bytes).
 void pack_plan(const stc_HACApK_leafmtxp *st, const Plan &plan, uint8_t *dst);

@@ -72,14 +72,15 @@ class Info(C.Structure):
 
 class SolveOpts(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iter", C.c_int), ("verbose", C.c_int),
-                ("batch", C.c_int), ("reserved", C.c_int * 11)]
+                ("batch", C.c_int), ("reserved0", C.c_int), ("inner_tol", C.c_double),
+                ("reserved", C.c_int * 8)]
 
 
 class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("bnorm", C.c_double),
                 ("relres", C.c_double), ("true_relres", C.c_double), ("seconds", C.c_double),
                 ("iter_kernel_seconds", C.c_double), ("iter_launches", C.c_int),
-                ("launches", C.c_int), ("reserved", C.c_int * 6)]
+                ("launches", C.c_int), ("outer", C.c_int), ("reserved", C.c_int * 5)]
 
 
 class BuildParams(C.Structure):
@@ -100,6 +101,8 @@ class BuildStats(C.Structure):
 KERNEL_PPOHBEM = 0
 KERNEL_LAPLACE = 1
 
+HBX_FP64, HBX_FP32 = 0, 1
+
 STATUS = {0: "HBX_OK", 1: "HBX_ERR_INVALID", 2: "HBX_ERR_NOMEM", 3: "HBX_ERR_CUDA",
           4: "HBX_ERR_TIMEOUT", 5: "HBX_ERR_BREAKDOWN", 6: "HBX_ERR_NOT_CONVERGED",
           7: "HBX_ERR_NONFINITE", 8: "HBX_ERR_UNSUPPORTED"}
@@ -118,6 +121,8 @@ ENGINE_SYMBOLS = [
     ("hbx_matvec_host", C.c_int, [_VP, _DP, _DP, C.c_int, _DP, _DP]),
     ("hbx_bicgstab", C.c_int, [_VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
     ("hbx_bicgstab_host", C.c_int, [_VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
+    ("hbx_bicgstab_refined", C.c_int, [_VP, _VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
+    ("hbx_bicgstab_refined_host", C.c_int, [_VP, _VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     ("hbx_gradient_host", C.c_int, [_VP, _VP, _DP, _DP, _DP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo),
                                     C.POINTER(SolveInfo)]),
     ("hbx_debug_phase_stamps", C.c_int, [_VP, C.POINTER(C.c_ulonglong), C.c_int]),

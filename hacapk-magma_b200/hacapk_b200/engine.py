@@ -29,11 +29,12 @@ def _check(status: int, where: str):
 class Engine:
     """Packed H-matrix resident on the current CUDA device."""
 
-    def __init__(self, st, nd: int, num_ctas: int = 0, transpose: bool = False):
-        """transpose=True packs H^T: products and solves with the adjoint."""
+    def __init__(self, st, nd: int, num_ctas: int = 0, transpose: bool = False, precision: int = 0):
+        """transpose=True packs H^T: products and solves with the adjoint.
+        precision=abi.HBX_FP32 stores the factors in float (half the bytes)."""
         self.lib = abi.engine_lib()
         opt = abi.Options()
-        opt.precision = 0
+        opt.precision = precision
         opt.num_ctas = num_ctas
         opt.transpose = 1 if transpose else 0
         h = C.c_void_p()
@@ -78,12 +79,13 @@ class Engine:
 
     # -- BiCGSTAB -------------------------------------------------------------
     @staticmethod
-    def _opts(tol, max_iter, verbose, batch):
+    def _opts(tol, max_iter, verbose, batch, inner_tol=0.0):
         o = abi.SolveOpts()
         o.tol = tol
         o.max_iter = max_iter
         o.verbose = verbose
         o.batch = batch
+        o.inner_tol = inner_tol
         return o
 
     @staticmethod
@@ -132,3 +134,27 @@ class Engine:
                                           abi.dptr(grad), C.byref(J), C.byref(o), C.byref(fi), C.byref(ai)),
                "hbx_gradient_host")
         return J.value, grad, sigma, self._info(fi), self._info(ai)
+
+    # -- mixed precision --------------------------------------------------------
+    def bicgstab_refined_host(self, low: "Engine", b: np.ndarray, u0: np.ndarray | None = None, tol: float = 1e-8,
+                              max_iter: int = 1000, inner_tol: float = 0.0, check: bool = True):
+        """FP64 iterative refinement (self: FP64 engine) around BiCGSTAB on
+        `low` (an FP32 engine of the same matrix); host vectors."""
+        b = np.ascontiguousarray(b, np.float64)
+        u = np.zeros(self.nd) if u0 is None else np.array(u0, np.float64, copy=True)
+        o = self._opts(tol, max_iter, 0, 8, inner_tol)
+        si = abi.SolveInfo()
+        st = self.lib.hbx_bicgstab_refined_host(self._h, low._h, abi.dptr(b), abi.dptr(u), C.byref(o), C.byref(si))
+        if check:
+            _check(st, "hbx_bicgstab_refined_host")
+        return u, self._info(si)
+
+    def bicgstab_refined_dev(self, low: "Engine", b_ptr: int, u_ptr: int, tol: float = 1e-8, max_iter: int = 1000,
+                             inner_tol: float = 0.0, stream: int = 0, check: bool = True) -> dict:
+        o = self._opts(tol, max_iter, 0, 8, inner_tol)
+        si = abi.SolveInfo()
+        st = self.lib.hbx_bicgstab_refined(self._h, low._h, C.c_void_p(b_ptr), C.c_void_p(u_ptr), C.byref(o),
+                                           C.byref(si), C.c_void_p(stream) if stream else None)
+        if check:
+            _check(st, "hbx_bicgstab_refined")
+        return self._info(si)

@@ -111,12 +111,17 @@ typedef enum hbx_status {
   HBX_ERR_UNSUPPORTED = 8    /* e.g. more than one MPI rank                */
 } hbx_status;
 
-enum { HBX_FP64 = 0 };
+/* Storage precision of the packed factors.  HBX_FP32 rounds every factor
+ * to float once, at hbx_create, and multiplies in float (four columns per
+ * 16-byte load), adding each run's products to double row sums; vectors,
+ * dot products and solver scalars stay double.  No counterpart in the
+ * reference, which is FP64 throughout. */
+enum { HBX_FP64 = 0, HBX_FP32 = 1 };
 
 typedef struct hbx_hmat hbx_hmat;
 
 typedef struct hbx_options {
-  int precision;   /* HBX_FP64 (only value accepted by this ABI version) */
+  int precision;   /* HBX_FP64 or HBX_FP32 (factor storage)               */
   int num_ctas;    /* persistent CTAs; 0 = one per SM                     */
   int transpose;   /* 1: the engine holds H^T (adjoint products and solves;
                       no counterpart in the reference)                    */
@@ -141,7 +146,10 @@ typedef struct hbx_solve_opts {
   int max_iter;        /* iteration limit (param[82] in the drop-in)             */
   int verbose;         /* >0: print the residual history like the reference     */
   int batch;           /* iterations per graph replay between host checks (0=8) */
-  int reserved[11];
+  int reserved0;
+  double inner_tol;    /* mixed-precision solve: relative residual reduction asked
+                          of each inner solve at most (0 = 1e-6)                 */
+  int reserved[8];
 } hbx_solve_opts;
 
 typedef struct hbx_solve_info {
@@ -155,7 +163,8 @@ typedef struct hbx_solve_info {
   int iter_launches;   /* iteration-kernel launches (includes the final
                           launches that only observe convergence)             */
   int launches;        /* all kernel launches of the solve                    */
-  int reserved[6];
+  int outer;           /* mixed-precision solve: refinement steps (FP64 residuals) */
+  int reserved[5];
 } hbx_solve_info;
 
 /* Packs the leaf list into the engine's per-CTA streaming layout and uploads
@@ -191,6 +200,21 @@ int hbx_matvec(hbx_hmat *h, double alpha, const double *x, double beta,
  * word (hbx_sync). */
 int hbx_matvec_noalloc(hbx_hmat *h, double alpha, const double *x, double beta,
                        const double *yin, double *y, void *stream);
+
+/* Mixed-precision BiCGSTAB (no counterpart in the reference): FP64
+ * iterative refinement around BiCGSTAB on `hl`, an engine created on the same
+ * leaf list with hbx_options.precision = HBX_FP32.  Each refinement step
+ * forms the residual r = b - H u with the FP64 engine `h`, solves H d = r on
+ * `hl` until its residual falls by max(opts->inner_tol, tol*||b||/||r||/2)
+ * and adds d to u, until ||b - H u|| / ||b|| < opts->tol (FP64, measured) or
+ * opts->max_iter inner steps in all.  info->iterations counts the inner
+ * steps, info->outer the refinement steps, info->true_relres is the final
+ * FP64 residual.  u: x0 in, solution out (device pointers, on `stream`). */
+int hbx_bicgstab_refined(hbx_hmat *h, hbx_hmat *hl, const double *b, double *u, const hbx_solve_opts *opts,
+                         hbx_solve_info *info, void *stream);
+/* The same with host vectors (copies inside). */
+int hbx_bicgstab_refined_host(hbx_hmat *h, hbx_hmat *hl, const double *b, double *u, const hbx_solve_opts *opts,
+                              hbx_solve_info *info);
 
 /* Adjoint sensitivity of J(g) = 0.5 ||sigma - sigma_t||^2 where H sigma = g
  * (no counterpart in the reference): solves H sigma = g with `h`, then

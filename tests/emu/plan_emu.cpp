@@ -3,8 +3,10 @@
 // way the sm_100a kernel does (P slabs -> zbu, D/U atom blocks -> y), checks
 // the layout invariants the kernel relies on (16-byte aligned streams, runs
 // back to back inside their CTA stream, gather segments covering each run's
-// stage exactly, heights <= 32, atoms partitioning the rows exactly once,
-// zbu written once before it is read), and returns y = H x.
+// stage exactly, heights <= 32 (64 for P slabs), atoms partitioning the rows
+// exactly once, zbu written once before it is read), and returns y = H x.
+// With FP32 storage it multiplies the float factors by the float-rounded
+// vector, as the kernel does, but sums in double.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -15,15 +17,15 @@
 
 using namespace hbx;
 
-extern "C" int emu_matvec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, const double *x, double *y,
-                          long long *stats, char *msg, int msglen) {
+extern "C" int emu_matvec_prec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int precision, const double *x,
+                               double *y, long long *stats, char *msg, int msglen) {
   auto bad = [&](const std::string &s) {
     std::snprintf(msg, msglen, "%s", s.c_str());
     return 1;
   };
   Plan plan;
   std::string err;
-  int rc = make_plan(st, nd, num_ctas, plan, err);
+  int rc = make_plan(st, nd, num_ctas, plan, err, precision);
   if (rc != 0) return bad("make_plan: " + err);
   std::vector<uint8_t> buf(plan.total_bytes, 0xAB);
   pack_plan(st, plan, buf.data());
@@ -32,7 +34,8 @@ extern "C" int emu_matvec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, c
   std::vector<int> owner(nd, -1);
   std::fill(y, y + nd, NAN);
   long long nruns = 0;
-  std::vector<double> stage(kStageCap), acc(kSlabMax);
+  const uint32_t G = group_cols(precision);
+  std::vector<double> stage(kStageBytes / elem_bytes(precision)), acc(kSlabMax);
 
   // structural checks of one CTA's records; returns "" when fine
   auto check_cta = [&](int c) -> std::string {
@@ -47,13 +50,15 @@ extern "C" int emu_matvec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, c
       const uint32_t want = k < ci.nr_p ? kRunP : (k < ci.nr_p + ci.nr_d ? kRunD : kRunU);
       if (run_kind(r) != want) return "run kind out of section order";
       if (r.nrow == 0 || r.nrow > (want == kRunP ? kSlabMax : kAtomMax)) return "run height outside 1..32 (1..64 for P)";
-      if (2u * r.npair > (uint32_t)kStageCap || r.vlen != 2u * r.npair) return "run width";
+      if (G * r.npanel * elem_bytes(precision) > (uint32_t)kStageBytes || r.vlen > G * r.npanel ||
+          (r.npanel > 0 && r.vlen + G <= G * r.npanel))
+        return "run width";
       if (r.nseg > kRunSegs) return "too many segments";
       if (r.rot >= kConsumerWarps) return "bad rotation";
       if (r.pos != pos || r.pos % 16 != 0) return "runs not back to back";
       pos += run_bytes(r);
-      if ((r.flags & kPadCol) && (!(r.flags & kLast) || r.npair == 0)) return "pad column outside a last run";
-      const uint32_t real = 2u * r.npair - ((r.flags & kPadCol) ? 1u : 0u);
+      if (r.vlen != G * r.npanel && !(r.flags & kLast)) return "zero columns outside a block's last run";
+      const uint32_t real = r.vlen;
       const uint64_t vmax = want == kRunU ? plan.zbu_len : (uint64_t)nd;
       std::vector<char> cov(real, 0);
       uint32_t d = 0;
@@ -81,13 +86,20 @@ extern "C" int emu_matvec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, c
     const RunRec &R = plan.recs[ci.rec_begin + k];
     const Run &r = R.hdr;
     for (uint32_t q = 0; q < r.nseg; ++q)
-      for (uint32_t e = 0; e < R.seg[q].len; ++e) stage[R.seg[q].dst + e] = vec[R.seg[q].src + e];
-    if (r.flags & kPadCol) stage[2u * r.npair - 1] = 0.0;
+      for (uint32_t e = 0; e < R.seg[q].len; ++e) {
+        const double v = vec[R.seg[q].src + e];
+        stage[R.seg[q].dst + e] = precision == kFP32 ? (double)(float)v : v;
+      }
+    for (uint32_t c = r.vlen; c < G * r.npanel; ++c) stage[c] = 0.0;
     if (r.flags & kFirst) std::fill(acc.begin(), acc.end(), 0.0);
     const double *d = reinterpret_cast<const double *>(buf.data() + ci.stream_off + r.pos);
-    for (uint32_t j = 0; j < r.npair; ++j)
+    const float *f = reinterpret_cast<const float *>(buf.data() + ci.stream_off + r.pos);
+    for (uint32_t j = 0; j < r.npanel; ++j)
       for (uint32_t i = 0; i < r.nrow; ++i)
-        acc[i] += d[((size_t)j * r.nrow + i) * 2] * stage[2 * j] + d[((size_t)j * r.nrow + i) * 2 + 1] * stage[2 * j + 1];
+        for (uint32_t c = 0; c < G; ++c) {
+          const size_t k = ((size_t)j * r.nrow + i) * G + c;
+          acc[i] += (precision == kFP32 ? (double)f[k] : d[k]) * stage[G * j + c];
+        }
     ++nruns;
   };
 
@@ -155,6 +167,11 @@ extern "C" int emu_matvec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, c
     stats[7] = (long long)plan.pad_bytes;
   }
   return 0;
+}
+
+extern "C" int emu_matvec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, const double *x, double *y,
+                          long long *stats, char *msg, int msglen) {
+  return emu_matvec_prec(st, nd, num_ctas, kFP64, x, y, stats, msg, msglen);
 }
 
 // The same walk over the packed layout of H^T (hbx_plan.cpp:transpose_leaves).

@@ -24,6 +24,8 @@ def emu(build_libs):
     lib.emu_matvec.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                C.POINTER(C.c_longlong), C.c_char_p, C.c_int]
     lib.emu_matvec_transposed.argtypes = lib.emu_matvec.argtypes
+    lib.emu_matvec_prec.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_char_p, C.c_int]
     return lib
 
 
@@ -183,3 +185,24 @@ def test_transposed_edge_cases(emu):
     assert rc == 0, msg
     ref = _dense_of(leaves, nd).T @ x
     assert np.abs(y - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("level,nc", [(3, 148), (4, 148), (3, 7)])
+def test_fp32_layout(emu, level, nc):
+    """FP32 storage: 4-column float panels with the same 16-byte rows; every
+    factor stored once (half the bytes), products within float rounding of
+    the FP64 oracle."""
+    import oracle
+    H = sphere(level)
+    x = np.random.default_rng(level + 70).standard_normal(H.nd)
+    y = np.zeros(H.nd)
+    stats = (C.c_longlong * 8)()
+    msg = C.create_string_buffer(512)
+    rc = emu.emu_matvec_prec(C.cast(H.st, C.c_void_p), H.nd, nc, 1, x.ctypes.data_as(C.POINTER(C.c_double)),
+                             y.ctypes.data_as(C.POINTER(C.c_double)), stats, msg, 512)
+    assert rc == 0, msg.value.decode()
+    ref = oracle.matvec(H.st, x)
+    assert np.abs(y - ref).max() <= 2e-6 * np.abs(ref).max()
+    d, lr = H.storage_words()
+    assert stats[6] == 4 * (d + lr) + stats[7]
+    assert stats[7] <= 0.05 * 4 * (d + lr)
