@@ -49,6 +49,7 @@ void free_engine(hbx_hmat *h) {
   cudaFree(h->d_stream);
   cudaFree(h->d_recs);
   cudaFree(h->d_ctas);
+  cudaFree(h->d_lite);
   cudaFree(h->d_atoms);
   cudaFree(h->d_zbu);
   cudaFree(h->d_gbar);
@@ -96,10 +97,12 @@ hbx::MatvecArgs matvec_args(hbx_hmat *h, double alpha, const double *x, double b
   a.stream = h->d_stream;
   a.recs = h->d_recs;
   a.ctas = h->d_ctas;
+  a.lite = h->d_lite;
   a.x = x;
   a.yin = yin;
   a.y = y;
   a.zbu = h->d_zbu;
+  a.zbu_len = h->plan.zbu_len;
   if (h->d_f32) {
     a.x32 = h->d_f32;
     a.zbu32 = h->d_f32 + 3 * (size_t)h->plan.nd;
@@ -233,12 +236,16 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hb
   if ((e = cudaMalloc(&h->d_recs, std::max<size_t>(1, P.recs.size()) * sizeof(hbx::RunRec))) != cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(run records)"));
   if ((e = cudaMalloc(&h->d_ctas, P.ctas.size() * sizeof(hbx::CtaInfo))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(ctas)"));
+  if ((e = cudaMalloc(&h->d_lite, std::max<size_t>(1, P.lite.size()) * sizeof(hbx::RunLite))) != cudaSuccess)
+    return bail(cuda_fail(e, "cudaMalloc(lite)"));
   if ((e = cudaMalloc(&h->d_atoms, std::max<size_t>(1, P.atoms.size()) * sizeof(hbx::Atom))) != cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(atoms)"));
-  if ((e = cudaMalloc(&h->d_zbu, std::max<uint64_t>(1, P.zbu_len) * sizeof(double))) != cudaSuccess)
+  // zbu twice: the two H-matvecs of a BiCGSTAB step write separate copies
+  if ((e = cudaMalloc(&h->d_zbu, 2 * std::max<uint64_t>(1, P.zbu_len) * sizeof(double))) != cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(zbu)"));
   if (P.precision == hbx::kFP32 &&
-      (e = cudaMalloc(&h->d_f32, (3 * (size_t)nd + std::max<uint64_t>(1, P.zbu_len)) * sizeof(float))) != cudaSuccess)
+      (e = cudaMalloc(&h->d_f32, (3 * (size_t)nd + 2 * std::max<uint64_t>(1, P.zbu_len)) * sizeof(float))) !=
+          cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(float copies)"));
   if ((e = cudaMalloc(&h->d_gbar, 4 * sizeof(unsigned))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(gbar)"));
   if ((e = cudaMalloc(&h->d_err, sizeof(int))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(err)"));
@@ -249,17 +256,23 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hb
     return bail(cuda_fail(e, "upload run records"));
   if ((e = cudaMemcpy(h->d_ctas, P.ctas.data(), P.ctas.size() * sizeof(hbx::CtaInfo), cudaMemcpyHostToDevice)) != cudaSuccess)
     return bail(cuda_fail(e, "upload ctas"));
+  if (!P.lite.empty() &&
+      (e = cudaMemcpy(h->d_lite, P.lite.data(), P.lite.size() * sizeof(hbx::RunLite), cudaMemcpyHostToDevice)) !=
+          cudaSuccess)
+    return bail(cuda_fail(e, "upload run summaries"));
   if (!P.atoms.empty() &&
       (e = cudaMemcpy(h->d_atoms, P.atoms.data(), P.atoms.size() * sizeof(hbx::Atom), cudaMemcpyHostToDevice)) != cudaSuccess)
     return bail(cuda_fail(e, "upload atoms"));
   cudaMemset(h->d_gbar, 0, 4 * sizeof(unsigned));
   cudaMemset(h->d_err, 0, sizeof(int));
-  cudaMemset(h->d_zbu, 0, std::max<uint64_t>(1, P.zbu_len) * sizeof(double));
+  cudaMemset(h->d_zbu, 0, 2 * std::max<uint64_t>(1, P.zbu_len) * sizeof(double));
   if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(cuda_fail(e, "hbx_create sync"));
   // host copies of the records and the packing tables are no longer needed
   h->num_runs = (long long)P.recs.size();
   h->plan.recs.clear();
   h->plan.recs.shrink_to_fit();
+  h->plan.lite.clear();
+  h->plan.lite.shrink_to_fit();
   h->plan.blocks.clear();
   h->plan.blocks.shrink_to_fit();
   h->plan.pieces.clear();
@@ -404,8 +417,10 @@ static hbx::BicgArgs bicg_args(hbx_hmat *h, const double *b, double *u, double t
   a.stream = h->d_stream;
   a.recs = h->d_recs;
   a.ctas = h->d_ctas;
+  a.lite = h->d_lite;
   a.atoms = h->d_atoms;
   a.zbu = h->d_zbu;
+  a.zbu_len = h->plan.zbu_len;
   a.gbar = h->d_gbar;
   a.err = h->d_err;
   a.timeout_ns = h->timeout_ns;

@@ -1,15 +1,17 @@
 // hbx_device.cuh -- sm_100a device building blocks of the streaming H-matvec.
 //
 //  * mbarrier + cp.async.bulk (1D TMA) ring: one producer thread copies the
-//    CTA's contiguous stream into NS shared-memory chunks; consumer warps
-//    wait on a chunk's "full" barrier, read it, and arrive on its "empty"
-//    barrier; the producer refills a slot once every consumer warp released
-//    it.  Every wait is bounded by a %globaltimer deadline; a wait that runs
-//    out sets an error bit and makes the waiter give up instead of hanging.
+//    CTA's contiguous stream into kRingChunks shared-memory chunks, as far
+//    ahead as the ring allows; consumer warps wait on a chunk's "full"
+//    barrier, read it and arrive on its "empty" barrier, so the copies go on
+//    while the consumers do the bookkeeping of a run.
+//  * Gather warps fill a ring of vector stage buffers (the x or zbu segments
+//    of a run) with cp.async; mbarriers hand a buffer to the consumers and
+//    back.
+//  * Every wait is bounded by a %globaltimer deadline; a wait that runs out
+//    sets an error bit and makes the waiter give up instead of hanging.
 //  * A sense-reversing grid barrier (count, generation) for the persistent
-//    cooperative grid, with split arrive / wait so work can be placed between
-//    the two, and the same bounded wait.
-//  * The block-row processor shared by the matvec and BiCGSTAB kernels.
+//    cooperative grid, with split arrive / wait and the same bounded wait.
 #pragma once
 
 #include <cstdint>
@@ -19,59 +21,52 @@
 namespace hbx {
 
 constexpr uint32_t kRingBytes = (uint32_t)kRingChunks * kChunkBytes;
-// Run records in flight: the gather warp bulk-copies the records it will
-// need this many runs ahead (they come from HBM: the matrix stream evicts
-// them from L2 between two matvecs).
-constexpr uint32_t kRecSlots = 8;
-// Block ends are summed kGroup at a time, after one CTA barrier for the
-// group; the partials of two groups fit in shared memory.
-#ifndef HBX_GROUP
-#define HBX_GROUP 2
+#ifndef HBX_GATHER_WARPS
+#define HBX_GATHER_WARPS 2
 #endif
-constexpr uint32_t kGroup = HBX_GROUP;
+constexpr int kGatherWarps = HBX_GATHER_WARPS;  // warps that stage run vectors
+constexpr uint32_t kRecSlots = 8;               // run records in flight per gather warp
+constexpr uint32_t kRedSlots = 4;               // block ends parked at once
+static_assert(kStages % kGatherWarps == 0, "a stage slot is always filled by the same gather warp");
+// consumer warps, the bulk-copy producer warp, the gather warps, the
+// grid-barrier warp and the block-sum warp
+constexpr int kProducerWarp = kConsumerWarps;
+constexpr int kGatherWarp0 = kConsumerWarps + 1;
+constexpr int kSyncWarp = kGatherWarp0 + kGatherWarps;
+constexpr int kSumWarp = kSyncWarp + 1;
+constexpr int kThreads = (kSumWarp + 1) * 32;
 
 // Shared-memory offset in the ring of stream byte p of absolute chunk c
 // (c = pass base + p / kChunkBytes).  The ring need not be a power of two.
 __device__ __forceinline__ uint32_t ring_off(uint32_t c, uint32_t p) {
   return (c % (uint32_t)kRingChunks) * (uint32_t)kChunkBytes + (p & (uint32_t)(kChunkBytes - 1));
 }
-// consumer warps, then the bulk-copy producer warp, then the gather warp
-constexpr int kProducerWarp = kConsumerWarps;
-constexpr int kGatherWarp = kConsumerWarps + 1;
-constexpr int kThreads = (kConsumerWarps + 2) * 32;
-// Chunks the producer prefetches into L2 beyond the ones in flight into the
-// ring.  The ring alone keeps kRingBytes in flight per SM, about what HBM
-// latency times the per-SM share of bandwidth needs, so any time consumers
-// hold a chunk shows up as lost bandwidth; the L2 prefetch keeps HBM busy
-// further ahead and turns the ring refills into L2 hits.
-#ifndef HBX_L2_AHEAD
-#define HBX_L2_AHEAD 0
-#endif
-constexpr uint32_t kL2Ahead = HBX_L2_AHEAD;
 
 // error bits written to the device error word
 enum : int { kErrPipeline = 1, kErrGridBarrier = 2, kErrProducer = 4 };
 
 struct SharedLayout {
   static constexpr uint32_t ring = 0;
-  static constexpr uint32_t full = kRingBytes;
-  static constexpr uint32_t empty = full + 8 * kRingChunks;
-  static constexpr uint32_t red = empty + 8 * kRingChunks;            // [2*kGroup][NW][64] double
-  static constexpr uint32_t scal = red + 2 * kGroup * kConsumerWarps * 64 * 8;  // 64 doubles of scratch
-  static constexpr uint32_t stage = scal + 64 * 8;                     // [kStages][kStageBytes]
-  static constexpr uint32_t rec = stage + kStages * kStageBytes;       // [kRecSlots] run records
-  static constexpr uint32_t rfull = rec + kRecSlots * kRecBytes;       // [kRecSlots] record landed
-  static constexpr uint32_t hdr = rfull + 8 * kRecSlots;               // [kStages] Run
-  static constexpr uint32_t sfull = hdr + kStages * 32;                // stage filled (gather warp)
-  static constexpr uint32_t sempty = sfull + 8 * kStages;              // stage consumed (consumer warps)
-  static constexpr uint32_t xready = sempty + 8 * kStages;             // a pass's x is complete grid-wide
-  static constexpr uint32_t garrive = xready + 8;                      // this CTA arrived on the grid barrier
-  static constexpr uint32_t gen = garrive + 8;                         // grid-barrier generation of that arrival
-  static constexpr uint32_t binfo = gen + 16;                          // [2*kGroup] pending block ends
-  static constexpr uint32_t bytes = binfo + 2 * kGroup * 8;
+  static constexpr uint32_t full = kRingBytes;                               // [kRingChunks] chunk landed
+  static constexpr uint32_t empty = full + 8 * kRingChunks;                  // [kRingChunks] chunk consumed
+  static constexpr uint32_t red = empty + 8 * kRingChunks;                   // [kRedSlots][NW][64] double
+  static constexpr uint32_t stage = red + kRedSlots * kConsumerWarps * 64 * 8;  // [kStages][kStageBytes]
+  static constexpr uint32_t lite = stage + kStages * kStageBytes;            // [kMaxCtaRuns] RunLite
+  static constexpr uint32_t rec = lite + kMaxCtaRuns * 16;                   // [kGatherWarps][kRecSlots] records
+  static constexpr uint32_t scal = rec + kGatherWarps * kRecSlots * kRecBytes;  // 64 doubles of scratch
+  static constexpr uint32_t sfull = scal + 64 * 8;                           // [kStages] stage filled
+  static constexpr uint32_t sempty = sfull + 8 * kStages;                    // [kStages] stage consumed
+  static constexpr uint32_t rfull = sempty + 8 * kStages;                    // [kGatherWarps][kRecSlots]
+  static constexpr uint32_t xready = rfull + 8 * kGatherWarps * kRecSlots;   // a pass's x is complete grid-wide
+  static constexpr uint32_t pdone = xready + 8;                              // the CTA's P blocks are summed
+  static constexpr uint32_t gdone = pdone + 8;                               // every CTA's zbu is complete
+  static constexpr uint32_t redfull = gdone + 8;                             // [kRedSlots] a block's partials parked
+  static constexpr uint32_t rdone = redfull + 8 * kRedSlots;                 // a pass's block sums are written
+  static constexpr uint32_t rsum = rdone + 8;                                // block ends summed so far
+  static constexpr uint32_t bytes = rsum + 16;
 };
-static_assert(SharedLayout::stage % 16 == 0 && SharedLayout::hdr % 16 == 0 && SharedLayout::sfull % 8 == 0 &&
-                  SharedLayout::rec % 16 == 0,
+static_assert(SharedLayout::red % 16 == 0 && SharedLayout::stage % 16 == 0 && SharedLayout::lite % 16 == 0 &&
+                  SharedLayout::rec % 16 == 0 && SharedLayout::sfull % 8 == 0,
               "shared-memory layout alignment");
 static_assert(SharedLayout::bytes <= 227 * 1024, "shared memory per CTA");
 
@@ -141,7 +136,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64
 }
 
 // Warp-uniform bounded wait: every lane observes the phase itself (so every
-// lane acquires the bulk-copied bytes) and the outcome is agreed on.
+// lane acquires the copied bytes) and the outcome is agreed on.
 __device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, uint64_t timeout_ns) {
   const bool ok = mbar_wait(bar, parity, timeout_ns);
   return __all_sync(0xffffffffu, ok);
@@ -155,11 +150,6 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
           smem_u32(dst)),
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
-}
-
-// Prefetch `bytes` (multiple of 16) of global memory into L2, no destination.
-__device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 
 // Ampere-style asynchronous gathers into shared memory (vector staging).
@@ -191,7 +181,15 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
   return v;
 }
 
-__device__ __forceinline__ double ld_cg(const double *p) { return __ldcg(p); }
+// CTA-scope acquire load / release store of a shared-memory word.
+__device__ __forceinline__ unsigned ld_acquire_s(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.cta.shared.u32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_s(unsigned *p, unsigned v) {
+  asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v) : "memory");
+}
 
 __device__ __forceinline__ double lds_f64(uint32_t addr) {
   double v;
@@ -238,11 +236,6 @@ __device__ __forceinline__ void producer_run(const uint8_t *src, uint32_t bytes,
                                              uint64_t timeout_ns) {
   const uint32_t K = (bytes + kChunkBytes - 1) >> kChunkLog;
   const uint32_t total = K * npass;
-  auto prefetch = [&](uint32_t g) {
-    const uint32_t off = (g % K) << kChunkLog;
-    bulk_prefetch_l2(src + off, min((uint32_t)kChunkBytes, bytes - off));
-  };
-  for (uint32_t g = kRingChunks; g < min(total, (uint32_t)kRingChunks + kL2Ahead); ++g) prefetch(g);
   uint32_t issued = 0;
   for (uint32_t g = 0; g < total; ++g) {
     const uint32_t s = g % kRingChunks;
@@ -258,7 +251,6 @@ __device__ __forceinline__ void producer_run(const uint8_t *src, uint32_t bytes,
     mbar_arrive_expect_tx(&full[s], nb);
     bulk_g2s(ring + ((size_t)s << kChunkLog), src + off, nb, &full[s]);
     issued = g + 1;
-    if (kL2Ahead > 0 && g + kRingChunks + kL2Ahead < total) prefetch(g + kRingChunks + kL2Ahead);
   }
   // Copies still in flight must land before the CTA exits.
   const uint32_t g0 = issued > (uint32_t)kRingChunks ? issued - kRingChunks : 0;
@@ -342,29 +334,9 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// ---- gather warp: for every run of the CTA, in order and for every pass,
-// copies the run header into hdr[slot] and gathers the run's vector segments
-// (x for P and D runs, zbu for U runs) into stage[slot] with 8-byte cp.async
-// (segments start anywhere; the warp copies long segments together and
-// short ones one per lane), kStages runs ahead of the consumers.  Lane l
-// holds 16 bytes of the 512-byte record: lanes 0-1 the header, lane l >= 2
-// segments 2(l-2) and 2(l-2)+1.  Before the first run of pass p it waits
-// until that pass's x is complete grid-wide (xready), and before the first U
-// run until every CTA's zbu is (this CTA's grid-barrier arrival, then the
-// barrier).  Every wait is bounded; on a timeout the warp flags the error
-// and stops, and the consumers' own bounded waits end the launch.
-struct GatherCtx {
-  const RunRec *recs;
-  uint32_t nr_p, nr_d, nr_u, npass;
-  const void *x0, *x1;  // x of pass 0 and pass 1 (float copies for FP32 engines)
-  const void *zbu;       // zbu (float copy for FP32 engines)
-  unsigned *gbar;
-  int *err;
-  uint64_t timeout_ns;
-};
-
-// Staging copies with cp.async: doubles for FP64 engines, the float copies
-// of the vectors for FP32 engines.
+// ---- gather warps ----------------------------------------------------------
+// Staging copies with cp.async: doubles for FP64 engines, the float copies of
+// the vectors for FP32 engines.
 template <bool kF32>
 __device__ __forceinline__ void stage_elems(uint8_t *st, uint32_t dst, const void *src, uint32_t e0, uint32_t len,
                                             uint32_t step) {
@@ -379,122 +351,98 @@ __device__ __forceinline__ void stage_elems(uint8_t *st, uint32_t dst, const voi
   }
 }
 
+struct GatherCtx {
+  const RunRec *recs;   // the CTA's records
+  uint32_t nr, nr_pd;   // runs of a pass; P + D runs (index of the first U run)
+  uint32_t npass;
+  const void *x0, *x1;  // the gathered vector of pass 0 and pass 1 (float copies for FP32 engines)
+  const void *z0, *z1;  // zbu of pass 0 and pass 1 (float copies for FP32 engines)
+  int *err;
+  uint64_t timeout_ns;
+};
+
+// Gather warp gi stages runs g = gi, gi + kGatherWarps, ... (g counted over
+// the passes) into stage slot g % kStages: it waits until the consumers have
+// given the slot back, copies each long segment with the whole warp and each
+// short one with one lane, clears the zero columns of the last panel, and
+// completes the slot's sfull barrier (32 cp.async arrivals + one plain
+// arrival).  Before its first run of a pass it waits for that pass's x
+// (xready), and before its first U run of a pass for the grid barrier that
+// completes zbu (gdone).  Run records arrive kRecSlots runs ahead by cp.async.
 template <bool kF32, class SM>
-__device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm) {
+__device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm, uint32_t gi) {
   const int lane = threadIdx.x & 31;
-  const uint32_t nruns = c.nr_p + c.nr_d + c.nr_u, total = nruns * c.npass;
-  if (total == 0) return;
-  // records g .. g + kRecSlots - 1 are in flight into slots g % kRecSlots
-  uint32_t issued = 0;
-  auto issue = [&](uint32_t gg) {
-    const uint32_t rs = gg % kRecSlots;
-    mbar_arrive_expect_tx(&sm.rfull[rs], (uint32_t)kRecBytes);
-    bulk_g2s(sm.rec + rs * kRecBytes, c.recs + (gg % nruns), (uint32_t)kRecBytes, &sm.rfull[rs]);
+  const uint32_t total = c.nr * c.npass;
+  uint8_t *recs = sm.rec + gi * kRecSlots * kRecBytes;
+  uint64_t *rfull = sm.rfull + gi * kRecSlots;
+  // the i-th run of this warp is g = gi + i * kGatherWarps
+  auto fetch = [&](uint32_t i) {
+    const uint32_t g = gi + i * kGatherWarps;
+    const uint8_t *src = reinterpret_cast<const uint8_t *>(c.recs + (g % c.nr));
+#pragma unroll
+    for (uint32_t o = 0; o < (uint32_t)kRecBytes; o += 512)
+      cp_async16cg(recs + (i % kRecSlots) * kRecBytes + o + lane * 16, src + o + lane * 16);
+    cp_async_arrive(&rfull[i % kRecSlots]);
   };
-  if (lane == 0)
-    for (uint32_t gg = 0; gg < min(total, kRecSlots); ++gg) issue(gg);
-  issued = min(total, kRecSlots);
-  uint32_t g = 0;
-  for (; g < total; ++g) {
-    const uint32_t k = g % nruns, pass = g / nruns;
-    const uint32_t rs = g % kRecSlots;
-    if (!warp_wait(&sm.rfull[rs], (g / kRecSlots) & 1, c.timeout_ns)) {
-      if (lane == 0) atomicOr(c.err, kErrProducer);
-      break;
-    }
-    const uint4 cur = reinterpret_cast<const uint4 *>(sm.rec + rs * kRecBytes)[lane];
-    __syncwarp();  // every lane has read the slot before it is refilled
-    if (g + kRecSlots < total) {
-      if (lane == 0) issue(g + kRecSlots);
-      issued = g + kRecSlots + 1;
-    }
-    bool ok = true;
-    if (k == 0) ok = warp_wait(sm.xready, pass & 1, c.timeout_ns);
-    if (ok && k == c.nr_p + c.nr_d) {  // first U run of the pass: zbu must be complete grid-wide
-      ok = warp_wait(sm.garrive, pass & 1, c.timeout_ns);
-      if (ok) {
-        int gok = 1;
-        if (lane == 0) gok = grid_wait(c.gbar, *sm.gen, c.timeout_ns) ? 1 : 0;
-        ok = __shfl_sync(0xffffffffu, gok, 0) != 0;
-        __syncwarp();
-        __threadfence();
-      }
+  const uint32_t nmine = total > gi ? (total - gi + kGatherWarps - 1) / kGatherWarps : 0;
+  for (uint32_t i = 0; i < nmine && i < kRecSlots; ++i) fetch(i);
+  int xpass = -1, upass = -1;  // passes whose x / zbu readiness this warp has observed
+  bool ok = true;
+  for (uint32_t i = 0; i < nmine && ok; ++i) {
+    const uint32_t g = gi + i * kGatherWarps, k = g % c.nr, pass = g / c.nr;
+    ok = warp_wait(&rfull[i % kRecSlots], (i / kRecSlots) & 1, c.timeout_ns);
+    // A parity wait only tells the current phase from the one before it, so
+    // the phases of xready and gdone are observed one pass after the other,
+    // also for passes in which this warp stages nothing.
+    for (; ok && xpass < (int)pass; ++xpass) ok = warp_wait(sm.xready, (uint32_t)(xpass + 1) & 1, c.timeout_ns);
+    const bool is_u = k >= c.nr_pd;
+    if (ok && is_u && upass < (int)pass) {
+      for (; ok && upass < (int)pass; ++upass) ok = warp_wait(sm.gdone, (uint32_t)(upass + 1) & 1, c.timeout_ns);
+      __threadfence();
     }
     const uint32_t slot = g % kStages;
     if (ok && g >= (uint32_t)kStages) ok = warp_wait(&sm.sempty[slot], ((g / kStages) - 1) & 1, c.timeout_ns);
-    if (!ok) {
-      if (lane == 0) atomicOr(c.err, kErrProducer);
-      ++g;  // this record was consumed
-      break;
-    }
-    if (lane < 2) reinterpret_cast<uint4 *>(sm.hdr + slot)[lane] = cur;
-    const uint32_t w2 = __shfl_sync(0xffffffffu, cur.z, 0);  // nrow | npanel << 16
-    const uint32_t w3 = __shfl_sync(0xffffffffu, cur.w, 0);  // flags | rot << 16
-    const uint32_t w4 = __shfl_sync(0xffffffffu, cur.x, 1);  // nseg | vlen << 16
-    const uint32_t nseg = w4 & 0xffffu, vlen = w4 >> 16;
-    const void *vec = (w3 & 0xffu) == kRunU ? c.zbu : ((pass & 1) ? c.x1 : c.x0);
-    const uint32_t esz = kF32 ? 4u : 8u;
+    if (!ok) break;
+    const uint8_t *rec = recs + (i % kRecSlots) * kRecBytes;
+    const Run h = *reinterpret_cast<const Run *>(rec);
+    const Seg *seg = reinterpret_cast<const Seg *>(rec + sizeof(Run));
+    const uint8_t *vec =
+        static_cast<const uint8_t *>(is_u ? ((pass & 1) ? c.z1 : c.z0) : ((pass & 1) ? c.x1 : c.x0));
+    constexpr uint32_t esz = kF32 ? 4u : 8u;
     uint8_t *st = sm.stage + slot * kStageBytes;
-    const uint32_t nlong = __shfl_sync(0xffffffffu, cur.w, 1);
-    // long segments: the whole warp copies each one (segment s sits in lane
-    // 2 + s/2 of the record, fields (x, y) for even s and (z, w) for odd s)
-    for (uint32_t q = 0; q < nlong; ++q) {
-      const int holder = 2 + (int)(q >> 1);
-      const uint32_t src = __shfl_sync(0xffffffffu, (q & 1) ? cur.z : cur.x, holder);
-      const uint32_t ld = __shfl_sync(0xffffffffu, (q & 1) ? cur.w : cur.y, holder);
-      const uint32_t len = ld & 0xffffu, dst = ld >> 16;
-      stage_elems<kF32>(st, dst, static_cast<const uint8_t *>(vec) + (size_t)src * esz, (uint32_t)lane, len, 32);
+    for (uint32_t q = 0; q < h.nlong; ++q) {
+      const Seg sg = seg[q];
+      stage_elems<kF32>(st, sg.dst, vec + (size_t)sg.src * esz, (uint32_t)lane, sg.len, 32);
     }
-    // short segments: lane i copies segment nlong + i (and nlong + 32 + i)
-    for (uint32_t base = nlong; base < nseg; base += 32) {
-      const uint32_t q = base + (uint32_t)lane;
-      const int holder = 2 + (int)((q >> 1) & 31u);  // only q < nseg <= 60 is used
-      const uint32_t sx = __shfl_sync(0xffffffffu, cur.x, holder);
-      const uint32_t sy = __shfl_sync(0xffffffffu, cur.y, holder);
-      const uint32_t sz = __shfl_sync(0xffffffffu, cur.z, holder);
-      const uint32_t sw = __shfl_sync(0xffffffffu, cur.w, holder);
-      if (q < nseg) {
-        const uint32_t src = (q & 1) ? sz : sx, ld = (q & 1) ? sw : sy;
-        const uint32_t len = ld & 0xffffu, dst = ld >> 16;
-        stage_elems<kF32>(st, dst, static_cast<const uint8_t *>(vec) + (size_t)src * esz, 0, len, 1);
-      }
+    for (uint32_t q = h.nlong + lane; q < h.nseg; q += 32) {
+      const Seg sg = seg[q];
+      stage_elems<kF32>(st, sg.dst, vec + (size_t)sg.src * esz, 0, sg.len, 1);
     }
-    // the zero columns that fill the last panel
-    const uint32_t vend = (w2 >> 16) * (kF32 ? 4u : 2u);
-    for (uint32_t e = vlen + (uint32_t)lane; e < vend; e += 32) {
+    const uint32_t vend = (uint32_t)h.npanel * (kF32 ? 4u : 2u);
+    for (uint32_t e = h.vlen + lane; e < vend; e += 32) {
       if (kF32) reinterpret_cast<float *>(st)[e] = 0.0f;
       else reinterpret_cast<double *>(st)[e] = 0.0;
     }
     cp_async_arrive(&sm.sfull[slot]);
     __syncwarp();
-    if (lane == 0) mbar_arrive(&sm.sfull[slot]);  // releases the header and the plain stores
+    if (lane == 0) mbar_arrive(&sm.sfull[slot]);  // releases the plain stores
+    __syncwarp();  // every lane has read the record before its slot is refilled
+    if (i + kRecSlots < nmine) fetch(i + kRecSlots);
   }
-  // record copies still in flight (only after an error) must land before exit
-  if (lane == 0)
-    for (uint32_t gg = g; gg < issued; ++gg) mbar_wait(&sm.rfull[gg % kRecSlots], (gg / kRecSlots) & 1, c.timeout_ns);
-  cp_async_wait_all();
+  if (!ok && lane == 0) atomicOr(c.err, kErrProducer);
+  cp_async_wait_all();  // copies in flight land before the warp exits
 }
 
-// ---- one run of a block: acc(lane) += sum over the run's panels of
-// B(lane, c) v(c).  Panel j (16h bytes, row i at 16i: two double columns or
-// four float columns) is read by warp (rot + j) mod NW, kUnroll panels per
-// iteration, so the 16 warps together hold a window of NW*kUnroll panels of
-// the ring; lanes >= h repeat row h-1 and their sums are never used.  FP32
-// panels are multiplied in float (four accumulators per row) and added to the
-// row's double accumulator at the end of the run.
-#ifndef HBX_UNROLL
-#define HBX_UNROLL 4
-#endif
-constexpr uint32_t kUnroll = HBX_UNROLL;
-
+// ---- panel arithmetic --------------------------------------------------------
 __device__ __forceinline__ float4 lds_f32x4(uint32_t addr) {
   float4 v;
   asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(addr));
   return v;
 }
 
-// Per-precision panel arithmetic: load a 16-byte stage group / panel row and
-// multiply-accumulate it.
+// A lane's accumulator for a row: FP64 panels (two double columns) add into
+// two doubles; FP32 panels (four float columns) into four floats, folded into
+// the double total at the end of every run.
 template <bool kF32>
 struct PanelMath;
 template <>
@@ -502,7 +450,12 @@ struct PanelMath<false> {
   using V = double2;
   struct Acc {
     double a0 = 0.0, a1 = 0.0;
-    __device__ __forceinline__ double sum() const { return a0 + a1; }
+    __device__ __forceinline__ double take() {
+      const double s = a0 + a1;
+      a0 = 0.0;
+      a1 = 0.0;
+      return s;
+    }
   };
   static __device__ __forceinline__ V ld(uint32_t addr) { return lds_f64x2(addr); }
   static __device__ __forceinline__ void fma(Acc &a, const V &m, const V &v) {
@@ -515,7 +468,11 @@ struct PanelMath<true> {
   using V = float4;
   struct Acc {
     float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-    __device__ __forceinline__ double sum() const { return ((double)a0 + (double)a1) + ((double)a2 + (double)a3); }
+    __device__ __forceinline__ double take() {
+      const double s = ((double)a0 + (double)a1) + ((double)a2 + (double)a3);
+      a0 = a1 = a2 = a3 = 0.f;
+      return s;
+    }
   };
   static __device__ __forceinline__ V ld(uint32_t addr) { return lds_f32x4(addr); }
   static __device__ __forceinline__ void fma(Acc &a, const V &m, const V &v) {
@@ -526,24 +483,35 @@ struct PanelMath<true> {
   }
 };
 
-// (18 warps of 576 threads leave 96 registers a thread: the two-row form
-// unrolls by 2 to stay within them.)
+// ---- one run of a consumer warp ------------------------------------------
+// The warp reads panels j = (w - rot) mod NW, j + NW, ... of the run (16h
+// bytes each; lane i reads row min(i, h-1), and row min(i + 32, h-1) of P
+// slabs taller than 32, 16 bytes each: two double or four float columns)
+// from the ring, kUnroll panels per iteration (two-row form: 2), and adds
+// their products with the staged vector into its accumulators; it adds the
+// run's sums of its rows to t0 (row i) and t1 (row i + 32).  Lanes past the
+// last row repeat it; their sums are never used.
+#ifndef HBX_UNROLL
+#define HBX_UNROLL 4
+#endif
+constexpr uint32_t kUnroll = HBX_UNROLL;
+
 template <bool kTwoRows, bool kF32>
-__device__ __forceinline__ void run_block_rows(const Run &run, uint32_t stage_s, Ring &R, double &acc, double &acc2) {
+__device__ __forceinline__ void run_rows(const RunLite &L, uint32_t stage_s, Ring &R, uint32_t w, double &t0,
+                                         double &t1) {
   using PM = PanelMath<kF32>;
   using V = typename PM::V;
   constexpr uint32_t NW = kConsumerWarps, U = kTwoRows ? 2 : kUnroll;
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t h = run.nrow, np = run.npanel;
-  if (np == 0) return;
+  const int lane = threadIdx.x & 31;
+  const uint32_t h = L.nrow, np = L.npanel;
   const uint32_t pb = 16u * h;
   const uint32_t lrow = 16u * min((uint32_t)lane, h - 1u);
   const uint32_t lrow2 = 16u * min((uint32_t)lane + 32u, h - 1u) - lrow;  // second row, relative
   const uint32_t ring_s = smem_u32(R.buf);
-  uint32_t j = (uint32_t)((w - (int)run.rot) & (int)(NW - 1));
+  uint32_t j = (w + NW - L.rot) % NW;
   typename PM::Acc a[U], b[kTwoRows ? U : 1];
   for (; j + (U - 1) * NW < np; j += U * NW) {
-    const uint32_t p0 = run.pos + j * pb;
+    const uint32_t p0 = L.pos + j * pb;
     R.ensure(p0, p0 + (U - 1) * NW * pb + pb);
     V v[U], m[U], m2[kTwoRows ? U : 1];
 #pragma unroll
@@ -571,7 +539,7 @@ __device__ __forceinline__ void run_block_rows(const Run &run, uint32_t stage_s,
     }
   }
   for (; j < np; j += NW) {
-    const uint32_t p0 = run.pos + j * pb;
+    const uint32_t p0 = L.pos + j * pb;
     R.ensure(p0, p0 + pb);
     const V vv = PM::ld(stage_s + 16u * j);
     const uint32_t pl = p0 + lrow;
@@ -581,23 +549,19 @@ __device__ __forceinline__ void run_block_rows(const Run &run, uint32_t stage_s,
       PM::fma(b[0], PM::ld(ring_s + ring_off(R.base + (p2 >> kChunkLog), p2)), vv);
     }
   }
-  double t = 0.0;
 #pragma unroll
-  for (uint32_t u = 0; u < U; ++u) t += a[u].sum();
-  acc += t;
+  for (uint32_t u = 0; u < U; ++u) t0 += a[u].take();
   if (kTwoRows) {
-    double t2 = 0.0;
 #pragma unroll
-    for (uint32_t u = 0; u < U; ++u) t2 += b[u].sum();
-    acc2 += t2;
+    for (uint32_t u = 0; u < U; ++u) t1 += b[u].take();
   }
 }
 
-// acc: row `lane` of the block; acc2: row lane + 32 (P slabs taller than 32).
 template <bool kF32>
-__device__ __forceinline__ void run_block(const Run &run, uint32_t stage_s, Ring &R, double &acc, double &acc2) {
-  if (run.nrow > 32) run_block_rows<true, kF32>(run, stage_s, R, acc, acc2);
-  else run_block_rows<false, kF32>(run, stage_s, R, acc, acc2);
+__device__ __forceinline__ void run_panels(const RunLite &L, uint32_t stage_s, Ring &R, uint32_t w, double &t0,
+                                           double &t1) {
+  if (L.nrow > 32) run_rows<true, kF32>(L, stage_s, R, w, t0, t1);
+  else run_rows<false, kF32>(L, stage_s, R, w, t0, t1);
 }
 
 // ---- compensated (Dot2) accumulation ------------------------------------------

@@ -34,12 +34,14 @@ struct MatvecArgs {
   const uint8_t *stream;
   const RunRec *recs;
   const CtaInfo *ctas;
+  const RunLite *lite;
   const double *x;
   const double *yin;
   double *y;
   double *zbu;
   const float *x32;  // FP32 engines: x rounded to float (gathered instead of x)
   float *zbu32;      // FP32 engines: zbu rounded to float (gathered by the U runs)
+  uint64_t zbu_len;
   double alpha, beta;
   unsigned *gbar;
   int *err;
@@ -51,14 +53,16 @@ struct BicgArgs {
   const uint8_t *stream;
   const RunRec *recs;
   const CtaInfo *ctas;
+  const RunLite *lite;
   const Atom *atoms;
-  double *zbu;
+  double *zbu;      // [2][zbu_len]: one copy per H-matvec of a step
+  uint64_t zbu_len;
   unsigned *gbar;
   int *err;
   unsigned long long timeout_ns;
   const double *b;
   double *u, *r, *rh, *p, *ap, *t, *at;
-  float *p32, *t32, *zbu32;  // FP32 engines: float copies of the matvec inputs
+  float *p32, *t32, *zbu32;  // FP32 engines: float copies of the matvec inputs (zbu32: [2][zbu_len])
   double *part;   // [num_ctas][kSlots][2]
   BicgState *state;
   double *hist;   // relres per iteration (max_iter + 1 entries)
@@ -97,6 +101,7 @@ struct hbx_hmat {
   hbx::RunRec *d_recs = nullptr;
   long long num_runs = 0;
   hbx::CtaInfo *d_ctas = nullptr;
+  hbx::RunLite *d_lite = nullptr;
   hbx::Atom *d_atoms = nullptr;
   double *d_zbu = nullptr;
   unsigned *d_gbar = nullptr;

@@ -9,13 +9,16 @@
 //               both H-matvecs, the vector updates and all dot products, with
 //               compensated (Dot2) partial sums reduced in a fixed order.
 //
-// All kernels run one CTA per SM: 16 consumer warps, one producer warp and
-// one descriptor warp.  The producer streams the CTA's packed runs through a
-// shared-memory ring with cp.async.bulk; consumer warps own interleaved
-// column pairs of every run (rotated so the work stays balanced) and
-// accumulate in registers.  Grid-wide dependencies (zbu complete, dot
-// products complete) use a bounded grid barrier; the launch is cooperative so
-// every CTA is resident.
+// All kernels run one CTA per SM: 16 consumer warps, a bulk-copy producer
+// warp, kGatherWarps gather warps, a grid-barrier warp and a block-sum warp.
+// The producer streams the CTA's packed runs through a shared-memory ring
+// with cp.async.bulk; the consumers take every 16th panel of every run
+// (rotated so the work stays balanced), multiply it by the run's staged
+// vector and accumulate in registers; at a block end they park their partial
+// sums and go on, and the block-sum warp adds them in a fixed order and
+// writes the rows.  Grid-wide dependencies (zbu complete, dot products
+// complete) use a bounded grid barrier; the launch is cooperative so every
+// CTA is resident.
 #include "hbx_device.cuh"
 #include "hbx_engine.h"
 
@@ -28,16 +31,14 @@ constexpr int kConsumerThreads = NW * 32;
 struct Smem {
   uint8_t *ring;
   uint64_t *full, *empty;
-  double *red;    // [2*kGroup][NW][64]
-  uint2 *binfo;   // [2*kGroup] (out, h | kind << 16) of the pending block ends
-  double *scal;   // 64 doubles
-  uint8_t *stage; // [kStages][kStageBytes]
-  uint8_t *rec;   // [kRecSlots] run records
-  uint64_t *rfull;
-  Run *hdr;       // [kStages] headers of the staged runs
-  uint64_t *sfull, *sempty;
-  uint64_t *xready, *garrive;
-  unsigned *gen;
+  double *red;     // [kRedSlots][NW][64] partial sums of a block end
+  uint8_t *stage;  // [kStages][kStageBytes]
+  RunLite *lite;   // the CTA's run summaries
+  uint8_t *rec;    // [kGatherWarps][kRecSlots] run records
+  double *scal;    // 64 doubles
+  uint64_t *sfull, *sempty, *rfull;
+  uint64_t *xready, *pdone, *gdone, *redfull, *rdone;
+  unsigned *rsum;
 };
 
 __device__ __forceinline__ Smem smem_layout(uint8_t *base) {
@@ -46,188 +47,216 @@ __device__ __forceinline__ Smem smem_layout(uint8_t *base) {
   s.full = reinterpret_cast<uint64_t *>(base + SharedLayout::full);
   s.empty = reinterpret_cast<uint64_t *>(base + SharedLayout::empty);
   s.red = reinterpret_cast<double *>(base + SharedLayout::red);
-  s.scal = reinterpret_cast<double *>(base + SharedLayout::scal);
   s.stage = base + SharedLayout::stage;
+  s.lite = reinterpret_cast<RunLite *>(base + SharedLayout::lite);
   s.rec = base + SharedLayout::rec;
-  s.rfull = reinterpret_cast<uint64_t *>(base + SharedLayout::rfull);
-  s.hdr = reinterpret_cast<Run *>(base + SharedLayout::hdr);
+  s.scal = reinterpret_cast<double *>(base + SharedLayout::scal);
   s.sfull = reinterpret_cast<uint64_t *>(base + SharedLayout::sfull);
   s.sempty = reinterpret_cast<uint64_t *>(base + SharedLayout::sempty);
+  s.rfull = reinterpret_cast<uint64_t *>(base + SharedLayout::rfull);
   s.xready = reinterpret_cast<uint64_t *>(base + SharedLayout::xready);
-  s.garrive = reinterpret_cast<uint64_t *>(base + SharedLayout::garrive);
-  s.gen = reinterpret_cast<unsigned *>(base + SharedLayout::gen);
-  s.binfo = reinterpret_cast<uint2 *>(base + SharedLayout::binfo);
+  s.pdone = reinterpret_cast<uint64_t *>(base + SharedLayout::pdone);
+  s.gdone = reinterpret_cast<uint64_t *>(base + SharedLayout::gdone);
+  s.redfull = reinterpret_cast<uint64_t *>(base + SharedLayout::redfull);
+  s.rdone = reinterpret_cast<uint64_t *>(base + SharedLayout::rdone);
+  s.rsum = reinterpret_cast<unsigned *>(base + SharedLayout::rsum);
   return s;
 }
 
-__device__ __forceinline__ void init_barriers(const Smem &s) {
+// Barriers, the block-sum counter and the CTA's run summaries (`lite`, nr of
+// them) in shared memory; every thread takes part.
+__device__ __forceinline__ void init_cta(const Smem &s, const RunLite *lite, uint32_t nr) {
   if (threadIdx.x == 0) {
     for (int i = 0; i < kRingChunks; ++i) {
       mbar_init(&s.full[i], 1);
       mbar_init(&s.empty[i], NW);
     }
     for (int i = 0; i < kStages; ++i) {
-      mbar_init(&s.sfull[i], 33);  // 32 cp.async arrivals of the gather warp + its lane 0
+      mbar_init(&s.sfull[i], 33);  // 32 cp.async arrivals of a gather warp + its lane 0
       mbar_init(&s.sempty[i], NW);
     }
-    for (uint32_t i = 0; i < kRecSlots; ++i) mbar_init(&s.rfull[i], 1);
+    for (int i = 0; i < kGatherWarps * (int)kRecSlots; ++i) mbar_init(&s.rfull[i], 32);
     mbar_init(s.xready, 1);
-    mbar_init(s.garrive, 1);
+    mbar_init(s.pdone, 1);
+    mbar_init(s.gdone, 1);
+    for (uint32_t i = 0; i < kRedSlots; ++i) mbar_init(&s.redfull[i], NW);
+    mbar_init(s.rdone, 1);
+    *s.rsum = 0;
     mbar_fence_init();
   }
+  const uint4 *src = reinterpret_cast<const uint4 *>(lite);
+  uint4 *dst = reinterpret_cast<uint4 *>(s.lite);
+  for (uint32_t k = threadIdx.x; k < nr; k += blockDim.x) dst[k] = __ldg(src + k);
   __syncthreads();
 }
 
-__device__ __forceinline__ uint32_t run_end(const Run &r) { return r.pos + run_bytes(r); }
+// ---- grid-barrier warp: once per pass, after the CTA's P blocks are summed
+// (pdone), arrive on the grid barrier, wait for it and release the U runs
+// (gdone).  The barrier latency stays off the consumer and gather warps.
+__device__ __forceinline__ void sync_warp(unsigned *gbar, uint32_t npass, const Smem &sm, int *err, uint64_t tmo) {
+  for (uint32_t p = 0; p < npass; ++p) {
+    if (!mbar_wait(sm.pdone, p & 1, tmo)) {
+      atomicOr(err, kErrPipeline);
+      return;  // the waits on gdone are bounded too
+    }
+    const unsigned gen = ld_acquire(&gbar[1]);
+    grid_arrive(gbar, gridDim.x);  // fences first: the CTA's zbu stores are visible grid-wide
+    if (!grid_wait(gbar, gen, tmo)) {
+      atomicOr(err, kErrGridBarrier);
+      return;
+    }
+    mbar_arrive(sm.gdone);
+  }
+}
 
-// Cross-warp sums of the finished blocks.  A warp that finishes its part of
-// a block writes its 64 partial sums (rows lane and lane + 32) to red buffer
-// nae % (2 kGroup); after
-// every kGroup blocks (and at the end of a section) one CTA barrier makes
-// them visible and warp (block mod NW) sums each pending block in warp order
-// and writes its rows:  kind P: zbu[out+i] = s;  D: y = alpha*s + beta*yin;
-// U: y += alpha*s.  A group's buffers are refilled only after the next
-// group's barrier, which its summing warps pass after they have summed.
-struct BlockEnds {
-  uint32_t nae = 0;   // blocks finished so far (the same in every warp)
-  uint32_t pend = 0;  // finished but not yet summed
+// Where the block sums of one H-matvec pass go.
+struct PassOut {
+  double alpha, beta;
+  const double *yin;
+  double *y, *zbu;
+  float *zbu32;     // FP32 engines: zbu rounded to float (what the U runs gather)
+  uint32_t pass;    // pass index within the launch (barrier parities)
+  uint32_t nblk_p;  // P blocks of the CTA
 };
 
-__device__ __forceinline__ void flush_block_ends(BlockEnds &B, const Smem &sm, double alpha, double beta,
-                                                 const double *yin, double *y, double *zbu, float *zbu32,
-                                                 const Ring &R) {
-  if (B.pend == 0) return;
+// End of a block for a consumer warp: park its row sums (rows lane and
+// lane + 32) in red slot nb mod kRedSlots, once the block-sum warp has
+// emptied it, and arrive on the slot's barrier.  Returns false after a
+// timed-out wait.
+__device__ __forceinline__ bool block_end(double t0, double t1, uint32_t &nb, const Smem &sm, int *err,
+                                          uint64_t tmo) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  named_bar(2, kConsumerThreads);
-  for (uint32_t q = B.nae - B.pend; q < B.nae; ++q) {
-    if ((uint32_t)w != q % NW || R.bad) continue;
-    const uint32_t b = q % (2 * kGroup);
-    const uint2 bi = sm.binfo[b];
-    const uint32_t h = bi.y & 0xffffu, kind = bi.y >> 16;
-    const double *rb = sm.red + b * (NW * 64);
-    for (uint32_t row = lane; row < h; row += 32) {
-      double s = rb[row];
+  const uint32_t slot = nb % kRedSlots;
+  int ok = 1;
+  if (nb >= kRedSlots && lane == 0 && ld_acquire_s(sm.rsum) + kRedSlots <= nb) {
+    const uint64_t ts = gtimer();
+    while (ld_acquire_s(sm.rsum) + kRedSlots <= nb) {
+      if (gtimer() - ts > tmo) {
+        ok = 0;
+        atomicOr(err, kErrPipeline);
+        break;
+      }
+    }
+  }
+  ++nb;
+  if (!__shfl_sync(0xffffffffu, ok, 0)) return false;
+  double *rb = sm.red + slot * (NW * 64) + w * 64;
+  rb[lane] = t0;
+  rb[32 + lane] = t1;
+  __syncwarp();
+  if (lane == 0) mbar_arrive(&sm.redfull[slot]);
+  return true;
+}
+
+// ---- block-sum warp: for every block end of every pass, in order, wait
+// until all consumer warps parked their partial sums, add them in warp order
+// and write the rows -- P: zbu = s;  D: y = alpha*s + beta*yin;  U: y +=
+// alpha*s (the atom's D block was summed before, in this same order) --
+// then free the slot.  After the pass's last P block it signals pdone (the
+// CTA's zbu rows are complete), after the pass's last block rdone.
+__device__ __forceinline__ void sum_warp(uint32_t nr, uint32_t npass, uint32_t nblk_p, const PassOut *outs,
+                                         const Smem &sm, int *err, uint64_t tmo) {
+  const int lane = threadIdx.x & 31;
+  uint32_t nb = 0;
+  for (uint32_t pass = 0; pass < npass; ++pass) {
+    const PassOut &o = outs[pass];
+    // Not before the pass has started: rdone must not run a phase ahead of
+    // the consumers' wait on it (a CTA without blocks would otherwise
+    // complete both passes' phases at once).
+    if (!warp_wait(sm.xready, pass & 1, tmo)) {
+      if (lane == 0) atomicOr(err, kErrPipeline);
+      return;
+    }
+    uint32_t np_done = 0;
+    for (uint32_t r = 0; r < nr; ++r) {
+      const RunLite L = sm.lite[r];
+      if (!(L.flags & kLast)) continue;
+      const uint32_t slot = nb % kRedSlots;
+      if (!warp_wait(&sm.redfull[slot], (nb / kRedSlots) & 1, tmo)) {
+        if (lane == 0) atomicOr(err, kErrPipeline);
+        return;  // the consumers' bounded waits end the launch
+      }
+      const uint32_t kind = L.flags & 0xffu;
+      const double *rb = sm.red + slot * (NW * 64);
+      for (uint32_t i = lane; i < L.nrow; i += 32) {
+        double s = rb[i];
 #pragma unroll
-      for (int k = 1; k < NW; ++k) s += rb[k * 64 + row];
-      const uint32_t r = bi.x + row;
-      if (kind == kRunP) {
-        zbu[r] = s;
-        if (zbu32) zbu32[r] = (float)s;
-        continue;
+        for (int k = 1; k < NW; ++k) s += rb[k * 64 + i];
+        const uint32_t row = L.out + i;
+        if (kind == kRunP) {
+          o.zbu[row] = s;
+          if (o.zbu32) o.zbu32[row] = (float)s;
+        } else if (kind == kRunD) {
+          double v = o.alpha * s;
+          if (o.beta != 0.0) v = fma(o.beta, o.yin[row], v);
+          o.y[row] = v;
+        } else {
+          o.y[row] = fma(o.alpha, s, o.y[row]);
+        }
       }
-      if (kind == kRunD) {
-        double v = alpha * s;
-        if (beta != 0.0) v = fma(beta, yin[r], v);
-        y[r] = v;
-      } else {
-        y[r] = fma(alpha, s, y[r]);
+      ++nb;
+      __syncwarp();
+      if (lane == 0) {
+        __threadfence_block();
+        st_release_s(sm.rsum, nb);  // the slot may be refilled
+        if (kind == kRunP && ++np_done == nblk_p) mbar_arrive(sm.pdone);  // the CTA's zbu rows are complete
       }
     }
-  }
-  B.pend = 0;
-}
-
-// End of a block: park this warp's partials; sum the group when it is full.
-// Before the barrier a warp gives back every ring chunk it will not read
-// again, so no warp waits at a barrier while holding chunks others need.
-__device__ __forceinline__ void block_end(const Run &run, double &acc, double &acc2, BlockEnds &B, const Smem &sm,
-                                          double alpha, double beta, const double *yin, double *y, double *zbu,
-                                          float *zbu32, Ring &R) {
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  R.release_below(R.base + (run_end(run) >> kChunkLog));
-  const uint32_t b = B.nae % (2 * kGroup);
-  sm.red[b * (NW * 64) + w * 64 + lane] = acc;
-  sm.red[b * (NW * 64) + w * 64 + 32 + lane] = acc2;
-  if (w == 0 && lane == 0) sm.binfo[b] = make_uint2(run.out, (uint32_t)run.nrow | (run_kind(run) << 16));
-  acc = 0.0;
-  acc2 = 0.0;
-  ++B.nae;
-  if (++B.pend == kGroup) flush_block_ends(B, sm, alpha, beta, yin, y, zbu, zbu32, R);
-}
-
-// Consumer view of the stage ring: run g (counted over sections and passes)
-// is in slot g % kStages.
-struct StageQ {
-  uint32_t g;
-};
-
-// Runs a section: waits for each run's staged vector, processes it, and
-// gives the slot back.  Before a wait the warp gives back the ring chunks of
-// the previous run, so no warp blocks while holding chunks the others need.
-// process(run, stage) returns the stream position where the run ends.
-template <class F>
-__device__ __forceinline__ void run_section(uint32_t nruns, StageQ &Q, const Smem &sm, Ring &R, int *err,
-                                            F &&process) {
-  uint32_t rend = 0;
-  for (uint32_t k = 0; k < nruns; ++k) {
-    const uint32_t g = Q.g + k, slot = g % kStages;
-    if (k > 0) R.release_below(R.base + (rend >> kChunkLog));
-    if (!R.bad && !warp_wait(&sm.sfull[slot], (g / kStages) & 1, R.timeout_ns)) {
-      R.bad = true;
-      if ((threadIdx.x & 31) == 0) atomicOr(err, kErrPipeline);
-    }
-    Run run = sm.hdr[slot];
-    if (R.bad) run.npanel = 0;  // after a timed-out wait: touch neither the stage nor the ring
-    rend = process(run, smem_u32(sm.stage + slot * kStageBytes));
     __syncwarp();
-    if ((threadIdx.x & 31) == 0) mbar_arrive(&sm.sempty[slot]);
+    if (lane == 0) mbar_arrive(sm.rdone);
   }
-  Q.g += nruns;
 }
 
-// One H-matvec over this CTA's stream (pass starting at absolute chunk R.base,
-// K chunks long).  The CTA arrives on the grid barrier after its P runs; the
-// gather warp waits for the barrier before it stages the first U run, so the
-// D runs hide the barrier latency.  Every warp has released the whole pass
-// when it returns.
+// One H-matvec pass of a consumer warp over the CTA's runs (the pass starts
+// at absolute ring chunk R.base and is K chunks long).  For every run the
+// warp waits for its staged vector, multiplies its panels (every 16th,
+// rotated), gives the stage slot back and, at a block end, parks its row
+// sums for the block-sum warp.  Before it can block, a warp gives back every
+// ring chunk below the run it is about to process, so no wait holds a chunk
+// another warp needs.  nb counts the block ends over the launch.
 template <bool kF32>
-__device__ __forceinline__ void matvec_body(Ring &R, StageQ &Q, uint32_t K, const CtaInfo &ci, double alpha,
-                                            double beta, const double *yin, double *y, double *zbu, float *zbu32,
-                                            unsigned *gbar, int *err, const Smem &sm, BlockEnds &B,
-                                            unsigned long long *prof = nullptr) {
+__device__ __forceinline__ void consume_pass(Ring &R, uint32_t K, uint32_t nr, uint32_t &nb, uint32_t pass,
+                                             const Smem &sm, int *err, uint64_t tmo) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  auto stamp = [&](int k) {
-    if (prof && w == 0 && lane == 0) prof[blockIdx.x * 16 + k] = gtimer();
-  };
-  stamp(0);
-  double acc = 0.0, acc2 = 0.0;
-  auto block = [&](const Run &run, uint32_t stage_s) {
-    run_block<kF32>(run, stage_s, R, acc, acc2);
-    if (run.flags & kLast) block_end(run, acc, acc2, B, sm, alpha, beta, yin, y, zbu, zbu32, R);
-    return run_end(run);
-  };
-  // ---- P: zbu = V^T x for this CTA's slabs
-  uint32_t pend = 0;
-  run_section(ci.nr_p, Q, sm, R, err, [&](const Run &run, uint32_t st) { return pend = block(run, st); });
-  R.release_below(R.base + (pend >> kChunkLog));
-  flush_block_ends(B, sm, alpha, beta, yin, y, zbu, zbu32, R);
-  stamp(1);
-  if (lane == 0) __threadfence();
-  named_bar(1, kConsumerThreads);
-  stamp(2);
-  unsigned gen = 0;
-  if (w == 0 && lane == 0) {
-    gen = ld_acquire(&gbar[1]);
-    *sm.gen = gen;
-    grid_arrive(gbar, gridDim.x);
-    mbar_arrive(sm.garrive);
+  bool bad = R.bad;
+  double t0 = 0.0, t1 = 0.0;  // this lane's block sums: rows lane and lane + 32
+  for (uint32_t r = 0; r < nr; ++r) {
+    const RunLite L = sm.lite[r];
+    const uint32_t g = pass * nr + r, slot = g % kStages;
+    R.release_below(R.base + (L.pos >> kChunkLog));
+    // Every warp observes every phase of the slot's barrier, panels or not: a
+    // warp that skipped phases could take an older completed phase for the
+    // one it waits on.
+    if (!bad && !warp_wait(&sm.sfull[slot], (g / kStages) & 1, tmo)) {
+      bad = true;
+      if (lane == 0) atomicOr(err, kErrPipeline);
+    }
+    if (!bad) run_panels<kF32>(L, smem_u32(sm.stage + slot * kStageBytes), R, (uint32_t)w, t0, t1);
+    bad = bad || R.bad;
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sm.sempty[slot]);
+    if (L.flags & kLast) {
+      R.release_below(R.base + ((L.pos + 16u * L.nrow * L.npanel) >> kChunkLog));
+      if (bad) ++nb;
+      else if (!block_end(t0, t1, nb, sm, err, tmo)) bad = true;
+      t0 = 0.0;
+      t1 = 0.0;
+    }
   }
-  // ---- D: dense rows of the owned atoms
-  uint32_t dend = pend;
-  run_section(ci.nr_d, Q, sm, R, err, [&](const Run &run, uint32_t st) { return dend = block(run, st); });
-  R.release_below(R.base + (dend >> kChunkLog));
-  flush_block_ends(B, sm, alpha, beta, yin, y, zbu, zbu32, R);
-  stamp(3);
-  stamp(4);
-  // ---- U: U rows of the owned atoms times zbu (staged after the grid barrier)
-  run_section(ci.nr_u, Q, sm, R, err, [&](const Run &run, uint32_t st) { return block(run, st); });
   R.release_below(R.base + K);
-  flush_block_ends(B, sm, alpha, beta, yin, y, zbu, zbu32, R);
-  // The barrier counts arrivals per instance: this CTA may arrive on the
-  // next instance only once this one is complete (a CTA without U runs has
-  // not waited for it yet).
-  if (w == 0 && lane == 0 && !grid_wait(gbar, gen, R.timeout_ns)) atomicOr(err, kErrGridBarrier);
-  stamp(5);
+}
+
+// The consumer warps' part of one H-matvec pass: the P-done signal of a CTA
+// without P blocks, the pass, then the wait for the block-sum warp (every
+// row of the pass is written) and, in warp 0, for the pass's grid barrier
+// (the caller's next grid barrier must not start before it completes).
+template <bool kF32>
+__device__ __forceinline__ void matvec_pass(Ring &R, uint32_t K, uint32_t nr, uint32_t &nb, const PassOut &o,
+                                            const Smem &sm, int *err, uint64_t tmo) {
+  if (o.nblk_p == 0 && threadIdx.x == 0) mbar_arrive(sm.pdone);
+  consume_pass<kF32>(R, K, nr, nb, o.pass, sm, err, tmo);
+  if (!warp_wait(sm.rdone, o.pass & 1, tmo) && (threadIdx.x & 31) == 0) atomicOr(err, kErrPipeline);
+  if (threadIdx.x < 32 && !warp_wait(sm.gdone, o.pass & 1, tmo) && threadIdx.x == 0) atomicOr(err, kErrGridBarrier);
 }
 
 template <bool kF32>
@@ -235,7 +264,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const Smem sm = smem_layout(smem_raw);
   const CtaInfo ci = a.ctas[blockIdx.x];
-  init_barriers(sm);
+  const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
+  const uint64_t t_start = a.prof ? gtimer() : 0;
+  init_cta(sm, a.lite + ci.rec_begin, nr);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
   if (w == kProducerWarp) {
@@ -243,21 +274,30 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
       producer_run(a.stream + ci.stream_off, ci.stream_bytes, 1, sm.ring, sm.full, sm.empty, a.err, a.timeout_ns);
     return;
   }
-  if (w == kGatherWarp) {
+  if (w >= kGatherWarp0 && w < kSyncWarp) {
     const void *xs = kF32 ? static_cast<const void *>(a.x32) : static_cast<const void *>(a.x);
     const void *zs = kF32 ? static_cast<const void *>(a.zbu32) : static_cast<const void *>(a.zbu);
-    const GatherCtx c{a.recs + ci.rec_begin, ci.nr_p, ci.nr_d, ci.nr_u, 1, xs, xs, zs, a.gbar, a.err,
-                      a.timeout_ns};
-    gather_warp<kF32>(c, sm);
+    const GatherCtx c{a.recs + ci.rec_begin, nr, ci.nr_p + ci.nr_d, 1, xs, xs, zs, zs, a.err, a.timeout_ns};
+    gather_warp<kF32>(c, sm, (uint32_t)(w - kGatherWarp0));
+    return;
+  }
+  if (w == kSyncWarp) {
+    if (lane == 0) sync_warp(a.gbar, 1, sm, a.err, a.timeout_ns);
+    return;
+  }
+  const PassOut o{a.alpha, a.beta, a.yin, a.y, a.zbu, kF32 ? a.zbu32 : nullptr, 0, ci.nblk_p};
+  if (w == kSumWarp) {
+    sum_warp(nr, 1, ci.nblk_p, &o, sm, a.err, a.timeout_ns);
     return;
   }
   if (threadIdx.x == 0) mbar_arrive(sm.xready);  // x is an input: ready from the start
+  uint32_t nb = 0;
   Ring R{sm.ring, sm.full, sm.empty, 0, 0, 0, a.timeout_ns, a.err, false};
-  StageQ Q{0};
-  BlockEnds B;
-  matvec_body<kF32>(R, Q, K, ci, a.alpha, a.beta, a.yin, a.y, a.zbu, kF32 ? a.zbu32 : nullptr, a.gbar, a.err, sm, B,
-                    a.prof);
-  R.drain(K);
+  matvec_pass<kF32>(R, K, nr, nb, o, sm, a.err, a.timeout_ns);
+  if (a.prof && threadIdx.x == 0) {
+    a.prof[blockIdx.x * 16 + 0] = t_start;
+    a.prof[blockIdx.x * 16 + 5] = gtimer();
+  }
 }
 
 // ---------------------------------------------------------------- BiCGSTAB
@@ -363,7 +403,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     if (a.prof && threadIdx.x == 0) a.prof[blockIdx.x * 16 + 8 + k] = gtimer();
   };
   const uint64_t t_start = a.prof ? gtimer() : 0;
-  init_barriers(sm);
+  const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
+  init_cta(sm, a.lite + ci.rec_begin, nr);
 
   // ---- S0: scalars of the previous step; stop test at the top of the loop
   // (HACApK_SOLVER.c:602-603).  Every CTA computes identical values: warps
@@ -435,18 +476,31 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
       producer_run(a.stream + ci.stream_off, ci.stream_bytes, 2, sm.ring, sm.full, sm.empty, a.err, a.timeout_ns);
     return;
   }
-  if (w == kGatherWarp) {
+  if (w >= kGatherWarp0 && w < kSyncWarp) {
     const void *x0 = kF32 ? static_cast<const void *>(a.p32) : static_cast<const void *>(a.p);
     const void *x1 = kF32 ? static_cast<const void *>(a.t32) : static_cast<const void *>(a.t);
-    const void *zs = kF32 ? static_cast<const void *>(a.zbu32) : static_cast<const void *>(a.zbu);
-    const GatherCtx c{a.recs + ci.rec_begin, ci.nr_p, ci.nr_d, ci.nr_u, 2, x0, x1, zs, a.gbar, a.err,
-                      a.timeout_ns};
-    gather_warp<kF32>(c, sm);
+    const void *z0 = kF32 ? static_cast<const void *>(a.zbu32) : static_cast<const void *>(a.zbu);
+    const void *z1 =
+        kF32 ? static_cast<const void *>(a.zbu32 + a.zbu_len) : static_cast<const void *>(a.zbu + a.zbu_len);
+    const GatherCtx c{a.recs + ci.rec_begin, nr, ci.nr_p + ci.nr_d, 2, x0, x1, z0, z1, a.err, a.timeout_ns};
+    gather_warp<kF32>(c, sm, (uint32_t)(w - kGatherWarp0));
+    return;
+  }
+  if (w == kSyncWarp) {
+    if (lane == 0) sync_warp(a.gbar, 2, sm, a.err, a.timeout_ns);
+    return;
+  }
+  // The two H-matvecs write separate zbu copies, so a U run of the second
+  // never reads a line of the first from L1.
+  const PassOut outs[2] = {{1.0, 0.0, nullptr, a.ap, a.zbu, kF32 ? a.zbu32 : nullptr, 0, ci.nblk_p},
+                           {1.0, 0.0, nullptr, a.at, a.zbu + a.zbu_len, kF32 ? a.zbu32 + a.zbu_len : nullptr, 1,
+                            ci.nblk_p}};
+  if (w == kSumWarp) {
+    sum_warp(nr, 2, ci.nblk_p, outs, sm, a.err, a.timeout_ns);
     return;
   }
   Ring R{sm.ring, sm.full, sm.empty, 0, 0, 0, a.timeout_ns, a.err, false};
-  StageQ Q{0};
-  BlockEnds B;
+  uint32_t nb = 0;
 
   // ---- S1: p = r + beta*(p - zeta*Ap)  (p = r on the first step)
   if (beta == 0.0) {
@@ -457,7 +511,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     });
   } else {
     for_own_rows(a.atoms, ci, [&](uint32_t r) {
-      const double v = fma(-zeta_prev, a.ap[r], a.p[r]) * beta;
+      // p through L2 only: a line of p cached in L1 here could hold rows of
+      // another CTA that the gather warps read after it rewrote them
+      const double v = fma(-zeta_prev, a.ap[r], __ldcg(&a.p[r])) * beta;
       const double pv = v + a.r[r];
       a.p[r] = pv;
       if (kF32) a.p32[r] = (float)pv;
@@ -465,7 +521,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
   __threadfence();
   grid_sync(a.gbar, a.err, a.timeout_ns, sm);
-  if (threadIdx.x == 0) mbar_arrive(sm.xready);  // p complete grid-wide: pass 1 may be staged
+  if (threadIdx.x == 0) mbar_arrive(sm.xready);  // p complete grid-wide: pass 0 may be gathered
   stamp(1);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.state->iter = iter + 1;
@@ -477,7 +533,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
 
   // ---- S2: Ap = H p;  rh . Ap
-  matvec_body<kF32>(R, Q, K, ci, 1.0, 0.0, nullptr, a.ap, a.zbu, kF32 ? a.zbu32 : nullptr, a.gbar, a.err, sm, B);
+  matvec_pass<kF32>(R, K, nr, nb, outs[0], sm, a.err, a.timeout_ns);
   stamp(2);
   {
     Acc2 acc[1] = {{0, 0}};
@@ -502,12 +558,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   });
   __threadfence();
   grid_sync(a.gbar, a.err, a.timeout_ns, sm);
-  if (threadIdx.x == 0) mbar_arrive(sm.xready);  // t complete grid-wide: pass 2 may be staged
+  if (threadIdx.x == 0) mbar_arrive(sm.xready);  // t complete grid-wide: pass 1 may be gathered
   stamp(4);
 
   // ---- S4: At = H t;  At . t,  At . At
   R.base = K;
-  matvec_body<kF32>(R, Q, K, ci, 1.0, 0.0, nullptr, a.at, a.zbu, kF32 ? a.zbu32 : nullptr, a.gbar, a.err, sm, B);
+  matvec_pass<kF32>(R, K, nr, nb, outs[1], sm, a.err, a.timeout_ns);
   stamp(5);
   {
     Acc2 acc[2] = {{0, 0}, {0, 0}};
@@ -555,7 +611,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     });
     cta_partials<2>(acc, a.part, kSlotRhoR, sm);
   }
-  R.drain(2 * K);
   stamp(7);
 }
 

@@ -347,8 +347,17 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
       do {
         uint32_t nc = std::min<uint32_t>(stage_cols, Wp - col);
         segments(M, col, std::min(col + nc, b.W), segs);
-        while (segs.size() > (size_t)kRunSegs) {  // too many pieces: take fewer columns
-          nc = std::max<uint32_t>(G, (nc / 2) / G * G);
+        if (segs.size() > (size_t)kRunSegs) {
+          // too many pieces: the widest run (a multiple of G columns) whose
+          // segments fit the record (the count grows with the width)
+          uint32_t lo = G, hi = nc - G;
+          while (lo < hi) {
+            const uint32_t mid = ((lo + hi + G) / 2) / G * G;
+            segments(M, col, std::min(col + mid, b.W), segs);
+            if (segs.size() <= (size_t)kRunSegs) lo = mid;
+            else hi = mid - G;
+          }
+          nc = lo;
           segments(M, col, std::min(col + nc, b.W), segs);
         }
         RunRec rec{};
@@ -367,6 +376,14 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
         r.col0 = col;
         std::copy(segs.begin(), segs.end(), rec.seg);
         plan.recs.push_back(rec);
+        RunLite L{};
+        L.pos = r.pos;
+        L.out = r.out;
+        L.npanel = r.npanel;
+        L.nrow = (uint8_t)r.nrow;
+        L.rot = (uint8_t)r.rot;
+        L.flags = r.flags;
+        plan.lite.push_back(L);
         plan.pad_bytes += (uint64_t)elem_bytes(precision) * b.h * (nc - r.vlen);
         pos += 16ull * b.h * r.npanel;
         rot = (rot + r.npanel) % kConsumerWarps;
@@ -376,11 +393,16 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
       return nr;
     };
     for (uint32_t b : pl) info.nr_p += emit_block(b);
+    info.nblk_p = (uint32_t)pl.size();
     for (uint32_t a : al) info.nr_d += emit_block(dblock[a]);
     for (uint32_t a : al)
       if (ublock[a] != 0xffffffffu) info.nr_u += emit_block(ublock[a]);
     if (pos > 0xfffffff0ull) {
       err = "a CTA stream exceeds 4 GiB; use more CTAs";
+      return HBX_ERR_INVALID;
+    }
+    if (info.nr_p + info.nr_d + info.nr_u > (uint32_t)kMaxCtaRuns) {
+      err = "a CTA holds more than " + std::to_string(kMaxCtaRuns) + " runs; use more CTAs";
       return HBX_ERR_INVALID;
     }
     info.stream_bytes = (uint32_t)pos;  // a multiple of 16 by construction

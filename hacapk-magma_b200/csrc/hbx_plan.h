@@ -24,18 +24,19 @@
 // A block is stored as panels of column groups, each h x G row-major with
 // 16-byte rows: G = 2 double columns (FP64 storage) or G = 4 float columns
 // (FP32 storage).  One 16-byte shared-memory load then gives a lane one row
-// of G columns, and the 32 lanes of a warp read h*16 consecutive bytes, free
-// of bank conflicts.  A block's last panel is filled with zero columns.  A
-// block's columns are cut into RUNS that fit the 8 KB vector stage buffer
-// (1024 doubles or 2048 floats); all CTA data is one
-// contiguous byte stream (P runs, then D runs, then U runs) that the kernel
-// moves into shared memory with 1D bulk copies, so every byte of H crosses
-// HBM once per matvec.
+// of G columns (and a second load row i + 32 in P slabs taller than 32), and
+// the 32 lanes of a warp read h*16 consecutive bytes, free of bank
+// conflicts.  A block's last panel is filled with zero columns.  A block's
+// columns are cut into RUNS that fit the 8 KB vector stage buffer (1024
+// doubles or 2048 floats) and a run record; all CTA data is one contiguous
+// byte stream (P runs, then D runs, then U runs) that the kernel moves into
+// shared memory with 1D bulk copies, so every byte of H crosses HBM once per
+// matvec.
 //
-// Each run has a fixed-size record (header + gather segments).  A gather
-// warp reads the records and fills a ring of kStages vector stage buffers
-// with cp.async, several runs ahead of the consumer warps, so no gather
-// latency and no CTA-wide barrier sits between two runs.
+// Each run has a fixed-size record (header + gather segments) and a 16-byte
+// summary (RunLite).  Gather warps read the records and fill a ring of
+// kStages vector stage buffers with cp.async, runs ahead of the consumer
+// warps; the consumer warps keep the CTA's summaries in shared memory.
 #pragma once
 
 #include <cstddef>
@@ -55,7 +56,7 @@ namespace hbx {
 
 constexpr int kAtomMax = 32;       // rows per D/U block (one lane per row)
 constexpr int kSlabMax = 64;       // rows per P slab (two rows per lane)
-constexpr int kConsumerWarps = 16; // warps that compute (+ a producer and a descriptor warp)
+constexpr int kConsumerWarps = 16; // warps that multiply (+ producer, gather, grid-barrier and block-sum warps)
 #ifndef HBX_CHUNK_LOG
 #define HBX_CHUNK_LOG 15
 #endif
@@ -67,14 +68,15 @@ constexpr int kChunkBytes = 1 << kChunkLog;
 constexpr int kRingChunks = HBX_RING_CHUNKS;  // 128 KB ring per CTA
 constexpr int kStageBytes = 8192;  // one vector stage buffer: 1024 doubles or 2048 floats
 constexpr int kStageCap = kStageBytes / 8;  // doubles per stage buffer
-constexpr int kRunSegs = 60;       // gather segments per run record
+constexpr int kRunSegs = 124;      // gather segments per run record
 constexpr int kSegShort = 32;      // a segment this long or shorter is copied by one gather lane;
                                    // a longer one by the whole gather warp
-constexpr int kRecBytes = 512;     // one run record: 32-byte header + kRunSegs segments (16 B per lane)
+constexpr int kRecBytes = 1024;    // one run record: 32-byte header + kRunSegs segments
 #ifndef HBX_STAGES
 #define HBX_STAGES 4
 #endif
 constexpr int kStages = HBX_STAGES;  // vector stage buffers: runs gathered ahead of the consumers
+constexpr int kMaxCtaRuns = 1024;    // run summaries a CTA keeps in shared memory
 
 enum RunKind : uint16_t { kRunP = 0, kRunD = 1, kRunU = 2 };
 enum RunFlags : uint16_t { kFirst = 0x100, kLast = 0x200 };
@@ -109,6 +111,19 @@ struct alignas(16) Run {
 };
 static_assert(sizeof(Run) == 32, "Run must stay 32 bytes");
 
+// What the consumer and block-sum warps need of a run (16 bytes, kept in
+// shared memory for the whole launch).
+struct alignas(16) RunLite {
+  uint32_t pos;     // byte offset of the run's panels in the CTA stream
+  uint32_t out;     // first output row: zbu index (P) or y row (D, U)
+  uint16_t npanel;  // column-group panels
+  uint8_t nrow;     // h: 1..32 (1..64 for P)
+  uint8_t rot;      // consumer warp that takes panel 0
+  uint16_t flags;   // RunKind | RunFlags
+  uint16_t pad;
+};
+static_assert(sizeof(RunLite) == 16, "RunLite layout");
+
 struct alignas(16) RunRec {
   Run hdr;
   Seg seg[kRunSegs];
@@ -121,10 +136,11 @@ HBX_HD inline uint32_t run_bytes(const Run &r) { return 16u * r.nrow * r.npanel;
 struct CtaInfo {
   uint64_t stream_off;    // byte offset of the CTA stream in the packed buffer
   uint32_t stream_bytes;  // multiple of 16
-  uint32_t rec_begin;     // first run record of the CTA (P, D, U runs in order)
+  uint32_t rec_begin;     // first run record (and summary) of the CTA (P, D, U runs in order)
   uint32_t nr_p, nr_d, nr_u;
   uint32_t atom_begin, n_atoms;  // owned atoms (rows written by this CTA)
-  uint32_t pad[7];
+  uint32_t nblk_p;               // P blocks (slabs) of the CTA
+  uint32_t pad[6];
 };
 static_assert(sizeof(CtaInfo) == 64, "CtaInfo layout");
 
@@ -153,6 +169,7 @@ struct Plan {
   int precision = kFP64;
   std::vector<Atom> atoms;          // in CTA order (atom_begin indexes this)
   std::vector<RunRec> recs;         // in CTA order
+  std::vector<RunLite> lite;        // one summary per record, same order
   std::vector<CtaInfo> ctas;
   std::vector<Block> blocks;
   std::vector<Piece> pieces;

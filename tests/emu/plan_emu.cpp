@@ -43,13 +43,18 @@ extern "C" int emu_matvec_prec(const stc_HACApK_leafmtxp *st, int nd, int num_ct
     if (ci.stream_off % 256 != 0 || ci.stream_bytes % 16 != 0) return "stream alignment";
     if (ci.stream_off + ci.stream_bytes > plan.total_bytes) return "stream outside buffer";
     const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
-    if ((uint64_t)ci.rec_begin + nr > plan.recs.size()) return "records outside the record array";
+    if ((uint64_t)ci.rec_begin + nr > plan.recs.size() || plan.lite.size() != plan.recs.size())
+      return "records outside the record array";
     uint32_t pos = 0;
     for (uint32_t k = 0; k < nr; ++k) {
       const Run &r = plan.recs[ci.rec_begin + k].hdr;
       const uint32_t want = k < ci.nr_p ? kRunP : (k < ci.nr_p + ci.nr_d ? kRunD : kRunU);
       if (run_kind(r) != want) return "run kind out of section order";
       if (r.nrow == 0 || r.nrow > (want == kRunP ? kSlabMax : kAtomMax)) return "run height outside 1..32 (1..64 for P)";
+      const RunLite &L = plan.lite[ci.rec_begin + k];
+      if (L.pos != r.pos || L.out != r.out || L.npanel != r.npanel || L.nrow != r.nrow || L.rot != r.rot ||
+          L.flags != r.flags)
+        return "run summary does not match its record";
       if (G * r.npanel * elem_bytes(precision) > (uint32_t)kStageBytes || r.vlen > G * r.npanel ||
           (r.npanel > 0 && r.vlen + G <= G * r.npanel))
         return "run width";
