@@ -310,6 +310,19 @@ __device__ __forceinline__ void for_own_rows(const Atom *atoms, const CtaInfo &c
   }
 }
 
+// The same with the warp's first atom (index w) already loaded (a0; h = 0
+// when the CTA owns fewer atoms), so the loop does not start with a
+// dependent load.
+template <class F>
+__device__ __forceinline__ void for_own_rows(const Atom *atoms, const CtaInfo &ci, const Atom &a0, F f) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if ((uint32_t)lane < a0.h) f(a0.r0 + lane);
+  for (uint32_t q = w + NW; q < ci.n_atoms; q += NW) {
+    const Atom A = atoms[ci.atom_begin + q];
+    if ((uint32_t)lane < A.h) f(A.r0 + lane);
+  }
+}
+
 // Per-CTA compensated partial sums of NS dot products over the owned rows.
 // acc[] holds the calling thread's partials; the result goes to part[cta][slot0+k].
 template <int NSL>
@@ -339,12 +352,25 @@ __device__ __forceinline__ void cta_partials(Acc2 (&acc)[NSL], double *part, int
 }
 
 // Total of one slot over all CTAs, same operation order in every CTA (full warp).
+// (The loads of a lane are issued together, then merged in CTA order; a
+// merge with a zero pair leaves the sum unchanged.)
 __device__ __forceinline__ double reduce_slot(const double *part, int ncta, int slot) {
+  constexpr int kBatch = 5;
   const int lane = threadIdx.x & 31;
   Acc2 a{0.0, 0.0};
-  for (int c = lane; c < ncta; c += 32) {
-    const double *src = part + ((size_t)c * kSlots + slot) * 2;
-    a = acc2_merge(a, Acc2{__ldcg(src), __ldcg(src + 1)});
+  for (int c0 = 0; c0 < ncta; c0 += 32 * kBatch) {
+    Acc2 v[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      const int c = c0 + lane + 32 * k;
+      v[k] = Acc2{0.0, 0.0};
+      if (c < ncta) {
+        const double *src = part + ((size_t)c * kSlots + slot) * 2;
+        v[k] = Acc2{__ldcg(src), __ldcg(src + 1)};
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) a = acc2_merge(a, v[k]);
   }
   a = warp_merge(a);
   return a.s + a.c;
@@ -404,6 +430,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   };
   const uint64_t t_start = a.prof ? gtimer() : 0;
   const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
+  // a consumer warp's first owned atom, loaded while the step's scalars are reduced
+  const Atom a0 = (w < NW && (uint32_t)w < ci.n_atoms) ? a.atoms[ci.atom_begin + w] : Atom{0, 0};
   init_cta(sm, a.lite + ci.rec_begin, nr);
 
   // ---- S0: scalars of the previous step; stop test at the top of the loop
@@ -504,13 +532,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
 
   // ---- S1: p = r + beta*(p - zeta*Ap)  (p = r on the first step)
   if (beta == 0.0) {
-    for_own_rows(a.atoms, ci, [&](uint32_t r) {
+    for_own_rows(a.atoms, ci, a0, [&](uint32_t r) {
       const double v = a.r[r];
       a.p[r] = v;
       if (kF32) a.p32[r] = (float)v;
     });
   } else {
-    for_own_rows(a.atoms, ci, [&](uint32_t r) {
+    for_own_rows(a.atoms, ci, a0, [&](uint32_t r) {
       // p through L2 only: a line of p cached in L1 here could hold rows of
       // another CTA that the gather warps read after it rewrote them
       const double v = fma(-zeta_prev, a.ap[r], __ldcg(&a.p[r])) * beta;
@@ -538,7 +566,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   {
     Acc2 acc[1] = {{0, 0}};
     named_bar(1, kConsumerThreads);
-    for_own_rows(a.atoms, ci, [&](uint32_t r) { dot2_add(acc[0], a.rh[r], a.ap[r]); });
+    for_own_rows(a.atoms, ci, a0, [&](uint32_t r) { dot2_add(acc[0], a.rh[r], a.ap[r]); });
     cta_partials<1>(acc, a.part, kSlotRhAp, sm);
   }
   grid_sync(a.gbar, a.err, a.timeout_ns, sm);
@@ -551,7 +579,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   stamp(3);
 
   // ---- S3: t = r - alpha*Ap
-  for_own_rows(a.atoms, ci, [&](uint32_t r) {
+  for_own_rows(a.atoms, ci, a0, [&](uint32_t r) {
     const double v = fma(-alpha, a.ap[r], a.r[r]);
     a.t[r] = v;
     if (kF32) a.t32[r] = (float)v;
@@ -568,7 +596,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   {
     Acc2 acc[2] = {{0, 0}, {0, 0}};
     named_bar(1, kConsumerThreads);
-    for_own_rows(a.atoms, ci, [&](uint32_t r) {
+    for_own_rows(a.atoms, ci, a0, [&](uint32_t r) {
       const double atv = a.at[r];
       dot2_add(acc[0], atv, a.t[r]);
       dot2_add(acc[1], atv, atv);
@@ -601,7 +629,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   // ---- S5: u += alpha*p + zeta*t;  r = t - zeta*At;  rh . r,  r . r
   {
     Acc2 acc[2] = {{0, 0}, {0, 0}};
-    for_own_rows(a.atoms, ci, [&](uint32_t r) {
+    for_own_rows(a.atoms, ci, a0, [&](uint32_t r) {
       const double uv = fma(alpha, a.p[r], a.u[r]);
       a.u[r] = fma(zeta, a.t[r], uv);
       const double rv = fma(-zeta, a.at[r], a.t[r]);
