@@ -62,7 +62,7 @@ struct SharedLayout {
   static constexpr uint32_t gdone = pdone + 8;                               // every CTA's zbu is complete
   static constexpr uint32_t redfull = gdone + 8;                             // [kRedSlots] a block's partials parked
   static constexpr uint32_t rdone = redfull + 8 * kRedSlots;                 // a pass's block sums are written
-  static constexpr uint32_t rsum = rdone + 8;                                // block ends summed so far
+  static constexpr uint32_t rsum = rdone + 8;                                // block ends summed so far; [1]: grid gen0
   static constexpr uint32_t bytes = rsum + 16;
 };
 static_assert(SharedLayout::red % 16 == 0 && SharedLayout::stage % 16 == 0 && SharedLayout::lite % 16 == 0 &&
@@ -204,25 +204,33 @@ __device__ __forceinline__ double2 lds_f64x2(uint32_t addr) {
   return v;
 }
 
-// ---- grid barrier: gbar[0] = arrivals, gbar[1] = generation ---------------
-__device__ __forceinline__ void grid_arrive(unsigned *gbar, unsigned nblocks) {
+// ---- grid barrier -----------------------------------------------------------
+// gbar[0] counts arrivals and gbar[1] completed barrier instances, both since
+// the words were last cleared and modulo 2^32.  A launch reads gbar[1] once
+// at its start (grid_gen0; no instance of the launch can complete before
+// every CTA has started), numbers its instances k = 0, 1, ... in the same
+// order in every CTA, and instance k is complete once gbar[0] has reached
+// nblocks * (gen0 + k + 1).  The last arriver also advances gbar[1] for the
+// next launch; nobody waits for that.  A CTA arrives on instance k + 1 only
+// after it has seen instance k complete.
+__device__ __forceinline__ unsigned grid_gen0(const unsigned *gbar) { return ld_acquire(&gbar[1]); }
+__device__ __forceinline__ unsigned grid_target(unsigned gen0, unsigned k, unsigned nblocks) {
+  return nblocks * (gen0 + k + 1u);
+}
+__device__ __forceinline__ void grid_arrive(unsigned *gbar, unsigned target) {
   __threadfence();
   const unsigned old = atomicAdd(&gbar[0], 1u);
-  if (old == nblocks - 1) {
-    atomicExch(&gbar[0], 0u);
-    __threadfence();
-    atomicAdd(&gbar[1], 1u);
-  }
+  if (old + 1u == target) atomicAdd(&gbar[1], 1u);
 }
 
 // The trailing fence (as in cooperative groups' grid sync) orders every later
 // load of the CTA -- after the caller's bar.sync -- behind the other CTAs'
 // pre-barrier writes.
-__device__ __forceinline__ bool grid_wait(const unsigned *gbar, unsigned gen, uint64_t timeout_ns) {
-  if (ld_acquire(&gbar[1]) == gen) {
+__device__ __forceinline__ bool grid_wait(const unsigned *gbar, unsigned target, uint64_t timeout_ns) {
+  if ((int)(ld_acquire(&gbar[0]) - target) < 0) {
     const uint64_t t0 = gtimer();
-    while (ld_acquire(&gbar[1]) == gen) {
-      __nanosleep(64);
+    while ((int)(ld_acquire(&gbar[0]) - target) < 0) {
+      __nanosleep(32);
       if (gtimer() - t0 > timeout_ns) return false;
     }
   }

@@ -63,9 +63,10 @@ __device__ __forceinline__ Smem smem_layout(uint8_t *base) {
   return s;
 }
 
-// Barriers, the block-sum counter and the CTA's run summaries (`lite`, nr of
-// them) in shared memory; every thread takes part.
-__device__ __forceinline__ void init_cta(const Smem &s, const RunLite *lite, uint32_t nr) {
+// Barriers, the block-sum counter, the launch's first grid-barrier generation
+// and the CTA's run summaries (`lite`, nr of them) in shared memory; every
+// thread takes part.
+__device__ __forceinline__ void init_cta(const Smem &s, const RunLite *lite, uint32_t nr, unsigned gen0) {
   if (threadIdx.x == 0) {
     for (int i = 0; i < kRingChunks; ++i) {
       mbar_init(&s.full[i], 1);
@@ -81,7 +82,8 @@ __device__ __forceinline__ void init_cta(const Smem &s, const RunLite *lite, uin
     mbar_init(s.gdone, 1);
     for (uint32_t i = 0; i < kRedSlots; ++i) mbar_init(&s.redfull[i], NW);
     mbar_init(s.rdone, 1);
-    *s.rsum = 0;
+    s.rsum[0] = 0;
+    s.rsum[1] = gen0;
     mbar_fence_init();
   }
   const uint4 *src = reinterpret_cast<const uint4 *>(lite);
@@ -93,15 +95,17 @@ __device__ __forceinline__ void init_cta(const Smem &s, const RunLite *lite, uin
 // ---- grid-barrier warp: once per pass, after the CTA's P blocks are summed
 // (pdone), arrive on the grid barrier, wait for it and release the U runs
 // (gdone).  The barrier latency stays off the consumer and gather warps.
-__device__ __forceinline__ void sync_warp(unsigned *gbar, uint32_t npass, const Smem &sm, int *err, uint64_t tmo) {
+// Pass p uses grid-barrier instance k0 + p * kstep of the launch.
+__device__ __forceinline__ void sync_warp(unsigned *gbar, uint32_t npass, uint32_t k0, uint32_t kstep, const Smem &sm,
+                                          int *err, uint64_t tmo) {
   for (uint32_t p = 0; p < npass; ++p) {
     if (!mbar_wait(sm.pdone, p & 1, tmo)) {
       atomicOr(err, kErrPipeline);
       return;  // the waits on gdone are bounded too
     }
-    const unsigned gen = ld_acquire(&gbar[1]);
-    grid_arrive(gbar, gridDim.x);  // fences first: the CTA's zbu stores are visible grid-wide
-    if (!grid_wait(gbar, gen, tmo)) {
+    const unsigned target = grid_target(sm.rsum[1], k0 + p * kstep, gridDim.x);
+    grid_arrive(gbar, target);  // fences first: the CTA's zbu stores are visible grid-wide
+    if (!grid_wait(gbar, target, tmo)) {
       atomicOr(err, kErrGridBarrier);
       return;
     }
@@ -266,7 +270,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   const CtaInfo ci = a.ctas[blockIdx.x];
   const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
   const uint64_t t_start = a.prof ? gtimer() : 0;
-  init_cta(sm, a.lite + ci.rec_begin, nr);
+  init_cta(sm, a.lite + ci.rec_begin, nr, threadIdx.x == 0 ? grid_gen0(a.gbar) : 0u);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
   if (w == kProducerWarp) {
@@ -282,7 +286,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
     return;
   }
   if (w == kSyncWarp) {
-    if (lane == 0) sync_warp(a.gbar, 1, sm, a.err, a.timeout_ns);
+    if (lane == 0) sync_warp(a.gbar, 1, 0, 0, sm, a.err, a.timeout_ns);
     return;
   }
   const PassOut o{a.alpha, a.beta, a.yin, a.y, a.zbu, kF32 ? a.zbu32 : nullptr, 0, ci.nblk_p};
@@ -376,14 +380,20 @@ __device__ __forceinline__ double reduce_slot(const double *part, int ncta, int 
   return a.s + a.c;
 }
 
-// Full grid barrier among the consumer warps of every CTA.
-__device__ __forceinline__ bool grid_sync(unsigned *gbar, int *err, uint64_t timeout_ns, const Smem &sm) {
+// Grid-barrier instances of one BiCGSTAB step, in order: p complete, zbu of
+// the first H-matvec complete, the r^.Ap partials, t complete, zbu of the
+// second H-matvec, the At.t / At.At partials.
+enum : unsigned { kGridP = 0, kGridPass0 = 1, kGridAlpha = 2, kGridT = 3, kGridPass1 = 4, kGridZeta = 5 };
+
+// Full grid barrier (instance k of the launch) among the consumer warps of
+// every CTA.
+__device__ __forceinline__ bool grid_sync(unsigned *gbar, unsigned k, int *err, uint64_t timeout_ns, const Smem &sm) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   named_bar(1, kConsumerThreads);
   if (w == 0 && lane == 0) {
-    const unsigned gen = ld_acquire(&gbar[1]);
-    grid_arrive(gbar, gridDim.x);
-    const bool ok = grid_wait(gbar, gen, timeout_ns);
+    const unsigned target = grid_target(sm.rsum[1], k, gridDim.x);
+    grid_arrive(gbar, target);
+    const bool ok = grid_wait(gbar, target, timeout_ns);
     if (!ok) atomicOr(err, kErrGridBarrier);
     sm.scal[62] = ok ? 1.0 : 0.0;
   }
@@ -432,7 +442,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
   // a consumer warp's first owned atom, loaded while the step's scalars are reduced
   const Atom a0 = (w < NW && (uint32_t)w < ci.n_atoms) ? a.atoms[ci.atom_begin + w] : Atom{0, 0};
-  init_cta(sm, a.lite + ci.rec_begin, nr);
+  init_cta(sm, a.lite + ci.rec_begin, nr, threadIdx.x == 0 ? grid_gen0(a.gbar) : 0u);
 
   // ---- S0: scalars of the previous step; stop test at the top of the loop
   // (HACApK_SOLVER.c:602-603).  Every CTA computes identical values: warps
@@ -515,7 +525,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     return;
   }
   if (w == kSyncWarp) {
-    if (lane == 0) sync_warp(a.gbar, 2, sm, a.err, a.timeout_ns);
+    if (lane == 0) sync_warp(a.gbar, 2, kGridPass0, kGridPass1 - kGridPass0, sm, a.err, a.timeout_ns);
     return;
   }
   // The two H-matvecs write separate zbu copies, so a U run of the second
@@ -548,7 +558,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     });
   }
   __threadfence();
-  grid_sync(a.gbar, a.err, a.timeout_ns, sm);
+  grid_sync(a.gbar, kGridP, a.err, a.timeout_ns, sm);
   if (threadIdx.x == 0) mbar_arrive(sm.xready);  // p complete grid-wide: pass 0 may be gathered
   stamp(1);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -569,7 +579,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     for_own_rows(a.atoms, ci, a0, [&](uint32_t r) { dot2_add(acc[0], a.rh[r], a.ap[r]); });
     cta_partials<1>(acc, a.part, kSlotRhAp, sm);
   }
-  grid_sync(a.gbar, a.err, a.timeout_ns, sm);
+  grid_sync(a.gbar, kGridAlpha, a.err, a.timeout_ns, sm);
   if (w == 0) {
     const double zden = reduce_slot(a.part, ncta, kSlotRhAp);
     if (lane == 0) sm.scal[8] = rho / zden;
@@ -585,7 +595,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     if (kF32) a.t32[r] = (float)v;
   });
   __threadfence();
-  grid_sync(a.gbar, a.err, a.timeout_ns, sm);
+  grid_sync(a.gbar, kGridT, a.err, a.timeout_ns, sm);
   if (threadIdx.x == 0) mbar_arrive(sm.xready);  // t complete grid-wide: pass 1 may be gathered
   stamp(4);
 
@@ -603,7 +613,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     });
     cta_partials<2>(acc, a.part, kSlotAtT, sm);
   }
-  grid_sync(a.gbar, a.err, a.timeout_ns, sm);
+  grid_sync(a.gbar, kGridZeta, a.err, a.timeout_ns, sm);
   if (w < 2) {  // the two sums side by side
     const double v = reduce_slot(a.part, ncta, w == 0 ? kSlotAtT : kSlotAtAt);
     if (lane == 0) sm.scal[10 + w] = v;
