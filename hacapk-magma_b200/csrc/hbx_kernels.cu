@@ -64,10 +64,12 @@ __device__ __forceinline__ Smem smem_layout(uint8_t *base) {
 }
 
 // Barriers, the block-sum counter, the launch's first grid-barrier generation
-// and the CTA's run summaries (`lite`, nr of them) in shared memory; every
-// thread takes part.
-__device__ __forceinline__ void init_cta(const Smem &s, const RunLite *lite, uint32_t nr, unsigned gen0) {
-  if (threadIdx.x == 0) {
+// and the CTA's run summaries (`lite`, nr of them) in shared memory.  Thread
+// t0 sets up the barriers; threads t0 and up copy the summaries.  The caller
+// synchronises the CTA afterwards.
+__device__ __forceinline__ void init_cta_part(const Smem &s, const RunLite *lite, uint32_t nr, const unsigned *gbar,
+                                              uint32_t t0) {
+  if (threadIdx.x == t0) {
     for (int i = 0; i < kRingChunks; ++i) {
       mbar_init(&s.full[i], 1);
       mbar_init(&s.empty[i], NW);
@@ -83,12 +85,17 @@ __device__ __forceinline__ void init_cta(const Smem &s, const RunLite *lite, uin
     for (uint32_t i = 0; i < kRedSlots; ++i) mbar_init(&s.redfull[i], NW);
     mbar_init(s.rdone, 1);
     s.rsum[0] = 0;
-    s.rsum[1] = gen0;
+    s.rsum[1] = grid_gen0(gbar);
     mbar_fence_init();
   }
+  if (threadIdx.x < t0) return;
   const uint4 *src = reinterpret_cast<const uint4 *>(lite);
   uint4 *dst = reinterpret_cast<uint4 *>(s.lite);
-  for (uint32_t k = threadIdx.x; k < nr; k += blockDim.x) dst[k] = __ldg(src + k);
+  for (uint32_t k = threadIdx.x - t0; k < nr; k += blockDim.x - t0) dst[k] = __ldg(src + k);
+}
+
+__device__ __forceinline__ void init_cta(const Smem &s, const RunLite *lite, uint32_t nr, const unsigned *gbar) {
+  init_cta_part(s, lite, nr, gbar, 0);
   __syncthreads();
 }
 
@@ -270,7 +277,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   const CtaInfo ci = a.ctas[blockIdx.x];
   const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
   const uint64_t t_start = a.prof ? gtimer() : 0;
-  init_cta(sm, a.lite + ci.rec_begin, nr, threadIdx.x == 0 ? grid_gen0(a.gbar) : 0u);
+  init_cta(sm, a.lite + ci.rec_begin, nr, a.gbar);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
   if (w == kProducerWarp) {
@@ -314,13 +321,10 @@ __device__ __forceinline__ void for_own_rows(const Atom *atoms, const CtaInfo &c
   }
 }
 
-// The same with the warp's first atom (index w) already loaded (a0; h = 0
-// when the CTA owns fewer atoms), so the loop does not start with a
-// dependent load.
+// The same over the warp's atoms after its first one (index w + NW, ...).
 template <class F>
-__device__ __forceinline__ void for_own_rows(const Atom *atoms, const CtaInfo &ci, const Atom &a0, F f) {
+__device__ __forceinline__ void for_more_rows(const Atom *atoms, const CtaInfo &ci, F f) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if ((uint32_t)lane < a0.h) f(a0.r0 + lane);
   for (uint32_t q = w + NW; q < ci.n_atoms; q += NW) {
     const Atom A = atoms[ci.atom_begin + q];
     if ((uint32_t)lane < A.h) f(A.r0 + lane);
@@ -440,9 +444,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   };
   const uint64_t t_start = a.prof ? gtimer() : 0;
   const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
-  // a consumer warp's first owned atom, loaded while the step's scalars are reduced
+  // A consumer warp's first owned atom and this lane's row of it: its vector
+  // entries stay in registers through the step, loaded while the step's
+  // scalars are reduced (the rows of further atoms are read where needed).
   const Atom a0 = (w < NW && (uint32_t)w < ci.n_atoms) ? a.atoms[ci.atom_begin + w] : Atom{0, 0};
-  init_cta(sm, a.lite + ci.rec_begin, nr, threadIdx.x == 0 ? grid_gen0(a.gbar) : 0u);
+  const bool own0 = (uint32_t)lane < a0.h;
+  const uint32_t row0 = a0.r0 + lane;
+  double c_r = 0.0, c_rh = 0.0, c_p = 0.0, c_ap = 0.0, c_u = 0.0, c_t = 0.0, c_at = 0.0;
+  if (own0) {
+    c_r = a.r[row0];
+    c_rh = a.rh[row0];
+    c_p = __ldcg(&a.p[row0]);  // see S1
+    c_ap = a.ap[row0];
+    c_u = a.u[row0];
+  }
+  // warps 4 and up set up the CTA while warps 0-3 reduce the scalars
+  init_cta_part(sm, a.lite + ci.rec_begin, nr, a.gbar, 128);
 
   // ---- S0: scalars of the previous step; stop test at the top of the loop
   // (HACApK_SOLVER.c:602-603).  Every CTA computes identical values: warps
@@ -541,14 +558,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   uint32_t nb = 0;
 
   // ---- S1: p = r + beta*(p - zeta*Ap)  (p = r on the first step)
+  if (own0) {
+    c_p = (beta == 0.0) ? c_r : fma(-zeta_prev, c_ap, c_p) * beta + c_r;
+    a.p[row0] = c_p;
+    if (kF32) a.p32[row0] = (float)c_p;
+  }
   if (beta == 0.0) {
-    for_own_rows(a.atoms, ci, a0, [&](uint32_t r) {
+    for_more_rows(a.atoms, ci, [&](uint32_t r) {
       const double v = a.r[r];
       a.p[r] = v;
       if (kF32) a.p32[r] = (float)v;
     });
   } else {
-    for_own_rows(a.atoms, ci, a0, [&](uint32_t r) {
+    for_more_rows(a.atoms, ci, [&](uint32_t r) {
       // p through L2 only: a line of p cached in L1 here could hold rows of
       // another CTA that the gather warps read after it rewrote them
       const double v = fma(-zeta_prev, a.ap[r], __ldcg(&a.p[r])) * beta;
@@ -576,7 +598,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   {
     Acc2 acc[1] = {{0, 0}};
     named_bar(1, kConsumerThreads);
-    for_own_rows(a.atoms, ci, a0, [&](uint32_t r) { dot2_add(acc[0], a.rh[r], a.ap[r]); });
+    if (own0) {
+      c_ap = a.ap[row0];
+      dot2_add(acc[0], c_rh, c_ap);
+    }
+    for_more_rows(a.atoms, ci, [&](uint32_t r) { dot2_add(acc[0], a.rh[r], a.ap[r]); });
     cta_partials<1>(acc, a.part, kSlotRhAp, sm);
   }
   grid_sync(a.gbar, kGridAlpha, a.err, a.timeout_ns, sm);
@@ -589,7 +615,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   stamp(3);
 
   // ---- S3: t = r - alpha*Ap
-  for_own_rows(a.atoms, ci, a0, [&](uint32_t r) {
+  if (own0) {
+    c_t = fma(-alpha, c_ap, c_r);
+    a.t[row0] = c_t;
+    if (kF32) a.t32[row0] = (float)c_t;
+  }
+  for_more_rows(a.atoms, ci, [&](uint32_t r) {
     const double v = fma(-alpha, a.ap[r], a.r[r]);
     a.t[r] = v;
     if (kF32) a.t32[r] = (float)v;
@@ -606,7 +637,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   {
     Acc2 acc[2] = {{0, 0}, {0, 0}};
     named_bar(1, kConsumerThreads);
-    for_own_rows(a.atoms, ci, a0, [&](uint32_t r) {
+    if (own0) {
+      c_at = a.at[row0];
+      dot2_add(acc[0], c_at, c_t);
+      dot2_add(acc[1], c_at, c_at);
+    }
+    for_more_rows(a.atoms, ci, [&](uint32_t r) {
       const double atv = a.at[r];
       dot2_add(acc[0], atv, a.t[r]);
       dot2_add(acc[1], atv, atv);
@@ -639,7 +675,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   // ---- S5: u += alpha*p + zeta*t;  r = t - zeta*At;  rh . r,  r . r
   {
     Acc2 acc[2] = {{0, 0}, {0, 0}};
-    for_own_rows(a.atoms, ci, a0, [&](uint32_t r) {
+    if (own0) {
+      a.u[row0] = fma(zeta, c_t, fma(alpha, c_p, c_u));
+      const double rv = fma(-zeta, c_at, c_t);
+      a.r[row0] = rv;
+      dot2_add(acc[0], c_rh, rv);
+      dot2_add(acc[1], rv, rv);
+    }
+    for_more_rows(a.atoms, ci, [&](uint32_t r) {
       const double uv = fma(alpha, a.p[r], a.u[r]);
       a.u[r] = fma(zeta, a.t[r], uv);
       const double rv = fma(-zeta, a.at[r], a.t[r]);
