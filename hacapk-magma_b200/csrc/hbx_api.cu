@@ -64,6 +64,7 @@ void free_engine(hbx_hmat *h) {
   cudaFree(h->d_hist);
   cudaFree(h->d_refine);
   cudaFree(h->d_f32);
+  cudaFree(h->d_zbum);
   if (h->h_pin) cudaFreeHost(h->h_pin);
   if (h->h_state) cudaFreeHost(h->h_state);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -180,6 +181,10 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hb
   if (nd <= 0) return fail(HBX_ERR_INVALID, "hbx_create: nd <= 0");
   if (opt && opt->precision != HBX_FP64 && opt->precision != HBX_FP32)
     return fail(HBX_ERR_UNSUPPORTED, "hbx_create: precision must be HBX_FP64 or HBX_FP32");
+  const int nrhs = (opt && opt->nrhs > 1) ? opt->nrhs : 1;
+  if (nrhs != 1 && nrhs != hbx::kNrhs) return fail(HBX_ERR_UNSUPPORTED, "hbx_create: nrhs must be 0, 1 or HBX_NRHS");
+  if (nrhs > 1 && opt->precision != HBX_FP32)
+    return fail(HBX_ERR_UNSUPPORTED, "hbx_create: a multi-RHS engine needs precision HBX_FP32");
   const double t0 = now_s();
   hbx_hmat *h = new (std::nothrow) hbx_hmat();
   if (!h) return fail(HBX_ERR_NOMEM, "hbx_create: host allocation");
@@ -190,6 +195,8 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hb
   if ((e = cudaGetDeviceProperties(&prop, h->device)) != cudaSuccess) return bail(cuda_fail(e, "cudaGetDeviceProperties"));
   if (prop.major < 10) return bail(fail(HBX_ERR_UNSUPPORTED, "hbx_create: needs an sm_100 device"));
   if ((e = hbx::configure_kernels()) != cudaSuccess) return bail(cuda_fail(e, "configure_kernels"));
+  if ((e = hbx::configure_matmat()) != cudaSuccess) return bail(cuda_fail(e, "configure_matmat"));
+  h->nrhs = nrhs;
   int coop = 0;
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->device);
   if (!coop) return bail(fail(HBX_ERR_UNSUPPORTED, "hbx_create: device lacks cooperative launch"));
@@ -214,7 +221,8 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hb
     st = &tleaves.container;
     h->transposed = 1;
   }
-  int st_plan = hbx::make_plan(st, nd, nc, h->plan, err, (opt && opt->precision == HBX_FP32) ? hbx::kFP32 : hbx::kFP64);
+  int st_plan = hbx::make_plan(st, nd, nc, h->plan, err, (opt && opt->precision == HBX_FP32) ? hbx::kFP32 : hbx::kFP64,
+                               nrhs > 1);
   if (st_plan != HBX_OK) return bail(fail(st_plan, "hbx_create: " + err));
   const hbx::Plan &P = h->plan;
 
@@ -247,6 +255,9 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hb
       (e = cudaMalloc(&h->d_f32, (3 * (size_t)nd + 2 * std::max<uint64_t>(1, P.zbu_len)) * sizeof(float))) !=
           cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(float copies)"));
+  if (nrhs > 1 &&
+      (e = cudaMalloc(&h->d_zbum, std::max<uint64_t>(1, P.zbu_len) * hbx::kNrhs * sizeof(float))) != cudaSuccess)
+    return bail(cuda_fail(e, "cudaMalloc(multi-RHS zbu)"));
   if ((e = cudaMalloc(&h->d_gbar, 4 * sizeof(unsigned))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(gbar)"));
   if ((e = cudaMalloc(&h->d_err, sizeof(int))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(err)"));
   if ((e = cudaMemcpy(h->d_stream, host.data(), P.total_bytes, cudaMemcpyHostToDevice)) != cudaSuccess)
@@ -320,10 +331,43 @@ int hbx_get_info(const hbx_hmat *h, hbx_info *info) {
   info->lowrank_words = (long long)P.lowrank_words;
   info->setup_seconds = h->setup_seconds;
   info->transposed = h->transposed;
+  info->nrhs = h->nrhs;
+  return HBX_OK;
+}
+
+// The single-vector calls on a multi-RHS engine (its stream is laid out for
+// the tensor-core product only).
+static int single_rhs(const hbx_hmat *h, const char *where) {
+  if (h && h->nrhs > 1) return fail(HBX_ERR_UNSUPPORTED, std::string(where) + ": a multi-RHS engine takes hbx_matmat only");
+  return HBX_OK;
+}
+
+int hbx_matmat(hbx_hmat *h, double alpha, const float *X, double beta, const double *Yin, double *Y, void *stream) {
+  if (!h || !X || !Y) return fail(HBX_ERR_INVALID, "hbx_matmat: NULL argument");
+  if (h->nrhs != hbx::kNrhs) return fail(HBX_ERR_UNSUPPORTED, "hbx_matmat: not a multi-RHS engine (hbx_options.nrhs)");
+  if (beta != 0.0 && !Yin) return fail(HBX_ERR_INVALID, "hbx_matmat: beta != 0 needs Yin");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  hbx::MatmatArgs a{};
+  a.stream = h->d_stream;
+  a.recs = h->d_recs;
+  a.ctas = h->d_ctas;
+  a.lite = h->d_lite;
+  a.x = X;
+  a.yin = Yin;
+  a.y = Y;
+  a.zbu = h->d_zbum;
+  a.alpha = alpha;
+  a.beta = beta;
+  a.gbar = h->d_gbar;
+  a.err = h->d_err;
+  a.timeout_ns = h->timeout_ns;
+  cudaError_t e = hbx::launch_matmat(a, h->num_ctas, s);
+  if (e != cudaSuccess) return cuda_fail(e, "hbx_matmat launch");
   return HBX_OK;
 }
 
 int hbx_matvec(hbx_hmat *h, double alpha, const double *x, double beta, const double *yin, double *y, void *stream) {
+  if (int rc = single_rhs(h, "hbx_matvec")) return rc;
   if (!h || !x || !y) return fail(HBX_ERR_INVALID, "hbx_matvec: NULL argument");
   if (beta != 0.0 && !yin) return fail(HBX_ERR_INVALID, "hbx_matvec: beta != 0 needs yin");
   cudaError_t e = mv_launch(h, matvec_args(h, alpha, x, beta, yin, y), (cudaStream_t)stream);
@@ -346,6 +390,7 @@ static void *g_noalloc_ptr[128] = {nullptr};
 int hbx_matvec_noalloc(hbx_hmat *h, double alpha, const double *x, double beta, const double *yin, double *y,
                        void *stream) {
   if (!h || !x || !y) return fail(HBX_ERR_INVALID, "hbx_matvec_noalloc: NULL argument");
+  if (int rc = single_rhs(h, "hbx_matvec_noalloc")) return rc;
   if (beta != 0.0 && !yin) return fail(HBX_ERR_INVALID, "hbx_matvec_noalloc: beta != 0 needs yin");
   if (h->plan.precision != hbx::kFP64)
     return fail(HBX_ERR_UNSUPPORTED, "hbx_matvec_noalloc: FP64 engines only (use hbx_matvec)");
@@ -391,6 +436,7 @@ int hbx_sync(hbx_hmat *h, void *stream) {
 int hbx_matvec_host(hbx_hmat *h, const double *zu, double *zau, int accumulate, double *kernel_seconds,
                     double *copy_seconds) {
   if (!h || !zu || !zau) return fail(HBX_ERR_INVALID, "hbx_matvec_host: NULL argument");
+  if (int rc = single_rhs(h, "hbx_matvec_host")) return rc;
   int st = ensure_host_staging(h);
   if (st != HBX_OK) return st;
   const size_t n = (size_t)h->plan.nd, bytes = n * sizeof(double);
@@ -480,6 +526,7 @@ static int get_graph(hbx_hmat *h, const hbx::BicgArgs &a, int batch) {
 
 // BiCGSTAB on device vectors b, u (u: x0 in / solution out), all on h->stream.
 static int bicgstab_dev(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info) {
+  if (int rc = single_rhs(h, "hbx_bicgstab")) return rc;
   const double tol = opts ? opts->tol : 1e-8;
   const int max_iter = opts ? opts->max_iter : 1000;
   const int verbose = opts ? opts->verbose : 0;
@@ -589,6 +636,8 @@ int hbx_bicgstab_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_o
 // residual; the last one is asked for no more than the outer tolerance needs.
 static int refined_dev(hbx_hmat *h, hbx_hmat *hl, const double *b, double *u, const hbx_solve_opts *opts,
                        hbx_solve_info *info) {
+  if (int rc = single_rhs(h, "hbx_bicgstab_refined")) return rc;
+  if (int rc = single_rhs(hl, "hbx_bicgstab_refined")) return rc;
   const double tol = opts ? opts->tol : 1e-8;
   const int max_iter = opts ? opts->max_iter : 1000;
   const double floor_tol = (opts && opts->inner_tol > 0.0) ? opts->inner_tol : 1e-6;
@@ -698,6 +747,8 @@ int hbx_gradient_host(hbx_hmat *h, hbx_hmat *ht, const double *g, const double *
                       double *grad, double *J, const hbx_solve_opts *opts, hbx_solve_info *fwd,
                       hbx_solve_info *adj) {
   if (!h || !ht || !g || !sigma_t || !sigma || !grad) return fail(HBX_ERR_INVALID, "hbx_gradient_host: NULL argument");
+  if (int rc = single_rhs(h, "hbx_gradient_host")) return rc;
+  if (int rc = single_rhs(ht, "hbx_gradient_host")) return rc;
   if (h->transposed || !ht->transposed)
     return fail(HBX_ERR_INVALID, "hbx_gradient_host: h must hold H and ht must hold H^T (hbx_options.transpose)");
   if (h->plan.nd != ht->plan.nd) return fail(HBX_ERR_INVALID, "hbx_gradient_host: h and ht differ in size");

@@ -239,13 +239,51 @@ __device__ __forceinline__ bool grid_wait(const unsigned *gbar, unsigned target,
 }
 
 // ---- producer: streams `npass` passes over the CTA's byte range ------------
-__device__ __forceinline__ void producer_run(const uint8_t *src, uint32_t bytes, uint32_t npass,
+// Chunk g of the launch (g = pass * K + k) covers stream bytes k * kChunkBytes
+// on, in ring slot g % kRingChunks.
+__device__ __forceinline__ void producer_issue(const uint8_t *src, uint32_t bytes, uint32_t K, uint32_t g,
+                                               uint8_t *ring, uint64_t *full) {
+  const uint32_t s = g % kRingChunks;
+  const uint32_t off = (g % K) << kChunkLog;
+  const uint32_t nb = min((uint32_t)kChunkBytes, bytes - off);
+  mbar_arrive_expect_tx(&full[s], nb);
+  bulk_g2s(ring + ((size_t)s << kChunkLog), src + off, nb, &full[s]);
+}
+
+// The producer thread's part of the CTA set-up, before the CTA's first
+// barrier: it sets up the ring's barriers and issues the first chunks (one
+// per ring slot, which needs no empty wait), so the stream is under way while
+// the other threads load the run summaries and reduce scalars.  Returns the
+// number of chunks issued; producer_run goes on from there.
+__device__ __forceinline__ uint32_t producer_start(const uint8_t *src, uint32_t bytes, uint32_t npass,
+                                                  uint8_t *ring, uint64_t *full, uint64_t *empty) {
+  for (int i = 0; i < kRingChunks; ++i) {
+    mbar_init(&full[i], 1);
+    mbar_init(&empty[i], kConsumerWarps);
+  }
+  mbar_fence_init();
+  const uint32_t K = (bytes + kChunkBytes - 1) >> kChunkLog;
+  const uint32_t n = min(K * npass, (uint32_t)kRingChunks);
+  for (uint32_t g = 0; g < n; ++g) producer_issue(src, bytes, K, g, ring, full);
+  return n;
+}
+
+// Bounded wait for chunks [g0, issued) -- copies still in flight must land
+// before the CTA exits.
+__device__ __forceinline__ void producer_drain(uint64_t *full, uint32_t issued, uint64_t timeout_ns) {
+  const uint32_t g0 = issued > (uint32_t)kRingChunks ? issued - kRingChunks : 0;
+  for (uint32_t g = g0; g < issued; ++g) mbar_wait(&full[g % kRingChunks], (g / kRingChunks) & 1, timeout_ns);
+}
+
+// The rest of the stream: chunk g once the consumers emptied chunk
+// g - kRingChunks.
+__device__ __forceinline__ void producer_run(const uint8_t *src, uint32_t bytes, uint32_t npass, uint32_t issued0,
                                              uint8_t *ring, uint64_t *full, uint64_t *empty, int *err,
                                              uint64_t timeout_ns) {
   const uint32_t K = (bytes + kChunkBytes - 1) >> kChunkLog;
   const uint32_t total = K * npass;
-  uint32_t issued = 0;
-  for (uint32_t g = 0; g < total; ++g) {
+  uint32_t issued = issued0;
+  for (uint32_t g = issued0; g < total; ++g) {
     const uint32_t s = g % kRingChunks;
     if (g >= (uint32_t)kRingChunks) {
       if (!mbar_wait(&empty[s], ((g / kRingChunks) - 1) & 1, timeout_ns)) {
@@ -253,16 +291,10 @@ __device__ __forceinline__ void producer_run(const uint8_t *src, uint32_t bytes,
         break;
       }
     }
-    const uint32_t k = g % K;
-    const uint32_t off = k << kChunkLog;
-    const uint32_t nb = min((uint32_t)kChunkBytes, bytes - off);
-    mbar_arrive_expect_tx(&full[s], nb);
-    bulk_g2s(ring + ((size_t)s << kChunkLog), src + off, nb, &full[s]);
+    producer_issue(src, bytes, K, g, ring, full);
     issued = g + 1;
   }
-  // Copies still in flight must land before the CTA exits.
-  const uint32_t g0 = issued > (uint32_t)kRingChunks ? issued - kRingChunks : 0;
-  for (uint32_t g = g0; g < issued; ++g) mbar_wait(&full[g % kRingChunks], (g / kRingChunks) & 1, timeout_ns);
+  producer_drain(full, issued, timeout_ns);
 }
 
 // ---- consumer-side ring state (one per warp) ------------------------------

@@ -71,6 +71,27 @@ struct BicgArgs {
   int max_iter;
 };
 
+// Multi-RHS product on the tensor cores (hbx_mrhs.cu): Y = alpha*H*X +
+// beta*Yin for kNrhs right-hand sides, rows of kNrhs values (RHS-contiguous).
+constexpr int kNrhs = 64;
+struct MatmatArgs {
+  const uint8_t *stream;  // packed with pair_panels (FP32)
+  const RunRec *recs;
+  const CtaInfo *ctas;
+  const RunLite *lite;
+  const float *x;     // [nd][kNrhs]
+  const double *yin;  // [nd][kNrhs], read when beta != 0
+  double *y;          // [nd][kNrhs]
+  float *zbu;         // [zbu_len][kNrhs]
+  double alpha, beta;
+  unsigned *gbar;
+  int *err;
+  unsigned long long timeout_ns;
+};
+size_t matmat_smem_bytes();
+cudaError_t configure_matmat();
+cudaError_t launch_matmat(const MatmatArgs &a, int num_ctas, cudaStream_t s);
+
 // Static scratch of hbx_matvec_noalloc (hbx_kernels.cu): 256 bytes of
 // barrier words, then room for kNoallocZbuMax zbu doubles.
 constexpr size_t kNoallocScratchBytes = size_t(1) << 20;
@@ -96,6 +117,8 @@ struct hbx_hmat {
   int device = 0;
   int num_ctas = 0;
   int transposed = 0;  // the packed stream holds H^T
+  int nrhs = 1;        // right-hand sides per product (kNrhs: multi-RHS engine, hbx_matmat only)
+  float *d_zbum = nullptr;  // multi-RHS engine: zbu for all right-hand sides [zbu_len][kNrhs]
   hbx::Plan plan;
   uint8_t *d_stream = nullptr;
   hbx::RunRec *d_recs = nullptr;

@@ -63,17 +63,13 @@ __device__ __forceinline__ Smem smem_layout(uint8_t *base) {
   return s;
 }
 
-// Barriers, the block-sum counter, the launch's first grid-barrier generation
-// and the CTA's run summaries (`lite`, nr of them) in shared memory.  Thread
-// t0 sets up the barriers; threads t0 and up copy the summaries.  The caller
-// synchronises the CTA afterwards.
+// Barriers (but the ring's: producer_start), the block-sum counter, the
+// launch's first grid-barrier generation and the CTA's run summaries (`lite`,
+// nr of them) in shared memory.  Thread t0 sets up the barriers; threads t0
+// and up copy the summaries.  The caller synchronises the CTA afterwards.
 __device__ __forceinline__ void init_cta_part(const Smem &s, const RunLite *lite, uint32_t nr, const unsigned *gbar,
                                               uint32_t t0) {
   if (threadIdx.x == t0) {
-    for (int i = 0; i < kRingChunks; ++i) {
-      mbar_init(&s.full[i], 1);
-      mbar_init(&s.empty[i], NW);
-    }
     for (int i = 0; i < kStages; ++i) {
       mbar_init(&s.sfull[i], 33);  // 32 cp.async arrivals of a gather warp + its lane 0
       mbar_init(&s.sempty[i], NW);
@@ -277,12 +273,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   const CtaInfo ci = a.ctas[blockIdx.x];
   const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
   const uint64_t t_start = a.prof ? gtimer() : 0;
+  uint32_t issued0 = 0;
+  if (threadIdx.x == kProducerWarp * 32)
+    issued0 = producer_start(a.stream + ci.stream_off, ci.stream_bytes, 1, sm.ring, sm.full, sm.empty);
   init_cta(sm, a.lite + ci.rec_begin, nr, a.gbar);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
   if (w == kProducerWarp) {
     if (lane == 0 && K > 0)
-      producer_run(a.stream + ci.stream_off, ci.stream_bytes, 1, sm.ring, sm.full, sm.empty, a.err, a.timeout_ns);
+      producer_run(a.stream + ci.stream_off, ci.stream_bytes, 1, issued0, sm.ring, sm.full, sm.empty, a.err,
+                   a.timeout_ns);
     return;
   }
   if (w >= kGatherWarp0 && w < kSyncWarp) {
@@ -458,7 +458,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     c_ap = a.ap[row0];
     c_u = a.u[row0];
   }
-  // warps 4 and up set up the CTA while warps 0-3 reduce the scalars
+  // the producer starts the stream of the first H-matvec, warps 4 and up set
+  // up the CTA and warps 0-3 reduce the scalars
+  uint32_t issued0 = 0;
+  if (threadIdx.x == kProducerWarp * 32)
+    issued0 = producer_start(a.stream + ci.stream_off, ci.stream_bytes, 2, sm.ring, sm.full, sm.empty);
   init_cta_part(sm, a.lite + ci.rec_begin, nr, a.gbar, 128);
 
   // ---- S0: scalars of the previous step; stop test at the top of the loop
@@ -519,7 +523,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     }
   }
   __syncthreads();
-  if (sm.scal[0] != 0.0) return;
+  if (sm.scal[0] != 0.0) {
+    if (threadIdx.x == kProducerWarp * 32) producer_drain(sm.full, issued0, a.timeout_ns);
+    return;
+  }
   if (a.prof && threadIdx.x == 0) a.prof[blockIdx.x * 16 + 8] = t_start;  // stamps of working steps only
   const double beta = sm.scal[2], zeta_prev = sm.scal[3], rho = sm.scal[4];
   const double relres = sm.scal[5], bnorm = sm.scal[7];
@@ -528,7 +535,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
   if (w == kProducerWarp) {
     if (lane == 0 && K > 0)
-      producer_run(a.stream + ci.stream_off, ci.stream_bytes, 2, sm.ring, sm.full, sm.empty, a.err, a.timeout_ns);
+      producer_run(a.stream + ci.stream_off, ci.stream_bytes, 2, issued0, sm.ring, sm.full, sm.empty, a.err,
+                   a.timeout_ns);
     return;
   }
   if (w >= kGatherWarp0 && w < kSyncWarp) {

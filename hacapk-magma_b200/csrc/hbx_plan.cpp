@@ -88,8 +88,10 @@ struct ColumnMap {
 };
 
 // Gather segments of block columns [c0, c1) (c1 <= W): contiguous vector
-// ranges merged; the ones longer than kSegShort are moved to the front.
-void segments(const ColumnMap &M, uint32_t c0, uint32_t c1, std::vector<Seg> &out) {
+// ranges merged, in stage order; with long_first the ones longer than
+// kSegShort are moved to the front (the single-RHS gather copies those with
+// the whole warp).
+void segments(const ColumnMap &M, uint32_t c0, uint32_t c1, std::vector<Seg> &out, bool long_first) {
   out.clear();
   uint32_t piece = 0, piece_c0 = 0;
   uint32_t c = c0;
@@ -107,7 +109,8 @@ void segments(const ColumnMap &M, uint32_t c0, uint32_t c1, std::vector<Seg> &ou
     out.push_back(Seg{src, (uint16_t)n, (uint16_t)(c - c0)});
     c += n;
   }
-  std::stable_partition(out.begin(), out.end(), [](const Seg &s) { return s.len > (uint32_t)kSegShort; });
+  if (long_first)
+    std::stable_partition(out.begin(), out.end(), [](const Seg &s) { return s.len > (uint32_t)kSegShort; });
 }
 
 uint32_t count_long(const std::vector<Seg> &segs) {
@@ -118,11 +121,17 @@ uint32_t count_long(const std::vector<Seg> &segs) {
 
 }  // namespace
 
-int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, std::string &err, int precision) {
+int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, std::string &err, int precision,
+              bool pair_panels) {
   plan = Plan();
   if (precision != kFP64 && precision != kFP32) { err = "unknown storage precision"; return HBX_ERR_INVALID; }
+  if (pair_panels && precision != kFP32) { err = "panel pairs need FP32 storage"; return HBX_ERR_INVALID; }
   plan.precision = precision;
+  plan.pair_panels = pair_panels;
   const uint32_t G = group_cols(precision);
+  // run widths are multiples of RG columns: whole panels, or whole panel
+  // pairs (the K = 8 of one TF32 tensor-core step) for the multi-RHS engine
+  const uint32_t RG = pair_panels ? 2 * G : G;
   const uint32_t stage_cols = kStageBytes / elem_bytes(precision);
   if (!st || nd <= 0 || num_ctas <= 0) { err = "null container, nd <= 0 or no CTAs"; return HBX_ERR_INVALID; }
   const int nlf = st->nlf;
@@ -333,7 +342,7 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
     uint32_t rot = 0;
     auto emit_block = [&](uint32_t bi) -> uint32_t {
       const Block &b = plan.blocks[bi];
-      const uint32_t Wp = (b.W + G - 1) / G * G;
+      const uint32_t Wp = (b.W + RG - 1) / RG * RG;
       ColumnMap M{plan, b, 0};
       uint32_t out = 0;
       if (b.kind == kRunP) {
@@ -346,19 +355,19 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
       uint32_t nr = 0, col = 0;
       do {
         uint32_t nc = std::min<uint32_t>(stage_cols, Wp - col);
-        segments(M, col, std::min(col + nc, b.W), segs);
+        segments(M, col, std::min(col + nc, b.W), segs, !pair_panels);
         if (segs.size() > (size_t)kRunSegs) {
-          // too many pieces: the widest run (a multiple of G columns) whose
+          // too many pieces: the widest run (a multiple of RG columns) whose
           // segments fit the record (the count grows with the width)
-          uint32_t lo = G, hi = nc - G;
+          uint32_t lo = RG, hi = nc - RG;
           while (lo < hi) {
-            const uint32_t mid = ((lo + hi + G) / 2) / G * G;
-            segments(M, col, std::min(col + mid, b.W), segs);
+            const uint32_t mid = ((lo + hi + RG) / 2) / RG * RG;
+            segments(M, col, std::min(col + mid, b.W), segs, !pair_panels);
             if (segs.size() <= (size_t)kRunSegs) lo = mid;
-            else hi = mid - G;
+            else hi = mid - RG;
           }
           nc = lo;
-          segments(M, col, std::min(col + nc, b.W), segs);
+          segments(M, col, std::min(col + nc, b.W), segs, !pair_panels);
         }
         RunRec rec{};
         Run &r = rec.hdr;
@@ -370,7 +379,7 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
         r.flags = (uint16_t)(b.kind | (col == 0 ? kFirst : 0) | (last ? kLast : 0));
         r.rot = (uint16_t)rot;
         r.nseg = (uint16_t)segs.size();
-        r.nlong = count_long(segs);
+        r.nlong = pair_panels ? 0 : count_long(segs);
         r.vlen = (uint16_t)(std::min(col + nc, b.W) - col);
         r.block = bi;
         r.col0 = col;

@@ -167,6 +167,7 @@ struct Plan {
   int nd = 0, nlf = 0, nlfkt = 0, ktmax = 0;
   int num_ctas = 0;
   int precision = kFP64;
+  bool pair_panels = false;         // multi-RHS layout (even panel counts, segments in stage order)
   std::vector<Atom> atoms;          // in CTA order (atom_begin indexes this)
   std::vector<RunRec> recs;         // in CTA order
   std::vector<RunLite> lite;        // one summary per record, same order
@@ -184,8 +185,10 @@ struct Plan {
 
 // Validates the leaf list and builds the plan.  Returns HBX_OK or an error
 // (message in `err`).
+// pair_panels (FP32 only): every run holds an even number of panels and its
+// segments stay in stage order -- the layout of the multi-RHS engine.
 int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, std::string &err,
-              int precision = kFP64);
+              int precision = kFP64, bool pair_panels = false);
 
 // Writes the packed stream of every CTA into `dst` (plan.total_bytes bytes).
 void pack_plan(const stc_HACApK_leafmtxp *st, const Plan &plan, uint8_t *dst);

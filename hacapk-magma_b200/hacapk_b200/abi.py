@@ -57,7 +57,7 @@ class LControl(C.Structure):
 
 
 class Options(C.Structure):
-    _fields_ = [("precision", C.c_int), ("num_ctas", C.c_int), ("transpose", C.c_int), ("reserved", C.c_int * 13)]
+    _fields_ = [("precision", C.c_int), ("num_ctas", C.c_int), ("transpose", C.c_int), ("nrhs", C.c_int), ("reserved", C.c_int * 12)]
 
 
 class Info(C.Structure):
@@ -67,7 +67,7 @@ class Info(C.Structure):
                 ("alg_bytes", C.c_longlong), ("alg_flops", C.c_longlong),
                 ("zbu_len", C.c_longlong), ("dense_words", C.c_longlong),
                 ("lowrank_words", C.c_longlong), ("setup_seconds", C.c_double),
-                ("transposed", C.c_int), ("reserved", C.c_int * 7)]
+                ("transposed", C.c_int), ("nrhs", C.c_int), ("reserved", C.c_int * 6)]
 
 
 class SolveOpts(C.Structure):
@@ -102,6 +102,7 @@ KERNEL_PPOHBEM = 0
 KERNEL_LAPLACE = 1
 
 HBX_FP64, HBX_FP32 = 0, 1
+HBX_NRHS = 64
 
 STATUS = {0: "HBX_OK", 1: "HBX_ERR_INVALID", 2: "HBX_ERR_NOMEM", 3: "HBX_ERR_CUDA",
           4: "HBX_ERR_TIMEOUT", 5: "HBX_ERR_BREAKDOWN", 6: "HBX_ERR_NOT_CONVERGED",
@@ -117,6 +118,7 @@ ENGINE_SYMBOLS = [
     ("hbx_get_info", C.c_int, [_VP, C.POINTER(Info)]),
     ("hbx_matvec", C.c_int, [_VP, C.c_double, _VP, C.c_double, _VP, _VP, _VP]),
     ("hbx_matvec_noalloc", C.c_int, [_VP, C.c_double, _VP, C.c_double, _VP, _VP, _VP]),
+    ("hbx_matmat", C.c_int, [_VP, C.c_double, _VP, C.c_double, _VP, _VP, _VP]),
     ("hbx_sync", C.c_int, [_VP, _VP]),
     ("hbx_matvec_host", C.c_int, [_VP, _DP, _DP, C.c_int, _DP, _DP]),
     ("hbx_bicgstab", C.c_int, [_VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),

@@ -29,14 +29,17 @@ def _check(status: int, where: str):
 class Engine:
     """Packed H-matrix resident on the current CUDA device."""
 
-    def __init__(self, st, nd: int, num_ctas: int = 0, transpose: bool = False, precision: int = 0):
+    def __init__(self, st, nd: int, num_ctas: int = 0, transpose: bool = False, precision: int = 0,
+                 nrhs: int = 0):
         """transpose=True packs H^T: products and solves with the adjoint.
-        precision=abi.HBX_FP32 stores the factors in float (half the bytes)."""
+        precision=abi.HBX_FP32 stores the factors in float (half the bytes).
+        nrhs=abi.HBX_NRHS (with HBX_FP32) makes a multi-RHS engine: matmat only."""
         self.lib = abi.engine_lib()
         opt = abi.Options()
         opt.precision = precision
         opt.num_ctas = num_ctas
         opt.transpose = 1 if transpose else 0
+        opt.nrhs = nrhs
         h = C.c_void_p()
         _check(self.lib.hbx_create(st, nd, C.byref(opt), C.byref(h)), "hbx_create")
         self._h = h
@@ -73,6 +76,14 @@ class Engine:
         _check(self.lib.hbx_matvec(self._h, alpha, C.c_void_p(x_ptr), beta,
                                    C.c_void_p(yin_ptr) if yin_ptr else None, C.c_void_p(y_ptr),
                                    C.c_void_p(stream) if stream else None), "hbx_matvec")
+
+    def matmat_dev(self, x_ptr: int, y_ptr: int, alpha: float = 1.0, beta: float = 0.0,
+                   yin_ptr: int | None = None, stream: int = 0):
+        """Y = alpha H X + beta Yin for HBX_NRHS right-hand sides: X nd x 64
+        floats, Y (and Yin) nd x 64 doubles, row-major device arrays."""
+        _check(self.lib.hbx_matmat(self._h, alpha, C.c_void_p(x_ptr), beta,
+                                   C.c_void_p(yin_ptr) if yin_ptr else None, C.c_void_p(y_ptr),
+                                   C.c_void_p(stream) if stream else None), "hbx_matmat")
 
     def sync(self, stream: int = 0):
         _check(self.lib.hbx_sync(self._h, C.c_void_p(stream) if stream else None), "hbx_sync")

@@ -125,8 +125,14 @@ typedef struct hbx_options {
   int num_ctas;    /* persistent CTAs; 0 = one per SM                     */
   int transpose;   /* 1: the engine holds H^T (adjoint products and solves;
                       no counterpart in the reference)                    */
-  int reserved[13];
+  int nrhs;        /* 0 or 1: single-vector engine (hbx_matvec, solves);
+                      HBX_NRHS: multi-RHS engine for hbx_matmat (needs
+                      precision = HBX_FP32; no counterpart in the reference) */
+  int reserved[12];
 } hbx_options;
+
+/* Right-hand sides of one hbx_matmat call on a multi-RHS engine. */
+#define HBX_NRHS 64
 
 typedef struct hbx_info {
   int nd, nlf, nlfkt, ktmax;
@@ -138,7 +144,8 @@ typedef struct hbx_info {
   long long dense_words, lowrank_words;
   double setup_seconds;
   int transposed;          /* 1 when the engine holds H^T                    */
-  int reserved[7];
+  int nrhs;                /* right-hand sides per product (1 or HBX_NRHS)   */
+  int reserved[6];
 } hbx_info;
 
 typedef struct hbx_solve_opts {
@@ -200,6 +207,17 @@ int hbx_matvec(hbx_hmat *h, double alpha, const double *x, double beta,
  * word (hbx_sync). */
 int hbx_matvec_noalloc(hbx_hmat *h, double alpha, const double *x, double beta,
                        const double *yin, double *y, void *stream);
+
+/* Y = alpha * H X + beta * Yin for HBX_NRHS right-hand sides at once, on an
+ * engine created with hbx_options.nrhs = HBX_NRHS (no counterpart in the
+ * reference, whose batched GEMV takes one vector).  X is nd x HBX_NRHS floats,
+ * Yin and Y nd x HBX_NRHS doubles, all row-major (the HBX_NRHS values of a row
+ * adjacent) on the device; beta == 0 ignores Yin.  The products run on the
+ * tensor cores (TF32 inputs: factors and X rounded to 10-bit mantissas, FP32
+ * accumulation): a relative error of order 1e-3 per entry, meant as the inner
+ * product of an iterative refinement.  One persistent launch on `stream`. */
+int hbx_matmat(hbx_hmat *h, double alpha, const float *X, double beta, const double *Yin, double *Y,
+               void *stream);
 
 /* Mixed-precision BiCGSTAB (no counterpart in the reference): FP64
  * iterative refinement around BiCGSTAB on `hl`, an engine created on the same

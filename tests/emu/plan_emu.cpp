@@ -17,15 +17,15 @@
 
 using namespace hbx;
 
-extern "C" int emu_matvec_prec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int precision, const double *x,
-                               double *y, long long *stats, char *msg, int msglen) {
+static int emu_run(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int precision, bool pairs, const double *x,
+                   double *y, long long *stats, char *msg, int msglen) {
   auto bad = [&](const std::string &s) {
     std::snprintf(msg, msglen, "%s", s.c_str());
     return 1;
   };
   Plan plan;
   std::string err;
-  int rc = make_plan(st, nd, num_ctas, plan, err, precision);
+  int rc = make_plan(st, nd, num_ctas, plan, err, precision, pairs);
   if (rc != 0) return bad("make_plan: " + err);
   std::vector<uint8_t> buf(plan.total_bytes, 0xAB);
   pack_plan(st, plan, buf.data());
@@ -55,8 +55,10 @@ extern "C" int emu_matvec_prec(const stc_HACApK_leafmtxp *st, int nd, int num_ct
       if (L.pos != r.pos || L.out != r.out || L.npanel != r.npanel || L.nrow != r.nrow || L.rot != r.rot ||
           L.flags != r.flags)
         return "run summary does not match its record";
+      // pair-panel runs (multi-RHS layout) are whole panel pairs
+      const uint32_t RG = pairs ? 2 * G : G;
       if (G * r.npanel * elem_bytes(precision) > (uint32_t)kStageBytes || r.vlen > G * r.npanel ||
-          (r.npanel > 0 && r.vlen + G <= G * r.npanel))
+          (r.npanel > 0 && r.vlen + RG <= G * r.npanel) || (pairs && r.npanel % 2 != 0))
         return "run width";
       if (r.nseg > kRunSegs) return "too many segments";
       if (r.rot >= kConsumerWarps) return "bad rotation";
@@ -71,7 +73,8 @@ extern "C" int emu_matvec_prec(const stc_HACApK_leafmtxp *st, int nd, int num_ct
       for (uint32_t q = 0; q < r.nseg; ++q) {
         const Seg &s = plan.recs[ci.rec_begin + k].seg[q];
         if (s.len == 0 || (uint32_t)s.dst + s.len > real) return "segment outside the stage";
-        if ((q < r.nlong) != (s.len > (uint32_t)kSegShort)) return "long segments not first";
+        if (pairs ? (r.nlong != 0 || s.dst != d) : ((q < r.nlong) != (s.len > (uint32_t)kSegShort)))
+          return pairs ? "pair-panel segments not in stage order" : "long segments not first";
         if ((uint64_t)s.src + s.len > vmax) return "segment source out of range";
         for (uint32_t e = 0; e < s.len; ++e) {
           if (cov[s.dst + e]) return "segments overlap";
@@ -172,6 +175,18 @@ extern "C" int emu_matvec_prec(const stc_HACApK_leafmtxp *st, int nd, int num_ct
     stats[7] = (long long)plan.pad_bytes;
   }
   return 0;
+}
+
+extern "C" int emu_matvec_prec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int precision, const double *x,
+                               double *y, long long *stats, char *msg, int msglen) {
+  return emu_run(st, nd, num_ctas, precision, false, x, y, stats, msg, msglen);
+}
+
+// The multi-RHS engine's layout (FP32 factors, runs of whole panel pairs,
+// segments in stage order), one right-hand side at a time.
+extern "C" int emu_matvec_pairs(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, const double *x, double *y,
+                                long long *stats, char *msg, int msglen) {
+  return emu_run(st, nd, num_ctas, kFP32, true, x, y, stats, msg, msglen);
 }
 
 extern "C" int emu_matvec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, const double *x, double *y,
