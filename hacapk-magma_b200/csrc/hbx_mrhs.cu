@@ -7,10 +7,11 @@
 //
 //   warps 0-3   epilogue: TMEM accumulator -> zbu (P blocks) or Y (D, U)
 //   warp 4      tcgen05: allocates TMEM; one thread issues the MMAs
-//   warp 5      bulk-copy producer of the stream ring (as in k_matvec)
-//   warps 6-9   gather: X (or zbu) columns of a run, 64 at a time, into a
-//               K-major operand stage [4-column chunk][rhs][4] (16 KB)
-//   warp 10     grid barrier between the P blocks and the U runs
+//   warp 5      bulk-copy producer of the stream ring (16 KB chunks)
+//   warps 6-13  gather: X (or zbu) columns of a run, 64 at a time, into a
+//               K-major operand stage [4-column chunk][rhs][4] (16 KB), one
+//               stage per warp
+//   warp 14     grid barrier between the P blocks and the U runs
 //
 // One MMA: D[rhs][row] += Xs[rhs][k..k+8] * Panel[row][k..k+8]^T with
 // M = 64 right-hand sides, N = the block's rows rounded up to 8, A (the
@@ -19,7 +20,9 @@
 // 8 rows 128 bytes on (SBO), the next 4 columns LBO on (1 KB for A, 16h for
 // B).  D lives in TMEM (M = 64: rhs m in lane (m mod 16) + 32 (m / 16)); two
 // 64-column accumulators let the epilogue of one block overlap the MMAs of
-// the next.  MMAs read the ring in place: a panel pair that runs past the
+// the next.  The ring is smaller than k_matvec's (the product is bound by
+// the X stages, not by the stream) and MMAs read it in place: a panel pair
+// that runs past the
 // ring's end reads a mirror of the first bytes of slot 0 that the producer
 // keeps behind the ring.  Rows of D past h come from bytes after the pair
 // and are never stored.
@@ -35,20 +38,25 @@ constexpr int kSliceCols = 64;                         // stage columns per slic
 constexpr int kSliceChunks = kSliceCols / 4;           // 4-column K chunks per slice
 constexpr int kChunkXBytes = kNrhs * 16;               // one chunk, all right-hand sides: 1 KB
 constexpr int kSliceBytes = kSliceChunks * kChunkXBytes;  // 16 KB
-constexpr int kXStages = 4;
+constexpr int kMChunkLog = 14;  // ring chunk: 16 KB
+constexpr int kMChunkBytes = 1 << kMChunkLog;
+constexpr int kMRingChunks = 4;
+constexpr uint32_t kMRingBytes = (uint32_t)kMRingChunks * kMChunkBytes;
+constexpr int kXStages = 8;
 constexpr int kMirrorBytes = 2304;  // >= 2 panels of 64 rows + 7 rows past them
 constexpr int kAccCols = 64;        // TMEM columns per accumulator (rows of a block <= 64)
 constexpr int kTmemCols = 2 * kAccCols;
-constexpr int kEpiWarps = 4, kMmaWarp = 4, kProdWarpM = 5, kGathWarp0 = 6, kGathWarps = 4, kSyncWarpM = 10;
+constexpr int kEpiWarps = 4, kMmaWarp = 4, kProdWarpM = 5, kGathWarp0 = 6, kGathWarps = 8, kSyncWarpM = 14;
+static_assert(kXStages == kGathWarps, "gather warp gi always fills stage gi");
 constexpr int kThreadsM = (kSyncWarpM + 1) * 32;
 
 struct MLayout {
   static constexpr uint32_t ring = 0;
-  static constexpr uint32_t xst = (kRingBytes + kMirrorBytes + 1023) / 1024 * 1024;  // [kXStages] slices
+  static constexpr uint32_t xst = (kMRingBytes + kMirrorBytes + 1023) / 1024 * 1024;  // [kXStages] slices
   static constexpr uint32_t rec = xst + kXStages * kSliceBytes;                       // [kGathWarps] records
   static constexpr uint32_t full = rec + kGathWarps * kRecBytes;
-  static constexpr uint32_t empty = full + 8 * kRingChunks;
-  static constexpr uint32_t xfull = empty + 8 * kRingChunks;
+  static constexpr uint32_t empty = full + 8 * kMRingChunks;
+  static constexpr uint32_t xfull = empty + 8 * kMRingChunks;
   static constexpr uint32_t xempty = xfull + 8 * kXStages;
   static constexpr uint32_t accfull = xempty + 8 * kXStages;
   static constexpr uint32_t accempty = accfull + 16;
@@ -105,28 +113,30 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
 // ---- producer with the ring-end mirror ------------------------------------
 __device__ __forceinline__ void mr_issue(const uint8_t *src, uint32_t bytes, uint32_t g, uint8_t *ring,
                                          uint64_t *full) {
-  const uint32_t s = g % kRingChunks;
-  const uint32_t off = g << kChunkLog;
-  const uint32_t nb = min((uint32_t)kChunkBytes, bytes - off);
+  const uint32_t s = g % kMRingChunks;
+  const uint32_t off = g << kMChunkLog;
+  const uint32_t nb = min((uint32_t)kMChunkBytes, bytes - off);
   const uint32_t nm = s == 0 ? min(nb, (uint32_t)kMirrorBytes) : 0u;
   mbar_arrive_expect_tx(&full[s], nb + nm);
-  bulk_g2s(ring + ((size_t)s << kChunkLog), src + off, nb, &full[s]);
-  if (nm) bulk_g2s(ring + kRingBytes, src + off, nm, &full[s]);
+  bulk_g2s(ring + ((size_t)s << kMChunkLog), src + off, nb, &full[s]);
+  if (nm) bulk_g2s(ring + kMRingBytes, src + off, nm, &full[s]);
 }
 
 __device__ __forceinline__ void mr_producer(const uint8_t *src, uint32_t bytes, uint8_t *ring, uint64_t *full,
                                             uint64_t *empty, int *err, uint64_t tmo) {
-  const uint32_t K = (bytes + kChunkBytes - 1) >> kChunkLog;
+  const uint32_t K = (bytes + kMChunkBytes - 1) >> kMChunkLog;
   uint32_t issued = 0;
   for (uint32_t g = 0; g < K; ++g) {
-    if (g >= (uint32_t)kRingChunks && !mbar_wait(&empty[g % kRingChunks], ((g / kRingChunks) - 1) & 1, tmo)) {
+    if (g >= (uint32_t)kMRingChunks && !mbar_wait(&empty[g % kMRingChunks], ((g / kMRingChunks) - 1) & 1, tmo)) {
       atomicOr(err, kErrProducer);
       break;
     }
     mr_issue(src, bytes, g, ring, full);
     issued = g + 1;
   }
-  producer_drain(full, issued, tmo);
+  // copies still in flight land before the CTA exits
+  const uint32_t g0 = issued > (uint32_t)kMRingChunks ? issued - kMRingChunks : 0;
+  for (uint32_t g = g0; g < issued; ++g) mbar_wait(&full[g % kMRingChunks], (g / kMRingChunks) & 1, tmo);
 }
 
 struct MSmem {
@@ -234,6 +244,9 @@ __device__ __forceinline__ void mr_gather(const MatmatArgs &a, const CtaInfo &ci
 }
 
 // ---- MMA thread ---------------------------------------------------------------
+// Per slice: wait for its X stage and for every ring chunk its panel pairs
+// touch (at most 16 KB of pairs, two chunks), then issue its MMAs back to
+// back with the descriptors advanced in place, and commit the stage back.
 __device__ __forceinline__ void mr_mma(const MatmatArgs &a, const RunLite *lite, uint32_t nr, uint32_t K,
                                        const MSmem &sm) {
   const uint64_t tmo = a.timeout_ns;
@@ -247,11 +260,11 @@ __device__ __forceinline__ void mr_mma(const MatmatArgs &a, const RunLite *lite,
   auto release_below = [&](uint32_t c) {
     while (ok && released < c) {
       if (waited <= released) {
-        ok = mbar_wait(&sm.full[released % kRingChunks], (released / kRingChunks) & 1, tmo);
+        ok = mbar_wait(&sm.full[released % kMRingChunks], (released / kMRingChunks) & 1, tmo);
         if (!ok) return;
         waited = released + 1;
       }
-      tc_commit(&sm.empty[released % kRingChunks]);
+      tc_commit(&sm.empty[released % kMRingChunks]);
       ++released;
     }
   };
@@ -261,33 +274,35 @@ __device__ __forceinline__ void mr_mma(const MatmatArgs &a, const RunLite *lite,
     const uint32_t h = L.nrow, n8 = (h + 7u) & ~7u, pb = 16u * h;
     const uint32_t idesc = idesc_tf32(kNrhs, n8);
     const uint32_t buf = nb & 1u;
+    const uint32_t dtm = tbase + buf * kAccCols;
     if (L.flags & kFirst) {
       // the epilogue has read this accumulator's previous block
       if (nb >= 2 && !(ok = mbar_wait(&sm.accempty[buf], ((nb >> 1) - 1) & 1, tmo))) break;
-      tc_fence_after();
       first = true;
     }
     const uint32_t nsl = run_slices(L), npair = L.npanel / 2u;
     for (uint32_t s = 0; s < nsl && ok; ++s, ++q) {
       const uint32_t slot = q % kXStages;
-      if (!(ok = mbar_wait(&sm.xfull[slot], (q / kXStages) & 1, tmo))) break;
+      const uint32_t p0 = s * (kSliceCols / 8), p1 = min(npair, p0 + kSliceCols / 8);
+      const uint32_t pos0 = L.pos + 2u * p0 * pb, pos1 = L.pos + 2u * p1 * pb;
+      release_below(pos0 >> kMChunkLog);
+      const uint32_t clast = (pos1 - 1u) >> kMChunkLog;
+      while (ok && waited <= clast) {
+        ok = mbar_wait(&sm.full[waited % kMRingChunks], (waited / kMRingChunks) & 1, tmo);
+        waited += ok ? 1u : 0u;
+      }
+      if (ok) ok = mbar_wait(&sm.xfull[slot], (q / kXStages) & 1, tmo);
+      if (!ok) break;
       tc_fence_after();
-      const uint32_t p1 = min(npair, (s + 1) * (kSliceCols / 8));
-      for (uint32_t p = s * (kSliceCols / 8); p < p1 && ok; ++p) {
-        const uint32_t pos = L.pos + 2u * p * pb;
-        const uint32_t c0 = pos >> kChunkLog, c1 = (pos + 2u * pb - 1u) >> kChunkLog;
-        release_below(c0);
-        while (ok && waited <= c1) {
-          ok = mbar_wait(&sm.full[waited % kRingChunks], (waited / kRingChunks) & 1, tmo);
-          waited += ok ? 1u : 0u;
-        }
-        if (!ok) break;
-        tc_fence_after();
-        const uint32_t a_addr = xst_s + slot * kSliceBytes + (2u * p - s * (kSliceCols / 4)) * kChunkXBytes;
-        const uint32_t b_addr = ring_s + (c0 % kRingChunks) * kChunkBytes + (pos & (kChunkBytes - 1));
-        mma_tf32(tbase + buf * kAccCols, smem_desc(a_addr, kChunkXBytes, 128), smem_desc(b_addr, pb, 128), idesc,
-                 first ? 0u : 1u);
+      uint64_t adesc = smem_desc(xst_s + slot * kSliceBytes, kChunkXBytes, 128);
+      uint32_t baddr = ring_s + ((pos0 >> kMChunkLog) % kMRingChunks) * kMChunkBytes + (pos0 & (kMChunkBytes - 1));
+      const uint64_t bhi = smem_desc(0, pb, 128);  // the descriptor without its address
+      for (uint32_t p = p0; p < p1; ++p) {
+        mma_tf32(dtm, adesc, bhi | (uint64_t)((baddr >> 4) & 0x3fffu), idesc, first ? 0u : 1u);
         first = false;
+        adesc += (2u * kChunkXBytes) >> 4;  // the next two K chunks of the stage
+        baddr += 2u * pb;
+        if (baddr >= ring_s + kMRingBytes) baddr -= kMRingBytes;  // a pair that starts past the ring's end
       }
       tc_commit(&sm.xempty[slot]);  // the stage slot is free once these MMAs are done
     }
@@ -371,10 +386,10 @@ __global__ void __launch_bounds__(kThreadsM, 1) k_matmat(MatmatArgs a) {
   const CtaInfo ci = a.ctas[blockIdx.x];
   const RunLite *lite = a.lite + ci.rec_begin;
   const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
-  const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
+  const uint32_t K = (ci.stream_bytes + kMChunkBytes - 1) >> kMChunkLog;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    for (int i = 0; i < kRingChunks; ++i) {
+    for (int i = 0; i < kMRingChunks; ++i) {
       mbar_init(&sm.full[i], 1);
       mbar_init(&sm.empty[i], 1);
     }
