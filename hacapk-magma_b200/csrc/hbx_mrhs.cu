@@ -53,8 +53,9 @@ constexpr int kThreadsM = (kSyncWarpM + 1) * 32;
 struct MLayout {
   static constexpr uint32_t ring = 0;
   static constexpr uint32_t xst = (kMRingBytes + kMirrorBytes + 1023) / 1024 * 1024;  // [kXStages] slices
-  static constexpr uint32_t rec = xst + kXStages * kSliceBytes;                       // [kGathWarps] records
-  static constexpr uint32_t full = rec + kGathWarps * kRecBytes;
+  static constexpr uint32_t rec = xst + kXStages * kSliceBytes;                       // [kGathWarps][2] records
+  static constexpr uint32_t lite = rec + 2 * kGathWarps * kRecBytes;                  // [kMaxPairRuns] summaries
+  static constexpr uint32_t full = lite + kMaxPairRuns * 16;
   static constexpr uint32_t empty = full + 8 * kMRingChunks;
   static constexpr uint32_t xfull = empty + 8 * kMRingChunks;
   static constexpr uint32_t xempty = xfull + 8 * kXStages;
@@ -103,13 +104,6 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar) {
                : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-               : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
 // ---- producer with the ring-end mirror ------------------------------------
 __device__ __forceinline__ void mr_issue(const uint8_t *src, uint32_t bytes, uint32_t g, uint8_t *ring,
                                          uint64_t *full) {
@@ -141,6 +135,7 @@ __device__ __forceinline__ void mr_producer(const uint8_t *src, uint32_t bytes, 
 
 struct MSmem {
   uint8_t *ring, *xst, *rec;
+  RunLite *lite;
   uint64_t *full, *empty, *xfull, *xempty, *accfull, *accempty, *pdone, *gdone, *mdone;
   uint32_t *tmem, *gen0;
 };
@@ -150,6 +145,7 @@ __device__ __forceinline__ MSmem mlayout(uint8_t *b) {
   s.ring = b + MLayout::ring;
   s.xst = b + MLayout::xst;
   s.rec = b + MLayout::rec;
+  s.lite = reinterpret_cast<RunLite *>(b + MLayout::lite);
   s.full = reinterpret_cast<uint64_t *>(b + MLayout::full);
   s.empty = reinterpret_cast<uint64_t *>(b + MLayout::empty);
   s.xfull = reinterpret_cast<uint64_t *>(b + MLayout::xfull);
@@ -178,32 +174,43 @@ __device__ __forceinline__ uint32_t run_slices(const RunLite &L) {
 // Lane (c = lane & 3, m0 = lane >> 2) copies column c of every 4-column chunk
 // for right-hand sides m0, m0 + 8, ...: consecutive lanes write consecutive
 // words of the stage.  A stage column past the run's real columns is zero.
-__device__ __forceinline__ void mr_gather(const MatmatArgs &a, const CtaInfo &ci, const RunLite *lite, uint32_t nr,
-                                          const MSmem &sm, uint32_t gi) {
+// The record of the next run with a slice of this warp is fetched into the
+// other of the warp's two record buffers while it stages the current one.
+__device__ __forceinline__ void mr_gather(const MatmatArgs &a, const CtaInfo &ci, uint32_t nr, const MSmem &sm,
+                                          uint32_t gi) {
   const int lane = threadIdx.x & 31;
   const uint32_t c4 = lane & 3, m0 = lane >> 2;
   const RunRec *recs = a.recs + ci.rec_begin;
-  uint8_t *myrec = sm.rec + gi * kRecBytes;
-  const Run &hdr = *reinterpret_cast<const Run *>(myrec);
-  const Seg *seg = reinterpret_cast<const Seg *>(myrec + sizeof(Run));
-  bool ok = true, zbu_ready = false;
-  uint32_t q = 0;
-  for (uint32_t r = 0; r < nr && ok; ++r) {
-    const RunLite L = lite[r];
-    const uint32_t nsl = run_slices(L);
-    const uint32_t mine0 = (gi + kGathWarps - q % kGathWarps) % kGathWarps;  // first own slice of the run
-    if (mine0 >= nsl) {
+  uint8_t *rbuf = sm.rec + gi * 2 * kRecBytes;
+  // the next run at or after r (slice counter q at r) that holds a slice of this warp
+  auto next_own = [&](uint32_t &r, uint32_t &q) {
+    for (; r < nr; ++r) {
+      const uint32_t nsl = run_slices(sm.lite[r]);
+      if ((gi + kGathWarps - q % kGathWarps) % kGathWarps < nsl) return;
       q += nsl;
-      continue;
     }
-    // the run record, once per run
-    {
-      const uint8_t *src = reinterpret_cast<const uint8_t *>(recs + r);
+  };
+  auto fetch = [&](uint32_t r, uint32_t b) {
+    const uint8_t *src = reinterpret_cast<const uint8_t *>(recs + r);
 #pragma unroll
-      for (uint32_t o = 0; o < (uint32_t)kRecBytes; o += 512) cp_async16cg(myrec + o + lane * 16, src + o + lane * 16);
-      cp_async_wait_all();
-      __syncwarp();
-    }
+    for (uint32_t o = 0; o < (uint32_t)kRecBytes; o += 512)
+      cp_async16cg(rbuf + b * kRecBytes + o + lane * 16, src + o + lane * 16);
+  };
+  bool ok = true, zbu_ready = false;
+  uint32_t r = 0, q = 0, b = 0;
+  next_own(r, q);
+  if (r < nr) fetch(r, 0);
+  while (ok && r < nr) {
+    const RunLite L = sm.lite[r];
+    const uint32_t nsl = run_slices(L), mine0 = (gi + kGathWarps - q % kGathWarps) % kGathWarps;
+    cp_async_wait_all();  // this run's record has landed
+    __syncwarp();
+    uint32_t rn = r + 1, qn = q + nsl;
+    next_own(rn, qn);
+    if (rn < nr) fetch(rn, b ^ 1u);
+    const uint8_t *rec = rbuf + b * kRecBytes;
+    const Run &hdr = *reinterpret_cast<const Run *>(rec);
+    const Seg *seg = reinterpret_cast<const Seg *>(rec + sizeof(Run));
     const uint32_t kind = L.flags & 0xffu, vlen = hdr.vlen, nseg = hdr.nseg;
     const float *vec = kind == kRunU ? a.zbu : a.x;
     if (kind == kRunU && !zbu_ready) {
@@ -237,7 +244,9 @@ __device__ __forceinline__ void mr_gather(const MatmatArgs &a, const CtaInfo &ci
       __syncwarp();
       if (lane == 0) mbar_arrive(&sm.xfull[slot]);
     }
-    q += nsl;
+    r = rn;
+    q = qn;
+    b ^= 1u;
   }
   if (!ok && lane == 0) atomicOr(a.err, kErrPipeline);
   cp_async_wait_all();
@@ -247,8 +256,8 @@ __device__ __forceinline__ void mr_gather(const MatmatArgs &a, const CtaInfo &ci
 // Per slice: wait for its X stage and for every ring chunk its panel pairs
 // touch (at most 16 KB of pairs, two chunks), then issue its MMAs back to
 // back with the descriptors advanced in place, and commit the stage back.
-__device__ __forceinline__ void mr_mma(const MatmatArgs &a, const RunLite *lite, uint32_t nr, uint32_t K,
-                                       const MSmem &sm) {
+__device__ __forceinline__ void mr_mma(const MatmatArgs &a, uint32_t nr, uint32_t K, const MSmem &sm) {
+  const RunLite *lite = sm.lite;
   const uint64_t tmo = a.timeout_ns;
   const uint32_t tbase = *sm.tmem;
   const uint32_t ring_s = smem_u32(sm.ring), xst_s = smem_u32(sm.xst);
@@ -319,8 +328,16 @@ __device__ __forceinline__ void mr_mma(const MatmatArgs &a, const RunLite *lite,
 }
 
 // ---- epilogue warps -----------------------------------------------------------
-__device__ __forceinline__ void mr_epilogue(const MatmatArgs &a, const RunLite *lite, uint32_t nr, uint32_t nblk_p,
-                                            const MSmem &sm) {
+// Warp w reads TMEM lanes 32w..32w+31 (rhs 16w + lane for lane < 16): all of
+// a block's columns (its rows) first, then, for D and U blocks, all the Y
+// values it updates, so each block costs one round trip of each kind.
+__device__ __forceinline__ void tmem_ld8_async(uint32_t taddr, uint32_t *r) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+}
+
+__device__ __forceinline__ void mr_epilogue(const MatmatArgs &a, uint32_t nr, uint32_t nblk_p, const MSmem &sm) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t m = 16u * w + lane;  // right-hand side of this thread's TMEM lane (lane < 16)
   const uint32_t tlane = (32u * (uint32_t)w) << 16;  // this warp's TMEM lane quarter
@@ -328,13 +345,13 @@ __device__ __forceinline__ void mr_epilogue(const MatmatArgs &a, const RunLite *
   if (nblk_p == 0 && lane == 0) mbar_arrive(sm.pdone);
   bool ok = true;
   for (uint32_t r = 0; r < nr && ok; ++r) {
-    const RunLite L = lite[r];
+    const RunLite L = sm.lite[r];
     if (!(L.flags & kLast)) continue;
+    const uint32_t h = L.nrow, kind = L.flags & 0xffu;
     if (empty_block(L)) {
       // no columns: D rows are beta * yin, P rows zero, U rows unchanged
-      const uint32_t kind = L.flags & 0xffu;
       if (lane < 16)
-        for (uint32_t i = 0; i < L.nrow; ++i) {
+        for (uint32_t i = 0; i < h; ++i) {
           const size_t o = (size_t)(L.out + i) * kNrhs + m;
           if (kind == kRunD) a.y[o] = a.beta != 0.0 ? a.beta * a.yin[o] : 0.0;
           else if (kind == kRunP) a.zbu[o] = 0.0f;
@@ -347,27 +364,31 @@ __device__ __forceinline__ void mr_epilogue(const MatmatArgs &a, const RunLite *
     ok = warp_wait(&sm.accfull[buf], (nb >> 1) & 1, a.timeout_ns);
     if (!ok) break;
     tc_fence_after();
-    const uint32_t h = L.nrow, kind = L.flags & 0xffu;
     const uint32_t taddr = *sm.tmem + tlane + buf * kAccCols;
-    for (uint32_t c0 = 0; c0 < h; c0 += 8) {
-      uint32_t v[8];
-      tmem_ld8(taddr + c0, v);
+    // 16 rows at a time: their columns from TMEM, then (D with beta, U) the
+    // Y values they update, then the stores
+    const bool add = kind == kRunU || (kind == kRunD && a.beta != 0.0);
+    const double *src = kind == kRunU ? a.y : a.yin;
+    const double c = kind == kRunU ? 1.0 : a.beta;
+    for (uint32_t r0 = 0; r0 < h; r0 += 16) {
+      uint32_t v[16];
+      tmem_ld8_async(taddr + r0, v);
+      if (r0 + 8 < h) tmem_ld8_async(taddr + r0 + 8, v + 8);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (lane < 16) {
+        const size_t o0 = (size_t)(L.out + r0) * kNrhs + m;
+        const uint32_t n = min(16u, h - r0);
+        if (kind == kRunP) {
 #pragma unroll
-        for (uint32_t j = 0; j < 8; ++j) {
-          const uint32_t i = c0 + j;
-          if (i >= h) break;
-          const float f = __uint_as_float(v[j]);
-          const size_t o = (size_t)(L.out + i) * kNrhs + m;
-          if (kind == kRunP) {
-            a.zbu[o] = f;
-          } else if (kind == kRunD) {
-            double y = a.alpha * (double)f;
-            if (a.beta != 0.0) y = fma(a.beta, a.yin[o], y);
-            a.y[o] = y;
-          } else {
-            a.y[o] = fma(a.alpha, (double)f, a.y[o]);
-          }
+          for (uint32_t i = 0; i < 16; ++i)
+            if (i < n) a.zbu[o0 + (size_t)i * kNrhs] = __uint_as_float(v[i]);
+        } else {
+          double old[16];
+#pragma unroll
+          for (uint32_t i = 0; i < 16; ++i) old[i] = (add && i < n) ? src[o0 + (size_t)i * kNrhs] : 0.0;
+#pragma unroll
+          for (uint32_t i = 0; i < 16; ++i)
+            if (i < n) a.y[o0 + (size_t)i * kNrhs] = fma(a.alpha, (double)__uint_as_float(v[i]), c * old[i]);
         }
       }
     }
@@ -384,7 +405,6 @@ __global__ void __launch_bounds__(kThreadsM, 1) k_matmat(MatmatArgs a) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const MSmem sm = mlayout(smem_raw);
   const CtaInfo ci = a.ctas[blockIdx.x];
-  const RunLite *lite = a.lite + ci.rec_begin;
   const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
   const uint32_t K = (ci.stream_bytes + kMChunkBytes - 1) >> kMChunkLog;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -407,6 +427,11 @@ __global__ void __launch_bounds__(kThreadsM, 1) k_matmat(MatmatArgs a) {
     *sm.gen0 = grid_gen0(a.gbar);
     mbar_fence_init();
   }
+  {  // the CTA's run summaries
+    const uint4 *src = reinterpret_cast<const uint4 *>(a.lite + ci.rec_begin);
+    uint4 *dst = reinterpret_cast<uint4 *>(sm.lite);
+    for (uint32_t k = threadIdx.x; k < nr; k += blockDim.x) dst[k] = __ldg(src + k);
+  }
   if (w == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(sm.tmem)),
                  "r"((uint32_t)kTmemCols)
@@ -422,7 +447,7 @@ __global__ void __launch_bounds__(kThreadsM, 1) k_matmat(MatmatArgs a) {
     return;
   }
   if (w >= kGathWarp0 && w < kGathWarp0 + kGathWarps) {
-    mr_gather(a, ci, lite, nr, sm, (uint32_t)(w - kGathWarp0));
+    mr_gather(a, ci, nr, sm, (uint32_t)(w - kGathWarp0));
     return;
   }
   if (w == kSyncWarpM) {
@@ -442,10 +467,10 @@ __global__ void __launch_bounds__(kThreadsM, 1) k_matmat(MatmatArgs a) {
     return;
   }
   if (w == kMmaWarp) {
-    if (lane == 0) mr_mma(a, lite, nr, K, sm);
+    if (lane == 0) mr_mma(a, nr, K, sm);
     __syncwarp();
   } else {
-    mr_epilogue(a, lite, nr, ci.nblk_p, sm);
+    mr_epilogue(a, nr, ci.nblk_p, sm);
   }
   // TMEM goes back once the MMAs are complete and the epilogue has read it
   tc_fence_before();

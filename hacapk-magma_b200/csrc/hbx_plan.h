@@ -77,6 +77,7 @@ constexpr int kRecBytes = 1024;    // one run record: 32-byte header + kRunSegs 
 #endif
 constexpr int kStages = HBX_STAGES;  // vector stage buffers: runs gathered ahead of the consumers
 constexpr int kMaxCtaRuns = 1024;    // run summaries a CTA keeps in shared memory
+constexpr int kMaxPairRuns = 512;    // the same for the multi-RHS engine (pair-panel plans)
 
 enum RunKind : uint16_t { kRunP = 0, kRunD = 1, kRunU = 2 };
 enum RunFlags : uint16_t { kFirst = 0x100, kLast = 0x200 };
