@@ -65,6 +65,13 @@ void free_engine(hbx_hmat *h) {
   cudaFree(h->d_refine);
   cudaFree(h->d_f32);
   cudaFree(h->d_zbum);
+  cudaFree(h->d_mrv);
+  cudaFree(h->d_mr32);
+  cudaFree(h->d_mrpart);
+  cudaFree(h->d_mrsc);
+  cudaFree(h->d_mrint);
+  cudaFree(h->d_mrdbl);
+  if (h->h_mrpin) cudaFreeHost(h->h_mrpin);
   if (h->h_pin) cudaFreeHost(h->h_pin);
   if (h->h_state) cudaFreeHost(h->h_state);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -806,6 +813,202 @@ static void release_for(stc_HACApK_leafmtxp *st) {
 void magma_init_(void) { cudaFree(nullptr); }
 
 void magma_finalize_(void) {}
+
+// ---- multi-RHS BiCGSTAB in FP64 iterative refinement ----------------------
+namespace {
+
+struct MrPinned {
+  hbx::MrScal sc[hbx::kNrhs];
+  double norm[hbx::kNrhs];
+  double thresh[hbx::kNrhs];
+  int mask[hbx::kNrhs];
+  int any;
+};
+
+int ensure_mr_workspace(hbx_hmat *hm) {
+  if (hm->d_mrv) return HBX_OK;
+  const size_t n = (size_t)hm->plan.nd * hbx::kNrhs;
+  HBX_CUDA(cudaMalloc(&hm->d_mrv, 10 * n * sizeof(double)));
+  HBX_CUDA(cudaMalloc(&hm->d_mr32, n * sizeof(float)));
+  HBX_CUDA(cudaMalloc(&hm->d_mrpart, (size_t)hbx::mr_row_blocks(hm->plan.nd) * 2 * hbx::kNrhs * sizeof(double)));
+  HBX_CUDA(cudaMalloc(&hm->d_mrsc, hbx::kNrhs * sizeof(hbx::MrScal)));
+  HBX_CUDA(cudaMalloc(&hm->d_mrint, (1 + hbx::kNrhs) * sizeof(int)));
+  HBX_CUDA(cudaMalloc(&hm->d_mrdbl, 2 * hbx::kNrhs * sizeof(double)));
+  HBX_CUDA(cudaMallocHost(&hm->h_mrpin, sizeof(MrPinned)));
+  return HBX_OK;
+}
+
+cudaError_t mr_matmat(void *ctx, const float *x, double *y, cudaStream_t s) {
+  hbx_hmat *hm = static_cast<hbx_hmat *>(ctx);
+  hbx::MatmatArgs a{};
+  a.stream = hm->d_stream;
+  a.recs = hm->d_recs;
+  a.ctas = hm->d_ctas;
+  a.lite = hm->d_lite;
+  a.x = x;
+  a.y = y;
+  a.zbu = hm->d_zbum;
+  a.alpha = 1.0;
+  a.beta = 0.0;
+  a.gbar = hm->d_gbar;
+  a.err = hm->d_err;
+  a.timeout_ns = hm->timeout_ns;
+  return hbx::launch_matmat(a, hm->num_ctas, s);
+}
+
+}  // namespace
+
+int hbx_bicgstab_multi(hbx_hmat *h, hbx_hmat *hm, const double *B, double *U, const hbx_solve_opts *opts,
+                       hbx_solve_info *info, void *stream) {
+  if (!h || !hm || !B || !U) return fail(HBX_ERR_INVALID, "hbx_bicgstab_multi: NULL argument");
+  if (int rc = single_rhs(h, "hbx_bicgstab_multi")) return rc;
+  if (hm->nrhs != hbx::kNrhs) return fail(HBX_ERR_UNSUPPORTED, "hbx_bicgstab_multi: hm is not a multi-RHS engine");
+  if (h->plan.precision != hbx::kFP64) return fail(HBX_ERR_UNSUPPORTED, "hbx_bicgstab_multi: h must hold FP64 factors");
+  if (h->plan.nd != hm->plan.nd || h->transposed != hm->transposed)
+    return fail(HBX_ERR_INVALID, "hbx_bicgstab_multi: h and hm differ (size or orientation)");
+  const double tol = opts ? opts->tol : 1e-8;
+  const int max_iter = opts ? opts->max_iter : 1000;
+  const double floor_tol = (opts && opts->inner_tol > 0.0) ? opts->inner_tol : 1e-3;
+  const int batch = (opts && opts->batch > 0) ? opts->batch : 4;
+  if (max_iter < 0 || !(tol >= 0.0)) return fail(HBX_ERR_INVALID, "hbx_bicgstab_multi: bad tol or max_iter");
+  int st = ensure_mr_workspace(hm);
+  if (st != HBX_OK) return st;
+  const int nd = h->plan.nd;
+  const size_t n = (size_t)nd * hbx::kNrhs;
+  double *r = hm->d_mrv, *rh = r + n, *p = rh + n, *ap = p + n, *t = ap + n, *at = t + n, *x = at + n, *R = x + n,
+         *T1 = R + n, *T2 = T1 + n;
+  double *d_thr = hm->d_mrdbl, *d_norm = hm->d_mrdbl + hbx::kNrhs;
+  int *d_any = hm->d_mrint, *d_mask = hm->d_mrint + 1;
+  MrPinned *pin = static_cast<MrPinned *>(hm->h_mrpin);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  auto norms = [&](const double *v) -> int {  // pin->norm[j] = ||v_j||^2
+    HBX_CUDA(hbx::mr_launch_dots(1, nd, v, v, nullptr, nullptr, hm->d_mrpart, s));
+    HBX_CUDA(hbx::mr_launch_colsum(nd, hm->d_mrpart, d_norm, s));
+    HBX_CUDA(cudaMemcpyAsync(pin->norm, d_norm, sizeof(pin->norm), cudaMemcpyDeviceToHost, s));
+    HBX_CUDA(cudaStreamSynchronize(s));
+    return HBX_OK;
+  };
+  HBX_CUDA(cudaEventRecord(hm->ev0, s));
+  if ((st = norms(B)) != HBX_OK) return st;
+  double bnorm[hbx::kNrhs], relres[hbx::kNrhs];
+  int done[hbx::kNrhs], status[hbx::kNrhs], iters[hbx::kNrhs];
+  for (int j = 0; j < hbx::kNrhs; ++j) {
+    bnorm[j] = std::sqrt(pin->norm[j]);
+    relres[j] = 1.0;
+    done[j] = 0;
+    status[j] = HBX_ERR_NOT_CONVERGED;
+    iters[j] = 0;
+  }
+  int outer = 0, launches = 1, steps = 0;
+  for (;;) {
+    // R = B - H U, FP64: one product per right-hand side still running
+    HBX_CUDA(hbx::mr_launch_transpose(nd, hbx::kNrhs, U, T1, s));
+    for (int j = 0; j < hbx::kNrhs; ++j)
+      if (!done[j]) HBX_CUDA(mv_launch(h, matvec_args(h, 1.0, T1 + (size_t)j * nd, 0.0, nullptr, T2 + (size_t)j * nd), s));
+    HBX_CUDA(hbx::mr_launch_resid(nd, B, T2, R, s));
+    if ((st = norms(R)) != HBX_OK) return st;
+    if ((st = check_device_error(h, s)) != HBX_OK) return st;
+    launches += 4 + hbx::kNrhs;
+    int running = 0, max_done_iters = 0;
+    for (int j = 0; j < hbx::kNrhs; ++j) {
+      if (done[j]) continue;
+      const double rn = std::sqrt(pin->norm[j]);
+      relres[j] = bnorm[j] > 0.0 ? rn / bnorm[j] : rn;
+      if (!std::isfinite(relres[j])) { done[j] = 1; status[j] = HBX_ERR_BREAKDOWN; continue; }
+      if (relres[j] < tol) { done[j] = 1; status[j] = HBX_OK; continue; }
+      if (iters[j] >= max_iter || outer >= 64) { done[j] = 1; continue; }
+      max_done_iters = std::max(max_done_iters, iters[j]);
+      ++running;
+    }
+    if (running == 0) break;
+    for (int j = 0; j < hbx::kNrhs; ++j) {
+      pin->mask[j] = !done[j];
+      pin->thresh[j] = done[j] ? 0.0 : std::max(floor_tol, 0.5 * tol / relres[j]) * relres[j] * (bnorm[j] > 0.0 ? bnorm[j] : 1.0);
+    }
+    HBX_CUDA(cudaMemcpyAsync(d_thr, pin->thresh, sizeof(pin->thresh), cudaMemcpyHostToDevice, s));
+    HBX_CUDA(cudaMemcpyAsync(d_mask, pin->mask, sizeof(pin->mask), cudaMemcpyHostToDevice, s));
+    HBX_CUDA(hbx::mr_launch_setup(nd, R, r, rh, p, ap, x, s));
+    HBX_CUDA(hbx::mr_launch_dots(1, nd, r, r, nullptr, nullptr, hm->d_mrpart, s));
+    HBX_CUDA(hbx::mr_launch_init(nd, hm->d_mrpart, d_thr, d_mask, hm->d_mrsc, d_any, s));
+    launches += 3;
+    hbx::MrStep a{};
+    a.nd = nd;
+    a.max_iter = std::max(1, max_iter - max_done_iters);
+    a.sc = hm->d_mrsc;
+    a.any_active = d_any;
+    a.r = r; a.rh = rh; a.p = p; a.ap = ap; a.t = t; a.at = at; a.x = x; a.part = hm->d_mrpart;
+    a.f32 = hm->d_mr32;
+    a.matmat = mr_matmat;
+    a.ctx = hm;
+    for (int k = 0; k < a.max_iter; k += batch) {
+      HBX_CUDA(cudaMemcpyAsync(&pin->any, d_any, sizeof(int), cudaMemcpyDeviceToHost, s));
+      HBX_CUDA(cudaStreamSynchronize(s));
+      if (!pin->any) break;
+      for (int b = 0; b < batch; ++b) HBX_CUDA(hbx::mr_launch_step(a, s));
+      launches += 10 * batch;
+      steps += batch;
+    }
+    HBX_CUDA(cudaMemcpyAsync(pin->sc, hm->d_mrsc, sizeof(pin->sc), cudaMemcpyDeviceToHost, s));
+    HBX_CUDA(hbx::mr_launch_add(nd, d_mask, x, U, s));
+    HBX_CUDA(cudaStreamSynchronize(s));
+    if ((st = check_device_error(hm, s)) != HBX_OK) return st;
+    ++launches;
+    for (int j = 0; j < hbx::kNrhs; ++j) {
+      if (done[j]) continue;
+      iters[j] += pin->sc[j].iters;
+      // an inner solve that broke down before its first step leaves nothing to refine
+      if (pin->sc[j].iters == 0 && pin->sc[j].status == HBX_ERR_BREAKDOWN) { done[j] = 1; status[j] = HBX_ERR_BREAKDOWN; }
+    }
+    ++outer;
+  }
+  HBX_CUDA(cudaEventRecord(hm->ev1, s));
+  HBX_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, hm->ev0, hm->ev1);
+  int worst = HBX_OK;
+  for (int j = 0; j < hbx::kNrhs; ++j) {
+    if (status[j] != HBX_OK && worst == HBX_OK) worst = status[j];
+    if (info) {
+      hbx_solve_info &I = info[j];
+      std::memset(&I, 0, sizeof(I));
+      I.iterations = iters[j];
+      I.outer = outer;
+      I.status = status[j];
+      I.bnorm = bnorm[j];
+      I.relres = relres[j];
+      I.true_relres = relres[j];
+      I.seconds = ms * 1e-3;
+      I.launches = launches;
+      I.iter_launches = steps;
+    }
+  }
+  if (worst != HBX_OK) return fail(worst, std::string("hbx_bicgstab_multi: ") + hbx_status_string(worst));
+  return HBX_OK;
+}
+
+
+int hbx_bicgstab_multi_host(hbx_hmat *h, hbx_hmat *hm, const double *B, double *U, const hbx_solve_opts *opts,
+                            hbx_solve_info *info) {
+  if (!h || !hm || !B || !U) return fail(HBX_ERR_INVALID, "hbx_bicgstab_multi_host: NULL argument");
+  if (hm->nrhs != hbx::kNrhs) return fail(HBX_ERR_UNSUPPORTED, "hbx_bicgstab_multi_host: hm is not a multi-RHS engine");
+  int st = ensure_mr_workspace(hm);
+  if (st != HBX_OK) return st;
+  const size_t bytes = (size_t)hm->plan.nd * hbx::kNrhs * sizeof(double);
+  double *dB = nullptr, *dU = nullptr;
+  HBX_CUDA(cudaMalloc(&dB, 2 * bytes));
+  dU = dB + (size_t)hm->plan.nd * hbx::kNrhs;
+  cudaStream_t s = hm->stream;
+  cudaError_t e = cudaMemcpyAsync(dB, B, bytes, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dU, U, bytes, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) { cudaFree(dB); return cuda_fail(e, "hbx_bicgstab_multi_host upload"); }
+  st = hbx_bicgstab_multi(h, hm, dB, dU, opts, info, s);
+  e = cudaMemcpyAsync(U, dU, bytes, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(dB);
+  if (e != cudaSuccess) return cuda_fail(e, "hbx_bicgstab_multi_host download");
+  return st;
+}
+
 
 void c_hacapk_adot_body_lfcpy_batch_sorted_(int *nd, stc_HACApK_leafmtxp *st_leafmtxp) {
   if (!nd || !st_leafmtxp) return;

@@ -92,6 +92,35 @@ size_t matmat_smem_bytes();
 cudaError_t configure_matmat();
 cudaError_t launch_matmat(const MatmatArgs &a, int num_ctas, cudaStream_t s);
 
+// Multi-RHS BiCGSTAB (hbx_mrhs_solve.cu): scalars of one right-hand side.
+struct MrScal {
+  double alpha, zeta, rho, beta, rr, rtol;
+  int active, iters, status, pad;
+};
+// One step for every right-hand side still running (10 launches, two of
+// them the product through `matmat`).
+struct MrStep {
+  int nd, max_iter;
+  MrScal *sc;
+  int *any_active;
+  double *r, *rh, *p, *ap, *t, *at, *x, *part;
+  float *f32;  // the product's input (p, then t, rounded to float)
+  cudaError_t (*matmat)(void *ctx, const float *x, double *y, cudaStream_t s);
+  void *ctx;
+};
+int mr_row_blocks(int nd);
+cudaError_t mr_launch_dots(int nq, int nd, const double *x0, const double *y0, const double *x1, const double *y1,
+                           double *part, cudaStream_t s);
+cudaError_t mr_launch_setup(int nd, const double *R, double *r, double *rh, double *p, double *ap, double *x,
+                            cudaStream_t s);
+cudaError_t mr_launch_init(int nd, const double *part, const double *thresh, const int *mask, MrScal *sc,
+                           int *any_active, cudaStream_t s);
+cudaError_t mr_launch_step(const MrStep &a, cudaStream_t s);
+cudaError_t mr_launch_colsum(int nd, const double *part, double *out, cudaStream_t s);
+cudaError_t mr_launch_transpose(int rows, int cols, const double *in, double *out, cudaStream_t s);
+cudaError_t mr_launch_resid(int nd, const double *B, const double *HU, double *R, cudaStream_t s);
+cudaError_t mr_launch_add(int nd, const int *mask, const double *D, double *U, cudaStream_t s);
+
 // Static scratch of hbx_matvec_noalloc (hbx_kernels.cu): 256 bytes of
 // barrier words, then room for kNoallocZbuMax zbu doubles.
 constexpr size_t kNoallocScratchBytes = size_t(1) << 20;
@@ -119,6 +148,14 @@ struct hbx_hmat {
   int transposed = 0;  // the packed stream holds H^T
   int nrhs = 1;        // right-hand sides per product (kNrhs: multi-RHS engine, hbx_matmat only)
   float *d_zbum = nullptr;  // multi-RHS engine: zbu for all right-hand sides [zbu_len][kNrhs]
+  // multi-RHS solver workspace (hbx_bicgstab_multi)
+  double *d_mrv = nullptr;      // r, rh, p, ap, t, at, x, R, and two kNrhs x nd scratch arrays
+  float *d_mr32 = nullptr;      // nd x kNrhs
+  double *d_mrpart = nullptr;   // [row blocks][2][kNrhs]
+  hbx::MrScal *d_mrsc = nullptr;
+  int *d_mrint = nullptr;       // any_active, mask[kNrhs]
+  double *d_mrdbl = nullptr;    // thresholds[kNrhs], norms[kNrhs]
+  void *h_mrpin = nullptr;      // pinned: MrScal[kNrhs], norms, thresholds, ints
   hbx::Plan plan;
   uint8_t *d_stream = nullptr;
   hbx::RunRec *d_recs = nullptr;

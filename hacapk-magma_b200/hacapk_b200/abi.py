@@ -119,6 +119,8 @@ ENGINE_SYMBOLS = [
     ("hbx_matvec", C.c_int, [_VP, C.c_double, _VP, C.c_double, _VP, _VP, _VP]),
     ("hbx_matvec_noalloc", C.c_int, [_VP, C.c_double, _VP, C.c_double, _VP, _VP, _VP]),
     ("hbx_matmat", C.c_int, [_VP, C.c_double, _VP, C.c_double, _VP, _VP, _VP]),
+    ("hbx_bicgstab_multi", C.c_int, [_VP, _VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
+    ("hbx_bicgstab_multi_host", C.c_int, [_VP, _VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     ("hbx_sync", C.c_int, [_VP, _VP]),
     ("hbx_matvec_host", C.c_int, [_VP, _DP, _DP, C.c_int, _DP, _DP]),
     ("hbx_bicgstab", C.c_int, [_VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),

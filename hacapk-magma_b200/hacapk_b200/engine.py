@@ -85,6 +85,32 @@ class Engine:
                                    C.c_void_p(yin_ptr) if yin_ptr else None, C.c_void_p(y_ptr),
                                    C.c_void_p(stream) if stream else None), "hbx_matmat")
 
+    def bicgstab_multi_host(self, multi: "Engine", B: np.ndarray, U0: np.ndarray | None = None, tol: float = 1e-8,
+                            max_iter: int = 1000, inner_tol: float = 0.0, batch: int = 0):
+        """Solves H U = B for HBX_NRHS right-hand sides (B: nd x 64) with
+        this FP64 engine for the refinement residuals and `multi` (a multi-RHS
+        engine) for the inner products; returns (U, [info dict per RHS])."""
+        B = np.ascontiguousarray(B, np.float64)
+        U = np.zeros_like(B) if U0 is None else np.array(U0, np.float64, copy=True, order="C")
+        infos = (abi.SolveInfo * abi.HBX_NRHS)()
+        o = self._opts(tol, max_iter, 0, batch, inner_tol)
+        st = self.lib.hbx_bicgstab_multi_host(self._h, multi._h, abi.dptr(B), abi.dptr(U), C.byref(o), infos)
+        res = [self._info(infos[j]) for j in range(abi.HBX_NRHS)]
+        if st not in (0, 5, 6):
+            _check(st, "hbx_bicgstab_multi_host")
+        return U, res
+
+    def bicgstab_multi_dev(self, multi: "Engine", B_ptr: int, U_ptr: int, tol: float = 1e-8, max_iter: int = 1000,
+                           inner_tol: float = 0.0, batch: int = 0, stream: int = 0, check: bool = True):
+        """Device-array form of bicgstab_multi_host (nd x 64 row-major doubles)."""
+        infos = (abi.SolveInfo * abi.HBX_NRHS)()
+        o = self._opts(tol, max_iter, 0, batch, inner_tol)
+        st = self.lib.hbx_bicgstab_multi(self._h, multi._h, C.c_void_p(B_ptr), C.c_void_p(U_ptr), C.byref(o), infos,
+                                         C.c_void_p(stream) if stream else None)
+        if check:
+            _check(st, "hbx_bicgstab_multi")
+        return [self._info(infos[j]) for j in range(abi.HBX_NRHS)]
+
     def sync(self, stream: int = 0):
         _check(self.lib.hbx_sync(self._h, C.c_void_p(stream) if stream else None), "hbx_sync")
 

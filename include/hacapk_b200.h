@@ -219,6 +219,28 @@ int hbx_matvec_noalloc(hbx_hmat *h, double alpha, const double *x, double beta,
 int hbx_matmat(hbx_hmat *h, double alpha, const float *X, double beta, const double *Yin, double *Y,
                void *stream);
 
+/* BiCGSTAB for HBX_NRHS right-hand sides at once (no counterpart in the
+ * reference): FP64 iterative refinement around the algorithm of
+ * c_hacapk_bicgstab_cax_lfmtx_gpu_ (HACApK_SOLVER.c:602-732) run for every
+ * right-hand side with its own scalars and its own stop test (a convergence
+ * mask) on `hm`, a multi-RHS engine (hbx_options.nrhs = HBX_NRHS) of the same
+ * leaf list, so both products of a step go through one tensor-core launch.
+ * Each refinement step forms R = B - H U with the FP64 engine `h` (one
+ * product per unconverged right-hand side), solves H D = R on `hm` until each
+ * residual falls by max(opts->inner_tol (0 = 1e-3), tol*||b||/||r||/2) and
+ * adds D to U; a right-hand side stops once its FP64 residual
+ * ||b - H u||/||b|| is below opts->tol, or after opts->max_iter inner steps.
+ * B and U are nd x HBX_NRHS doubles, row-major, on the device (U: x0 in,
+ * solutions out); info (nullable) receives HBX_NRHS entries, one per
+ * right-hand side (iterations = its inner steps, outer = refinement steps,
+ * true_relres = its final FP64 residual).  Returns HBX_OK when every
+ * right-hand side converged. */
+int hbx_bicgstab_multi(hbx_hmat *h, hbx_hmat *hm, const double *B, double *U, const hbx_solve_opts *opts,
+                       hbx_solve_info *info, void *stream);
+/* The same with host arrays (copies inside, on an internal stream). */
+int hbx_bicgstab_multi_host(hbx_hmat *h, hbx_hmat *hm, const double *B, double *U, const hbx_solve_opts *opts,
+                            hbx_solve_info *info);
+
 /* Mixed-precision BiCGSTAB (no counterpart in the reference): FP64
  * iterative refinement around BiCGSTAB on `hl`, an engine created on the same
  * leaf list with hbx_options.precision = HBX_FP32.  Each refinement step

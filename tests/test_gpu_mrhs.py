@@ -101,3 +101,46 @@ def test_multi_rhs_needs_fp32(gpu, build_libs):
     H = sphere(3)
     with pytest.raises(HbxError):
         Engine(H.st, H.nd, precision=abi.HBX_FP64, nrhs=abi.HBX_NRHS)
+
+
+@pytest.mark.parametrize("level", [3, 4])
+def test_multi_rhs_solve_reaches_fp64_tolerance(gpu, build_libs, level):
+    """hbx_bicgstab_multi: 64 right-hand sides (the unit-potential rhs of the
+    BEM config plus 63 N(0,1) ones) solved to 1e-8 in the FP64 norm, each
+    checked with the FP64 oracle product."""
+    import oracle
+    from hacapk_b200 import configs
+    from hacapk_b200.engine import Engine
+    H, b = configs.c1(level)
+    E64 = Engine(H.st, H.nd)
+    Em = _engine(H)
+    rng = np.random.default_rng(2)
+    B = rng.standard_normal((H.nd, 64))
+    B[:, 0] = b
+    U, infos = E64.bicgstab_multi_host(Em, B, tol=1e-8, max_iter=500)
+    worst = 0.0
+    for j in range(64):
+        assert infos[j]["status"] == 0, (j, infos[j])
+        ref = oracle.matvec(H.st, U[:, j])
+        rel = np.linalg.norm(B[:, j] - ref) / np.linalg.norm(B[:, j])
+        assert rel < 1e-8, (j, rel)
+        assert abs(rel - infos[j]["true_relres"]) <= 1e-3 * rel + 1e-15
+        worst = max(worst, rel)
+    its = [i["iterations"] for i in infos]
+    print(f"L{level}: 64 RHS, worst FP64 residual {worst:.2e}, inner steps {min(its)}..{max(its)}, "
+          f"refinement steps {infos[0]['outer']}")
+
+
+def test_multi_rhs_solve_masks_converged_columns(gpu, build_libs):
+    """A right-hand side that is zero converges at once (x = 0) and leaves
+    the others unchanged: the convergence mask holds it still."""
+    from hacapk_b200 import configs
+    from hacapk_b200.engine import Engine
+    H, b = configs.c1(3)
+    E64 = Engine(H.st, H.nd)
+    Em = _engine(H)
+    B = np.random.default_rng(3).standard_normal((H.nd, 64))
+    B[:, 7] = 0.0
+    U, infos = E64.bicgstab_multi_host(Em, B, tol=1e-8)
+    assert np.all(U[:, 7] == 0.0) and infos[7]["iterations"] == 0
+    assert all(i["status"] == 0 for i in infos)
