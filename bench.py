@@ -218,6 +218,7 @@ def run_ours(args, world, rank, local):
     E.sync(s)
     mv_us = m0.elapsed_time(m1) / reps * 1e3
     mv_gbs = info["alg_bytes"] / (mv_us * 1e-6) / 1e9
+    forms = None if args.no_forms else measure_forms(H, b, E, args, dev, stream, ms / 1e3)
     out = {
         "metric": METRIC,
         "value": ms / 1e3,
@@ -257,8 +258,77 @@ def run_ours(args, world, rank, local):
         "clocks": clk,
         "gpu_launches": launches,
     }
+    if forms is not None:
+        out["forms"] = forms
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(H, b, args)
+    return out
+
+
+def measure_forms(H, b, E, args, dev, stream, fp64_solve_s):
+    """The precision and batching forms beside the FP64 solve (same matrix,
+    same tolerance, verified by the FP64 residual): FP32 factors inside FP64
+    refinement, and 64 right-hand sides at once on the tensor cores."""
+    import numpy as np
+    import torch
+    from hacapk_b200 import abi
+    from hacapk_b200.engine import Engine
+    s = stream.cuda_stream
+    n = H.nd
+    reps = 3
+    out = {}
+    # FP32 factors, FP64 refinement, single right-hand side
+    E32 = Engine(H.st, n, precision=abi.HBX_FP32)
+    bd = torch.from_numpy(b).to(dev)
+    ud = torch.zeros(n, dtype=torch.float64, device=dev)
+    best, inf = 1e9, None
+    for _ in range(reps + 1):
+        ud.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        inf = E.bicgstab_refined_dev(E32, bd.data_ptr(), ud.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
+        torch.cuda.synchronize(dev)
+        best = min(best, time.perf_counter() - t0)
+    out["fp32_refined"] = {"solve_s": best, "true_relres": inf["true_relres"], "inner_iterations": inf["iterations"],
+                           "outer": inf["outer"], "speedup_vs_fp64": fp64_solve_s / best}
+    E32.close()
+    # 64 right-hand sides: the rhs above plus 63 seeded N(0,1) ones
+    Em = Engine(H.st, n, precision=abi.HBX_FP32, nrhs=abi.HBX_NRHS)
+    rng = np.random.default_rng(2)
+    B = rng.standard_normal((n, abi.HBX_NRHS))
+    B[:, 0] = b
+    Bd = torch.from_numpy(B).to(dev)
+    Ud = torch.zeros_like(Bd)
+    best, infos = 1e9, None
+    for _ in range(reps + 1):
+        Ud.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        infos = E.bicgstab_multi_dev(Em, Bd.data_ptr(), Ud.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
+        torch.cuda.synchronize(dev)
+        best = min(best, time.perf_counter() - t0)
+    X = torch.randn(n, abi.HBX_NRHS, device=dev).float()
+    Y = torch.zeros(n, abi.HBX_NRHS, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        Em.matmat_dev(X.data_ptr(), Y.data_ptr(), stream=s)
+    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0.record(stream)
+    for _ in range(20):
+        Em.matmat_dev(X.data_ptr(), Y.data_ptr(), stream=s)
+    m1.record(stream)
+    torch.cuda.synchronize(dev)
+    Em.sync(s)
+    mm_us = m0.elapsed_time(m1) / 20 * 1e3
+    its = [i["iterations"] for i in infos]
+    out["mrhs64"] = {
+        "rhs": abi.HBX_NRHS, "solve_s": best, "per_rhs_s": best / abi.HBX_NRHS,
+        "speedup_vs_fp64_per_rhs": fp64_solve_s * abi.HBX_NRHS / best,
+        "worst_true_relres": max(i["true_relres"] for i in infos), "converged": sum(i["status"] == 0 for i in infos),
+        "inner_iterations": [min(its), max(its)], "outer": infos[0]["outer"],
+        "matmat_us": mm_us, "matmat_tf32_tflops": abi.HBX_NRHS * Em.info["alg_flops"] / (mm_us * 1e-6) / 1e12,
+        "matmat_per_rhs_gbs": abi.HBX_NRHS * E.info["alg_bytes"] / 2 / (mm_us * 1e-6) / 1e9,
+    }
+    Em.close()
     return out
 
 
@@ -319,6 +389,7 @@ def main():
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--max-iter", type=int, default=2000)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-forms", action="store_true", help="skip the FP32-refined and 64-RHS forms")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
