@@ -332,6 +332,23 @@ def measure_forms(H, b, E, args, dev, stream, fp64_solve_s):
     return out
 
 
+def profile_matmat(args):
+    """Five 64-RHS products on the C1 workload, nothing timed: the command
+    the ncu summary of k_matmat is taken from."""
+    import torch
+    from hacapk_b200 import abi, configs
+    from hacapk_b200.engine import Engine
+    H, _ = configs.c1(args.level)
+    E = Engine(H.st, H.nd, precision=abi.HBX_FP32, nrhs=abi.HBX_NRHS)
+    X = torch.randn(H.nd, abi.HBX_NRHS, device="cuda").float()
+    Y = torch.zeros(H.nd, abi.HBX_NRHS, dtype=torch.float64, device="cuda")
+    for _ in range(5):
+        E.matmat_dev(X.data_ptr(), Y.data_ptr())
+    torch.cuda.synchronize()
+    E.sync()
+    print(json.dumps({"profile_matmat": True, "stream_bytes": E.info["stream_bytes"]}), flush=True)
+
+
 def cpu_baseline(H, b, args):
     """The compiled reference CPU H-matvec (HACApK_MAGMA.c:5-57, one thread as
     written) inside the BiCGSTAB of HACApK_SOLVER.c:254-417: one full solve."""
@@ -390,7 +407,12 @@ def main():
     ap.add_argument("--max-iter", type=int, default=2000)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-forms", action="store_true", help="skip the FP32-refined and 64-RHS forms")
+    ap.add_argument("--profile-matmat", action="store_true",
+                    help="only run five 64-RHS tensor-core products (a short command for ncu)")
     args = ap.parse_args()
+    if args.profile_matmat:
+        profile_matmat(args)
+        return
     world, rank, local = dist_setup()
     if args.impl == "reference":
         out = run_reference(args, world, rank)
