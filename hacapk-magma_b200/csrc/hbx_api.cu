@@ -72,6 +72,12 @@ void free_engine(hbx_hmat *h) {
   cudaFree(h->d_mrint);
   cudaFree(h->d_mrdbl);
   if (h->h_mrpin) cudaFreeHost(h->h_mrpin);
+  cudaFree(h->d_inst_off);
+  cudaFree(h->d_rinst);
+  cudaFree(h->d_btv);
+  cudaFree(h->d_btsc);
+  cudaFree(h->d_btdbl);
+  cudaFree(h->d_btany);
   if (h->h_pin) cudaFreeHost(h->h_pin);
   if (h->h_state) cudaFreeHost(h->h_state);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -181,7 +187,41 @@ const char *hbx_status_string(int status) {
 
 const char *hbx_last_error(void) { return g_last_error.c_str(); }
 
+static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hbx_hmat **out);
+
 int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hbx_hmat **out) {
+  return create_engine(st, nd, opt, out);
+}
+
+int hbx_create_batch(const stc_HACApK_leafmtxp *const *st, const int *nd, int count, const hbx_options *opt,
+                     hbx_hmat **out) {
+  if (!out) return fail(HBX_ERR_INVALID, "hbx_create_batch: out is NULL");
+  *out = nullptr;
+  if (opt && opt->nrhs > 1) return fail(HBX_ERR_UNSUPPORTED, "hbx_create_batch: a batch engine takes one vector");
+  hbx::CombinedLeaves cl;
+  std::string err;
+  int rc = hbx::combine_leaves(st, nd, count, cl, err);
+  if (rc != HBX_OK) return fail(rc, "hbx_create_batch: " + err);
+  hbx_hmat *h = nullptr;
+  rc = create_engine(&cl.container, cl.off[count], opt, &h);
+  if (rc != HBX_OK) return rc;
+  h->inst_off = cl.off;
+  std::vector<int> rinst((size_t)cl.off[count]);
+  for (int k = 0; k < count; ++k)
+    for (int i = cl.off[k]; i < cl.off[k + 1]; ++i) rinst[i] = k;
+  cudaError_t e;
+  if ((e = cudaMalloc(&h->d_inst_off, (count + 1) * sizeof(int))) != cudaSuccess ||
+      (e = cudaMalloc(&h->d_rinst, rinst.size() * sizeof(int))) != cudaSuccess ||
+      (e = cudaMemcpy(h->d_inst_off, cl.off.data(), (count + 1) * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(h->d_rinst, rinst.data(), rinst.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess) {
+    free_engine(h);
+    return cuda_fail(e, "hbx_create_batch: instance tables");
+  }
+  *out = h;
+  return HBX_OK;
+}
+
+static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hbx_hmat **out) {
   if (!out) return fail(HBX_ERR_INVALID, "hbx_create: out is NULL");
   *out = nullptr;
   if (!st) return fail(HBX_ERR_INVALID, "hbx_create: container is NULL");
@@ -339,6 +379,7 @@ int hbx_get_info(const hbx_hmat *h, hbx_info *info) {
   info->setup_seconds = h->setup_seconds;
   info->transposed = h->transposed;
   info->nrhs = h->nrhs;
+  info->instances = h->inst_off.empty() ? 1 : (int)h->inst_off.size() - 1;
   return HBX_OK;
 }
 
@@ -901,10 +942,15 @@ int hbx_bicgstab_multi(hbx_hmat *h, hbx_hmat *hm, const double *B, double *U, co
   }
   int outer = 0, launches = 1, steps = 0;
   for (;;) {
-    // R = B - H U, FP64: one product per right-hand side still running
+    // R = B - H U, FP64: one product per right-hand side still running whose
+    // U is not zero (x0 = 0 makes the first residual B itself)
+    if ((st = norms(U)) != HBX_OK) return st;
     HBX_CUDA(hbx::mr_launch_transpose(nd, hbx::kNrhs, U, T1, s));
-    for (int j = 0; j < hbx::kNrhs; ++j)
-      if (!done[j]) HBX_CUDA(mv_launch(h, matvec_args(h, 1.0, T1 + (size_t)j * nd, 0.0, nullptr, T2 + (size_t)j * nd), s));
+    for (int j = 0; j < hbx::kNrhs; ++j) {
+      if (done[j]) continue;
+      if (pin->norm[j] == 0.0) HBX_CUDA(cudaMemsetAsync(T2 + (size_t)j * nd, 0, (size_t)nd * sizeof(double), s));
+      else HBX_CUDA(mv_launch(h, matvec_args(h, 1.0, T1 + (size_t)j * nd, 0.0, nullptr, T2 + (size_t)j * nd), s));
+    }
     HBX_CUDA(hbx::mr_launch_resid(nd, B, T2, R, s));
     if ((st = norms(R)) != HBX_OK) return st;
     if ((st = check_device_error(h, s)) != HBX_OK) return st;
@@ -1006,6 +1052,129 @@ int hbx_bicgstab_multi_host(hbx_hmat *h, hbx_hmat *hm, const double *B, double *
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   cudaFree(dB);
   if (e != cudaSuccess) return cuda_fail(e, "hbx_bicgstab_multi_host download");
+  return st;
+}
+
+
+// ---- batched BiCGSTAB over the instances of a block-diagonal engine -----------
+namespace {
+
+cudaError_t bt_matvec(void *ctx, const double *x, double *y, cudaStream_t s) {
+  hbx_hmat *h = static_cast<hbx_hmat *>(ctx);
+  return mv_launch(h, matvec_args(h, 1.0, x, 0.0, nullptr, y), s);
+}
+
+int ensure_bt_workspace(hbx_hmat *h, int count) {
+  const size_t n = (size_t)h->plan.nd;
+  if (!h->d_inst_off) {  // a plain engine is one instance
+    const int off[2] = {0, h->plan.nd};
+    h->inst_off.assign(off, off + 2);
+    HBX_CUDA(cudaMalloc(&h->d_inst_off, 2 * sizeof(int)));
+    HBX_CUDA(cudaMemcpy(h->d_inst_off, off, 2 * sizeof(int), cudaMemcpyHostToDevice));
+    HBX_CUDA(cudaMalloc(&h->d_rinst, n * sizeof(int)));
+    HBX_CUDA(cudaMemset(h->d_rinst, 0, n * sizeof(int)));
+  }
+  if (!h->d_btv) {
+    HBX_CUDA(cudaMalloc(&h->d_btv, 6 * n * sizeof(double)));
+    HBX_CUDA(cudaMalloc(&h->d_btsc, count * sizeof(hbx::MrScal)));
+    HBX_CUDA(cudaMalloc(&h->d_btdbl, 5 * (size_t)count * sizeof(double)));
+    HBX_CUDA(cudaMalloc(&h->d_btany, sizeof(int)));
+  }
+  return HBX_OK;
+}
+
+}  // namespace
+
+int hbx_bicgstab_batch(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info,
+                       void *stream) {
+  if (!h || !b || !u) return fail(HBX_ERR_INVALID, "hbx_bicgstab_batch: NULL argument");
+  if (int rc = single_rhs(h, "hbx_bicgstab_batch")) return rc;
+  const double tol = opts ? opts->tol : 1e-8;
+  const int max_iter = opts ? opts->max_iter : 1000;
+  const int batch = (opts && opts->batch > 0) ? opts->batch : 8;
+  if (max_iter < 0 || !(tol >= 0.0)) return fail(HBX_ERR_INVALID, "hbx_bicgstab_batch: bad tol or max_iter");
+  const int count = h->inst_off.empty() ? 1 : (int)h->inst_off.size() - 1;
+  int st = ensure_bt_workspace(h, count);
+  if (st != HBX_OK) return st;
+  const size_t n = (size_t)h->plan.nd;
+  double *r = h->d_btv, *rh = r + n, *p = rh + n, *ap = p + n, *t = ap + n, *at = t + n;
+  double *dots = h->d_btdbl, *bnorm = dots + 2 * (size_t)count, *tnorm = bnorm + count;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  HBX_CUDA(cudaEventRecord(h->ev0, s));
+  // r = b - H u, rh = r, p = Ap = 0; the stop test of every instance
+  HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, r), s));
+  HBX_CUDA(hbx::bt_launch_setup(n, r, rh, p, ap, s));
+  HBX_CUDA(hbx::bt_launch_dots(2, count, h->d_inst_off, r, r, b, b, dots, s));
+  HBX_CUDA(hbx::bt_launch_init(count, dots, tol, max_iter, h->d_btsc, bnorm, h->d_btany, s));
+  hbx::BtStep a{};
+  a.n = n;
+  a.count = count;
+  a.max_iter = max_iter;
+  a.off = h->d_inst_off;
+  a.rinst = h->d_rinst;
+  a.sc = h->d_btsc;
+  a.any_active = h->d_btany;
+  a.r = r; a.rh = rh; a.p = p; a.ap = ap; a.t = t; a.at = at; a.u = u; a.dots = dots; a.bnorm = bnorm;
+  a.matvec = bt_matvec;
+  a.ctx = h;
+  int any = 0, steps = 0, launches = 4;
+  for (;;) {
+    HBX_CUDA(cudaMemcpyAsync(&any, h->d_btany, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HBX_CUDA(cudaStreamSynchronize(s));
+    if (!any || steps >= max_iter) break;
+    for (int k = 0; k < batch; ++k) HBX_CUDA(hbx::bt_launch_step(a, s));
+    steps += batch;
+    launches += 11 * batch;
+  }
+  HBX_CUDA(cudaEventRecord(h->ev1, s));
+  // the true residual of every instance: ||b - H u|| / ||b||
+  HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, r), s));
+  HBX_CUDA(hbx::bt_launch_dots(1, count, h->d_inst_off, r, r, nullptr, nullptr, tnorm, s));
+  std::vector<hbx::MrScal> sc(count);
+  std::vector<double> hb(2 * (size_t)count);
+  HBX_CUDA(cudaMemcpyAsync(sc.data(), h->d_btsc, count * sizeof(hbx::MrScal), cudaMemcpyDeviceToHost, s));
+  HBX_CUDA(cudaMemcpyAsync(hb.data(), bnorm, 2 * (size_t)count * sizeof(double), cudaMemcpyDeviceToHost, s));
+  HBX_CUDA(cudaStreamSynchronize(s));
+  if ((st = check_device_error(h, s)) != HBX_OK) return st;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  int worst = HBX_OK;
+  for (int k = 0; k < count; ++k) {
+    const double bn = hb[k], tr = std::sqrt(hb[count + k]);
+    const int stk = sc[k].status;
+    if (stk != HBX_OK && worst == HBX_OK) worst = stk;
+    if (info) {
+      hbx_solve_info &I = info[k];
+      std::memset(&I, 0, sizeof(I));
+      I.iterations = sc[k].iters;
+      I.status = stk;
+      I.bnorm = bn;
+      I.relres = bn > 0.0 ? std::sqrt(sc[k].rr) / bn : 0.0;
+      I.true_relres = bn > 0.0 ? tr / bn : tr;
+      I.seconds = ms * 1e-3;
+      I.iter_launches = steps;
+      I.launches = launches + 2;
+    }
+  }
+  if (worst != HBX_OK) return fail(worst, std::string("hbx_bicgstab_batch: ") + hbx_status_string(worst));
+  return HBX_OK;
+}
+
+int hbx_bicgstab_batch_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts,
+                            hbx_solve_info *info) {
+  if (!h || !b || !u) return fail(HBX_ERR_INVALID, "hbx_bicgstab_batch_host: NULL argument");
+  const size_t bytes = (size_t)h->plan.nd * sizeof(double);
+  double *d = nullptr;
+  HBX_CUDA(cudaMalloc(&d, 2 * bytes));
+  cudaStream_t s = h->stream;
+  cudaError_t e = cudaMemcpyAsync(d, b, bytes, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d + h->plan.nd, u, bytes, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) { cudaFree(d); return cuda_fail(e, "hbx_bicgstab_batch_host upload"); }
+  int st = hbx_bicgstab_batch(h, d, d + h->plan.nd, opts, info, s);
+  e = cudaMemcpyAsync(u, d + h->plan.nd, bytes, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(e, "hbx_bicgstab_batch_host download");
   return st;
 }
 

@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "hbx_plan.h"
 
@@ -121,6 +122,25 @@ cudaError_t mr_launch_transpose(int rows, int cols, const double *in, double *ou
 cudaError_t mr_launch_resid(int nd, const double *B, const double *HU, double *R, cudaStream_t s);
 cudaError_t mr_launch_add(int nd, const int *mask, const double *D, double *U, cudaStream_t s);
 
+// Batched BiCGSTAB over the instances of a block-diagonal engine
+// (hbx_batch.cu); one MrScal per instance, rtol = the relative tolerance.
+struct BtStep {
+  size_t n;
+  int count, max_iter;
+  const int *off, *rinst;  // instance row offsets [count + 1], instance of every row
+  MrScal *sc;
+  int *any_active;
+  double *r, *rh, *p, *ap, *t, *at, *u, *dots, *bnorm;
+  cudaError_t (*matvec)(void *ctx, const double *x, double *y, cudaStream_t s);
+  void *ctx;
+};
+cudaError_t bt_launch_dots(int nq, int count, const int *off, const double *x0, const double *y0, const double *x1,
+                           const double *y1, double *out, cudaStream_t s);
+cudaError_t bt_launch_setup(size_t n, const double *r, double *rh, double *p, double *ap, cudaStream_t s);
+cudaError_t bt_launch_init(int count, const double *dots, double tol, int max_iter, MrScal *sc, double *bnorm,
+                           int *any_active, cudaStream_t s);
+cudaError_t bt_launch_step(const BtStep &a, cudaStream_t s);
+
 // Static scratch of hbx_matvec_noalloc (hbx_kernels.cu): 256 bytes of
 // barrier words, then room for kNoallocZbuMax zbu doubles.
 constexpr size_t kNoallocScratchBytes = size_t(1) << 20;
@@ -156,6 +176,14 @@ struct hbx_hmat {
   int *d_mrint = nullptr;       // any_active, mask[kNrhs]
   double *d_mrdbl = nullptr;    // thresholds[kNrhs], norms[kNrhs]
   void *h_mrpin = nullptr;      // pinned: MrScal[kNrhs], norms, thresholds, ints
+  // block-diagonal batch of independent instances (hbx_create_batch)
+  std::vector<int> inst_off;    // row offsets, count + 1 entries (empty: one instance)
+  int *d_inst_off = nullptr;    // the same on the device
+  int *d_rinst = nullptr;       // instance of every row
+  double *d_btv = nullptr;      // r, rh, p, ap, t, at (6 nd)
+  hbx::MrScal *d_btsc = nullptr;
+  double *d_btdbl = nullptr;    // dots [count][2], bnorm [count], true norms [count]
+  int *d_btany = nullptr;
   hbx::Plan plan;
   uint8_t *d_stream = nullptr;
   hbx::RunRec *d_recs = nullptr;

@@ -548,4 +548,49 @@ int transpose_leaves(const stc_HACApK_leafmtxp *st, int nd, TransposedLeaves &ou
   return HBX_OK;
 }
 
+int combine_leaves(const stc_HACApK_leafmtxp *const *st, const int *nd, int count, CombinedLeaves &out,
+                   std::string &err) {
+  out = CombinedLeaves();
+  if (!st || !nd || count <= 0) { err = "no instances"; return HBX_ERR_INVALID; }
+  out.off.assign(count + 1, 0);
+  size_t nleaves = 0;
+  int nlfkt = 0, ktmax = 0;
+  for (int k = 0; k < count; ++k) {
+    const stc_HACApK_leafmtxp *c = st[k];
+    if (!c || nd[k] <= 0) { err = "instance " + std::to_string(k) + ": null container or nd <= 0"; return HBX_ERR_INVALID; }
+    if (c->nlf < 0 || (c->nlf > 0 && (!c->st_lf || c->st_lf_stride < (int)sizeof(stc_HACApK_leafmtx)))) {
+      err = "instance " + std::to_string(k) + ": bad leaf array (nlf, st_lf or st_lf_stride)";
+      return HBX_ERR_INVALID;
+    }
+    if ((long long)out.off[k] + nd[k] > 0x7fffffffLL) { err = "combined size exceeds 2^31"; return HBX_ERR_INVALID; }
+    out.off[k + 1] = out.off[k] + nd[k];
+    nleaves += (size_t)c->nlf;
+    nlfkt += c->nlfkt;
+    ktmax = std::max(ktmax, c->ktmax);
+  }
+  out.leaves.reserve(std::max<size_t>(1, nleaves));
+  for (int k = 0; k < count; ++k) {
+    const stc_HACApK_leafmtxp *c = st[k];
+    for (int ip = 0; ip < c->nlf; ++ip) {
+      stc_HACApK_leafmtx t = *leaf_at(c, ip);
+      if (t.nstrtl < 1 || t.nstrtt < 1 || t.nstrtl - 1 + t.ndl > nd[k] || t.nstrtt - 1 + t.ndt > nd[k]) {
+        err = "instance " + std::to_string(k) + ", leaf " + std::to_string(ip) + ": outside [1, nd]";
+        return HBX_ERR_INVALID;
+      }
+      t.nstrtl += out.off[k];
+      t.nstrtt += out.off[k];
+      out.leaves.push_back(t);
+    }
+  }
+  if (out.leaves.empty()) out.leaves.resize(1);
+  std::memset(&out.container, 0, sizeof(out.container));
+  out.container.nd = out.off[count];
+  out.container.nlf = (int)nleaves;
+  out.container.nlfkt = nlfkt;
+  out.container.ktmax = ktmax;
+  out.container.st_lf_stride = (int)sizeof(stc_HACApK_leafmtx);
+  out.container.st_lf = out.leaves.data();
+  return HBX_OK;
+}
+
 }  // namespace hbx

@@ -206,4 +206,16 @@ struct TransposedLeaves {
 };
 int transpose_leaves(const stc_HACApK_leafmtxp *st, int nd, TransposedLeaves &out, std::string &err);
 
+// The leaves of `count` independent H-matrices as one block-diagonal leaf
+// list: instance k's rows and columns move by off[k] = nd[0] + ... +
+// nd[k-1] (off[count] = the total size).  The factors are not copied: the
+// combined leaves point at the instances' own data.
+struct CombinedLeaves {
+  std::vector<stc_HACApK_leafmtx> leaves;
+  std::vector<int> off;
+  stc_HACApK_leafmtxp container{};
+};
+int combine_leaves(const stc_HACApK_leafmtxp *const *st, const int *nd, int count, CombinedLeaves &out,
+                   std::string &err);
+
 }  // namespace hbx

@@ -67,7 +67,7 @@ class Info(C.Structure):
                 ("alg_bytes", C.c_longlong), ("alg_flops", C.c_longlong),
                 ("zbu_len", C.c_longlong), ("dense_words", C.c_longlong),
                 ("lowrank_words", C.c_longlong), ("setup_seconds", C.c_double),
-                ("transposed", C.c_int), ("nrhs", C.c_int), ("reserved", C.c_int * 6)]
+                ("transposed", C.c_int), ("nrhs", C.c_int), ("instances", C.c_int), ("reserved", C.c_int * 5)]
 
 
 class SolveOpts(C.Structure):
@@ -114,11 +114,15 @@ _IP = C.POINTER(C.c_int)
 # (name, restype, argtypes) of every symbol the engine library exports.
 ENGINE_SYMBOLS = [
     ("hbx_create", C.c_int, [C.POINTER(LeafMtxP), C.c_int, C.POINTER(Options), C.POINTER(_VP)]),
+    ("hbx_create_batch", C.c_int, [C.POINTER(C.POINTER(LeafMtxP)), _IP, C.c_int, C.POINTER(Options),
+                                   C.POINTER(_VP)]),
     ("hbx_destroy", C.c_int, [_VP]),
     ("hbx_get_info", C.c_int, [_VP, C.POINTER(Info)]),
     ("hbx_matvec", C.c_int, [_VP, C.c_double, _VP, C.c_double, _VP, _VP, _VP]),
     ("hbx_matvec_noalloc", C.c_int, [_VP, C.c_double, _VP, C.c_double, _VP, _VP, _VP]),
     ("hbx_matmat", C.c_int, [_VP, C.c_double, _VP, C.c_double, _VP, _VP, _VP]),
+    ("hbx_bicgstab_batch", C.c_int, [_VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
+    ("hbx_bicgstab_batch_host", C.c_int, [_VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     ("hbx_bicgstab_multi", C.c_int, [_VP, _VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
     ("hbx_bicgstab_multi_host", C.c_int, [_VP, _VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     ("hbx_sync", C.c_int, [_VP, _VP]),

@@ -7,13 +7,17 @@ the Laplace single layer 1/(4 pi r) with the analytic flat-triangle integral
 
   C1  plain FP64: icosphere L5 (20,480 faces), leaf 32, eta 2, ACA+ 1e-5,
       rhs = 1 + N(0, (1e-3)^2) per element (seed 0), BiCGSTAB to 1e-8.
+  C5  uneven batch: `count` ellipsoids (256 in the config), semi-axes
+      U(0.3, 3), subdivision levels drawn uniformly from {2, 3, 4, 5} (so the
+      sizes 320 .. 20,480 are log-uniform), seed 5; leaf 32, eta 2, ACA+ 1e-5;
+      rhs of instance k = 1 + N(0, (1e-3)^2) per element with seed 5 + k.
 """
 from __future__ import annotations
 
 import numpy as np
 
 from . import abi
-from .hmatrix import HostHMatrix, icosphere
+from .hmatrix import HostHMatrix, ellipsoid, icosphere
 
 
 def rhs_unit_plus_noise(n: int, seed: int = 0, sigma: float = 1e-3) -> np.ndarray:
@@ -32,3 +36,17 @@ def c1(level: int = 5, nthreads: int = 0):
     H = laplace_sphere(level, 32, 2.0, 1e-5, nthreads)
     b = H.to_cluster(rhs_unit_plus_noise(H.nd, seed=0))
     return H, b
+
+
+def c5(count: int = 256, seed: int = 5, max_level: int = 5, nthreads: int = 0):
+    """[(H-matrix, rhs in cluster order)] of configuration C5: `count` independent
+    ellipsoids of uneven sizes (the batch form's workload)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        level = int(rng.integers(2, max_level + 1))
+        axes = rng.uniform(0.3, 3.0, 3)
+        H = HostHMatrix(ellipsoid(level, axes), leaf_size=32, eta=2.0, aca_eps=1e-5,
+                        kernel=abi.KERNEL_LAPLACE, nthreads=nthreads)
+        out.append((H, H.to_cluster(rhs_unit_plus_noise(H.nd, seed=seed + k))))
+    return out

@@ -48,6 +48,52 @@ class Engine:
         _check(self.lib.hbx_get_info(h, C.byref(inf)), "hbx_get_info")
         self.info = {f: getattr(inf, f) for f, _ in abi.Info._fields_ if f != "reserved"}
 
+    @classmethod
+    def batch(cls, hmats, num_ctas: int = 0, precision: int = 0) -> "Engine":
+        """One engine over independent H-matrices (objects with .st and .nd):
+        block-diagonal, instance k at rows off[k]..off[k+1] (self.offsets)."""
+        self = cls.__new__(cls)
+        self.lib = abi.engine_lib()
+        opt = abi.Options()
+        opt.precision = precision
+        opt.num_ctas = num_ctas
+        k = len(hmats)
+        sts = (C.POINTER(abi.LeafMtxP) * k)(*[C.cast(H.st, C.POINTER(abi.LeafMtxP)) for H in hmats])
+        nds = (C.c_int * k)(*[int(H.nd) for H in hmats])
+        h = C.c_void_p()
+        _check(self.lib.hbx_create_batch(sts, nds, k, C.byref(opt), C.byref(h)), "hbx_create_batch")
+        self._h = h
+        self.offsets = np.concatenate([[0], np.cumsum([int(H.nd) for H in hmats])]).astype(np.int64)
+        self.nd = int(self.offsets[-1])
+        inf = abi.Info()
+        _check(self.lib.hbx_get_info(h, C.byref(inf)), "hbx_get_info")
+        self.info = {f: getattr(inf, f) for f, _ in abi.Info._fields_ if f != "reserved"}
+        return self
+
+    def bicgstab_batch_host(self, b: np.ndarray, u0: np.ndarray | None = None, tol: float = 1e-8,
+                            max_iter: int = 1000, batch: int = 0):
+        """Every instance of a batch engine solved at once; returns (u, [info per instance])."""
+        b = np.ascontiguousarray(b, np.float64)
+        u = np.zeros(self.nd) if u0 is None else np.array(u0, np.float64, copy=True)
+        k = self.info["instances"]
+        infos = (abi.SolveInfo * k)()
+        o = self._opts(tol, max_iter, 0, batch)
+        st = self.lib.hbx_bicgstab_batch_host(self._h, abi.dptr(b), abi.dptr(u), C.byref(o), infos)
+        if st not in (0, 5, 6):
+            _check(st, "hbx_bicgstab_batch_host")
+        return u, [self._info(infos[j]) for j in range(k)]
+
+    def bicgstab_batch_dev(self, b_ptr: int, u_ptr: int, tol: float = 1e-8, max_iter: int = 1000, batch: int = 0,
+                           stream: int = 0, check: bool = True):
+        k = self.info["instances"]
+        infos = (abi.SolveInfo * k)()
+        o = self._opts(tol, max_iter, 0, batch)
+        st = self.lib.hbx_bicgstab_batch(self._h, C.c_void_p(b_ptr), C.c_void_p(u_ptr), C.byref(o), infos,
+                                         C.c_void_p(stream) if stream else None)
+        if check:
+            _check(st, "hbx_bicgstab_batch")
+        return [self._info(infos[j]) for j in range(k)]
+
     def close(self):
         if getattr(self, "_h", None):
             self.lib.hbx_destroy(self._h)

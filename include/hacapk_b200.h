@@ -145,7 +145,8 @@ typedef struct hbx_info {
   double setup_seconds;
   int transposed;          /* 1 when the engine holds H^T                    */
   int nrhs;                /* right-hand sides per product (1 or HBX_NRHS)   */
-  int reserved[6];
+  int instances;           /* independent H-matrices (hbx_create_batch)     */
+  int reserved[5];
 } hbx_info;
 
 typedef struct hbx_solve_opts {
@@ -179,6 +180,16 @@ typedef struct hbx_solve_info {
  * c_hacapk_adot_body_lfcpy_batch_sorted_ (HACApK_BATCH_SORT.c:86-858). */
 int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt,
                hbx_hmat **out);
+/* One engine over `count` independent H-matrices (no counterpart in the
+ * reference, which holds one body): their leaves form one block-diagonal
+ * H, instance k owning rows and columns [off_k, off_k + nd[k]) with
+ * off_k = nd[0] + ... + nd[k-1], so hbx_matvec multiplies every body in one
+ * persistent launch and hbx_bicgstab_batch solves them all at once.  Vectors
+ * are the instances' vectors (each in its own cluster order) one after the
+ * other.  Same options as hbx_create except nrhs. */
+int hbx_create_batch(const stc_HACApK_leafmtxp *const *st, const int *nd, int count, const hbx_options *opt,
+                     hbx_hmat **out);
+
 /* Frees device and host state (HACApK_BATCH.c:812-859). */
 int hbx_destroy(hbx_hmat *h);
 int hbx_get_info(const hbx_hmat *h, hbx_info *info);
@@ -218,6 +229,23 @@ int hbx_matvec_noalloc(hbx_hmat *h, double alpha, const double *x, double beta,
  * product of an iterative refinement.  One persistent launch on `stream`. */
 int hbx_matmat(hbx_hmat *h, double alpha, const float *X, double beta, const double *Yin, double *Y,
                void *stream);
+
+/* BiCGSTAB of every instance of a batch engine at once (no counterpart in the
+ * reference): each instance runs the algorithm of HACApK_SOLVER.c:602-732
+ * with its own scalars and stops on its own when ||r||/||b|| of its rows is
+ * below opts->tol (checked before every step, as HACApK_SOLVER.c:631) or
+ * after opts->max_iter steps (a convergence mask: its rows of the products
+ * are zero from then on).  Both products of a step are one block-diagonal
+ * launch each.  b, u: device vectors of the engine's size (u: x0 in, solutions
+ * out); info (nullable) receives one entry per instance, true_relres being
+ * recomputed as ||b - H u||/||b|| after the solve.  On a plain engine this is
+ * BiCGSTAB with plain (not compensated) dot products.  Returns HBX_OK when
+ * every instance converged. */
+int hbx_bicgstab_batch(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info,
+                       void *stream);
+/* The same with host vectors (copies inside). */
+int hbx_bicgstab_batch_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts,
+                            hbx_solve_info *info);
 
 /* BiCGSTAB for HBX_NRHS right-hand sides at once (no counterpart in the
  * reference): FP64 iterative refinement around the algorithm of

@@ -189,6 +189,18 @@ extern "C" int emu_matvec_pairs(const stc_HACApK_leafmtxp *st, int nd, int num_c
   return emu_run(st, nd, num_ctas, kFP32, true, x, y, stats, msg, msglen);
 }
 
+// Several independent H-matrices as one block-diagonal engine layout.
+extern "C" int emu_matvec_batch(const stc_HACApK_leafmtxp *const *st, const int *nd, int count, int num_ctas,
+                                const double *x, double *y, long long *stats, char *msg, int msglen) {
+  CombinedLeaves cl;
+  std::string err;
+  if (combine_leaves(st, nd, count, cl, err) != 0) {
+    std::snprintf(msg, msglen, "combine_leaves: %s", err.c_str());
+    return 1;
+  }
+  return emu_run(&cl.container, cl.off[count], num_ctas, kFP64, false, x, y, stats, msg, msglen);
+}
+
 extern "C" int emu_matvec(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, const double *x, double *y,
                           long long *stats, char *msg, int msglen) {
   return emu_matvec_prec(st, nd, num_ctas, kFP64, x, y, stats, msg, msglen);

@@ -27,6 +27,8 @@ def emu(build_libs):
     lib.emu_matvec_prec.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double),
                                     C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_char_p, C.c_int]
     lib.emu_matvec_pairs.argtypes = lib.emu_matvec.argtypes
+    lib.emu_matvec_batch.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_int, C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_char_p, C.c_int]
     return lib
 
 
@@ -229,3 +231,28 @@ def test_pair_panel_layout(emu, level, nc):
     d, lr = H.storage_words()
     assert stats[6] == 4 * (d + lr) + stats[7]
     assert stats[7] <= 0.12 * 4 * (d + lr)
+
+
+@pytest.mark.parametrize("nc", [148, 5])
+def test_block_diagonal_batch_layout(emu, nc):
+    """Independent H-matrices of different sizes packed as one block-diagonal
+    leaf list (hbx_create_batch's layout): the packed product is each
+    instance's oracle product, one after the other."""
+    import oracle
+    from hacapk_b200 import hmatrix
+    Hs = [hmatrix.HostHMatrix(hmatrix.ellipsoid(lv, ax), leaf_size=32, eta=2.0, aca_eps=1e-5)
+          for lv, ax in [(2, (1.0, 0.5, 2.0)), (3, (0.4, 1.2, 0.9)), (2, (2.5, 2.5, 0.3)), (3, (1.0, 1.0, 1.0))]]
+    nds = [H.nd for H in Hs]
+    x = np.random.default_rng(11).standard_normal(sum(nds))
+    sts = (C.c_void_p * len(Hs))(*[C.cast(H.st, C.c_void_p) for H in Hs])
+    ndarr = (C.c_int * len(Hs))(*nds)
+    y = np.zeros(sum(nds))
+    stats = (C.c_longlong * 8)()
+    msg = C.create_string_buffer(512)
+    rc = emu.emu_matvec_batch(sts, ndarr, len(Hs), nc, x.ctypes.data_as(C.POINTER(C.c_double)),
+                              y.ctypes.data_as(C.POINTER(C.c_double)), stats, msg, 512)
+    assert rc == 0, msg.value.decode()
+    off = np.concatenate([[0], np.cumsum(nds)])
+    for k, H in enumerate(Hs):
+        ref = oracle.matvec(H.st, x[off[k]:off[k + 1]])
+        assert np.abs(y[off[k]:off[k + 1]] - ref).max() <= 1e-13 * np.abs(ref).max()
