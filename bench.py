@@ -329,6 +329,47 @@ def measure_forms(H, b, E, args, dev, stream, fp64_solve_s):
         "matmat_per_rhs_gbs": abi.HBX_NRHS * E.info["alg_bytes"] / 2 / (mm_us * 1e-6) / 1e9,
     }
     Em.close()
+    # uneven batch: a 64-instance sample of C5 (the config's 256 need a minute of
+    # host construction), solved in one block-diagonal engine and one by one
+    from hacapk_b200 import configs
+    t0 = time.time()
+    inst = configs.c5(count=args.c5_count)
+    t_build = time.time() - t0
+    Eb = Engine.batch([Hk for Hk, _ in inst])
+    bb = torch.from_numpy(np.concatenate([bk for _, bk in inst])).to(dev)
+    ub = torch.zeros_like(bb)
+    best, infos = 1e9, None
+    for _ in range(reps + 1):
+        ub.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        infos = Eb.bicgstab_batch_dev(bb.data_ptr(), ub.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
+        torch.cuda.synchronize(dev)
+        best = min(best, time.perf_counter() - t0)
+    stream_gb = Eb.info["stream_bytes"] / 1e9
+    Eb.close()
+    one = 0.0
+    for Hk, bk in inst:
+        Ek = Engine(Hk.st, Hk.nd)
+        bd = torch.from_numpy(bk).to(dev)
+        ud = torch.zeros_like(bd)
+        tk = 1e9
+        for _ in range(2):
+            ud.zero_()
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            Ek.bicgstab_dev(bd.data_ptr(), ud.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
+            torch.cuda.synchronize(dev)
+            tk = min(tk, time.perf_counter() - t0)
+        one += tk
+        Ek.close()
+    its = [i["iterations"] for i in infos]
+    out["batch_c5"] = {
+        "instances": len(inst), "n_total": int(sum(Hk.nd for Hk, _ in inst)), "stream_gb": stream_gb,
+        "solve_s": best, "one_by_one_s": one, "speedup": one / best,
+        "iterations": [min(its), max(its)], "worst_true_relres": max(i["true_relres"] for i in infos),
+        "converged": sum(i["status"] == 0 for i in infos), "host_build_s": t_build,
+    }
     return out
 
 
@@ -406,7 +447,8 @@ def main():
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--max-iter", type=int, default=2000)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--no-forms", action="store_true", help="skip the FP32-refined and 64-RHS forms")
+    ap.add_argument("--no-forms", action="store_true", help="skip the FP32-refined, 64-RHS and batch forms")
+    ap.add_argument("--c5-count", type=int, default=64, help="instances of the uneven-batch sample (C5: 256)")
     ap.add_argument("--profile-matmat", action="store_true",
                     help="only run five 64-RHS tensor-core products (a short command for ncu)")
     args = ap.parse_args()
