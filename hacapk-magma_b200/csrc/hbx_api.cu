@@ -268,8 +268,11 @@ static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_option
     st = &tleaves.container;
     h->transposed = 1;
   }
+  hbx::PlanCosts costs;
+  if (opt && opt->block_cost > 0) costs.block = (uint64_t)opt->block_cost;
+  if (opt && opt->run_cost > 0) costs.run = (uint64_t)opt->run_cost;
   int st_plan = hbx::make_plan(st, nd, nc, h->plan, err, (opt && opt->precision == HBX_FP32) ? hbx::kFP32 : hbx::kFP64,
-                               nrhs > 1);
+                               nrhs > 1, costs);
   if (st_plan != HBX_OK) return bail(fail(st_plan, "hbx_create: " + err));
   const hbx::Plan &P = h->plan;
 
@@ -380,6 +383,82 @@ int hbx_get_info(const hbx_hmat *h, hbx_info *info) {
   info->transposed = h->transposed;
   info->nrhs = h->nrhs;
   info->instances = h->inst_off.empty() ? 1 : (int)h->inst_off.size() - 1;
+  info->block_cost = (int)P.costs.block;
+  info->run_cost = (int)P.costs.run;
+  return HBX_OK;
+}
+
+int hbx_autotune(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *base, int reps, hbx_options *best,
+                 double *best_us, double *default_us) {
+  if (!st || nd <= 0) return fail(HBX_ERR_INVALID, "hbx_autotune: null container or nd <= 0");
+  if (reps <= 0) reps = 20;
+  hbx_options b0{};
+  if (base) b0 = *base;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const bool multi = b0.nrhs > 1;
+  const int nrows = nd;
+  // vectors for the timed products (contents do not change the time)
+  const size_t nx = (size_t)nrows * (multi ? hbx::kNrhs : 1);
+  void *x = nullptr;
+  double *y = nullptr;
+  HBX_CUDA(cudaMalloc(&x, nx * sizeof(double)));
+  if (cudaMalloc(&y, nx * sizeof(double)) != cudaSuccess) {
+    cudaFree(x);
+    return fail(HBX_ERR_NOMEM, "hbx_autotune: vectors");
+  }
+  cudaMemset(x, 0, nx * sizeof(double));
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  struct Cand { int block, run, ctas; };
+  std::vector<Cand> cands;
+  for (int bc : {0, 2048, 32768})
+    for (int rc : {0, 1024, 16384}) cands.push_back({bc, rc, 0});
+  cands.push_back({0, 0, std::max(1, sms - 4)});
+  double t_best = 1e30, t_def = -1.0;
+  hbx_options o_best = b0;
+  int rc_all = HBX_OK;
+  for (const Cand &c : cands) {
+    hbx_options o = b0;
+    o.block_cost = c.block;
+    o.run_cost = c.run;
+    o.num_ctas = c.ctas;
+    hbx_hmat *h = nullptr;
+    int rc = hbx_create(st, nd, &o, &h);
+    if (rc != HBX_OK) { rc_all = rc; continue; }
+    auto launch = [&]() {
+      return multi ? hbx_matmat(h, 1.0, static_cast<const float *>(x), 0.0, nullptr, y, s)
+                   : hbx_matvec(h, 1.0, static_cast<const double *>(x), 0.0, nullptr, y, s);
+    };
+    for (int k = 0; k < 3 && rc == HBX_OK; ++k) rc = launch();
+    cudaEventRecord(e0, s);
+    for (int k = 0; k < reps && rc == HBX_OK; ++k) rc = launch();
+    cudaEventRecord(e1, s);
+    if (rc == HBX_OK) rc = hbx_sync(h, s);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    hbx_destroy(h);
+    if (rc != HBX_OK) { rc_all = rc; continue; }
+    const double us = 1e3 * ms / reps;
+    if (c.block == 0 && c.run == 0 && c.ctas == 0) t_def = us;
+    if (us < t_best) {
+      t_best = us;
+      o_best = o;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(s);
+  cudaFree(x);
+  cudaFree(y);
+  if (t_best >= 1e30) return fail(rc_all != HBX_OK ? rc_all : HBX_ERR_INVALID, "hbx_autotune: no candidate ran");
+  if (best) *best = o_best;
+  if (best_us) *best_us = t_best;
+  if (default_us) *default_us = t_def;
   return HBX_OK;
 }
 

@@ -38,14 +38,7 @@ bool dense_active(const stc_HACApK_leafmtx *s) { return s->ltmtx == 2 && s->ndl 
 // Bytes-equivalent fixed costs of a block and of a run, for balancing only
 // (the latency of a block end or a run switch, at the per-SM share of HBM
 // bandwidth).
-#ifndef HBX_BLOCK_COST
-#define HBX_BLOCK_COST 8192
-#endif
-#ifndef HBX_RUN_COST
-#define HBX_RUN_COST 4096
-#endif
-constexpr uint64_t kBlockOverhead = HBX_BLOCK_COST;
-constexpr uint64_t kRunOverhead = HBX_RUN_COST;
+
 
 // Min-heap load balancer (longest processing time first).
 struct Bins {
@@ -64,9 +57,9 @@ struct Bins {
   }
 };
 
-uint64_t block_cost(uint32_t h, uint32_t W, int prec) {
+uint64_t block_cost(uint32_t h, uint32_t W, int prec, const PlanCosts &c) {
   const uint64_t g = group_cols(prec), wp = (W + g - 1) / g * g;
-  return (uint64_t)elem_bytes(prec) * h * wp + kBlockOverhead + kRunOverhead * (1 + wp * elem_bytes(prec) / kStageBytes);
+  return (uint64_t)elem_bytes(prec) * h * wp + c.block + c.run * (1 + wp * elem_bytes(prec) / kStageBytes);
 }
 
 // Vector index of block column c (c < W): P -> x index, D -> x index, U -> zbu index.
@@ -122,8 +115,9 @@ uint32_t count_long(const std::vector<Seg> &segs) {
 }  // namespace
 
 int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, std::string &err, int precision,
-              bool pair_panels) {
+              bool pair_panels, const PlanCosts &costs) {
   plan = Plan();
+  plan.costs = costs;
   if (precision != kFP64 && precision != kFP32) { err = "unknown storage precision"; return HBX_ERR_INVALID; }
   if (pair_panels && precision != kFP32) { err = "panel pairs need FP32 storage"; return HBX_ERR_INVALID; }
   plan.precision = precision;
@@ -289,7 +283,7 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
     }
     dblock[a] = (uint32_t)plan.blocks.size();
     plan.blocks.push_back(b);
-    acost[a] = block_cost(b.h, b.W, precision);
+    acost[a] = block_cost(b.h, b.W, precision, costs);
     if (ucnt[a + 1] > ucnt[a]) {
       // zbu order, so that the segments of one column group merge
       std::sort(uleaf.begin() + ucnt[a], uleaf.begin() + ucnt[a + 1],
@@ -303,7 +297,7 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
       }
       ublock[a] = (uint32_t)plan.blocks.size();
       plan.blocks.push_back(u);
-      acost[a] += block_cost(u.h, u.W, precision);
+      acost[a] += block_cost(u.h, u.W, precision, costs);
     }
   }
 
@@ -313,10 +307,10 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
   {
     std::vector<uint32_t> order(pblocks);
     std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
-      return block_cost(plan.blocks[x].h, plan.blocks[x].W, precision) >
-             block_cost(plan.blocks[y].h, plan.blocks[y].W, precision);
+      return block_cost(plan.blocks[x].h, plan.blocks[x].W, precision, costs) >
+             block_cost(plan.blocks[y].h, plan.blocks[y].W, precision, costs);
     });
-    for (uint32_t b : order) cta_p[bins.take(block_cost(plan.blocks[b].h, plan.blocks[b].W, precision))].push_back(b);
+    for (uint32_t b : order) cta_p[bins.take(block_cost(plan.blocks[b].h, plan.blocks[b].W, precision, costs))].push_back(b);
     std::vector<int> aorder(natoms);
     std::iota(aorder.begin(), aorder.end(), 0);
     std::stable_sort(aorder.begin(), aorder.end(), [&](int x, int y) { return acost[x] > acost[y]; });

@@ -163,12 +163,26 @@ struct Piece {
   uint32_t leaf, c0, n, vsrc;
 };
 
+// The balancing cost model: a block costs its bytes plus `block` plus `run`
+// per stage-full of columns (the fixed work of a block end and of a run).
+#ifndef HBX_BLOCK_COST
+#define HBX_BLOCK_COST 8192
+#endif
+#ifndef HBX_RUN_COST
+#define HBX_RUN_COST 4096
+#endif
+struct PlanCosts {
+  uint64_t block = HBX_BLOCK_COST;
+  uint64_t run = HBX_RUN_COST;
+};
+
 // Host-side plan: everything needed to pack and launch.
 struct Plan {
   int nd = 0, nlf = 0, nlfkt = 0, ktmax = 0;
   int num_ctas = 0;
   int precision = kFP64;
   bool pair_panels = false;         // multi-RHS layout (even panel counts, segments in stage order)
+  PlanCosts costs;                  // the balancing cost model the plan was made with
   std::vector<Atom> atoms;          // in CTA order (atom_begin indexes this)
   std::vector<RunRec> recs;         // in CTA order
   std::vector<RunLite> lite;        // one summary per record, same order
@@ -189,7 +203,7 @@ struct Plan {
 // pair_panels (FP32 only): every run holds an even number of panels and its
 // segments stay in stage order -- the layout of the multi-RHS engine.
 int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, std::string &err,
-              int precision = kFP64, bool pair_panels = false);
+              int precision = kFP64, bool pair_panels = false, const PlanCosts &costs = PlanCosts());
 
 // Writes the packed stream of every CTA into `dst` (plan.total_bytes bytes).
 void pack_plan(const stc_HACApK_leafmtxp *st, const Plan &plan, uint8_t *dst);

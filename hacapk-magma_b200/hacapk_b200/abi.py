@@ -57,7 +57,8 @@ class LControl(C.Structure):
 
 
 class Options(C.Structure):
-    _fields_ = [("precision", C.c_int), ("num_ctas", C.c_int), ("transpose", C.c_int), ("nrhs", C.c_int), ("reserved", C.c_int * 12)]
+    _fields_ = [("precision", C.c_int), ("num_ctas", C.c_int), ("transpose", C.c_int), ("nrhs", C.c_int),
+                ("block_cost", C.c_int), ("run_cost", C.c_int), ("reserved", C.c_int * 10)]
 
 
 class Info(C.Structure):
@@ -67,7 +68,8 @@ class Info(C.Structure):
                 ("alg_bytes", C.c_longlong), ("alg_flops", C.c_longlong),
                 ("zbu_len", C.c_longlong), ("dense_words", C.c_longlong),
                 ("lowrank_words", C.c_longlong), ("setup_seconds", C.c_double),
-                ("transposed", C.c_int), ("nrhs", C.c_int), ("instances", C.c_int), ("reserved", C.c_int * 5)]
+                ("transposed", C.c_int), ("nrhs", C.c_int), ("instances", C.c_int),
+                ("block_cost", C.c_int), ("run_cost", C.c_int), ("reserved", C.c_int * 3)]
 
 
 class SolveOpts(C.Structure):
@@ -116,6 +118,8 @@ ENGINE_SYMBOLS = [
     ("hbx_create", C.c_int, [C.POINTER(LeafMtxP), C.c_int, C.POINTER(Options), C.POINTER(_VP)]),
     ("hbx_create_batch", C.c_int, [C.POINTER(C.POINTER(LeafMtxP)), _IP, C.c_int, C.POINTER(Options),
                                    C.POINTER(_VP)]),
+    ("hbx_autotune", C.c_int, [C.POINTER(LeafMtxP), C.c_int, C.POINTER(Options), C.c_int, C.POINTER(Options), _DP,
+                               _DP]),
     ("hbx_destroy", C.c_int, [_VP]),
     ("hbx_get_info", C.c_int, [_VP, C.POINTER(Info)]),
     ("hbx_matvec", C.c_int, [_VP, C.c_double, _VP, C.c_double, _VP, _VP, _VP]),

@@ -29,8 +29,23 @@ def _check(status: int, where: str):
 class Engine:
     """Packed H-matrix resident on the current CUDA device."""
 
+    @staticmethod
+    def autotune(st, nd: int, precision: int = 0, nrhs: int = 0, transpose: bool = False, reps: int = 20):
+        """Times a grid of CTA schedules on the current device (hbx_autotune);
+        returns (keyword options for Engine(...) of the fastest, its us, the default's us)."""
+        lib = abi.engine_lib()
+        base = abi.Options()
+        base.precision = precision
+        base.nrhs = nrhs
+        base.transpose = 1 if transpose else 0
+        best = abi.Options()
+        tb, td = C.c_double(0.0), C.c_double(0.0)
+        _check(lib.hbx_autotune(st, nd, C.byref(base), reps, C.byref(best), C.byref(tb), C.byref(td)), "hbx_autotune")
+        kw = {"num_ctas": best.num_ctas, "block_cost": best.block_cost, "run_cost": best.run_cost}
+        return kw, tb.value, td.value
+
     def __init__(self, st, nd: int, num_ctas: int = 0, transpose: bool = False, precision: int = 0,
-                 nrhs: int = 0):
+                 nrhs: int = 0, block_cost: int = 0, run_cost: int = 0):
         """transpose=True packs H^T: products and solves with the adjoint.
         precision=abi.HBX_FP32 stores the factors in float (half the bytes).
         nrhs=abi.HBX_NRHS (with HBX_FP32) makes a multi-RHS engine: matmat only."""
@@ -40,6 +55,8 @@ class Engine:
         opt.num_ctas = num_ctas
         opt.transpose = 1 if transpose else 0
         opt.nrhs = nrhs
+        opt.block_cost = block_cost
+        opt.run_cost = run_cost
         h = C.c_void_p()
         _check(self.lib.hbx_create(st, nd, C.byref(opt), C.byref(h)), "hbx_create")
         self._h = h

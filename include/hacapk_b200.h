@@ -128,7 +128,10 @@ typedef struct hbx_options {
   int nrhs;        /* 0 or 1: single-vector engine (hbx_matvec, solves);
                       HBX_NRHS: multi-RHS engine for hbx_matmat (needs
                       precision = HBX_FP32; no counterpart in the reference) */
-  int reserved[12];
+  int block_cost;  /* balancing cost model of the CTA schedule: the fixed   */
+  int run_cost;    /* cost of a block end and of a run, in bytes (0 = the
+                      defaults 8192 and 4096; hbx_autotune picks them)      */
+  int reserved[10];
 } hbx_options;
 
 /* Right-hand sides of one hbx_matmat call on a multi-RHS engine. */
@@ -146,7 +149,8 @@ typedef struct hbx_info {
   int transposed;          /* 1 when the engine holds H^T                    */
   int nrhs;                /* right-hand sides per product (1 or HBX_NRHS)   */
   int instances;           /* independent H-matrices (hbx_create_batch)     */
-  int reserved[5];
+  int block_cost, run_cost; /* the CTA schedule's cost model in use          */
+  int reserved[3];
 } hbx_info;
 
 typedef struct hbx_solve_opts {
@@ -189,6 +193,18 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt,
  * other.  Same options as hbx_create except nrhs. */
 int hbx_create_batch(const stc_HACApK_leafmtxp *const *st, const int *nd, int count, const hbx_options *opt,
                      hbx_hmat **out);
+
+/* Autotuner of the CTA schedule (no counterpart in the reference, whose
+ * size-class batches are fixed by HACApK_BATCH_SORT.c): builds engines for a
+ * grid of schedules -- the planner's block and run costs, and the number of
+ * CTAs -- with `base`'s precision, orientation and nrhs, times the product
+ * of each on the current device (hbx_matvec, or hbx_matmat for a multi-RHS
+ * base; 3 untimed and `reps` timed launches, CUDA events) and returns in
+ * `best` the options of the fastest, in `best_us` its time and in
+ * `default_us` the time of the defaults (both nullable).  Takes about one
+ * engine build per candidate (nine to twelve). */
+int hbx_autotune(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *base, int reps, hbx_options *best,
+                 double *best_us, double *default_us);
 
 /* Frees device and host state (HACApK_BATCH.c:812-859). */
 int hbx_destroy(hbx_hmat *h);
