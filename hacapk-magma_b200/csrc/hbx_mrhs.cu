@@ -287,6 +287,7 @@ __device__ __forceinline__ void mr_mma(const MatmatArgs &a, uint32_t nr, uint32_
     if (L.flags & kFirst) {
       // the epilogue has read this accumulator's previous block
       if (nb >= 2 && !(ok = mbar_wait(&sm.accempty[buf], ((nb >> 1) - 1) & 1, tmo))) break;
+      tc_fence_after();  // the epilogue's TMEM reads come before these MMAs' writes
       first = true;
     }
     const uint32_t nsl = run_slices(L), npair = L.npanel / 2u;
@@ -302,7 +303,6 @@ __device__ __forceinline__ void mr_mma(const MatmatArgs &a, uint32_t nr, uint32_
       }
       if (ok) ok = mbar_wait(&sm.xfull[slot], (q / kXStages) & 1, tmo);
       if (!ok) break;
-      tc_fence_after();
       uint64_t adesc = smem_desc(xst_s + slot * kSliceBytes, kChunkXBytes, 128);
       uint32_t baddr = ring_s + ((pos0 >> kMChunkLog) % kMRingChunks) * kMChunkBytes + (pos0 & (kMChunkBytes - 1));
       const uint64_t bhi = smem_desc(0, pb, 128);  // the descriptor without its address
