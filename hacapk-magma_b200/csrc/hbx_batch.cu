@@ -20,7 +20,7 @@
 namespace hbx {
 namespace {
 
-constexpr int kBt = 256;
+constexpr int kBt = 1024;  // threads of a per-body dot block
 
 // out[k][q] = x_q . y_q over the rows of instance k
 template <int NQ>

@@ -57,10 +57,39 @@ __global__ void __launch_bounds__(kVecThreads) k_mr_dots(int nd, int rpb, const 
   block_partials<NQ>(acc, part, j);
 }
 
-__device__ __forceinline__ double sum_part(const double *part, int nblk, int nq, int k, int j) {
-  double v = 0.0;
-  for (int b = 0; b < nblk; ++b) v += part[((size_t)b * nq + k) * kNrhs + j];
-  return v;
+// The scalar kernels run kScalThreads = 8 lanes per right-hand side: lane l
+// of RHS j sums the partials of blocks l, l + 8, ... (two accumulators, so
+// its loads overlap), then lane 0 adds the 8 lane sums in lane order -- a
+// fixed order, the same on every run.
+constexpr int kSumLanes = 8;
+constexpr int kScalThreads = kSumLanes * kNrhs;  // 512
+
+// out[q] (valid in lane 0 of each RHS, threads 0..kNrhs-1) = sum over the
+// blocks of part[b][q0 + q][j] for q < NQ; j = threadIdx.x % kNrhs.
+template <int NQ>
+__device__ __forceinline__ void sum_parts(const double *part, int nblk, int nq, int q0, double (&out)[NQ]) {
+  __shared__ double lanes[NQ][kScalThreads];
+  const int j = threadIdx.x % kNrhs, l = threadIdx.x / kNrhs;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double a0 = 0.0, a1 = 0.0;
+    int b = l;
+    for (; b + kSumLanes < nblk; b += 2 * kSumLanes) {
+      a0 += part[((size_t)b * nq + q0 + q) * kNrhs + j];
+      a1 += part[((size_t)(b + kSumLanes) * nq + q0 + q) * kNrhs + j];
+    }
+    if (b < nblk) a0 += part[((size_t)b * nq + q0 + q) * kNrhs + j];
+    lanes[q][threadIdx.x] = a0 + a1;
+  }
+  __syncthreads();
+  if (l == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      double v = lanes[q][j];
+      for (int k = 1; k < kSumLanes; ++k) v += lanes[q][k * kNrhs + j];
+      out[q] = v;
+    }
+  }
 }
 
 // r = rh = R, p = ap = x = 0
@@ -83,9 +112,10 @@ __global__ void k_mr_init(const double *part, int nblk, const double *thresh, co
   const int j = threadIdx.x;
   __shared__ int any;
   if (j == 0) any = 0;
-  __syncthreads();
+  double sums[1];
+  sum_parts<1>(part, nblk, 1, 0, sums);
   if (j < kNrhs) {
-    const double rr = sum_part(part, nblk, 1, 0, j);
+    const double rr = sums[0];
     MrScal q{};
     q.rho = rr;
     q.rr = rr;
@@ -118,8 +148,10 @@ __global__ void __launch_bounds__(kVecThreads) k_mr_p(size_t n, const MrScal *s,
 // alpha = rho / (rh . Ap)
 __global__ void k_mr_alpha(const double *part, int nblk, MrScal *s) {
   const int j = threadIdx.x;
+  double sums[1];
+  sum_parts<1>(part, nblk, 1, 0, sums);
   if (j >= kNrhs || !s[j].active) return;
-  const double d = sum_part(part, nblk, 1, 0, j);
+  const double d = sums[0];
   const double alpha = s[j].rho / d;
   if (d == 0.0 || !isfinite(alpha)) {
     s[j].active = 0;
@@ -147,8 +179,10 @@ __global__ void __launch_bounds__(kVecThreads) k_mr_t(size_t n, const MrScal *s,
 // zeta = (At . t) / (At . At)
 __global__ void k_mr_zeta(const double *part, int nblk, MrScal *s) {
   const int j = threadIdx.x;
+  double sums[2];
+  sum_parts<2>(part, nblk, 2, 0, sums);
   if (j >= kNrhs || !s[j].active) return;
-  const double tt = sum_part(part, nblk, 2, 0, j), aa = sum_part(part, nblk, 2, 1, j);
+  const double tt = sums[0], aa = sums[1];
   const double zeta = aa != 0.0 ? tt / aa : 0.0;
   if (!isfinite(zeta)) {
     s[j].active = 0;
@@ -185,10 +219,11 @@ __global__ void k_mr_beta(const double *part, int nblk, int max_iter, MrScal *s,
   const int j = threadIdx.x;
   __shared__ int any;
   if (j == 0) any = 0;
-  __syncthreads();
+  double sums[2];
+  sum_parts<2>(part, nblk, 2, 0, sums);
   if (j < kNrhs && s[j].active) {
     MrScal q = s[j];
-    const double rho_new = sum_part(part, nblk, 2, 0, j), rr = sum_part(part, nblk, 2, 1, j);
+    const double rho_new = sums[0], rr = sums[1];
     q.iters += 1;
     q.rr = rr;
     if (!isfinite(rr)) {
@@ -219,7 +254,9 @@ __global__ void k_mr_beta(const double *part, int nblk, int max_iter, MrScal *s,
 // out[j] = sum of part[.][0][j]  (norms of the outer loop)
 __global__ void k_mr_colsum(const double *part, int nblk, double *out) {
   const int j = threadIdx.x;
-  if (j < kNrhs) out[j] = sum_part(part, nblk, 1, 0, j);
+  double sums[1];
+  sum_parts<1>(part, nblk, 1, 0, sums);
+  if (j < kNrhs) out[j] = sums[0];
 }
 
 // out (cols x rows) = in (rows x cols), 32 x 32 tiles
@@ -284,7 +321,7 @@ cudaError_t mr_launch_setup(int nd, const double *R, double *r, double *rh, doub
 
 cudaError_t mr_launch_init(int nd, const double *part, const double *thresh, const int *mask, MrScal *sc,
                            int *any_active, cudaStream_t s) {
-  k_mr_init<<<1, kNrhs, 0, s>>>(part, mr_row_blocks(nd), thresh, mask, sc, any_active);
+  k_mr_init<<<1, kScalThreads, 0, s>>>(part, mr_row_blocks(nd), thresh, mask, sc, any_active);
   return cudaGetLastError();
 }
 
@@ -295,18 +332,18 @@ cudaError_t mr_launch_step(const MrStep &a, cudaStream_t s) {
   k_mr_p<<<grid_for(n), kVecThreads, 0, s>>>(n, a.sc, a.r, a.p, a.ap, a.f32);
   if ((e = a.matmat(a.ctx, a.f32, a.ap, s)) != cudaSuccess) return e;
   k_mr_dots<1><<<nblk, kVecThreads, 0, s>>>(a.nd, rpb, a.rh, a.ap, nullptr, nullptr, a.part);
-  k_mr_alpha<<<1, kNrhs, 0, s>>>(a.part, nblk, a.sc);
+  k_mr_alpha<<<1, kScalThreads, 0, s>>>(a.part, nblk, a.sc);
   k_mr_t<<<grid_for(n), kVecThreads, 0, s>>>(n, a.sc, a.r, a.ap, a.t, a.f32);
   if ((e = a.matmat(a.ctx, a.f32, a.at, s)) != cudaSuccess) return e;
   k_mr_dots<2><<<nblk, kVecThreads, 0, s>>>(a.nd, rpb, a.at, a.t, a.at, a.at, a.part);
-  k_mr_zeta<<<1, kNrhs, 0, s>>>(a.part, nblk, a.sc);
+  k_mr_zeta<<<1, kScalThreads, 0, s>>>(a.part, nblk, a.sc);
   k_mr_xr<<<nblk, kVecThreads, 0, s>>>(a.nd, rpb, a.sc, a.p, a.t, a.at, a.rh, a.x, a.r, a.part);
-  k_mr_beta<<<1, kNrhs, 0, s>>>(a.part, nblk, a.max_iter, a.sc, a.any_active);
+  k_mr_beta<<<1, kScalThreads, 0, s>>>(a.part, nblk, a.max_iter, a.sc, a.any_active);
   return cudaGetLastError();
 }
 
 cudaError_t mr_launch_colsum(int nd, const double *part, double *out, cudaStream_t s) {
-  k_mr_colsum<<<1, kNrhs, 0, s>>>(part, mr_row_blocks(nd), out);
+  k_mr_colsum<<<1, kScalThreads, 0, s>>>(part, mr_row_blocks(nd), out);
   return cudaGetLastError();
 }
 
