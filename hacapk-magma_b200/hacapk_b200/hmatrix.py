@@ -86,6 +86,43 @@ def read_pbs(path: str) -> Mesh:
     return Mesh(np.ascontiguousarray(xyz), np.ascontiguousarray(faces), dble)
 
 
+def write_vtk(path: str, mesh: Mesh, values: np.ndarray, name: str = "solve") -> None:
+    """Writes the mesh and one value per face (in the mesh's own face order,
+    e.g. HostHMatrix.from_cluster(u)) as a legacy ASCII VTK unstructured grid
+    of triangles -- the output of Print_result in bem-bb-fw-HACApK-0.4.2.f90
+    (:755-855): POINTS, CELLS, CELL_TYPES (5 = triangle) and CELL_DATA with
+    one scalar field."""
+    values = np.asarray(values, np.float64)
+    if values.shape != (mesh.nofc,):
+        raise ValueError(f"need one value per face ({mesh.nofc}), got {values.shape}")
+    nv, nf = mesh.xyz.shape[0], mesh.nofc
+    lines = ["# vtk DataFile Version 2.0", "B200 H-matrix BiCGSTAB result", "ASCII",
+             "DATASET UNSTRUCTURED_GRID", f"POINTS {nv} double"]
+    lines += [f"{x:.16e} {y:.16e} {z:.16e}" for x, y, z in mesh.xyz]
+    lines.append(f"CELLS {nf} {4 * nf}")
+    lines += [f"3 {a} {b} {c}" for a, b, c in mesh.faces]
+    lines.append(f"CELL_TYPES {nf}")
+    lines += ["5"] * nf
+    lines += [f"CELL_DATA {nf}", f"SCALARS {name} double 1", "LOOKUP_TABLE default"]
+    lines += [f"{v:.17e}" for v in values]
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def read_vtk_cell_scalars(path: str):
+    """(points, triangles, values) of a file written by write_vtk."""
+    tok = open(path).read().split("\n")
+    i = tok.index(next(t for t in tok if t.startswith("POINTS")))
+    nv = int(tok[i].split()[1])
+    xyz = np.array([[float(v) for v in t.split()] for t in tok[i + 1:i + 1 + nv]])
+    i = tok.index(next(t for t in tok if t.startswith("CELLS")))
+    nf = int(tok[i].split()[1])
+    tri = np.array([[int(v) for v in t.split()[1:]] for t in tok[i + 1:i + 1 + nf]], np.int32)
+    i = tok.index("LOOKUP_TABLE default")
+    vals = np.array([float(t) for t in tok[i + 1:i + 1 + nf]])
+    return xyz, tri, vals
+
+
 def default_params() -> abi.BuildParams:
     p = abi.BuildParams()
     abi.build_lib().hbx_build_default_params(C.byref(p))

@@ -143,3 +143,26 @@ def test_oracle_bicgstab_zero_rhs_and_limits(build_libs):
     b = np.random.default_rng(5).standard_normal(H.nd)
     u, n, hist, _ = oracle.bicgstab(H.st, b, tol=1e-30, max_iter=3, kind="restated")
     assert n == 3
+
+
+def test_reference_input_end_to_end_to_vtk(build_libs, tmp_path):
+    """The reference's own mesh input (bem-bb_inputs/input_1ts.pbs, ppohBEM
+    kernel as in its runs) read, built, solved (CPU oracle BiCGSTAB to 1e-8)
+    and written as the VTK result file of Print_result; the file reads back
+    with the same points, triangles and values."""
+    path = os.path.join(REFERENCE, "bem-bb_inputs", "input_1ts.pbs")
+    if not os.path.exists(path):
+        pytest.skip("reference mesh not available")
+    import oracle
+    from hacapk_b200 import abi, hmatrix
+    m = hmatrix.read_pbs(path)
+    H = hmatrix.HostHMatrix(m, leaf_size=15, eta=2.0, aca_eps=1e-6, kernel=abi.KERNEL_PPOHBEM)
+    b = H.to_cluster(np.ones(H.nd))
+    u, n, hist, _ = oracle.bicgstab(H.st, b, tol=1e-8, max_iter=500, kind="restated")
+    assert hist[n] < 1e-8
+    sol = H.from_cluster(u)
+    out = str(tmp_path / "result.vtk")
+    hmatrix.write_vtk(out, m, sol)
+    xyz, tri, vals = hmatrix.read_vtk_cell_scalars(out)
+    assert np.array_equal(tri, m.faces) and np.allclose(xyz, m.xyz, rtol=0, atol=1e-15)
+    assert np.array_equal(vals, sol)
