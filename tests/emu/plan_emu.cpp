@@ -18,14 +18,14 @@
 using namespace hbx;
 
 static int emu_run(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int precision, bool pairs, const double *x,
-                   double *y, long long *stats, char *msg, int msglen) {
+                   double *y, long long *stats, char *msg, int msglen, const PlanCosts &costs = PlanCosts()) {
   auto bad = [&](const std::string &s) {
     std::snprintf(msg, msglen, "%s", s.c_str());
     return 1;
   };
   Plan plan;
   std::string err;
-  int rc = make_plan(st, nd, num_ctas, plan, err, precision, pairs);
+  int rc = make_plan(st, nd, num_ctas, plan, err, precision, pairs, costs);
   if (rc != 0) return bad("make_plan: " + err);
   std::vector<uint8_t> buf(plan.total_bytes, 0xAB);
   pack_plan(st, plan, buf.data());
@@ -187,6 +187,16 @@ extern "C" int emu_matvec_prec(const stc_HACApK_leafmtxp *st, int nd, int num_ct
 extern "C" int emu_matvec_pairs(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, const double *x, double *y,
                                 long long *stats, char *msg, int msglen) {
   return emu_run(st, nd, num_ctas, kFP32, true, x, y, stats, msg, msglen);
+}
+
+// The layout under another balancing cost model (what hbx_autotune tries).
+extern "C" int emu_matvec_costs(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, long long block_cost,
+                                long long run_cost, const double *x, double *y, long long *stats, char *msg,
+                                int msglen) {
+  PlanCosts c;
+  c.block = (uint64_t)block_cost;
+  c.run = (uint64_t)run_cost;
+  return emu_run(st, nd, num_ctas, kFP64, false, x, y, stats, msg, msglen, c);
 }
 
 // Several independent H-matrices as one block-diagonal engine layout.

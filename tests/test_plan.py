@@ -29,6 +29,8 @@ def emu(build_libs):
     lib.emu_matvec_pairs.argtypes = lib.emu_matvec.argtypes
     lib.emu_matvec_batch.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_int, C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_char_p, C.c_int]
+    lib.emu_matvec_costs.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_longlong, C.c_longlong, C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_char_p, C.c_int]
     return lib
 
 
@@ -256,3 +258,45 @@ def test_block_diagonal_batch_layout(emu, nc):
     for k, H in enumerate(Hs):
         ref = oracle.matvec(H.st, x[off[k]:off[k + 1]])
         assert np.abs(y[off[k]:off[k + 1]] - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("block_cost,run_cost", [(1, 1), (2048, 1024), (32768, 16384), (1 << 20, 1)])
+def test_cost_models_keep_the_layout_valid(emu, block_cost, run_cost):
+    """Every balancing cost model the autotuner may pick gives a valid layout
+    (the emulator's structural checks) with the oracle's product: the model
+    only moves blocks between CTAs."""
+    import oracle
+    H = sphere(4)
+    x = np.random.default_rng(block_cost % 97).standard_normal(H.nd)
+    y = np.zeros(H.nd)
+    stats = (C.c_longlong * 8)()
+    msg = C.create_string_buffer(512)
+    rc = emu.emu_matvec_costs(C.cast(H.st, C.c_void_p), H.nd, 148, block_cost, run_cost,
+                              x.ctypes.data_as(C.POINTER(C.c_double)), y.ctypes.data_as(C.POINTER(C.c_double)),
+                              stats, msg, 512)
+    assert rc == 0, msg.value.decode()
+    ref = oracle.matvec(H.st, x)
+    assert np.abs(y - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_batch_layout_rejects_bad_instances(emu):
+    """combine_leaves refuses a missing container, a non-positive size and a
+    leaf outside its instance's [1, nd]."""
+    from hacapk_b200 import hmatrix
+    H = hmatrix.HostHMatrix(hmatrix.ellipsoid(2, (1.0, 1.0, 1.0)), leaf_size=32, eta=2.0, aca_eps=1e-5)
+    x = np.zeros(2 * H.nd)
+    y = np.zeros(2 * H.nd)
+    stats = (C.c_longlong * 8)()
+    msg = C.create_string_buffer(512)
+
+    def run(sts, nds):
+        arr = (C.c_void_p * len(sts))(*sts)
+        nd = (C.c_int * len(nds))(*nds)
+        return emu.emu_matvec_batch(arr, nd, len(sts), 148, x.ctypes.data_as(C.POINTER(C.c_double)),
+                                    y.ctypes.data_as(C.POINTER(C.c_double)), stats, msg, 512)
+
+    st = C.cast(H.st, C.c_void_p).value
+    assert run([st, st], [H.nd, H.nd]) == 0
+    assert run([st, None], [H.nd, H.nd]) != 0 and b"null container" in msg.value
+    assert run([st, st], [H.nd, 0]) != 0 and b"nd <= 0" in msg.value
+    assert run([st, st], [H.nd, H.nd - 1]) != 0 and b"outside [1, nd]" in msg.value
