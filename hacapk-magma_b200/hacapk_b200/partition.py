@@ -1,0 +1,158 @@
+"""Row-partitioned H-matvec across ranks: the reference's MPI scheme.
+
+* Row cuts at leaf row starts, balanced by stored words (HACApK_setcutrow,
+  m_HACApK_base.f90:540-581): walking the leaves in row order, a cut is set
+  at the first row of the leaf whose cumulative words pass the next multiple
+  of total / nranks.  The reference balances before the fill with a nominal
+  rank for every low-rank leaf; here the leaves are filled, so their own
+  ranks are counted.
+* Each rank keeps the leaves whose first row lies in its range
+  (HACApK_generate_frame_leafmtx, m_HACApK_base.f90:511-521) and multiplies
+  them on its own device.
+* One combination per product.  The reference all-gathers row segments
+  (MPI_Allgatherv, HACApK_SOLVER.c:106-251); a leaf that starts in one range
+  can reach rows of the next, so here the ranks' full-length partial products
+  are all-gathered and summed in rank order -- exact whatever the leaves'
+  extent, and the same sum on every rank and every run.  The vectors of the
+  solve are replicated, as in the reference's flat solver.
+
+The local product is a callable built by a factory, so the same plumbing runs
+an engine per GPU over NCCL or the CPU checker over gloo.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Callable
+
+import numpy as np
+
+from . import abi
+
+
+def _leaf_ptr(st, ip: int) -> abi.LeafMtx:
+    c = st.contents
+    base = C.cast(c.st_lf, C.c_void_p).value
+    return abi.LeafMtx.from_address(base + ip * c.st_lf_stride)
+
+
+def leaf_words(L: abi.LeafMtx) -> int:
+    """Stored words of a leaf: ndl*ndt dense, kt*(ndl+ndt) low-rank."""
+    return int(L.ndl) * int(L.ndt) if L.ltmtx == 2 else int(L.kt) * (int(L.ndl) + int(L.ndt))
+
+
+def row_cuts(st, nd: int, nranks: int) -> list[int]:
+    """cuts[0] = 0 < ... < cuts[nranks] = nd; rank r owns rows [cuts[r], cuts[r+1])."""
+    nlf = st.contents.nlf
+    leaves = [_leaf_ptr(st, ip) for ip in range(nlf)]
+    order = sorted(range(nlf), key=lambda ip: (leaves[ip].nstrtl, leaves[ip].nstrtt))
+    total = sum(leaf_words(L) for L in leaves)
+    per = total // max(1, nranks)
+    cuts = [0] * (nranks + 1)
+    cuts[nranks] = nd
+    acc, ip_cut = 0, 1
+    for ip in order:
+        L = leaves[ip]
+        acc += leaf_words(L)
+        if ip_cut < nranks and acc > per * ip_cut and L.nstrtl - 1 > cuts[ip_cut - 1]:
+            cuts[ip_cut] = L.nstrtl - 1
+            ip_cut += 1
+    for r in range(ip_cut, nranks):  # fewer leaf starts than ranks: empty ranges at the end
+        cuts[r] = nd
+    return cuts
+
+
+class LeafSubset:
+    """A leaf list holding the leaves of `st` whose first row (0-based) lies in
+    [r0, r1), in the reference C layout; the factors are not copied."""
+
+    def __init__(self, st, nd: int, r0: int, r1: int):
+        c = st.contents
+        keep = [ip for ip in range(c.nlf) if r0 <= _leaf_ptr(st, ip).nstrtl - 1 < r1]
+        self._arr = (abi.LeafMtx * max(1, len(keep)))()
+        for k, ip in enumerate(keep):
+            C.memmove(C.addressof(self._arr[k]), C.addressof(_leaf_ptr(st, ip)), C.sizeof(abi.LeafMtx))
+        self._cont = abi.LeafMtxP()
+        self._cont.nd = nd
+        self._cont.nlf = len(keep)
+        self._cont.nlfkt = sum(1 for ip in keep if _leaf_ptr(st, ip).ltmtx == 1)
+        self._cont.ktmax = max([_leaf_ptr(st, ip).kt for ip in keep] + [0])
+        self._cont.st_lf_stride = C.sizeof(abi.LeafMtx)
+        self._cont.st_lf = C.cast(self._arr, C.POINTER(abi.LeafMtx))
+        self.st = C.pointer(self._cont)
+        self.nd = nd
+        self.nlf = len(keep)
+
+
+class RowPartitionedMatvec:
+    """y = H x with the leaves split over the ranks of a torch.distributed
+    group.  `local_factory(st, nd)` returns the rank's product x -> y over its
+    own leaves (full-length y, zero on rows none of them touch); x and y are
+    torch tensors on the rank's device (CPU for gloo, CUDA for NCCL)."""
+
+    def __init__(self, st, nd: int, local_factory: Callable, group=None):
+        import torch.distributed as dist
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+        self.cuts = row_cuts(st, nd, self.world)
+        self.subset = LeafSubset(st, nd, self.cuts[self.rank], self.cuts[self.rank + 1])
+        self.local = local_factory(self.subset.st, nd)
+        self.nd = nd
+
+    def __call__(self, x):
+        import torch
+        import torch.distributed as dist
+        y = self.local(x)
+        parts = [torch.empty_like(y) for _ in range(self.world)]
+        dist.all_gather(parts, y, group=self.group)
+        out = parts[0].clone()
+        for p in parts[1:]:  # rank order: the same sum on every rank
+            out += p
+        return out
+
+
+def engine_product(st, nd: int):
+    """Local product of one rank on its GPU: an engine over the rank's leaves."""
+    import torch
+    from .engine import Engine
+    E = Engine(st, nd)
+
+    def prod(x):
+        y = torch.empty_like(x)
+        E.matvec_dev(x.data_ptr(), y.data_ptr(), stream=torch.cuda.current_stream().cuda_stream)
+        return y
+    prod.engine = E
+    return prod
+
+
+def bicgstab(matvec: Callable, b, tol: float = 1e-8, max_iter: int = 1000):
+    """BiCGSTAB of HACApK_SOLVER.c:254-417 on replicated vectors (torch
+    tensors), the product given by `matvec`; returns (u, steps, relres)."""
+    import torch
+    u = torch.zeros_like(b)
+    r = b - matvec(u)
+    rh = r.clone()
+    p = torch.zeros_like(b)
+    ap = torch.zeros_like(b)
+    bnorm = float(torch.linalg.norm(b))
+    rho_old = alpha = zeta = 1.0
+    steps = 0
+    relres = float(torch.linalg.norm(r)) / bnorm if bnorm > 0 else 0.0
+    while relres >= tol and steps < max_iter:
+        rho = float(torch.dot(rh, r))
+        if steps == 0:
+            p = r.clone()
+        else:
+            beta = (alpha / zeta) * (rho / rho_old)
+            p = r + beta * (p - zeta * ap)
+        ap = matvec(p)
+        alpha = rho / float(torch.dot(rh, ap))
+        t = r - alpha * ap
+        at = matvec(t)
+        zeta = float(torch.dot(at, t)) / float(torch.dot(at, at))
+        u = u + alpha * p + zeta * t
+        r = t - zeta * at
+        rho_old = rho
+        steps += 1
+        relres = float(torch.linalg.norm(r)) / bnorm
+    return u, steps, relres

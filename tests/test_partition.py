@@ -1,0 +1,87 @@
+"""The row-partitioned product on the CPU (gloo, world size 2): the
+reference's MPI scheme (cuts by stored words at leaf row starts,
+m_HACApK_base.f90:511-581; one combination per product,
+HACApK_SOLVER.c:106-251) with the oracle as every rank's local product.  The
+same plumbing runs an engine per GPU over NCCL; that form is not run here
+(one GPU per call on this pool)."""
+import multiprocessing as mp
+import os
+import socket
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _build():
+    sys.path.insert(0, os.path.join(ROOT, "hacapk-magma_b200"))
+    sys.path.insert(0, ROOT)
+    from hacapk_b200 import configs
+    return configs.c1(3)
+
+
+def test_row_cuts_assign_every_leaf_once(build_libs):
+    from conftest import sphere
+    from hacapk_b200 import partition
+    H = sphere(4)
+    total = sum(partition.leaf_words(H.leaf(ip)) for ip in range(H.nlf))
+    starts = {H.leaf(ip).nstrtl - 1 for ip in range(H.nlf)}
+    for nranks in (2, 3, 8):
+        cuts = partition.row_cuts(H.st, H.nd, nranks)
+        assert cuts[0] == 0 and cuts[-1] == H.nd and all(a < b for a, b in zip(cuts, cuts[1:]))
+        assert all(c in starts for c in cuts[1:-1])
+        subs = [partition.LeafSubset(H.st, H.nd, cuts[r], cuts[r + 1]) for r in range(nranks)]
+        assert sum(s.nlf for s in subs) == H.nlf
+        words = [sum(partition.leaf_words(s.st.contents.st_lf[k]) for k in range(s.nlf)) for s in subs]
+        assert sum(words) == total
+        assert max(words) <= 1.5 * total / nranks
+
+
+def _rank_main(rank, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE="2", RANK=str(rank))
+    H, b = _build()
+    import torch
+    import torch.distributed as dist
+    import oracle
+    from hacapk_b200 import partition
+    dist.init_process_group("gloo")
+    mv = partition.RowPartitionedMatvec(
+        H.st, H.nd, lambda st, nd: (lambda x: torch.from_numpy(oracle.matvec(st, x.numpy()))))
+    x = torch.from_numpy(np.random.default_rng(3).standard_normal(H.nd))
+    y = mv(x).numpy()
+    u, steps, relres = partition.bicgstab(mv, torch.from_numpy(b), tol=1e-8, max_iter=500)
+    q.put((rank, y, u.numpy(), steps, relres, mv.subset.nlf))
+    dist.destroy_process_group()
+
+
+def test_partitioned_product_and_solve_gloo(build_libs):
+    import oracle
+    import torch
+    from hacapk_b200 import partition
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_rank_main, args=(r, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    got = sorted((q.get(timeout=300) for _ in ps), key=lambda t: t[0])
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    H, b = _build()
+    x = np.random.default_rng(3).standard_normal(H.nd)
+    ref = oracle.matvec(H.st, x)
+    for rank, y, u, steps, relres, nlf in got:
+        assert 0 < nlf < H.nlf  # each rank holds part of the leaves
+        assert np.abs(y - ref).max() <= 1e-13 * np.abs(ref).max()
+    # both ranks hold the same solution (replicated vectors, same sums)
+    assert np.array_equal(got[0][2], got[1][2]) and got[0][3] == got[1][3]
+    # against the same solve with the whole product on one process
+    _, n1, rel1 = partition.bicgstab(lambda v: torch.from_numpy(oracle.matvec(H.st, v.numpy())),
+                                      torch.from_numpy(b), tol=1e-8, max_iter=500)
+    assert abs(got[0][3] - n1) <= 1 and got[0][4] < 1e-8
+    rel = np.linalg.norm(b - oracle.matvec(H.st, got[0][2])) / np.linalg.norm(b)
+    assert rel < 1.05e-8
