@@ -85,3 +85,31 @@ def test_partitioned_product_and_solve_gloo(build_libs):
     assert abs(got[0][3] - n1) <= 1 and got[0][4] < 1e-8
     rel = np.linalg.norm(b - oracle.matvec(H.st, got[0][2])) / np.linalg.norm(b)
     assert rel < 1.05e-8
+
+
+import pytest  # noqa: E402
+
+
+@pytest.mark.gpu
+def test_rank_subsets_as_engines_on_one_gpu(gpu, build_libs):
+    """The GPU side of the partitioned form without the collective: each
+    rank's leaf subset as its own engine (engine_product), their products
+    summed in rank order, equal the oracle's product."""
+    import pytest
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    import oracle
+    from hacapk_b200 import configs, partition
+    H, _ = configs.c1(4)
+    cuts = partition.row_cuts(H.st, H.nd, 3)
+    subs = [partition.LeafSubset(H.st, H.nd, cuts[r], cuts[r + 1]) for r in range(3)]
+    prods = [partition.engine_product(s.st, H.nd) for s in subs]
+    x = np.random.default_rng(8).standard_normal(H.nd)
+    xd = torch.from_numpy(x).cuda()
+    y = prods[0](xd).clone()
+    for pr in prods[1:]:
+        y += pr(xd)
+    torch.cuda.synchronize()
+    ref = oracle.matvec(H.st, x)
+    assert np.abs(y.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
