@@ -156,3 +156,71 @@ def bicgstab(matvec: Callable, b, tol: float = 1e-8, max_iter: int = 1000):
         steps += 1
         relres = float(torch.linalg.norm(r)) / bnorm
     return u, steps, relres
+
+
+def diagonal_scaling(st, nd: int) -> np.ndarray:
+    """1/sqrt(|a_ii|) from the diagonal of the leaves that sit on the diagonal
+    (nstrtl == nstrtt, dense), the right scaling of the pipelined solver of
+    HACApK_SOLVER_PIPE.c:233-253 (1 where no dense diagonal leaf covers a row)."""
+    d = np.zeros(nd)
+    for ip in range(st.contents.nlf):
+        L = _leaf_ptr(st, ip)
+        if L.ltmtx == 2 and L.nstrtl == L.nstrtt and L.ndl > 0:
+            a = np.ctypeslib.as_array(L.a1, shape=(L.ndl * L.ndt,))
+            n = min(L.ndl, L.ndt)
+            d[L.nstrtl - 1:L.nstrtl - 1 + n] = a[np.arange(n) * (L.ndt + 1)]
+    out = np.ones(nd)
+    nz = d != 0.0
+    out[nz] = 1.0 / np.sqrt(np.abs(d[nz]))
+    return out
+
+
+def bicgstab_pipelined(matvec: Callable, b, tol: float = 1e-8, max_iter: int = 1000, scale=None):
+    """Pipelined BiCGSTAB of HACApK_SOLVER_PIPE.c:144-600 ("version 1") on
+    replicated vectors (torch tensors): the products of the auxiliary vectors
+    s = A p and z = A s are carried by recurrences, so a step has two
+    products (v = A z and t = A w) and two reduction points (zeta, then five
+    dot products for beta and alpha) instead of four.  `scale` (a tensor,
+    e.g. diagonal_scaling) applies the reference's right scaling: the solver
+    iterates on A diag(scale) and returns u = diag(scale) x.  Returns
+    (u, steps, relres) with relres the recursive residual."""
+    import torch
+    D = scale if scale is not None else None
+    op = (lambda v: matvec(D * v)) if D is not None else matvec
+    x = torch.zeros_like(b)
+    r = b - op(x)
+    r0 = r.clone()
+    w = op(r)
+    t = op(w)
+    bnorm = float(torch.linalg.norm(b))
+    znorm = float(torch.dot(r, r))
+    alpha = znorm / float(torch.dot(w, r))
+    beta = zeta = 0.0
+    relres = (znorm ** 0.5) / bnorm if bnorm > 0 else 0.0
+    p = s = z = None
+    steps = 0
+    while relres >= tol and steps < max_iter:
+        if steps == 0:
+            p, s, z = r.clone(), w.clone(), t.clone()
+        else:
+            p = r + beta * (p - zeta * s)
+            s = w + beta * (s - zeta * z)
+            z = t + beta * (z - zeta * v)
+        q = r - alpha * s
+        y = w - alpha * z
+        zeta = float(torch.dot(y, q)) / float(torch.dot(y, y))
+        v = op(z)
+        x = x + alpha * p + zeta * q
+        r = q - zeta * y
+        w = y - zeta * (t - alpha * v)
+        znorm_old = znorm
+        znorm = float(torch.dot(r, r0))
+        zw, zs, zz = float(torch.dot(w, r0)), float(torch.dot(s, r0)), float(torch.dot(z, r0))
+        rr = float(torch.dot(r, r))
+        beta = (alpha / zeta) * (znorm / znorm_old)
+        alpha = znorm / (zw + beta * zs - beta * zeta * zz)
+        t = op(w)
+        steps += 1
+        relres = (rr ** 0.5) / bnorm
+    u = D * x if D is not None else x
+    return u, steps, relres

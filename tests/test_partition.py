@@ -113,3 +113,21 @@ def test_rank_subsets_as_engines_on_one_gpu(gpu, build_libs):
     torch.cuda.synchronize()
     ref = oracle.matvec(H.st, x)
     assert np.abs(y.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_pipelined_bicgstab_converges_like_the_flat_solver(build_libs):
+    """The pipelined solver of HACApK_SOLVER_PIPE.c (two reduction points a
+    step) reaches 1e-8 in the FP64 residual within a few steps of the flat
+    solver, with and without the reference's diagonal right scaling."""
+    import oracle
+    import torch
+    from hacapk_b200 import partition
+    H, b = _build()
+    mv = lambda v: torch.from_numpy(oracle.matvec(H.st, v.numpy()))  # noqa: E731
+    bt = torch.from_numpy(b)
+    _, n_flat, _ = partition.bicgstab(mv, bt, tol=1e-8, max_iter=500)
+    for scale in (None, torch.from_numpy(partition.diagonal_scaling(H.st, H.nd))):
+        u, n, relres = partition.bicgstab_pipelined(mv, bt, tol=1e-8, max_iter=500, scale=scale)
+        true = np.linalg.norm(b - oracle.matvec(H.st, u.numpy())) / np.linalg.norm(b)
+        assert relres < 1e-8 and true < 1e-7, (scale is None, relres, true)
+        assert abs(n - n_flat) <= max(3, n_flat // 4), (n, n_flat)
