@@ -300,3 +300,38 @@ def test_batch_layout_rejects_bad_instances(emu):
     assert run([st, None], [H.nd, H.nd]) != 0 and b"null container" in msg.value
     assert run([st, st], [H.nd, 0]) != 0 and b"nd <= 0" in msg.value
     assert run([st, st], [H.nd, H.nd - 1]) != 0 and b"outside [1, nd]" in msg.value
+
+
+def test_pair_panel_layout_edge_cases(emu):
+    """The multi-RHS layout on the edge leaves of test_edge_cases plus an atom
+    that only low-rank leaves touch (its D block is empty: one run of no
+    panels) and an empty leaf list: runs stay whole panel pairs, the float
+    product matches the dense one within float rounding."""
+    rng = np.random.default_rng(19)
+    nd = 100
+    leaves = [
+        (2, 0, 1, 40, 1, 100, rng.standard_normal(40 * 100)),
+        (1, 0, 41, 30, 1, 50, np.zeros(0)),
+        (1, 3, 41, 30, 51, 50, rng.standard_normal(3 * (30 + 50))),
+        (1, 70, 71, 30, 1, 100, rng.standard_normal(70 * 130)),
+        (2, 0, 41, 30, 1, 50, rng.standard_normal(30 * 50)),
+    ]
+    P, keep = _custom(leaves, nd)
+    x = rng.standard_normal(nd)
+    ref = _dense_of(leaves, nd) @ x
+    for nc in (1, 5, 148):
+        y = np.zeros(nd)
+        stats = (C.c_longlong * 8)()
+        msg = C.create_string_buffer(512)
+        rc = emu.emu_matvec_pairs(C.cast(C.pointer(P), C.c_void_p), nd, nc, x.ctypes.data_as(C.POINTER(C.c_double)),
+                                  y.ctypes.data_as(C.POINTER(C.c_double)), stats, msg, 512)
+        assert rc == 0, msg.value.decode()
+        assert np.abs(y - ref).max() <= 2e-6 * np.abs(ref).max()
+    P0, keep0 = _custom([], 33)
+    y = np.ones(33)
+    stats = (C.c_longlong * 8)()
+    msg = C.create_string_buffer(512)
+    rc = emu.emu_matvec_pairs(C.cast(C.pointer(P0), C.c_void_p), 33, 148, np.ones(33).ctypes.data_as(C.POINTER(C.c_double)),
+                              y.ctypes.data_as(C.POINTER(C.c_double)), stats, msg, 512)
+    assert rc == 0, msg.value.decode()
+    assert np.all(y == 0.0)
