@@ -219,7 +219,9 @@ def run_ours(args, world, rank, local):
     E.sync(s)
     mv_us = m0.elapsed_time(m1) / reps * 1e3
     mv_gbs = info["alg_bytes"] / (mv_us * 1e-6) / 1e9
-    forms = None if args.no_forms else measure_forms(H, b, E, args, dev, stream, ms / 1e3)
+    # the forms are a single-GPU report (like cpu_baseline): the scaling runs
+    # time the FP64 solve only
+    forms = None if (args.no_forms or world > 1) else measure_forms(H, b, E, args, dev, stream, ms / 1e3)
     out = {
         "metric": METRIC,
         "value": ms / 1e3,
