@@ -352,7 +352,7 @@ int hbx_destroy(hbx_hmat *h) {
 // Diagnostics: copies the per-CTA phase stamps of the last k_matvec
 // (HBX_PROFILE=1 at create time) into out[num_ctas*8]; returns the count.
 int hbx_debug_phase_stamps(hbx_hmat *h, unsigned long long *out, int cap) {
-  if (!h || !out || !h->d_prof) return 0;
+  if (!h || !out || !h->d_prof || cap <= 0) return 0;
   const int n = std::min(cap, h->num_ctas * 16);
   cudaDeviceSynchronize();
   cudaMemcpy(out, h->d_prof, (size_t)n * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
@@ -945,16 +945,18 @@ struct MrPinned {
   int any;
 };
 
+// Each buffer is tested on its own, so a call after a failed allocation
+// completes the set instead of running on a null pointer.
 int ensure_mr_workspace(hbx_hmat *hm) {
-  if (hm->d_mrv) return HBX_OK;
   const size_t n = (size_t)hm->plan.nd * hbx::kNrhs;
-  HBX_CUDA(cudaMalloc(&hm->d_mrv, 10 * n * sizeof(double)));
-  HBX_CUDA(cudaMalloc(&hm->d_mr32, n * sizeof(float)));
-  HBX_CUDA(cudaMalloc(&hm->d_mrpart, (size_t)hbx::mr_row_blocks(hm->plan.nd) * 2 * hbx::kNrhs * sizeof(double)));
-  HBX_CUDA(cudaMalloc(&hm->d_mrsc, hbx::kNrhs * sizeof(hbx::MrScal)));
-  HBX_CUDA(cudaMalloc(&hm->d_mrint, (1 + hbx::kNrhs) * sizeof(int)));
-  HBX_CUDA(cudaMalloc(&hm->d_mrdbl, 2 * hbx::kNrhs * sizeof(double)));
-  HBX_CUDA(cudaMallocHost(&hm->h_mrpin, sizeof(MrPinned)));
+  if (!hm->d_mrv) HBX_CUDA(cudaMalloc(&hm->d_mrv, 10 * n * sizeof(double)));
+  if (!hm->d_mr32) HBX_CUDA(cudaMalloc(&hm->d_mr32, n * sizeof(float)));
+  if (!hm->d_mrpart)
+    HBX_CUDA(cudaMalloc(&hm->d_mrpart, (size_t)hbx::mr_row_blocks(hm->plan.nd) * 2 * hbx::kNrhs * sizeof(double)));
+  if (!hm->d_mrsc) HBX_CUDA(cudaMalloc(&hm->d_mrsc, hbx::kNrhs * sizeof(hbx::MrScal)));
+  if (!hm->d_mrint) HBX_CUDA(cudaMalloc(&hm->d_mrint, (1 + hbx::kNrhs) * sizeof(int)));
+  if (!hm->d_mrdbl) HBX_CUDA(cudaMalloc(&hm->d_mrdbl, 2 * hbx::kNrhs * sizeof(double)));
+  if (!hm->h_mrpin) HBX_CUDA(cudaMallocHost(&hm->h_mrpin, sizeof(MrPinned)));
   return HBX_OK;
 }
 
@@ -984,8 +986,8 @@ int hbx_bicgstab_multi(hbx_hmat *h, hbx_hmat *hm, const double *B, double *U, co
   if (int rc = single_rhs(h, "hbx_bicgstab_multi")) return rc;
   if (hm->nrhs != hbx::kNrhs) return fail(HBX_ERR_UNSUPPORTED, "hbx_bicgstab_multi: hm is not a multi-RHS engine");
   if (h->plan.precision != hbx::kFP64) return fail(HBX_ERR_UNSUPPORTED, "hbx_bicgstab_multi: h must hold FP64 factors");
-  if (h->plan.nd != hm->plan.nd || h->transposed != hm->transposed)
-    return fail(HBX_ERR_INVALID, "hbx_bicgstab_multi: h and hm differ (size or orientation)");
+  if (h->plan.nd != hm->plan.nd || h->transposed != hm->transposed || h->device != hm->device)
+    return fail(HBX_ERR_INVALID, "hbx_bicgstab_multi: h and hm differ (size, orientation or device)");
   const double tol = opts ? opts->tol : 1e-8;
   const int max_iter = opts ? opts->max_iter : 1000;
   const double floor_tol = (opts && opts->inner_tol > 0.0) ? opts->inner_tol : 1e-3;
@@ -1143,22 +1145,23 @@ cudaError_t bt_matvec(void *ctx, const double *x, double *y, cudaStream_t s) {
   return mv_launch(h, matvec_args(h, 1.0, x, 0.0, nullptr, y), s);
 }
 
+// A plain engine is one instance.  Its tables are published (inst_off set)
+// only once both are on the device, and each work buffer is tested on its
+// own, so a call after a failed allocation never runs on a null pointer.
 int ensure_bt_workspace(hbx_hmat *h, int count) {
   const size_t n = (size_t)h->plan.nd;
-  if (!h->d_inst_off) {  // a plain engine is one instance
+  if (h->inst_off.empty()) {
     const int off[2] = {0, h->plan.nd};
-    h->inst_off.assign(off, off + 2);
-    HBX_CUDA(cudaMalloc(&h->d_inst_off, 2 * sizeof(int)));
+    if (!h->d_inst_off) HBX_CUDA(cudaMalloc(&h->d_inst_off, 2 * sizeof(int)));
+    if (!h->d_rinst) HBX_CUDA(cudaMalloc(&h->d_rinst, n * sizeof(int)));
     HBX_CUDA(cudaMemcpy(h->d_inst_off, off, 2 * sizeof(int), cudaMemcpyHostToDevice));
-    HBX_CUDA(cudaMalloc(&h->d_rinst, n * sizeof(int)));
     HBX_CUDA(cudaMemset(h->d_rinst, 0, n * sizeof(int)));
+    h->inst_off.assign(off, off + 2);
   }
-  if (!h->d_btv) {
-    HBX_CUDA(cudaMalloc(&h->d_btv, 6 * n * sizeof(double)));
-    HBX_CUDA(cudaMalloc(&h->d_btsc, count * sizeof(hbx::MrScal)));
-    HBX_CUDA(cudaMalloc(&h->d_btdbl, 5 * (size_t)count * sizeof(double)));
-    HBX_CUDA(cudaMalloc(&h->d_btany, sizeof(int)));
-  }
+  if (!h->d_btv) HBX_CUDA(cudaMalloc(&h->d_btv, 6 * n * sizeof(double)));
+  if (!h->d_btsc) HBX_CUDA(cudaMalloc(&h->d_btsc, count * sizeof(hbx::MrScal)));
+  if (!h->d_btdbl) HBX_CUDA(cudaMalloc(&h->d_btdbl, 5 * (size_t)count * sizeof(double)));
+  if (!h->d_btany) HBX_CUDA(cudaMalloc(&h->d_btany, sizeof(int)));
   return HBX_OK;
 }
 
