@@ -59,22 +59,41 @@ def ncu_traffic(kernel: str):
 
 
 class Clocks:
-    """nvidia-smi sampler for the timed region."""
+    """nvidia-smi sampler for the timed region.  start() returns once the
+    sampler has written its first line (nvidia-smi takes a good part of a
+    second to come up, longer than a short timed region), and that line is
+    dropped: the samples kept are the ones taken from the start of the timed
+    region to stop()."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    INTERVAL_MS = 50
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, exe: str = "nvidia-smi"):
         self.index = index
+        self.exe = exe
         self.proc = None
 
-    def start(self):
+    def start(self, ready_timeout_s: float = 10.0):
+        import select
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+            self.proc = subprocess.Popen([self.exe, "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", str(self.INTERVAL_MS)],
                                          stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
         except OSError:
             self.proc = None
+            return
+        # the sample taken before the timed region, read from the descriptor
+        # itself (communicate() reads the descriptor, not the text buffer)
+        fd = self.proc.stdout.fileno()
+        deadline = time.monotonic() + ready_timeout_s
+        while True:
+            left = deadline - time.monotonic()
+            if left <= 0 or not select.select([fd], [], [], left)[0]:
+                break
+            ch = os.read(fd, 1)
+            if not ch or ch == b"\n":
+                break
 
     def stop(self) -> dict:
         if self.proc is None:
