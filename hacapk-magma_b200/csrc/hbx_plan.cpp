@@ -59,7 +59,7 @@ struct Bins {
 
 uint64_t block_cost(uint32_t h, uint32_t W, int prec, const PlanCosts &c) {
   const uint64_t g = group_cols(prec), wp = (W + g - 1) / g * g;
-  return (uint64_t)elem_bytes(prec) * h * wp + c.block + c.run * (1 + wp * elem_bytes(prec) / kStageBytes);
+  return (uint64_t)elem_bytes(prec) * h * wp + c.block + c.run * (1 + wp * stage_elem_bytes(prec) / kStageBytes);
 }
 
 // Vector index of block column c (c < W): P -> x index, D -> x index, U -> zbu index.
@@ -118,7 +118,10 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
               bool pair_panels, const PlanCosts &costs) {
   plan = Plan();
   plan.costs = costs;
-  if (precision != kFP64 && precision != kFP32) { err = "unknown storage precision"; return HBX_ERR_INVALID; }
+  if (precision != kFP64 && precision != kFP32 && precision != kBF16) {
+    err = "unknown storage precision";
+    return HBX_ERR_INVALID;
+  }
   if (pair_panels && precision != kFP32) { err = "panel pairs need FP32 storage"; return HBX_ERR_INVALID; }
   plan.precision = precision;
   plan.pair_panels = pair_panels;
@@ -126,7 +129,7 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
   // run widths are multiples of RG columns: whole panels, or whole panel
   // pairs (the K = 8 of one TF32 tensor-core step) for the multi-RHS engine
   const uint32_t RG = pair_panels ? 2 * G : G;
-  const uint32_t stage_cols = kStageBytes / elem_bytes(precision);
+  const uint32_t stage_cols = kStageBytes / stage_elem_bytes(precision);
   if (!st || nd <= 0 || num_ctas <= 0) { err = "null container, nd <= 0 or no CTAs"; return HBX_ERR_INVALID; }
   const int nlf = st->nlf;
   if (nlf < 0 || (nlf > 0 && (!st->st_lf || st->st_lf_stride < (int)sizeof(stc_HACApK_leafmtx)))) {
@@ -430,13 +433,15 @@ void pack_plan(const stc_HACApK_leafmtxp *st, const Plan &plan, uint8_t *dst) {
       const Run &r = plan.recs[info.rec_begin + k].hdr;
       const Block &b = plan.blocks[r.block];
       const uint32_t h = r.nrow, G = group_cols(plan.precision), ncol = G * r.npanel;
-      const bool f32 = plan.precision == kFP32;
+      const int prec = plan.precision;
       double *d = reinterpret_cast<double *>(base + r.pos);
       float *f = reinterpret_cast<float *>(base + r.pos);
+      uint16_t *hb = reinterpret_cast<uint16_t *>(base + r.pos);
       // element (row i, run column cc): panel cc/G, row i, slot cc%G (16-byte rows)
       auto put = [&](uint32_t i, uint32_t cc, double v) {
         const size_t k = ((size_t)(cc / G) * h + i) * G + cc % G;
-        if (f32) f[k] = (float)v;
+        if (prec == kBF16) hb[k] = bf16_from_double(v);
+        else if (prec == kFP32) f[k] = (float)v;
         else d[k] = v;
       };
       if (b.kind == kRunP) {

@@ -22,13 +22,15 @@
 // between the two so that the barrier latency is hidden.
 //
 // A block is stored as panels of column groups, each h x G row-major with
-// 16-byte rows: G = 2 double columns (FP64 storage) or G = 4 float columns
-// (FP32 storage).  One 16-byte shared-memory load then gives a lane one row
-// of G columns (and a second load row i + 32 in P slabs taller than 32), and
+// 16-byte rows: G = 2 double columns (FP64 storage), G = 4 float columns
+// (FP32 storage) or G = 8 bfloat16 columns (BF16 storage).  One 16-byte
+// shared-memory load then gives a lane one row of G columns (and a second
+// load row i + 32 in P slabs taller than 32), and
 // the 32 lanes of a warp read h*16 consecutive bytes, free of bank
 // conflicts.  A block's last panel is filled with zero columns.  A block's
 // columns are cut into RUNS that fit the 8 KB vector stage buffer (1024
-// doubles or 2048 floats) and a run record; all CTA data is one contiguous
+// doubles, or 2048 floats for FP32 and BF16 storage, whose vectors are
+// staged as float) and a run record; all CTA data is one contiguous
 // byte stream (P runs, then D runs, then U runs) that the kernel moves into
 // shared memory with 1D bulk copies, so every byte of H crosses HBM once per
 // matvec.
@@ -41,6 +43,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -83,10 +86,45 @@ enum RunKind : uint16_t { kRunP = 0, kRunD = 1, kRunU = 2 };
 enum RunFlags : uint16_t { kFirst = 0x100, kLast = 0x200 };
 
 // Storage precision of the packed factors.  A panel row is always 16 bytes:
-// two double columns or four float columns.
-enum Precision : int { kFP64 = 0, kFP32 = 1 };
-HBX_HD inline uint32_t group_cols(int prec) { return prec == kFP32 ? 4u : 2u; }
-HBX_HD inline uint32_t elem_bytes(int prec) { return prec == kFP32 ? 4u : 8u; }
+// two double, four float or eight bfloat16 columns.  The gathered vectors
+// are double for FP64 storage and float otherwise.
+enum Precision : int { kFP64 = 0, kFP32 = 1, kBF16 = 2 };
+HBX_HD constexpr uint32_t group_cols(int prec) { return prec == kBF16 ? 8u : (prec == kFP32 ? 4u : 2u); }
+HBX_HD constexpr uint32_t elem_bytes(int prec) { return prec == kBF16 ? 2u : (prec == kFP32 ? 4u : 8u); }
+HBX_HD constexpr uint32_t stage_elem_bytes(int prec) { return prec == kFP64 ? 8u : 4u; }
+
+// bfloat16: the high half of a float.  Storage rounds a double to the
+// nearest bfloat16, ties to even, in one step (no intermediate float
+// rounding); bfloat16 has float's exponent range, so every factor keeps 8
+// significant bits whatever its magnitude.  Values below float's normal
+// range go through float.
+inline uint16_t bf16_from_double(double v) {
+  uint64_t b;
+  std::memcpy(&b, &v, sizeof b);
+  const uint64_t mag = b & 0x7fffffffffffffffull;
+  if (mag >= 0x7ff0000000000000ull || mag < 0x3810000000000000ull) {  // inf/nan or below 2^-126
+    const float f = (float)v;
+    uint32_t u;
+    std::memcpy(&u, &f, sizeof u);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40u);  // quiet nan
+    return (uint16_t)((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
+  }
+  // keep 7 fraction bits of the 52: round the low 45 bits to nearest, ties to even
+  b += (1ull << 44) - 1ull + ((b >> 45) & 1ull);
+  b &= ~((1ull << 45) - 1ull);
+  double r;
+  std::memcpy(&r, &b, sizeof r);
+  const float f = (float)r;  // exact, or +-inf past float's range
+  uint32_t u;
+  std::memcpy(&u, &f, sizeof u);
+  return (uint16_t)(u >> 16);
+}
+inline float bf16_to_float(uint16_t h) {  // host side (the kernels shift in registers)
+  const uint32_t u = (uint32_t)h << 16;
+  float f;
+  std::memcpy(&f, &u, sizeof f);
+  return f;
+}
 
 // Gather segment: stage[dst + e] = vec[src + e], e < len (vec = x or zbu).
 struct Seg {

@@ -5,8 +5,8 @@
 // back to back inside their CTA stream, gather segments covering each run's
 // stage exactly, heights <= 32 (64 for P slabs), atoms partitioning the rows
 // exactly once, zbu written once before it is read), and returns y = H x.
-// With FP32 storage it multiplies the float factors by the float-rounded
-// vector, as the kernel does, but sums in double.
+// With FP32 or BF16 storage it multiplies the float (bfloat16) factors by
+// the float-rounded vector, as the kernel does, but sums in double.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -35,7 +35,7 @@ static int emu_run(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int prec
   std::fill(y, y + nd, NAN);
   long long nruns = 0;
   const uint32_t G = group_cols(precision);
-  std::vector<double> stage(kStageBytes / elem_bytes(precision)), acc(kSlabMax);
+  std::vector<double> stage(kStageBytes / stage_elem_bytes(precision)), acc(kSlabMax);
 
   // structural checks of one CTA's records; returns "" when fine
   auto check_cta = [&](int c) -> std::string {
@@ -57,7 +57,7 @@ static int emu_run(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int prec
         return "run summary does not match its record";
       // pair-panel runs (multi-RHS layout) are whole panel pairs
       const uint32_t RG = pairs ? 2 * G : G;
-      if (G * r.npanel * elem_bytes(precision) > (uint32_t)kStageBytes || r.vlen > G * r.npanel ||
+      if (G * r.npanel * stage_elem_bytes(precision) > (uint32_t)kStageBytes || r.vlen > G * r.npanel ||
           (r.npanel > 0 && r.vlen + RG <= G * r.npanel) || (pairs && r.npanel % 2 != 0))
         return "run width";
       if (r.nseg > kRunSegs) return "too many segments";
@@ -96,17 +96,20 @@ static int emu_run(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int prec
     for (uint32_t q = 0; q < r.nseg; ++q)
       for (uint32_t e = 0; e < R.seg[q].len; ++e) {
         const double v = vec[R.seg[q].src + e];
-        stage[R.seg[q].dst + e] = precision == kFP32 ? (double)(float)v : v;
+        stage[R.seg[q].dst + e] = precision != kFP64 ? (double)(float)v : v;
       }
     for (uint32_t c = r.vlen; c < G * r.npanel; ++c) stage[c] = 0.0;
     if (r.flags & kFirst) std::fill(acc.begin(), acc.end(), 0.0);
     const double *d = reinterpret_cast<const double *>(buf.data() + ci.stream_off + r.pos);
     const float *f = reinterpret_cast<const float *>(buf.data() + ci.stream_off + r.pos);
+    const uint16_t *hb = reinterpret_cast<const uint16_t *>(buf.data() + ci.stream_off + r.pos);
     for (uint32_t j = 0; j < r.npanel; ++j)
       for (uint32_t i = 0; i < r.nrow; ++i)
         for (uint32_t c = 0; c < G; ++c) {
           const size_t k = ((size_t)j * r.nrow + i) * G + c;
-          acc[i] += (precision == kFP32 ? (double)f[k] : d[k]) * stage[G * j + c];
+          const double m = precision == kBF16 ? (double)bf16_to_float(hb[k])
+                                              : (precision == kFP32 ? (double)f[k] : d[k]);
+          acc[i] += m * stage[G * j + c];
         }
     ++nruns;
   };
@@ -227,3 +230,7 @@ extern "C" int emu_matvec_transposed(const stc_HACApK_leafmtxp *st, int nd, int 
   }
   return emu_matvec(&tl.container, nd, num_ctas, x, y, stats, msg, msglen);
 }
+
+// bfloat16 rounding of the packer, one value at a time (checked against an
+// independent restatement in the tests).
+extern "C" unsigned emu_bf16_from_double(double v) { return bf16_from_double(v); }

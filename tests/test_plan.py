@@ -31,6 +31,8 @@ def emu(build_libs):
                                      C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_char_p, C.c_int]
     lib.emu_matvec_costs.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_longlong, C.c_longlong, C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_char_p, C.c_int]
+    lib.emu_bf16_from_double.argtypes = [C.c_double]
+    lib.emu_bf16_from_double.restype = C.c_uint
     return lib
 
 
@@ -211,6 +213,58 @@ def test_fp32_layout(emu, level, nc):
     d, lr = H.storage_words()
     assert stats[6] == 4 * (d + lr) + stats[7]
     assert stats[7] <= 0.05 * 4 * (d + lr)
+
+
+def _bf16_reference(v: np.ndarray) -> np.ndarray:
+    """bfloat16 bits of v rounded to 8 significant bits, to nearest with ties
+    to even, in one step from the double (frexp/rint restatement, float's
+    normal range)."""
+    m, e = np.frexp(v)                      # v = m 2^e, 0.5 <= |m| < 1
+    r = np.ldexp(np.rint(np.ldexp(m, 8)), e - 8)
+    return (r.astype(np.float32).view(np.uint32) >> 16).astype(np.uint32)
+
+
+def test_bf16_rounding(emu):
+    """The packer's double -> bfloat16 rounding against an independent
+    restatement: random values over many magnitudes, and exact ties and
+    near-ties, where rounding through float first would give another result
+    (1 + 2^-8 + 2^-40 rounds up; via float it would be a tie, rounded down)."""
+    rng = np.random.default_rng(11)
+    v = rng.standard_normal(20000) * np.exp2(rng.integers(-60, 60, 20000))
+    ties = np.array([1 + 2.0**-8, 1 + 3 * 2.0**-8, -(1 + 2.0**-8), 1 + 2.0**-8 + 2.0**-40,
+                     1 + 2.0**-8 - 2.0**-40, 3.0 * (1 + 2.0**-8), 0.75 * (1 + 5 * 2.0**-9)])
+    v = np.concatenate([v, ties, [0.0, 1.0, -2.5, 65504.0, 1e-30]])
+    got = np.array([emu.emu_bf16_from_double(float(t)) for t in v], dtype=np.uint32)
+    assert np.array_equal(got, _bf16_reference(v))
+    assert emu.emu_bf16_from_double(1 + 2.0**-8 + 2.0**-40) == 0x3F81  # up: not a tie in the double
+    assert emu.emu_bf16_from_double(1 + 2.0**-8) == 0x3F80             # a tie: to even
+    assert emu.emu_bf16_from_double(-0.0) == 0x8000
+
+
+@pytest.mark.parametrize("level,nc", [(3, 148), (4, 148), (3, 7), (3, 1)])
+def test_bf16_layout(emu, level, nc):
+    """BF16 storage: 8-column bfloat16 panels with the same 16-byte rows,
+    vectors staged as float; every factor stored once (a quarter of the FP64
+    bytes).  bfloat16 keeps 8 significant bits (unit roundoff 2^-9), so the
+    product is compared with the FP64 oracle in the relative 2-norm against
+    a bound of 2^-8 (measured values printed); run widths stay within the
+    2048-float stage."""
+    import oracle
+    H = sphere(level)
+    x = np.random.default_rng(level + 80).standard_normal(H.nd)
+    y = np.zeros(H.nd)
+    stats = (C.c_longlong * 8)()
+    msg = C.create_string_buffer(512)
+    rc = emu.emu_matvec_prec(C.cast(H.st, C.c_void_p), H.nd, nc, 2, x.ctypes.data_as(C.POINTER(C.c_double)),
+                             y.ctypes.data_as(C.POINTER(C.c_double)), stats, msg, 512)
+    assert rc == 0, msg.value.decode()
+    ref = oracle.matvec(H.st, x)
+    rel = np.linalg.norm(y - ref) / np.linalg.norm(ref)
+    d, lr = H.storage_words()
+    print(f"L{level} nc={nc}: BF16 relative error {rel:.2e}, padding {stats[7] / (2 * (d + lr)):.3f}")
+    assert rel <= 2.0**-8
+    assert stats[6] == 2 * (d + lr) + stats[7]
+    assert stats[7] <= 0.15 * 2 * (d + lr)
 
 
 @pytest.mark.parametrize("level,nc", [(3, 148), (4, 148), (3, 7), (3, 1)])
