@@ -130,9 +130,9 @@ hbx::MatvecArgs matvec_args(hbx_hmat *h, double alpha, const double *x, double b
   return a;
 }
 
-// One H-matvec launch; an FP32 engine first rounds x into its float copy.
+// One H-matvec launch; an FP32 or BF16 engine first rounds x into its float copy.
 cudaError_t mv_launch(hbx_hmat *h, const hbx::MatvecArgs &a, cudaStream_t s) {
-  if (h->plan.precision == hbx::kFP32) {
+  if (h->plan.precision != hbx::kFP64) {
     cudaError_t e = hbx::launch_to_float(a.x, h->d_f32, (size_t)h->plan.nd, s);
     if (e != cudaSuccess) return e;
   }
@@ -226,8 +226,13 @@ static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_option
   *out = nullptr;
   if (!st) return fail(HBX_ERR_INVALID, "hbx_create: container is NULL");
   if (nd <= 0) return fail(HBX_ERR_INVALID, "hbx_create: nd <= 0");
-  if (opt && opt->precision != HBX_FP64 && opt->precision != HBX_FP32)
-    return fail(HBX_ERR_UNSUPPORTED, "hbx_create: precision must be HBX_FP64 or HBX_FP32");
+  if (opt && opt->precision != HBX_FP64 && opt->precision != HBX_FP32 && opt->precision != HBX_BF16)
+    return fail(HBX_ERR_UNSUPPORTED, "hbx_create: precision must be HBX_FP64, HBX_FP32 or HBX_BF16");
+  if (opt && opt->precision == HBX_BF16) {
+    const char *on = std::getenv("HBX_EXPERIMENTAL_BF16");
+    if (!on || std::atoi(on) != 1)
+      return fail(HBX_ERR_UNSUPPORTED, "hbx_create: HBX_BF16 is experimental (set HBX_EXPERIMENTAL_BF16=1)");
+  }
   const int nrhs = (opt && opt->nrhs > 1) ? opt->nrhs : 1;
   if (nrhs != 1 && nrhs != hbx::kNrhs) return fail(HBX_ERR_UNSUPPORTED, "hbx_create: nrhs must be 0, 1 or HBX_NRHS");
   if (nrhs > 1 && opt->precision != HBX_FP32)
@@ -271,8 +276,9 @@ static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_option
   hbx::PlanCosts costs;
   if (opt && opt->block_cost > 0) costs.block = (uint64_t)opt->block_cost;
   if (opt && opt->run_cost > 0) costs.run = (uint64_t)opt->run_cost;
-  int st_plan = hbx::make_plan(st, nd, nc, h->plan, err, (opt && opt->precision == HBX_FP32) ? hbx::kFP32 : hbx::kFP64,
-                               nrhs > 1, costs);
+  const int prec = !opt ? hbx::kFP64
+                        : (opt->precision == HBX_BF16 ? hbx::kBF16 : (opt->precision == HBX_FP32 ? hbx::kFP32 : hbx::kFP64));
+  int st_plan = hbx::make_plan(st, nd, nc, h->plan, err, prec, nrhs > 1, costs);
   if (st_plan != HBX_OK) return bail(fail(st_plan, "hbx_create: " + err));
   const hbx::Plan &P = h->plan;
 
@@ -301,7 +307,7 @@ static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_option
   // zbu twice: the two H-matvecs of a BiCGSTAB step write separate copies
   if ((e = cudaMalloc(&h->d_zbu, 2 * std::max<uint64_t>(1, P.zbu_len) * sizeof(double))) != cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(zbu)"));
-  if (P.precision == hbx::kFP32 &&
+  if (P.precision != hbx::kFP64 &&
       (e = cudaMalloc(&h->d_f32, (3 * (size_t)nd + 2 * std::max<uint64_t>(1, P.zbu_len)) * sizeof(float))) !=
           cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(float copies)"));
@@ -370,7 +376,7 @@ int hbx_get_info(const hbx_hmat *h, hbx_info *info) {
   info->num_ctas = h->num_ctas;
   info->num_atoms = (int)P.atoms.size();
   info->num_runs = (int)h->num_runs;
-  info->precision = P.precision == hbx::kFP32 ? HBX_FP32 : HBX_FP64;
+  info->precision = P.precision == hbx::kBF16 ? HBX_BF16 : (P.precision == hbx::kFP32 ? HBX_FP32 : HBX_FP64);
   uint64_t sb = 0;
   for (const auto &c : P.ctas) sb += c.stream_bytes;
   info->stream_bytes = (long long)sb;

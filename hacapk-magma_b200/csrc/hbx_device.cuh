@@ -409,8 +409,9 @@ struct GatherCtx {
 // arrival).  Before its first run of a pass it waits for that pass's x
 // (xready), and before its first U run of a pass for the grid barrier that
 // completes zbu (gdone).  Run records arrive kRecSlots runs ahead by cp.async.
-template <bool kF32, class SM>
+template <int kPrec, class SM>
 __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm, uint32_t gi) {
+  constexpr bool kF32 = kPrec != kFP64;  // float copies of the vectors (FP32 and BF16 storage)
   const int lane = threadIdx.x & 31;
   const uint32_t total = c.nr * c.npass;
   uint8_t *recs = sm.rec + gi * kRecSlots * kRecBytes;
@@ -458,7 +459,7 @@ __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm, ui
       const Seg sg = seg[q];
       stage_elems<kF32>(st, sg.dst, vec + (size_t)sg.src * esz, 0, sg.len, 1);
     }
-    const uint32_t vend = (uint32_t)h.npanel * (kF32 ? 4u : 2u);
+    const uint32_t vend = (uint32_t)h.npanel * group_cols(kPrec);
     for (uint32_t e = h.vlen + lane; e < vend; e += 32) {
       if (kF32) reinterpret_cast<float *>(st)[e] = 0.0f;
       else reinterpret_cast<double *>(st)[e] = 0.0;
@@ -481,13 +482,16 @@ __device__ __forceinline__ float4 lds_f32x4(uint32_t addr) {
 }
 
 // A lane's accumulator for a row: FP64 panels (two double columns) add into
-// two doubles; FP32 panels (four float columns) into four floats, folded into
-// the double total at the end of every run.
-template <bool kF32>
+// two doubles; FP32 panels (four float columns) and BF16 panels (eight
+// bfloat16 columns) into four floats, folded into the double total at the end
+// of every run.  V is a panel's slice of the staged vector (ldv: panel j),
+// M one 16-byte panel row (ldm).
+template <int kPrec>
 struct PanelMath;
 template <>
-struct PanelMath<false> {
+struct PanelMath<kFP64> {
   using V = double2;
+  using M = double2;
   struct Acc {
     double a0 = 0.0, a1 = 0.0;
     __device__ __forceinline__ double take() {
@@ -497,15 +501,17 @@ struct PanelMath<false> {
       return s;
     }
   };
-  static __device__ __forceinline__ V ld(uint32_t addr) { return lds_f64x2(addr); }
-  static __device__ __forceinline__ void fma(Acc &a, const V &m, const V &v) {
+  static __device__ __forceinline__ V ldv(uint32_t stage_s, uint32_t j) { return lds_f64x2(stage_s + 16u * j); }
+  static __device__ __forceinline__ M ldm(uint32_t addr) { return lds_f64x2(addr); }
+  static __device__ __forceinline__ void fma(Acc &a, const M &m, const V &v) {
     a.a0 = ::fma(m.x, v.x, a.a0);
     a.a1 = ::fma(m.y, v.y, a.a1);
   }
 };
 template <>
-struct PanelMath<true> {
+struct PanelMath<kFP32> {
   using V = float4;
+  using M = float4;
   struct Acc {
     float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
     __device__ __forceinline__ double take() {
@@ -514,34 +520,70 @@ struct PanelMath<true> {
       return s;
     }
   };
-  static __device__ __forceinline__ V ld(uint32_t addr) { return lds_f32x4(addr); }
-  static __device__ __forceinline__ void fma(Acc &a, const V &m, const V &v) {
+  static __device__ __forceinline__ V ldv(uint32_t stage_s, uint32_t j) { return lds_f32x4(stage_s + 16u * j); }
+  static __device__ __forceinline__ M ldm(uint32_t addr) { return lds_f32x4(addr); }
+  static __device__ __forceinline__ void fma(Acc &a, const M &m, const V &v) {
     a.a0 = fmaf(m.x, v.x, a.a0);
     a.a1 = fmaf(m.y, v.y, a.a1);
     a.a2 = fmaf(m.z, v.z, a.a2);
     a.a3 = fmaf(m.w, v.w, a.a3);
   }
 };
+// A 32-bit word of a BF16 panel row holds columns 2k (low half) and 2k + 1
+// (high half); a bfloat16 is the high half of a float, so widening is a
+// shift or a mask.  Panel j's eight staged floats lie at 32 j bytes.
+template <>
+struct PanelMath<kBF16> {
+  struct V {
+    float4 lo, hi;
+  };
+  using M = uint4;
+  using Acc = PanelMath<kFP32>::Acc;
+  static __device__ __forceinline__ V ldv(uint32_t stage_s, uint32_t j) {
+    return V{lds_f32x4(stage_s + 32u * j), lds_f32x4(stage_s + 32u * j + 16u)};
+  }
+  static __device__ __forceinline__ M ldm(uint32_t addr) {
+    uint4 v;
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr));
+    return v;
+  }
+  static __device__ __forceinline__ float lo(uint32_t w) { return __uint_as_float(w << 16); }
+  static __device__ __forceinline__ float hi(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
+  static __device__ __forceinline__ void fma(Acc &a, const M &m, const V &v) {
+    a.a0 = fmaf(lo(m.x), v.lo.x, a.a0);
+    a.a1 = fmaf(hi(m.x), v.lo.y, a.a1);
+    a.a2 = fmaf(lo(m.y), v.lo.z, a.a2);
+    a.a3 = fmaf(hi(m.y), v.lo.w, a.a3);
+    a.a0 = fmaf(lo(m.z), v.hi.x, a.a0);
+    a.a1 = fmaf(hi(m.z), v.hi.y, a.a1);
+    a.a2 = fmaf(lo(m.w), v.hi.z, a.a2);
+    a.a3 = fmaf(hi(m.w), v.hi.w, a.a3);
+  }
+};
 
 // ---- one run of a consumer warp ------------------------------------------
 // The warp reads panels j = (w - rot) mod NW, j + NW, ... of the run (16h
 // bytes each; lane i reads row min(i, h-1), and row min(i + 32, h-1) of P
-// slabs taller than 32, 16 bytes each: two double or four float columns)
-// from the ring, kUnroll panels per iteration (two-row form: 2), and adds
-// their products with the staged vector into its accumulators; it adds the
-// run's sums of its rows to t0 (row i) and t1 (row i + 32).  Lanes past the
-// last row repeat it; their sums are never used.
+// slabs taller than 32, 16 bytes each: two double, four float or eight
+// bfloat16 columns) from the ring, kUnroll panels per iteration (BF16:
+// kUnroll / 2; two-row form: 2), and adds their products with the staged
+// vector into its accumulators; it adds the run's sums of its rows to t0
+// (row i) and t1 (row i + 32).  Lanes past the last row repeat it; their
+// sums are never used.
 #ifndef HBX_UNROLL
 #define HBX_UNROLL 4
 #endif
 constexpr uint32_t kUnroll = HBX_UNROLL;
 
-template <bool kTwoRows, bool kF32>
+template <bool kTwoRows, int kPrec>
 __device__ __forceinline__ void run_rows(const RunLite &L, uint32_t stage_s, Ring &R, uint32_t w, double &t0,
                                          double &t1) {
-  using PM = PanelMath<kF32>;
+  using PM = PanelMath<kPrec>;
   using V = typename PM::V;
-  constexpr uint32_t NW = kConsumerWarps, U = kTwoRows ? 2 : kUnroll;
+  using M = typename PM::M;
+  // panels per iteration: BF16 panels are twice as wide as FP32 ones, so
+  // half as many give the same columns per iteration
+  constexpr uint32_t NW = kConsumerWarps, U = kTwoRows ? 2 : (kPrec == kBF16 ? kUnroll / 2 : kUnroll);
   const int lane = threadIdx.x & 31;
   const uint32_t h = L.nrow, np = L.npanel;
   const uint32_t pb = 16u * h;
@@ -553,23 +595,24 @@ __device__ __forceinline__ void run_rows(const RunLite &L, uint32_t stage_s, Rin
   for (; j + (U - 1) * NW < np; j += U * NW) {
     const uint32_t p0 = L.pos + j * pb;
     R.ensure(p0, p0 + (U - 1) * NW * pb + pb);
-    V v[U], m[U], m2[kTwoRows ? U : 1];
+    V v[U];
+    M m[U], m2[kTwoRows ? U : 1];
 #pragma unroll
-    for (uint32_t u = 0; u < U; ++u) v[u] = PM::ld(stage_s + 16u * (j + u * NW));
+    for (uint32_t u = 0; u < U; ++u) v[u] = PM::ldv(stage_s, j + u * NW);
     const uint32_t pl = p0 + lrow;
     const uint32_t q = ring_off(R.base + (pl >> kChunkLog), pl);
     if (q + (U - 1) * NW * pb + (kTwoRows ? lrow2 : 0u) + 16u <= kRingBytes) {  // no wrap around the ring end
 #pragma unroll
       for (uint32_t u = 0; u < U; ++u) {
-        m[u] = PM::ld(ring_s + q + u * NW * pb);
-        if (kTwoRows) m2[u] = PM::ld(ring_s + q + u * NW * pb + lrow2);
+        m[u] = PM::ldm(ring_s + q + u * NW * pb);
+        if (kTwoRows) m2[u] = PM::ldm(ring_s + q + u * NW * pb + lrow2);
       }
     } else {
 #pragma unroll
       for (uint32_t u = 0; u < U; ++u) {
         const uint32_t pu = pl + u * NW * pb;
-        m[u] = PM::ld(ring_s + ring_off(R.base + (pu >> kChunkLog), pu));
-        if (kTwoRows) m2[u] = PM::ld(ring_s + ring_off(R.base + ((pu + lrow2) >> kChunkLog), pu + lrow2));
+        m[u] = PM::ldm(ring_s + ring_off(R.base + (pu >> kChunkLog), pu));
+        if (kTwoRows) m2[u] = PM::ldm(ring_s + ring_off(R.base + ((pu + lrow2) >> kChunkLog), pu + lrow2));
       }
     }
 #pragma unroll
@@ -581,12 +624,12 @@ __device__ __forceinline__ void run_rows(const RunLite &L, uint32_t stage_s, Rin
   for (; j < np; j += NW) {
     const uint32_t p0 = L.pos + j * pb;
     R.ensure(p0, p0 + pb);
-    const V vv = PM::ld(stage_s + 16u * j);
+    const V vv = PM::ldv(stage_s, j);
     const uint32_t pl = p0 + lrow;
-    PM::fma(a[0], PM::ld(ring_s + ring_off(R.base + (pl >> kChunkLog), pl)), vv);
+    PM::fma(a[0], PM::ldm(ring_s + ring_off(R.base + (pl >> kChunkLog), pl)), vv);
     if (kTwoRows) {
       const uint32_t p2 = pl + lrow2;
-      PM::fma(b[0], PM::ld(ring_s + ring_off(R.base + (p2 >> kChunkLog), p2)), vv);
+      PM::fma(b[0], PM::ldm(ring_s + ring_off(R.base + (p2 >> kChunkLog), p2)), vv);
     }
   }
 #pragma unroll
@@ -597,11 +640,11 @@ __device__ __forceinline__ void run_rows(const RunLite &L, uint32_t stage_s, Rin
   }
 }
 
-template <bool kF32>
+template <int kPrec>
 __device__ __forceinline__ void run_panels(const RunLite &L, uint32_t stage_s, Ring &R, uint32_t w, double &t0,
                                            double &t1) {
-  if (L.nrow > 32) run_rows<true, kF32>(L, stage_s, R, w, t0, t1);
-  else run_rows<false, kF32>(L, stage_s, R, w, t0, t1);
+  if (L.nrow > 32) run_rows<true, kPrec>(L, stage_s, R, w, t0, t1);
+  else run_rows<false, kPrec>(L, stage_s, R, w, t0, t1);
 }
 
 // ---- compensated (Dot2) accumulation ------------------------------------------

@@ -221,7 +221,7 @@ __device__ __forceinline__ void sum_warp(uint32_t nr, uint32_t npass, uint32_t n
 // sums for the block-sum warp.  Before it can block, a warp gives back every
 // ring chunk below the run it is about to process, so no wait holds a chunk
 // another warp needs.  nb counts the block ends over the launch.
-template <bool kF32>
+template <int kPrec>
 __device__ __forceinline__ void consume_pass(Ring &R, uint32_t K, uint32_t nr, uint32_t &nb, uint32_t pass,
                                              const Smem &sm, int *err, uint64_t tmo) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -238,7 +238,7 @@ __device__ __forceinline__ void consume_pass(Ring &R, uint32_t K, uint32_t nr, u
       bad = true;
       if (lane == 0) atomicOr(err, kErrPipeline);
     }
-    if (!bad) run_panels<kF32>(L, smem_u32(sm.stage + slot * kStageBytes), R, (uint32_t)w, t0, t1);
+    if (!bad) run_panels<kPrec>(L, smem_u32(sm.stage + slot * kStageBytes), R, (uint32_t)w, t0, t1);
     bad = bad || R.bad;
     __syncwarp();
     if (lane == 0) mbar_arrive(&sm.sempty[slot]);
@@ -257,17 +257,20 @@ __device__ __forceinline__ void consume_pass(Ring &R, uint32_t K, uint32_t nr, u
 // without P blocks, the pass, then the wait for the block-sum warp (every
 // row of the pass is written) and, in warp 0, for the pass's grid barrier
 // (the caller's next grid barrier must not start before it completes).
-template <bool kF32>
+template <int kPrec>
 __device__ __forceinline__ void matvec_pass(Ring &R, uint32_t K, uint32_t nr, uint32_t &nb, const PassOut &o,
                                             const Smem &sm, int *err, uint64_t tmo) {
   if (o.nblk_p == 0 && threadIdx.x == 0) mbar_arrive(sm.pdone);
-  consume_pass<kF32>(R, K, nr, nb, o.pass, sm, err, tmo);
+  consume_pass<kPrec>(R, K, nr, nb, o.pass, sm, err, tmo);
   if (!warp_wait(sm.rdone, o.pass & 1, tmo) && (threadIdx.x & 31) == 0) atomicOr(err, kErrPipeline);
   if (threadIdx.x < 32 && !warp_wait(sm.gdone, o.pass & 1, tmo) && threadIdx.x == 0) atomicOr(err, kErrGridBarrier);
 }
 
-template <bool kF32>
+// kPrec: storage precision of the factors; FP32 and BF16 engines gather the
+// float copies of the vectors.
+template <int kPrec>
 __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
+  constexpr bool kF32 = kPrec != kFP64;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const Smem sm = smem_layout(smem_raw);
   const CtaInfo ci = a.ctas[blockIdx.x];
@@ -289,7 +292,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
     const void *xs = kF32 ? static_cast<const void *>(a.x32) : static_cast<const void *>(a.x);
     const void *zs = kF32 ? static_cast<const void *>(a.zbu32) : static_cast<const void *>(a.zbu);
     const GatherCtx c{a.recs + ci.rec_begin, nr, ci.nr_p + ci.nr_d, 1, xs, xs, zs, zs, a.err, a.timeout_ns};
-    gather_warp<kF32>(c, sm, (uint32_t)(w - kGatherWarp0));
+    gather_warp<kPrec>(c, sm, (uint32_t)(w - kGatherWarp0));
     return;
   }
   if (w == kSyncWarp) {
@@ -304,7 +307,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   if (threadIdx.x == 0) mbar_arrive(sm.xready);  // x is an input: ready from the start
   uint32_t nb = 0;
   Ring R{sm.ring, sm.full, sm.empty, 0, 0, 0, a.timeout_ns, a.err, false};
-  matvec_pass<kF32>(R, K, nr, nb, o, sm, a.err, a.timeout_ns);
+  matvec_pass<kPrec>(R, K, nr, nb, o, sm, a.err, a.timeout_ns);
   if (a.prof && threadIdx.x == 0) {
     a.prof[blockIdx.x * 16 + 0] = t_start;
     a.prof[blockIdx.x * 16 + 5] = gtimer();
@@ -432,8 +435,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_setup(BicgArgs a) {
   }
 }
 
-template <bool kF32>
+template <int kPrec>
 __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
+  constexpr bool kF32 = kPrec != kFP64;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const Smem sm = smem_layout(smem_raw);
   const CtaInfo ci = a.ctas[blockIdx.x];
@@ -546,7 +550,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     const void *z1 =
         kF32 ? static_cast<const void *>(a.zbu32 + a.zbu_len) : static_cast<const void *>(a.zbu + a.zbu_len);
     const GatherCtx c{a.recs + ci.rec_begin, nr, ci.nr_p + ci.nr_d, 2, x0, x1, z0, z1, a.err, a.timeout_ns};
-    gather_warp<kF32>(c, sm, (uint32_t)(w - kGatherWarp0));
+    gather_warp<kPrec>(c, sm, (uint32_t)(w - kGatherWarp0));
     return;
   }
   if (w == kSyncWarp) {
@@ -601,7 +605,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
 
   // ---- S2: Ap = H p;  rh . Ap
-  matvec_pass<kF32>(R, K, nr, nb, outs[0], sm, a.err, a.timeout_ns);
+  matvec_pass<kPrec>(R, K, nr, nb, outs[0], sm, a.err, a.timeout_ns);
   stamp(2);
   {
     Acc2 acc[1] = {{0, 0}};
@@ -640,7 +644,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
 
   // ---- S4: At = H t;  At . t,  At . At
   R.base = K;
-  matvec_pass<kF32>(R, K, nr, nb, outs[1], sm, a.err, a.timeout_ns);
+  matvec_pass<kPrec>(R, K, nr, nb, outs[1], sm, a.err, a.timeout_ns);
   stamp(5);
   {
     Acc2 acc[2] = {{0, 0}, {0, 0}};
@@ -746,11 +750,13 @@ size_t kernel_smem_bytes() { return SharedLayout::bytes; }
 cudaError_t configure_kernels() {
   const int smem = (int)SharedLayout::bytes;
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_matvec<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(k_matvec<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_matvec<kFP64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_matvec<kFP32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_matvec<kBF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_bicg_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(k_bicg_iter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(k_bicg_iter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_bicg_iter<kFP64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_bicg_iter<kFP32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_bicg_iter<kBF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_dot_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
   return cudaSuccess;
 }
@@ -771,7 +777,8 @@ static cudaError_t launch_coop(void (*kern)(Args), const Args &a, int num_ctas, 
 }
 
 cudaError_t launch_matvec(const MatvecArgs &a, int num_ctas, cudaStream_t s, int precision) {
-  return precision == kFP32 ? launch_coop(k_matvec<true>, a, num_ctas, s) : launch_coop(k_matvec<false>, a, num_ctas, s);
+  if (precision == kBF16) return launch_coop(k_matvec<kBF16>, a, num_ctas, s);
+  return precision == kFP32 ? launch_coop(k_matvec<kFP32>, a, num_ctas, s) : launch_coop(k_matvec<kFP64>, a, num_ctas, s);
 }
 
 cudaError_t launch_bicg_setup(const BicgArgs &a, int num_ctas, cudaStream_t s) {
@@ -780,8 +787,9 @@ cudaError_t launch_bicg_setup(const BicgArgs &a, int num_ctas, cudaStream_t s) {
 }
 
 cudaError_t launch_bicg_iter(const BicgArgs &a, int num_ctas, cudaStream_t s, int precision) {
-  return precision == kFP32 ? launch_coop(k_bicg_iter<true>, a, num_ctas, s)
-                            : launch_coop(k_bicg_iter<false>, a, num_ctas, s);
+  if (precision == kBF16) return launch_coop(k_bicg_iter<kBF16>, a, num_ctas, s);
+  return precision == kFP32 ? launch_coop(k_bicg_iter<kFP32>, a, num_ctas, s)
+                            : launch_coop(k_bicg_iter<kFP64>, a, num_ctas, s);
 }
 
 cudaError_t launch_to_float(const double *x, float *y, size_t n, cudaStream_t s) {

@@ -103,7 +103,7 @@ class BuildStats(C.Structure):
 KERNEL_PPOHBEM = 0
 KERNEL_LAPLACE = 1
 
-HBX_FP64, HBX_FP32 = 0, 1
+HBX_FP64, HBX_FP32, HBX_BF16 = 0, 1, 2
 HBX_NRHS = 64
 
 STATUS = {0: "HBX_OK", 1: "HBX_ERR_INVALID", 2: "HBX_ERR_NOMEM", 3: "HBX_ERR_CUDA",

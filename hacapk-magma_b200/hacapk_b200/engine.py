@@ -47,7 +47,9 @@ class Engine:
     def __init__(self, st, nd: int, num_ctas: int = 0, transpose: bool = False, precision: int = 0,
                  nrhs: int = 0, block_cost: int = 0, run_cost: int = 0):
         """transpose=True packs H^T: products and solves with the adjoint.
-        precision=abi.HBX_FP32 stores the factors in float (half the bytes).
+        precision=abi.HBX_FP32 stores the factors in float (half the bytes),
+        abi.HBX_BF16 in bfloat16 (a quarter; experimental: needs the
+        environment variable HBX_EXPERIMENTAL_BF16=1).
         nrhs=abi.HBX_NRHS (with HBX_FP32) makes a multi-RHS engine: matmat only."""
         self.lib = abi.engine_lib()
         opt = abi.Options()
@@ -239,7 +241,7 @@ class Engine:
     def bicgstab_refined_host(self, low: "Engine", b: np.ndarray, u0: np.ndarray | None = None, tol: float = 1e-8,
                               max_iter: int = 1000, inner_tol: float = 0.0, check: bool = True):
         """FP64 iterative refinement (self: FP64 engine) around BiCGSTAB on
-        `low` (an FP32 engine of the same matrix); host vectors."""
+        `low` (an FP32 or BF16 engine of the same matrix); host vectors."""
         b = np.ascontiguousarray(b, np.float64)
         u = np.zeros(self.nd) if u0 is None else np.array(u0, np.float64, copy=True)
         o = self._opts(tol, max_iter, 0, 8, inner_tol)

@@ -114,14 +114,20 @@ typedef enum hbx_status {
 /* Storage precision of the packed factors.  HBX_FP32 rounds every factor
  * to float once, at hbx_create, and multiplies in float (four columns per
  * 16-byte load), adding each run's products to double row sums; vectors,
- * dot products and solver scalars stay double.  No counterpart in the
+ * dot products and solver scalars stay double.  HBX_BF16 rounds every
+ * factor to bfloat16 (8 significant bits, nearest, ties to even) and
+ * multiplies the widened factors by float vectors in float, eight columns
+ * per 16-byte load: a quarter of the FP64 bytes.  bfloat16 has float's
+ * exponent range, so no per-leaf scale is needed to keep the factors in
+ * range.  HBX_BF16 is experimental: hbx_create accepts it only with the
+ * environment variable HBX_EXPERIMENTAL_BF16=1.  No counterpart in the
  * reference, which is FP64 throughout. */
-enum { HBX_FP64 = 0, HBX_FP32 = 1 };
+enum { HBX_FP64 = 0, HBX_FP32 = 1, HBX_BF16 = 2 };
 
 typedef struct hbx_hmat hbx_hmat;
 
 typedef struct hbx_options {
-  int precision;   /* HBX_FP64 or HBX_FP32 (factor storage)               */
+  int precision;   /* HBX_FP64, HBX_FP32 or HBX_BF16 (factor storage)     */
   int num_ctas;    /* persistent CTAs; 0 = one per SM                     */
   int transpose;   /* 1: the engine holds H^T (adjoint products and solves;
                       no counterpart in the reference)                    */
@@ -141,7 +147,8 @@ typedef struct hbx_info {
   int nd, nlf, nlfkt, ktmax;
   int num_ctas, num_atoms, num_runs, precision;
   long long stream_bytes;  /* packed factor bytes streamed per matvec        */
-  long long alg_bytes;     /* algorithmic bytes per single-RHS matvec (B_H)  */
+  long long alg_bytes;     /* algorithmic bytes per single-RHS matvec with
+                              FP64 factors (B_H), whatever the storage       */
   long long alg_flops;     /* 2*(sum dense ndl*ndt + sum kt*(ndl+ndt))       */
   long long zbu_len;       /* sum of kt over low-rank leaves                  */
   long long dense_words, lowrank_words;

@@ -5,6 +5,8 @@ float; hbx_bicgstab_refined wraps BiCGSTAB on it in FP64 iterative
 refinement.  Errors are stated against the FP64 oracle (the reference's own
 CPU product, HACApK_MAGMA.c:5-57): the FP32 product within 1e-6 of it, the
 refined solution's FP64 residual ||b - H u||/||b|| below the tolerance."""
+import os
+
 import numpy as np
 import pytest
 
@@ -59,3 +61,53 @@ def test_fp32_plain_bicgstab_and_rejects_mismatch(gpu, build_libs):
     E64_small = Engine(H2.st, H2.nd)
     with pytest.raises(HbxError):
         E64_small.bicgstab_refined_host(E32, b2)
+
+
+# ---- BF16 storage (experimental: the engine needs HBX_EXPERIMENTAL_BF16=1) ----
+_bf16 = pytest.mark.skipif(os.environ.get("HBX_EXPERIMENTAL_BF16") != "1",
+                           reason="HBX_BF16 engines are experimental: set HBX_EXPERIMENTAL_BF16=1")
+
+
+@_bf16
+@pytest.mark.parametrize("level", [3, 5])
+def test_bf16_matvec_error_against_fp64_oracle(gpu, build_libs, level):
+    """bfloat16 factors (8 significant bits, unit roundoff 2^-9) times the
+    float-rounded vector, float accumulation within a run: the product is
+    within 2^-8 of the FP64 oracle in the relative 2-norm (measured value
+    printed), streams a quarter of the FP64 bytes plus panel padding, and is
+    bit-identical on repeat."""
+    import oracle
+    from hacapk_b200 import abi, configs
+    from hacapk_b200.engine import Engine
+    H, _ = configs.c1(level)
+    E16 = Engine(H.st, H.nd, precision=abi.HBX_BF16)
+    E64 = Engine(H.st, H.nd)
+    assert E16.info["precision"] == abi.HBX_BF16
+    assert E16.info["stream_bytes"] <= 0.27 * E64.info["stream_bytes"]
+    x = np.random.default_rng(level + 16).standard_normal(H.nd)
+    y, _, _ = E16.matvec_host(x)
+    ref = oracle.matvec(H.st, x)
+    rel = np.linalg.norm(y - ref) / np.linalg.norm(ref)
+    print(f"L{level}: BF16 product relative error {rel:.2e}")
+    assert rel <= 2.0**-8
+    y2, _, _ = E16.matvec_host(x)
+    assert np.array_equal(y, y2)
+
+
+@_bf16
+@pytest.mark.parametrize("level", [3, 4])
+def test_bf16_refined_solve_reaches_fp64_tolerance(gpu, build_libs, level):
+    """BiCGSTAB on the BF16 engine inside FP64 iterative refinement reaches
+    1e-8 in the FP64 residual, recomputed by the oracle."""
+    import oracle
+    from hacapk_b200 import abi, configs
+    from hacapk_b200.engine import Engine
+    H, b = configs.c1(level)
+    E64 = Engine(H.st, H.nd)
+    E16 = Engine(H.st, H.nd, precision=abi.HBX_BF16)
+    u, info = E64.bicgstab_refined_host(E16, b, tol=1e-8, max_iter=1000, inner_tol=1e-2)
+    assert info["status"] == 0
+    relres = np.linalg.norm(b - oracle.matvec(H.st, u)) / np.linalg.norm(b)
+    print(f"L{level}: BF16 refined: {info['outer']} refinement steps, {info['iterations']} inner steps, "
+          f"FP64 residual {relres:.2e}")
+    assert relres < 1.05e-8
