@@ -7,6 +7,10 @@ the Laplace single layer 1/(4 pi r) with the analytic flat-triangle integral
 
   C1  plain FP64: icosphere L5 (20,480 faces), leaf 32, eta 2, ACA+ 1e-5,
       rhs = 1 + N(0, (1e-3)^2) per element (seed 0), BiCGSTAB to 1e-8.
+  C2  precision: icosphere L7 (327,680 faces) and, as a second body, an
+      ellipsoid of the same subdivision level with semi-axes U(0.5, 2)
+      (seed 1), centred on the x axis so that the gap between the two
+      surfaces along x is 3; leaf 32, eta 2, ACA+ 1e-6; rhs as C1.
   C5  uneven batch: `count` ellipsoids (256 in the config), semi-axes
       U(0.3, 3), subdivision levels drawn uniformly from {2, 3, 4, 5} (so the
       sizes 320 .. 20,480 are log-uniform), seed 5; leaf 32, eta 2, ACA+ 1e-5;
@@ -17,7 +21,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import abi
-from .hmatrix import HostHMatrix, ellipsoid, icosphere
+from .hmatrix import HostHMatrix, concat, ellipsoid, icosphere
 
 
 def rhs_unit_plus_noise(n: int, seed: int = 0, sigma: float = 1e-3) -> np.ndarray:
@@ -34,6 +38,18 @@ def laplace_sphere(level: int, leaf_size: int = 32, eta: float = 2.0, aca_eps: f
 def c1(level: int = 5, nthreads: int = 0):
     """(H-matrix, rhs in cluster order) of configuration C1 (level 5 by default)."""
     H = laplace_sphere(level, 32, 2.0, 1e-5, nthreads)
+    b = H.to_cluster(rhs_unit_plus_noise(H.nd, seed=0))
+    return H, b
+
+
+def c2(level: int = 7, seed: int = 1, gap: float = 3.0, aca_eps: float = 1e-6, nthreads: int = 0):
+    """(H-matrix, rhs in cluster order) of configuration C2: the unit
+    icosphere and a seeded ellipsoid of the same level, one H-matrix over
+    both bodies."""
+    axes = np.random.default_rng(seed).uniform(0.5, 2.0, 3)
+    body2 = ellipsoid(level, axes, center=(1.0 + gap + axes[0], 0.0, 0.0))
+    H = HostHMatrix(concat(icosphere(level), body2), leaf_size=32, eta=2.0, aca_eps=aca_eps,
+                    kernel=abi.KERNEL_LAPLACE, nthreads=nthreads)
     b = H.to_cluster(rhs_unit_plus_noise(H.nd, seed=0))
     return H, b
 

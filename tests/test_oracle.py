@@ -137,6 +137,28 @@ def test_oracle_bicgstab_converges(build_libs):
         assert n2 == n and np.array_equal(u2, u)
 
 
+def test_two_body_precision_workload(build_libs):
+    """C2 (the precision form's workload) at level 3: the sphere and the
+    seeded ellipsoid are disjoint with the stated gap along x, the H-matrix
+    over both bodies reproduces the dense operator to the ACA tolerance
+    (1e-6), and the oracle's BiCGSTAB reaches 1e-8."""
+    import oracle
+    from hacapk_b200 import configs
+    from hacapk_b200.hmatrix import ellipsoid, icosphere
+    H, b = configs.c2(3)
+    sphere3 = icosphere(3)
+    assert H.nd == 2 * sphere3.nofc
+    axes = np.random.default_rng(1).uniform(0.5, 2.0, 3)
+    body2 = ellipsoid(3, axes, center=(1.0 + 3.0 + axes[0], 0.0, 0.0))
+    assert body2.xyz[:, 0].min() - sphere3.xyz[:, 0].max() >= 3.0 - 1e-12
+    A = H.dense()
+    x = np.random.default_rng(6).standard_normal(H.nd)
+    err = np.linalg.norm(A @ x - oracle.matvec(H.st, x)) / np.linalg.norm(A @ x)
+    assert err < 1e-5
+    u, n, hist, _ = oracle.bicgstab(H.st, b, tol=1e-8, max_iter=500, kind="restated")
+    assert np.linalg.norm(b - oracle.matvec(H.st, u)) / np.linalg.norm(b) < 1.01e-8
+
+
 def test_oracle_bicgstab_zero_rhs_and_limits(build_libs):
     import oracle
     H = sphere(2)
