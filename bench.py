@@ -408,6 +408,78 @@ def measure_forms(H, b, E, args, dev, stream, fp64_solve_s):
     return out
 
 
+def precision_workload(args):
+    """The precision form on its own workload (C2 at --precision-level: the
+    sphere and the seeded ellipsoid, ACA+ 1e-6), one JSON line: the FP64
+    solve, FP32 factors in FP64 refinement and, when HBX_EXPERIMENTAL_BF16=1,
+    BF16 factors in FP64 refinement (inner tolerance 1e-2); for each, the
+    standalone product's time and stream rate and the solve's time, step
+    counts and FP64 residual.  Solves are timed by the host clock around
+    each call, best of three after one untimed run."""
+    import torch
+    from hacapk_b200 import abi, configs
+    from hacapk_b200.engine import Engine
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    s = stream.cuda_stream
+    t0 = time.time()
+    H, b = configs.c2(args.precision_level)
+    t_build = time.time() - t0
+    n = H.nd
+    bd = torch.from_numpy(b).to(dev)
+    ud = torch.zeros(n, dtype=torch.float64, device=dev)
+    peak, peak_kind = peaks()
+
+    def best_of(fn):
+        best, res = 1e9, None
+        for _ in range(4):
+            ud.zero_()
+            torch.cuda.synchronize(dev)
+            t = time.perf_counter()
+            res = fn()
+            torch.cuda.synchronize(dev)
+            best = min(best, time.perf_counter() - t)
+        return best, res
+
+    def product(Ek):
+        x = torch.randn(n, dtype=torch.float64, device=dev)
+        y = torch.empty_like(x)
+        for _ in range(3):
+            Ek.matvec_dev(x.data_ptr(), y.data_ptr(), stream=s)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(20):
+            Ek.matvec_dev(x.data_ptr(), y.data_ptr(), stream=s)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        Ek.sync(s)
+        us = e0.elapsed_time(e1) / 20 * 1e3
+        return {"us": us, "stream_gb": Ek.info["stream_bytes"] / 1e9,
+                "stream_gbs": Ek.info["stream_bytes"] / (us * 1e-6) / 1e9,
+                "frac_of_" + peak_kind + "_peak": Ek.info["stream_bytes"] / (us * 1e-6) / 1e9 / peak}
+
+    E = Engine(H.st, n)
+    t64, inf = best_of(lambda: E.bicgstab_dev(bd.data_ptr(), ud.data_ptr(), tol=args.tol, max_iter=args.max_iter,
+                                              stream=s))
+    out = {"workload": f"C2: icosphere L{args.precision_level} + seeded ellipsoid, ACA+ 1e-6", "n": n,
+           "host_build_s": t_build,
+           "fp64": {"solve_s": t64, "iterations": inf["iterations"], "true_relres": inf["true_relres"],
+                    "product": product(E)}}
+    forms = [("fp32_refined", abi.HBX_FP32, 0.0)]
+    if os.environ.get("HBX_EXPERIMENTAL_BF16") == "1":
+        forms.append(("bf16_refined", abi.HBX_BF16, 1e-2))
+    for name, prec, inner in forms:
+        El = Engine(H.st, n, precision=prec)
+        tl, inf = best_of(lambda: E.bicgstab_refined_dev(El, bd.data_ptr(), ud.data_ptr(), tol=args.tol,
+                                                         max_iter=args.max_iter, inner_tol=inner, stream=s))
+        out[name] = {"solve_s": tl, "speedup_vs_fp64": t64 / tl, "outer": inf["outer"],
+                     "inner_iterations": inf["iterations"], "true_relres": inf["true_relres"],
+                     "product": product(El)}
+        El.close()
+    E.close()
+    print(json.dumps(out), flush=True)
+
+
 def profile_matmat(args):
     """Five 64-RHS products on the C1 workload, nothing timed: the command
     the ncu summary of k_matmat is taken from."""
@@ -486,9 +558,14 @@ def main():
     ap.add_argument("--c5-count", type=int, default=64, help="instances of the uneven-batch sample (C5: 256)")
     ap.add_argument("--profile-matmat", action="store_true",
                     help="only run five 64-RHS tensor-core products (a short command for ncu)")
+    ap.add_argument("--precision-level", type=int, default=0,
+                    help="only time the precision form on C2 at this level (7: the config; one GPU)")
     args = ap.parse_args()
     if args.profile_matmat:
         profile_matmat(args)
+        return
+    if args.precision_level > 0:
+        precision_workload(args)
         return
     world, rank, local = dist_setup()
     if args.impl == "reference":
