@@ -127,7 +127,9 @@ def engine_product(st, nd: int):
 
 def bicgstab(matvec: Callable, b, tol: float = 1e-8, max_iter: int = 1000):
     """BiCGSTAB of HACApK_SOLVER.c:254-417 on replicated vectors (torch
-    tensors), the product given by `matvec`; returns (u, steps, relres)."""
+    tensors), the product given by `matvec`; returns (u, steps, relres).  A
+    breakdown (a zero denominator) ends the loop with the last iterate, whose
+    relres then stays at or above tol."""
     import torch
     u = torch.zeros_like(b)
     r = b - matvec(u)
@@ -135,10 +137,14 @@ def bicgstab(matvec: Callable, b, tol: float = 1e-8, max_iter: int = 1000):
     p = torch.zeros_like(b)
     ap = torch.zeros_like(b)
     bnorm = float(torch.linalg.norm(b))
+    if bnorm == 0.0:  # u = 0 solves it (whatever tol)
+        return u, 0, 0.0
     rho_old = alpha = zeta = 1.0
     steps = 0
     relres = float(torch.linalg.norm(r)) / bnorm if bnorm > 0 else 0.0
     while relres >= tol and steps < max_iter:
+        if steps > 0 and (zeta == 0.0 or rho_old == 0.0):
+            break
         rho = float(torch.dot(rh, r))
         if steps == 0:
             p = r.clone()
@@ -146,10 +152,14 @@ def bicgstab(matvec: Callable, b, tol: float = 1e-8, max_iter: int = 1000):
             beta = (alpha / zeta) * (rho / rho_old)
             p = r + beta * (p - zeta * ap)
         ap = matvec(p)
-        alpha = rho / float(torch.dot(rh, ap))
+        den = float(torch.dot(rh, ap))
+        if den == 0.0:
+            break
+        alpha = rho / den
         t = r - alpha * ap
         at = matvec(t)
-        zeta = float(torch.dot(at, t)) / float(torch.dot(at, at))
+        aa = float(torch.dot(at, at))
+        zeta = float(torch.dot(at, t)) / aa if aa != 0.0 else 0.0
         u = u + alpha * p + zeta * t
         r = t - zeta * at
         rho_old = rho
@@ -183,18 +193,22 @@ def bicgstab_pipelined(matvec: Callable, b, tol: float = 1e-8, max_iter: int = 1
     dot products for beta and alpha) instead of four.  `scale` (a tensor,
     e.g. diagonal_scaling) applies the reference's right scaling: the solver
     iterates on A diag(scale) and returns u = diag(scale) x.  Returns
-    (u, steps, relres) with relres the recursive residual."""
+    (u, steps, relres) with relres the recursive residual.  A breakdown (a
+    zero denominator) ends the loop with the last iterate."""
     import torch
     D = scale if scale is not None else None
     op = (lambda v: matvec(D * v)) if D is not None else matvec
     x = torch.zeros_like(b)
+    if float(torch.linalg.norm(b)) == 0.0:  # u = 0 solves it (whatever tol)
+        return x, 0, 0.0
     r = b - op(x)
     r0 = r.clone()
     w = op(r)
     t = op(w)
     bnorm = float(torch.linalg.norm(b))
     znorm = float(torch.dot(r, r))
-    alpha = znorm / float(torch.dot(w, r))
+    wr = float(torch.dot(w, r))
+    alpha = znorm / wr if wr != 0.0 else 0.0
     beta = zeta = 0.0
     relres = (znorm ** 0.5) / bnorm if bnorm > 0 else 0.0
     p = s = z = None
@@ -208,7 +222,10 @@ def bicgstab_pipelined(matvec: Callable, b, tol: float = 1e-8, max_iter: int = 1
             z = t + beta * (z - zeta * v)
         q = r - alpha * s
         y = w - alpha * z
-        zeta = float(torch.dot(y, q)) / float(torch.dot(y, y))
+        yy = float(torch.dot(y, y))
+        if yy == 0.0 or alpha == 0.0:
+            break
+        zeta = float(torch.dot(y, q)) / yy
         v = op(z)
         x = x + alpha * p + zeta * q
         r = q - zeta * y
@@ -217,8 +234,13 @@ def bicgstab_pipelined(matvec: Callable, b, tol: float = 1e-8, max_iter: int = 1
         znorm = float(torch.dot(r, r0))
         zw, zs, zz = float(torch.dot(w, r0)), float(torch.dot(s, r0)), float(torch.dot(z, r0))
         rr = float(torch.dot(r, r))
+        if zeta == 0.0 or znorm_old == 0.0:
+            steps += 1
+            relres = (rr ** 0.5) / bnorm
+            break
         beta = (alpha / zeta) * (znorm / znorm_old)
-        alpha = znorm / (zw + beta * zs - beta * zeta * zz)
+        den = zw + beta * zs - beta * zeta * zz
+        alpha = znorm / den if den != 0.0 else 0.0
         t = op(w)
         steps += 1
         relres = (rr ** 0.5) / bnorm

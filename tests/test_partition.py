@@ -131,3 +131,23 @@ def test_pipelined_bicgstab_converges_like_the_flat_solver(build_libs):
         true = np.linalg.norm(b - oracle.matvec(H.st, u.numpy())) / np.linalg.norm(b)
         assert relres < 1e-8 and true < 1e-7, (scale is None, relres, true)
         assert abs(n - n_flat) <= max(3, n_flat // 4), (n, n_flat)
+
+
+def test_solvers_stop_at_a_breakdown():
+    """A skew-symmetric operator gives b^T A b = 0: the first denominator of
+    both host-side solvers is zero.  They stop there and return the start
+    iterate (relres 1) instead of raising; a zero rhs takes no step."""
+    import torch
+    from hacapk_b200.partition import bicgstab, bicgstab_pipelined
+    n = 6
+    A = torch.zeros(n, n, dtype=torch.float64)
+    for i in range(0, n, 2):
+        A[i, i + 1], A[i + 1, i] = 1.0, -1.0
+    mv = lambda v: A @ v  # noqa: E731
+    b = torch.arange(1.0, n + 1, dtype=torch.float64)
+    for solve in (bicgstab, bicgstab_pipelined):
+        u, steps, relres = solve(mv, b, tol=1e-8, max_iter=50)
+        assert steps == 0 and relres == pytest.approx(1.0) and torch.all(u == 0)
+        for tol in (1e-8, 0.0):
+            u, steps, relres = solve(mv, torch.zeros(n, dtype=torch.float64), tol=tol)
+            assert steps == 0 and relres == 0.0 and torch.all(u == 0)
