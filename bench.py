@@ -507,7 +507,34 @@ def cpu_baseline(H, b, args):
     dt = time.perf_counter() - t0
     return {"value": dt, "unit": "s", "cores": 1, "kind": "reference" if kind == "ref" else "port",
             "sample": f"one full C1 solve on the host: {n} iterations, matvec time {mv_s:.2f} s",
-            "iterations": n}
+            "iterations": n, "host_matvec": host_matvecs(H)}
+
+
+def host_matvecs(H, seconds: float = 2.0) -> dict:
+    """The reference's CPU products on the host cores, ms per H-matvec (each
+    repeated for about `seconds`): the CPU-BLAS path of HACApK_MAGMA.c:140-187
+    (one dgemv per leaf; OpenBLAS as bundled with scipy stands in for MKL) on
+    one thread and on every core, and the OpenMP product of
+    m_HACApK_solve.f90:203-253 (restated in C) on every core."""
+    import oracle
+    from threadpoolctl import threadpool_limits
+    cores = len(os.sched_getaffinity(0))
+    x = np.random.default_rng(0).standard_normal(H.nd)
+
+    def per_call(fn):
+        fn()
+        t0, k = time.perf_counter(), 0
+        while time.perf_counter() - t0 < seconds:
+            fn()
+            k += 1
+        return (time.perf_counter() - t0) / k * 1e3
+
+    out = {"cores": cores}
+    for nt in (1, cores):
+        with threadpool_limits(limits=nt, user_api="blas"):
+            out[f"blas_gemv_ms_{nt}_threads"] = per_call(lambda: oracle.matvec_blas(H.st, x))
+    out[f"omp_ms_{cores}_threads"] = per_call(lambda: oracle.matvec_omp(H.st, x, nthreads=cores))
+    return out
 
 
 def run_reference(args, world, rank):
