@@ -228,3 +228,21 @@ class HostHMatrix:
             else:
                 d += L.ndl * L.ndt
         return d, lr
+
+    def accuracy(self) -> tuple[float, float]:
+        """(||A - H||_F, ||A||_F) over the leaves, as HACApK_accuracy_leafmtx
+        (m_HACApK_base.f90:614-673) reports them: a low-rank leaf adds its
+        exact entries to ||A|| and their difference from U V^T to ||A - H||;
+        a dense leaf, which holds the exact entries, adds them to ||A|| only."""
+        zh = za = 0.0
+        for ip in range(self.nlf):
+            kind, nstrtl, ndl, nstrtt, ndt, kt, data = self.leaf_arrays(ip)
+            if kind == 1:
+                U, V = data
+                A = self.dense(nstrtl - 1, ndl, nstrtt - 1, ndt)
+                za += float(np.sum(A * A))
+                E = A - U @ V.T
+                zh += float(np.sum(E * E))
+            else:
+                za += float(np.sum(data * data))
+        return float(np.sqrt(zh)), float(np.sqrt(za))

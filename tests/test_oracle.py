@@ -124,6 +124,25 @@ def test_hmatrix_approximates_dense(build_libs):
     assert err < 1e-4
 
 
+@pytest.mark.parametrize("aca_eps", [1e-5, 1e-7])
+def test_accuracy_check_matches_the_assembled_matrix(build_libs, aca_eps):
+    """The reference's H-matrix accuracy check (HACApK_accuracy_leafmtx,
+    m_HACApK_base.f90:614-673) restated: its ||A - H||_F / ||A||_F equals
+    the one of the H-matrix assembled densely from its leaves against the
+    exact operator, and it follows the ACA+ tolerance."""
+    H = sphere(3, aca_eps=aca_eps)
+    zh, za = H.accuracy()
+    A = H.dense()
+    Hd = np.zeros_like(A)
+    for ip in range(H.nlf):
+        kind, r0, nr, c0, nc, kt, data = H.leaf_arrays(ip)
+        Hd[r0 - 1:r0 - 1 + nr, c0 - 1:c0 - 1 + nc] = data[0] @ data[1].T if kind == 1 else data
+    assert za == pytest.approx(np.linalg.norm(A), rel=1e-12)
+    assert zh / za == pytest.approx(np.linalg.norm(A - Hd) / np.linalg.norm(A), rel=1e-6, abs=1e-15)
+    assert zh / za < 10 * aca_eps
+    print(f"ACA+ {aca_eps:.0e}: ||A - H||_F / ||A||_F = {zh / za:.2e}")
+
+
 def test_oracle_bicgstab_converges(build_libs):
     import oracle
     from hacapk_b200 import configs
