@@ -63,6 +63,23 @@ def test_matvec_c1_full_size_and_deterministic(gpu, build_libs):
     assert relerr(hc, 2.5 * hx + hz) <= 1e-13
 
 
+def test_reference_self_check_with_unit_vector(gpu, build_libs):
+    """The reference's own CPU-vs-GPU check (m_HACApK_solve.f90:705-735):
+    x = 1, error(CPU-GPU) = ||y_cpu - y_gpu||_2 / ||y_cpu||_2, on the C1
+    matrix through hbx_matvec_host."""
+    import oracle
+    from hacapk_b200 import configs
+    from hacapk_b200.engine import Engine
+    H, _ = configs.c1(5)
+    E = Engine(H.st, H.nd)
+    x = np.ones(H.nd)
+    y_cpu = oracle.matvec(H.st, x)
+    y_gpu, _, _ = E.matvec_host(x)
+    err = np.linalg.norm(y_cpu - y_gpu) / np.linalg.norm(y_cpu)
+    print(f"error(CPU-GPU) = {err:.3e}")
+    assert err <= TOL
+
+
 def test_device_api_alpha_beta_and_aliasing(gpu, build_libs):
     import torch
     import oracle
