@@ -1,4 +1,4 @@
-"""The row-partitioned product on the CPU (gloo, world size 2): the
+"""The row-partitioned product on the CPU (gloo, world sizes 2 and 3): the
 reference's MPI scheme (cuts by stored words at leaf row starts,
 m_HACApK_base.f90:511-581; one combination per product,
 HACApK_SOLVER.c:106-251) with the oracle as every rank's local product.  The
@@ -10,6 +10,7 @@ import socket
 import sys
 
 import numpy as np
+import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -38,8 +39,8 @@ def test_row_cuts_assign_every_leaf_once(build_libs):
         assert max(words) <= 1.5 * total / nranks
 
 
-def _rank_main(rank, port, q):
-    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE="2", RANK=str(rank))
+def _rank_main(rank, world, pipelined, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world), RANK=str(rank))
     H, b = _build()
     import torch
     import torch.distributed as dist
@@ -50,12 +51,18 @@ def _rank_main(rank, port, q):
         H.st, H.nd, lambda st, nd: (lambda x: torch.from_numpy(oracle.matvec(st, x.numpy()))))
     x = torch.from_numpy(np.random.default_rng(3).standard_normal(H.nd))
     y = mv(x).numpy()
-    u, steps, relres = partition.bicgstab(mv, torch.from_numpy(b), tol=1e-8, max_iter=500)
+    solve = partition.bicgstab_pipelined if pipelined else partition.bicgstab
+    u, steps, relres = solve(mv, torch.from_numpy(b), tol=1e-8, max_iter=500)
     q.put((rank, y, u.numpy(), steps, relres, mv.subset.nlf))
     dist.destroy_process_group()
 
 
-def test_partitioned_product_and_solve_gloo(build_libs):
+@pytest.mark.parametrize("world,pipelined", [(2, False), (3, True)])
+def test_partitioned_product_and_solve_gloo(build_libs, world, pipelined):
+    """Every rank's combined product equals the oracle's; all ranks hold the
+    same solution, reached in a step count within one of the same solver
+    over the whole product on one process (the flat solver at world size 2,
+    the pipelined one at 3), below 1e-8 in the FP64 residual."""
     import oracle
     import torch
     from hacapk_b200 import partition
@@ -64,7 +71,7 @@ def test_partitioned_product_and_solve_gloo(build_libs):
         port = s.getsockname()[1]
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    ps = [ctx.Process(target=_rank_main, args=(r, port, q)) for r in range(2)]
+    ps = [ctx.Process(target=_rank_main, args=(r, world, pipelined, port, q)) for r in range(world)]
     for p in ps:
         p.start()
     got = sorted((q.get(timeout=300) for _ in ps), key=lambda t: t[0])
@@ -77,17 +84,15 @@ def test_partitioned_product_and_solve_gloo(build_libs):
     for rank, y, u, steps, relres, nlf in got:
         assert 0 < nlf < H.nlf  # each rank holds part of the leaves
         assert np.abs(y - ref).max() <= 1e-13 * np.abs(ref).max()
-    # both ranks hold the same solution (replicated vectors, same sums)
-    assert np.array_equal(got[0][2], got[1][2]) and got[0][3] == got[1][3]
+    # every rank holds the same solution (replicated vectors, same sums)
+    assert all(np.array_equal(got[0][2], g[2]) and got[0][3] == g[3] for g in got[1:])
     # against the same solve with the whole product on one process
-    _, n1, rel1 = partition.bicgstab(lambda v: torch.from_numpy(oracle.matvec(H.st, v.numpy())),
-                                      torch.from_numpy(b), tol=1e-8, max_iter=500)
+    solve = partition.bicgstab_pipelined if pipelined else partition.bicgstab
+    _, n1, rel1 = solve(lambda v: torch.from_numpy(oracle.matvec(H.st, v.numpy())),
+                        torch.from_numpy(b), tol=1e-8, max_iter=500)
     assert abs(got[0][3] - n1) <= 1 and got[0][4] < 1e-8
     rel = np.linalg.norm(b - oracle.matvec(H.st, got[0][2])) / np.linalg.norm(b)
     assert rel < 1.05e-8
-
-
-import pytest  # noqa: E402
 
 
 @pytest.mark.gpu
