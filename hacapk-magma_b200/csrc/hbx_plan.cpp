@@ -115,7 +115,7 @@ uint32_t count_long(const std::vector<Seg> &segs) {
 }  // namespace
 
 int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, std::string &err, int precision,
-              bool pair_panels, const PlanCosts &costs) {
+              bool pair_panels, const PlanCosts &costs, int merge_keep) {
   plan = Plan();
   plan.costs = costs;
   if (precision != kFP64 && precision != kFP32 && precision != kBF16) {
@@ -123,6 +123,7 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
     return HBX_ERR_INVALID;
   }
   if (pair_panels && precision != kFP32) { err = "panel pairs need FP32 storage"; return HBX_ERR_INVALID; }
+  if (pair_panels && merge_keep >= 0) { err = "merged D+U blocks need the single-vector layout"; return HBX_ERR_INVALID; }
   plan.precision = precision;
   plan.pair_panels = pair_panels;
   const uint32_t G = group_cols(precision);
@@ -202,6 +203,7 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
     plan.group_leaf_begin[ngroups] = (uint32_t)plan.group_leaves.size();
   }
   if (ktsum > 0xffffffffull || (uint64_t)nd > 0xffffffffull) { err = "zbu length exceeds 2^32"; return HBX_ERR_INVALID; }
+  if (merge_keep >= 0 && ktsum >= kSegZbu) { err = "zbu length reaches 2^31 (merged blocks)"; return HBX_ERR_INVALID; }
 
   // ---- P blocks: slabs of <= 64 stacked rows
   std::vector<uint32_t> pblocks;
@@ -334,7 +336,19 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
     info.rec_begin = (uint32_t)plan.recs.size();
     info.atom_begin = (uint32_t)plan.atoms.size();
     info.n_atoms = (uint32_t)al.size();
-    for (uint32_t a : al) plan.atoms.push_back(atoms[a]);
+    // merge_keep >= 0: atoms with low-rank rows past the first merge_keep
+    // take one kRunDU block; the atom list follows the blocks' order
+    std::vector<uint32_t> split, merged;
+    {
+      uint32_t with_u = 0;
+      for (uint32_t a : al) {
+        const bool has_u = ublock[a] != 0xffffffffu;
+        if (merge_keep >= 0 && has_u && with_u++ >= (uint32_t)merge_keep) merged.push_back(a);
+        else split.push_back(a);
+      }
+    }
+    for (uint32_t a : split) plan.atoms.push_back(atoms[a]);
+    for (uint32_t a : merged) plan.atoms.push_back(atoms[a]);
     uint64_t pos = 0;
     uint32_t rot = 0;
     auto emit_block = [&](uint32_t bi) -> uint32_t {
@@ -400,9 +414,24 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
     };
     for (uint32_t b : pl) info.nr_p += emit_block(b);
     info.nblk_p = (uint32_t)pl.size();
-    for (uint32_t a : al) info.nr_d += emit_block(dblock[a]);
-    for (uint32_t a : al)
+    for (uint32_t a : split) info.nr_d += emit_block(dblock[a]);
+    for (uint32_t a : split)
       if (ublock[a] != 0xffffffffu) info.nr_u += emit_block(ublock[a]);
+    for (uint32_t a : merged) {
+      const Block d = plan.blocks[dblock[a]], u = plan.blocks[ublock[a]];
+      Block m{kRunDU, d.h, d.a, 0, d.W + u.W, (uint32_t)plan.pieces.size(), d.npiece + u.npiece};
+      for (uint32_t q = 0; q < d.npiece; ++q) {
+        const Piece pc = plan.pieces[d.piece_begin + q];
+        plan.pieces.push_back(pc);
+      }
+      for (uint32_t q = 0; q < u.npiece; ++q) {
+        Piece pc = plan.pieces[u.piece_begin + q];
+        pc.vsrc |= kSegZbu;
+        plan.pieces.push_back(pc);
+      }
+      plan.blocks.push_back(m);
+      info.nr_u += emit_block((uint32_t)plan.blocks.size() - 1);
+    }
     if (pos > 0xfffffff0ull) {
       err = "a CTA stream exceeds 4 GiB; use more CTAs";
       return HBX_ERR_INVALID;
@@ -481,7 +510,8 @@ void pack_plan(const stc_HACApK_leafmtxp *st, const Plan &plan, uint8_t *dst) {
         const int ro = (int)atom_r0 - (s->nstrtl - 1);
         for (uint32_t i = 0; i < h; ++i) {
           double v;
-          if (b.kind == kRunD) v = s->a1[(size_t)lc + (size_t)(ro + (int)i) * s->ndt];  // A(il, it) = a1[it + il*ndt]
+          if (b.kind == kRunD || (b.kind == kRunDU && s->ltmtx == 2))
+            v = s->a1[(size_t)lc + (size_t)(ro + (int)i) * s->ndt];  // A(il, it) = a1[it + il*ndt]
           else v = a2_of(s)[(size_t)(ro + (int)i) + (size_t)lc * s->ndl];              // U(i, l) = a2[i + l*ndl]
           put(i, cc, v);
         }

@@ -82,7 +82,11 @@ constexpr int kStages = HBX_STAGES;  // vector stage buffers: runs gathered ahea
 constexpr int kMaxCtaRuns = 1024;    // run summaries a CTA keeps in shared memory
 constexpr int kMaxPairRuns = 512;    // the same for the multi-RHS engine (pair-panel plans)
 
-enum RunKind : uint16_t { kRunP = 0, kRunD = 1, kRunU = 2 };
+// kRunDU: an atom's dense and low-rank columns in one block (x segments,
+// then zbu segments marked by kSegZbu), placed in the U section; only plans
+// made with merge_keep >= 0 hold it, and the kernels do not take it yet.
+enum RunKind : uint16_t { kRunP = 0, kRunD = 1, kRunU = 2, kRunDU = 3 };
+constexpr uint32_t kSegZbu = 0x80000000u;  // kRunDU segment source: zbu (else x)
 enum RunFlags : uint16_t { kFirst = 0x100, kLast = 0x200 };
 
 // Storage precision of the packed factors.  A panel row is always 16 bytes:
@@ -240,8 +244,14 @@ struct Plan {
 // (message in `err`).
 // pair_panels (FP32 only): every run holds an even number of panels and its
 // segments stay in stage order -- the layout of the multi-RHS engine.
+// merge_keep >= 0 (single-vector layouts only): every atom with low-rank
+// rows, except the first merge_keep such atoms of each CTA, gets one kRunDU
+// block in place of its D and U blocks; the CTA's atom list then holds the
+// atoms of its D blocks, then those of its kRunDU blocks.  The default, -1,
+// keeps every atom split.
 int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, std::string &err,
-              int precision = kFP64, bool pair_panels = false, const PlanCosts &costs = PlanCosts());
+              int precision = kFP64, bool pair_panels = false, const PlanCosts &costs = PlanCosts(),
+              int merge_keep = -1);
 
 // Writes the packed stream of every CTA into `dst` (plan.total_bytes bytes).
 void pack_plan(const stc_HACApK_leafmtxp *st, const Plan &plan, uint8_t *dst);

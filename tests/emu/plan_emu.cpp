@@ -18,14 +18,15 @@
 using namespace hbx;
 
 static int emu_run(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int precision, bool pairs, const double *x,
-                   double *y, long long *stats, char *msg, int msglen, const PlanCosts &costs = PlanCosts()) {
+                   double *y, long long *stats, char *msg, int msglen, const PlanCosts &costs = PlanCosts(),
+                   int merge_keep = -1) {
   auto bad = [&](const std::string &s) {
     std::snprintf(msg, msglen, "%s", s.c_str());
     return 1;
   };
   Plan plan;
   std::string err;
-  int rc = make_plan(st, nd, num_ctas, plan, err, precision, pairs, costs);
+  int rc = make_plan(st, nd, num_ctas, plan, err, precision, pairs, costs, merge_keep);
   if (rc != 0) return bad("make_plan: " + err);
   std::vector<uint8_t> buf(plan.total_bytes, 0xAB);
   pack_plan(st, plan, buf.data());
@@ -48,7 +49,8 @@ static int emu_run(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int prec
     uint32_t pos = 0;
     for (uint32_t k = 0; k < nr; ++k) {
       const Run &r = plan.recs[ci.rec_begin + k].hdr;
-      const uint32_t want = k < ci.nr_p ? kRunP : (k < ci.nr_p + ci.nr_d ? kRunD : kRunU);
+      uint32_t want = k < ci.nr_p ? kRunP : (k < ci.nr_p + ci.nr_d ? kRunD : kRunU);
+      if (want == kRunU && run_kind(r) == kRunDU) want = kRunDU;  // merged blocks sit in the U section
       if (run_kind(r) != want) return "run kind out of section order";
       if (r.nrow == 0 || r.nrow > (want == kRunP ? kSlabMax : kAtomMax)) return "run height outside 1..32 (1..64 for P)";
       const RunLite &L = plan.lite[ci.rec_begin + k];
@@ -67,6 +69,7 @@ static int emu_run(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int prec
       if (r.vlen != G * r.npanel && !(r.flags & kLast)) return "zero columns outside a block's last run";
       const uint32_t real = r.vlen;
       const uint64_t vmax = want == kRunU ? plan.zbu_len : (uint64_t)nd;
+      const bool du = want == kRunDU;
       std::vector<char> cov(real, 0);
       uint32_t d = 0;
       if (r.nlong > r.nseg) return "nlong > nseg";
@@ -75,7 +78,9 @@ static int emu_run(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int prec
         if (s.len == 0 || (uint32_t)s.dst + s.len > real) return "segment outside the stage";
         if (pairs ? (r.nlong != 0 || s.dst != d) : ((q < r.nlong) != (s.len > (uint32_t)kSegShort)))
           return pairs ? "pair-panel segments not in stage order" : "long segments not first";
-        if ((uint64_t)s.src + s.len > vmax) return "segment source out of range";
+        const bool z = du && (s.src & kSegZbu);
+        const uint64_t src = du ? (s.src & ~kSegZbu) : s.src;
+        if (src + s.len > (du ? (z ? plan.zbu_len : (uint64_t)nd) : vmax)) return "segment source out of range";
         for (uint32_t e = 0; e < s.len; ++e) {
           if (cov[s.dst + e]) return "segments overlap";
           cov[s.dst + e] = 1;
@@ -90,12 +95,15 @@ static int emu_run(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int prec
     return "";
   };
   // one run: gather, multiply its pair panels, finish the block on its last run
+  // vec: the run's vector; a kRunDU run picks x or zbu per segment
   auto run_one = [&](const CtaInfo &ci, uint32_t k, const double *vec) {
     const RunRec &R = plan.recs[ci.rec_begin + k];
     const Run &r = R.hdr;
+    const bool du = run_kind(r) == kRunDU;
     for (uint32_t q = 0; q < r.nseg; ++q)
       for (uint32_t e = 0; e < R.seg[q].len; ++e) {
-        const double v = vec[R.seg[q].src + e];
+        const uint32_t sv = R.seg[q].src;
+        const double v = du ? ((sv & kSegZbu) ? zbu[(sv & ~kSegZbu) + e] : x[sv + e]) : vec[sv + e];
         stage[R.seg[q].dst + e] = precision != kFP64 ? (double)(float)v : v;
       }
     for (uint32_t c = r.vlen; c < G * r.npanel; ++c) stage[c] = 0.0;
@@ -139,9 +147,10 @@ static int emu_run(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int prec
     const CtaInfo &ci = plan.ctas[c];
     uint32_t owned = 0;
     for (uint32_t k = ci.nr_p; k < ci.nr_p + ci.nr_d + ci.nr_u; ++k) {
-      const bool is_u = k >= ci.nr_p + ci.nr_d;
-      run_one(ci, k, is_u ? zbu.data() : x);
       const Run &r = plan.recs[ci.rec_begin + k].hdr;
+      const bool is_du = run_kind(r) == kRunDU;
+      const bool is_u = k >= ci.nr_p + ci.nr_d && !is_du;  // adds to rows an earlier D block wrote
+      run_one(ci, k, is_u ? zbu.data() : x);
       if (!(r.flags & kLast)) continue;
       for (uint32_t i = 0; i < r.nrow; ++i) {
         const uint32_t row = r.out + i;
@@ -234,3 +243,60 @@ extern "C" int emu_matvec_transposed(const stc_HACApK_leafmtxp *st, int nd, int 
 // bfloat16 rounding of the packer, one value at a time (checked against an
 // independent restatement in the tests).
 extern "C" unsigned emu_bf16_from_double(double v) { return bf16_from_double(v); }
+
+// FNV-1a digest of everything a plan hands to the device: run records, run
+// summaries, CTA table, owned atoms and the packed stream.
+extern "C" unsigned long long emu_plan_digest(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int precision,
+                                              int pairs) {
+  Plan plan;
+  std::string err;
+  if (make_plan(st, nd, num_ctas, plan, err, precision, pairs != 0) != 0) return 0;
+  std::vector<uint8_t> buf(plan.total_bytes, 0);
+  pack_plan(st, plan, buf.data());
+  unsigned long long h = 1469598103934665603ull;
+  auto mix = [&](const void *p, size_t n) {
+    const uint8_t *b = static_cast<const uint8_t *>(p);
+    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+  };
+  mix(plan.recs.data(), plan.recs.size() * sizeof(RunRec));
+  mix(plan.lite.data(), plan.lite.size() * sizeof(RunLite));
+  mix(plan.ctas.data(), plan.ctas.size() * sizeof(CtaInfo));
+  mix(plan.atoms.data(), plan.atoms.size() * sizeof(Atom));
+  mix(buf.data(), buf.size());
+  return h;
+}
+
+// The layout with merged D+U blocks (make_plan's merge_keep), FP64 or any
+// storage precision.
+extern "C" int emu_matvec_merged(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int precision, int merge_keep,
+                                 const double *x, double *y, long long *stats, char *msg, int msglen) {
+  return emu_run(st, nd, num_ctas, precision, false, x, y, stats, msg, msglen, PlanCosts(), merge_keep);
+}
+
+// Per-CTA stream bytes and run counts of a plan (merge_keep as make_plan's).
+extern "C" int emu_plan_cta_table(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int precision, int merge_keep,
+                                  long long *bytes, int *runs) {
+  Plan plan;
+  std::string err;
+  if (make_plan(st, nd, num_ctas, plan, err, precision, false, PlanCosts(), merge_keep) != 0) return 1;
+  for (int c = 0; c < num_ctas; ++c) {
+    bytes[c] = plan.ctas[c].stream_bytes;
+    runs[c] = (int)(plan.ctas[c].nr_p + plan.ctas[c].nr_d + plan.ctas[c].nr_u);
+  }
+  return 0;
+}
+
+// Per-CTA run counts by section (P, D, U) of a plan.
+extern "C" int emu_plan_cta_sections(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int precision,
+                                     int merge_keep, int *np, int *ndr, int *nu, int *natoms) {
+  Plan plan;
+  std::string err;
+  if (make_plan(st, nd, num_ctas, plan, err, precision, false, PlanCosts(), merge_keep) != 0) return 1;
+  for (int c = 0; c < num_ctas; ++c) {
+    np[c] = (int)plan.ctas[c].nr_p;
+    ndr[c] = (int)plan.ctas[c].nr_d;
+    nu[c] = (int)plan.ctas[c].nr_u;
+    natoms[c] = (int)plan.ctas[c].n_atoms;
+  }
+  return 0;
+}

@@ -31,6 +31,8 @@ def emu(build_libs):
                                      C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_char_p, C.c_int]
     lib.emu_matvec_costs.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_longlong, C.c_longlong, C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_char_p, C.c_int]
+    lib.emu_matvec_merged.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_char_p, C.c_int]
     lib.emu_bf16_from_double.argtypes = [C.c_double]
     lib.emu_bf16_from_double.restype = C.c_uint
     return lib
@@ -389,3 +391,59 @@ def test_pair_panel_layout_edge_cases(emu):
                               y.ctypes.data_as(C.POINTER(C.c_double)), stats, msg, 512)
     assert rc == 0, msg.value.decode()
     assert np.all(y == 0.0)
+
+
+def _merged(emu, H, nc, keep, precision=0, seed=0):
+    x = np.random.default_rng(seed).standard_normal(H.nd)
+    y = np.zeros(H.nd)
+    stats = (C.c_longlong * 8)()
+    msg = C.create_string_buffer(512)
+    rc = emu.emu_matvec_merged(C.cast(H.st, C.c_void_p), H.nd, nc, precision, keep,
+                               x.ctypes.data_as(C.POINTER(C.c_double)), y.ctypes.data_as(C.POINTER(C.c_double)),
+                               stats, msg, 512)
+    return rc, msg.value.decode(), x, y, list(stats)
+
+
+@pytest.mark.parametrize("level,nc,keep", [(3, 148, 0), (3, 148, 1), (4, 148, 0), (4, 148, 2), (3, 7, 1),
+                                           (3, 1, 0), (4, 300, 0)])
+def test_merged_du_layout(emu, level, nc, keep):
+    """Merged D+U blocks (make_plan's merge_keep): an atom's dense and
+    low-rank columns in one block in the U section, each gather segment
+    marked with its source.  The layout keeps every invariant the emulator
+    checks (rows written once, by the CTA that owns them; the atom list in
+    the order of the blocks that first write them), reproduces the oracle,
+    packs the same factor bytes and needs no more runs than the split layout
+    (fewer when every atom merges: at 148 CTAs these matrices hold few
+    atoms with low-rank rows per CTA, so merge_keep = 1 or 2 may leave all
+    split)."""
+    import oracle
+    H = sphere(level)
+    rc, msg, x, y, st_m = _merged(emu, H, nc, keep, seed=level + nc)
+    assert rc == 0, msg
+    ref = oracle.matvec(H.st, x)
+    assert np.abs(y - ref).max() <= 1e-14 * np.abs(ref).max()
+    rc, msg, _, _, st_s = _merged(emu, H, nc, -1, seed=level + nc)
+    assert rc == 0, msg
+    d, lr = H.storage_words()
+    assert st_m[6] == 8 * (d + lr) + st_m[7]   # every factor packed once
+    assert st_m[1] <= st_s[1]                   # never more runs;
+    if keep == 0:                               # fewer when every atom with U rows merges
+        assert st_m[1] < st_s[1]
+    print(f"L{level} nc={nc} keep={keep}: runs {st_s[1]} -> {st_m[1]}")
+
+
+def test_merged_du_layout_other_precisions_and_rejects_pairs(emu):
+    import oracle
+    H = sphere(3)
+    for prec, tol in ((1, 2e-6), (2, 2.0**-8)):
+        rc, msg, x, y, _ = _merged(emu, H, 148, 0, precision=prec, seed=prec)
+        assert rc == 0, msg
+        ref = oracle.matvec(H.st, x)
+        assert np.linalg.norm(y - ref) / np.linalg.norm(ref) <= tol
+    # the multi-RHS layout has no merged form
+    stats = (C.c_longlong * 8)()
+    msg = C.create_string_buffer(512)
+    x = np.zeros(H.nd)
+    y = np.zeros(H.nd)
+    assert emu.emu_matvec_pairs(C.cast(H.st, C.c_void_p), H.nd, 148, x.ctypes.data_as(C.POINTER(C.c_double)),
+                                y.ctypes.data_as(C.POINTER(C.c_double)), stats, msg, 512) == 0
