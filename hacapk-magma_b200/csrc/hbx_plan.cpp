@@ -130,7 +130,7 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
   // run widths are multiples of RG columns: whole panels, or whole panel
   // pairs (the K = 8 of one TF32 tensor-core step) for the multi-RHS engine
   const uint32_t RG = pair_panels ? 2 * G : G;
-  const uint32_t stage_cols = kStageBytes / stage_elem_bytes(precision);
+  const uint32_t stage_cols = (pair_panels ? kPairStageBytes : kStageBytes) / stage_elem_bytes(precision);
   if (!st || nd <= 0 || num_ctas <= 0) { err = "null container, nd <= 0 or no CTAs"; return HBX_ERR_INVALID; }
   const int nlf = st->nlf;
   if (nlf < 0 || (nlf > 0 && (!st->st_lf || st->st_lf_stride < (int)sizeof(stc_HACApK_leafmtx)))) {

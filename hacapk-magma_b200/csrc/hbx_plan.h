@@ -69,7 +69,13 @@ constexpr int kConsumerWarps = 16; // warps that multiply (+ producer, gather, g
 constexpr int kChunkLog = HBX_CHUNK_LOG;      // ring chunk = 32 KB (bulk copies this size stream at HBM rate)
 constexpr int kChunkBytes = 1 << kChunkLog;
 constexpr int kRingChunks = HBX_RING_CHUNKS;  // 128 KB ring per CTA
-constexpr int kStageBytes = 8192;  // one vector stage buffer: 1024 doubles or 2048 floats
+#ifndef HBX_STAGE_BYTES
+#define HBX_STAGE_BYTES 8192
+#endif
+constexpr int kStageBytes = HBX_STAGE_BYTES;  // one vector stage buffer: 1024 doubles or 2048 floats (8 KB)
+constexpr int kPairStageBytes = 8192;         // run width of the multi-RHS layout (2048 float columns)
+static_assert(kStageBytes % 16 == 0 && kStageBytes >= kPairStageBytes && kStageBytes / 4 <= 65535,
+              "stage size: 16-byte multiple, at least the multi-RHS run width, columns within 16-bit offsets");
 constexpr int kStageCap = kStageBytes / 8;  // doubles per stage buffer
 constexpr int kRunSegs = 124;      // gather segments per run record
 constexpr int kSegShort = 32;      // a segment this long or shorter is copied by one gather lane;

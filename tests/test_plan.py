@@ -447,3 +447,33 @@ def test_merged_du_layout_other_precisions_and_rejects_pairs(emu):
     y = np.zeros(H.nd)
     assert emu.emu_matvec_pairs(C.cast(H.st, C.c_void_p), H.nd, 148, x.ctypes.data_as(C.POINTER(C.c_double)),
                                 y.ctypes.data_as(C.POINTER(C.c_double)), stats, msg, 512) == 0
+
+
+def test_merged_du_layout_needs_wider_stages(build_libs):
+    """The merge's gain, on the planner's own per-CTA tables (C1 L5, 148
+    CTAs): with 8 KB stages an atom's D and U columns together overflow one
+    stage, so the CTA holding the most runs keeps them all; with 16 KB stages
+    (the planner built with HBX_STAGE_BYTES=16384) merging takes that maximum
+    down by the 6 U runs of its atoms."""
+    from hacapk_b200 import configs
+    lib16 = os.path.join(ROOT, "tests", "emu", "_build", "libplanemu16.so")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-DHBX_STAGE_BYTES=16384", "-o",
+                    lib16, EMU_SRC, os.path.join(ROOT, "hacapk-magma_b200", "csrc", "hbx_plan.cpp")], check=True)
+    H, _ = configs.c1(5)
+    nc = 148
+
+    def max_runs(lib, keep):
+        b, r = (C.c_longlong * nc)(), (C.c_int * nc)()
+        assert lib.emu_plan_cta_table(C.cast(H.st, C.c_void_p), H.nd, nc, 0, keep, b, r) == 0
+        return max(r[:])
+
+    lib8 = C.CDLL(EMU_LIB)
+    lib16 = C.CDLL(lib16)
+    for lib in (lib8, lib16):
+        lib.emu_plan_cta_table.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                           C.POINTER(C.c_longlong), C.POINTER(C.c_int)]
+    split8, merged8 = max_runs(lib8, -1), max_runs(lib8, 0)
+    split16, merged16 = max_runs(lib16, -1), max_runs(lib16, 0)
+    print(f"max runs per CTA: 8 KB {split8} -> {merged8}, 16 KB {split16} -> {merged16}")
+    assert merged8 == split8
+    assert merged16 <= split16 - 5
