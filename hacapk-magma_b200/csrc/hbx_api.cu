@@ -127,6 +127,7 @@ hbx::MatvecArgs matvec_args(hbx_hmat *h, double alpha, const double *x, double b
   a.err = h->d_err;
   a.timeout_ns = h->timeout_ns;
   a.prof = h->d_prof;
+  a.keep_frac = h->keep_frac;
   return a;
 }
 
@@ -256,6 +257,10 @@ static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_option
   int nc = (opt && opt->num_ctas > 0) ? opt->num_ctas : max_ctas;
   if (nc > max_ctas) return bail(fail(HBX_ERR_INVALID, "hbx_create: num_ctas exceeds co-resident CTAs"));
   h->num_ctas = nc;
+  // L2 budget for the factor stream's pass-to-pass residency (MB): 24 by
+  // default, HBX_L2_KEEP_MB overrides (0 turns the cache hints off)
+  const char *keep = std::getenv("HBX_L2_KEEP_MB");
+  const double keep_mb = keep ? std::atof(keep) : 24.0;
   const char *tmo = std::getenv("HBX_TIMEOUT_MS");
   if (tmo) h->timeout_ns = (unsigned long long)(std::atof(tmo) * 1e6);
   const char *prof = std::getenv("HBX_PROFILE");
@@ -281,6 +286,14 @@ static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_option
   int st_plan = hbx::make_plan(st, nd, nc, h->plan, err, prec, nrhs > 1, costs);
   if (st_plan != HBX_OK) return bail(fail(st_plan, "hbx_create: " + err));
   const hbx::Plan &P = h->plan;
+  // L2 residency of the factor stream: the head of every CTA's stream, in
+  // all keep_mb megabytes, is read with the evict_last policy so that it
+  // stays in L2 from one product to the next; the rest streams with
+  // evict_first (HBX_L2_KEEP_MB; 0 = plain copies)
+  if (keep_mb > 0.0 && P.total_bytes > 0) {
+    const double f = keep_mb * 1e6 / (double)P.total_bytes;
+    h->keep_frac = f >= 1.0 ? 65536u : (uint32_t)(f * 65536.0);
+  }
 
   std::vector<uint8_t> host;
   try {
@@ -622,6 +635,7 @@ static hbx::BicgArgs bicg_args(hbx_hmat *h, const double *b, double *u, double t
   a.prof = h->d_prof;
   a.tol = tol;
   a.max_iter = max_iter;
+  a.keep_frac = h->keep_frac;
   return a;
 }
 

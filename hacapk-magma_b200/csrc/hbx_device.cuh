@@ -25,7 +25,10 @@ constexpr uint32_t kRingBytes = (uint32_t)kRingChunks * kChunkBytes;
 #define HBX_GATHER_WARPS 2
 #endif
 constexpr int kGatherWarps = HBX_GATHER_WARPS;  // warps that stage run vectors
-constexpr uint32_t kRecSlots = 8;               // run records in flight per gather warp
+#ifndef HBX_REC_SLOTS
+#define HBX_REC_SLOTS 8
+#endif
+constexpr uint32_t kRecSlots = HBX_REC_SLOTS;   // run records in flight per gather warp
 constexpr uint32_t kRedSlots = 4;               // block ends parked at once
 static_assert(kStages % kGatherWarps == 0, "a stage slot is always filled by the same gather warp");
 // consumer warps, the bulk-copy producer warp, the gather warps, the
@@ -62,8 +65,14 @@ struct SharedLayout {
   static constexpr uint32_t gdone = pdone + 8;                               // every CTA's zbu is complete
   static constexpr uint32_t redfull = gdone + 8;                             // [kRedSlots] a block's partials parked
   static constexpr uint32_t rdone = redfull + 8 * kRedSlots;                 // a pass's block sums are written
-  static constexpr uint32_t rsum = rdone + 8;                                // block ends summed so far; [1]: grid gen0
-  static constexpr uint32_t bytes = rsum + 16;
+  // [0] block ends summed so far; [1] the launch's first grid-barrier
+  // generation; [2] passes whose x is ready; [3] passes whose zbu is
+  // complete grid-wide (the gather warps wait on these two counters, not on
+  // xready / gdone: a gather warp can reach its first wait of a kind after
+  // both of the launch's phases completed, where a parity wait would take
+  // the finished second phase for the one it wants and never return)
+  static constexpr uint32_t rsum = rdone + 8;
+  static constexpr uint32_t bytes = rsum + 16 + 16;
 };
 static_assert(SharedLayout::red % 16 == 0 && SharedLayout::stage % 16 == 0 && SharedLayout::lite % 16 == 0 &&
                   SharedLayout::rec % 16 == 0 && SharedLayout::sfull % 8 == 0,
@@ -152,6 +161,30 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 
+// The same with an L2 cache-eviction hint (a createpolicy value).
+__device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, uint32_t bytes, uint64_t *bar,
+                                              uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+      : "memory");
+}
+
+// L2 policies of the streamed factors: the part of a CTA's stream that is
+// kept in L2 from one pass to the next (evict_last), and the rest, which
+// passes through L2 without displacing it or the vectors (evict_first).
+__device__ __forceinline__ uint64_t l2_policy_keep() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_stream() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
 // Ampere-style asynchronous gathers into shared memory (vector staging).
 // 8-byte copies go through L1 (.ca); 16-byte copies bypass it (.cg).
 __device__ __forceinline__ void cp_async4(void *dst, const void *src) {
@@ -189,6 +222,23 @@ __device__ __forceinline__ unsigned ld_acquire_s(const unsigned *p) {
 }
 __device__ __forceinline__ void st_release_s(unsigned *p, unsigned v) {
   asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v) : "memory");
+}
+
+// Bounded wait until a CTA counter in shared memory reaches `need`; every
+// lane acquires it.  Warp-uniform outcome.
+__device__ __forceinline__ bool count_wait(const unsigned *cnt, unsigned need, uint64_t timeout_ns) {
+  bool ok = true;
+  if (ld_acquire_s(cnt) < need) {
+    const uint64_t t0 = gtimer();
+    while (ld_acquire_s(cnt) < need) {
+      __nanosleep(64);
+      if (gtimer() - t0 > timeout_ns) {
+        ok = false;
+        break;
+      }
+    }
+  }
+  return __all_sync(0xffffffffu, ok);
 }
 
 __device__ __forceinline__ double lds_f64(uint32_t addr) {
@@ -240,14 +290,24 @@ __device__ __forceinline__ bool grid_wait(const unsigned *gbar, unsigned target,
 
 // ---- producer: streams `npass` passes over the CTA's byte range ------------
 // Chunk g of the launch (g = pass * K + k) covers stream bytes k * kChunkBytes
-// on, in ring slot g % kRingChunks.
-__device__ __forceinline__ void producer_issue(const uint8_t *src, uint32_t bytes, uint32_t K, uint32_t g,
-                                               uint8_t *ring, uint64_t *full) {
+// on, in ring slot g % kRingChunks.  `keep` > 0: the chunks that start below
+// byte `keep` of the CTA's stream are read with the evict_last policy (they
+// stay in L2 for the next pass), the others with evict_first; keep == 0
+// issues plain copies.
+struct StreamSrc {
+  const uint8_t *src;
+  uint32_t bytes, keep;
+};
+__device__ __forceinline__ void producer_issue(const StreamSrc &ss, uint32_t K, uint32_t g, uint8_t *ring,
+                                               uint64_t *full) {
   const uint32_t s = g % kRingChunks;
   const uint32_t off = (g % K) << kChunkLog;
-  const uint32_t nb = min((uint32_t)kChunkBytes, bytes - off);
+  const uint32_t nb = min((uint32_t)kChunkBytes, ss.bytes - off);
   mbar_arrive_expect_tx(&full[s], nb);
-  bulk_g2s(ring + ((size_t)s << kChunkLog), src + off, nb, &full[s]);
+  if (ss.keep == 0) bulk_g2s(ring + ((size_t)s << kChunkLog), ss.src + off, nb, &full[s]);
+  else
+    bulk_g2s_hint(ring + ((size_t)s << kChunkLog), ss.src + off, nb, &full[s],
+                  off < ss.keep ? l2_policy_keep() : l2_policy_stream());
 }
 
 // The producer thread's part of the CTA set-up, before the CTA's first
@@ -255,16 +315,16 @@ __device__ __forceinline__ void producer_issue(const uint8_t *src, uint32_t byte
 // per ring slot, which needs no empty wait), so the stream is under way while
 // the other threads load the run summaries and reduce scalars.  Returns the
 // number of chunks issued; producer_run goes on from there.
-__device__ __forceinline__ uint32_t producer_start(const uint8_t *src, uint32_t bytes, uint32_t npass,
-                                                  uint8_t *ring, uint64_t *full, uint64_t *empty) {
+__device__ __forceinline__ uint32_t producer_start(const StreamSrc &ss, uint32_t npass, uint8_t *ring,
+                                                  uint64_t *full, uint64_t *empty) {
   for (int i = 0; i < kRingChunks; ++i) {
     mbar_init(&full[i], 1);
     mbar_init(&empty[i], kConsumerWarps);
   }
   mbar_fence_init();
-  const uint32_t K = (bytes + kChunkBytes - 1) >> kChunkLog;
+  const uint32_t K = (ss.bytes + kChunkBytes - 1) >> kChunkLog;
   const uint32_t n = min(K * npass, (uint32_t)kRingChunks);
-  for (uint32_t g = 0; g < n; ++g) producer_issue(src, bytes, K, g, ring, full);
+  for (uint32_t g = 0; g < n; ++g) producer_issue(ss, K, g, ring, full);
   return n;
 }
 
@@ -277,10 +337,9 @@ __device__ __forceinline__ void producer_drain(uint64_t *full, uint32_t issued, 
 
 // The rest of the stream: chunk g once the consumers emptied chunk
 // g - kRingChunks.
-__device__ __forceinline__ void producer_run(const uint8_t *src, uint32_t bytes, uint32_t npass, uint32_t issued0,
-                                             uint8_t *ring, uint64_t *full, uint64_t *empty, int *err,
-                                             uint64_t timeout_ns) {
-  const uint32_t K = (bytes + kChunkBytes - 1) >> kChunkLog;
+__device__ __forceinline__ void producer_run(const StreamSrc &ss, uint32_t npass, uint32_t issued0, uint8_t *ring,
+                                             uint64_t *full, uint64_t *empty, int *err, uint64_t timeout_ns) {
+  const uint32_t K = (ss.bytes + kChunkBytes - 1) >> kChunkLog;
   const uint32_t total = K * npass;
   uint32_t issued = issued0;
   for (uint32_t g = issued0; g < total; ++g) {
@@ -291,7 +350,7 @@ __device__ __forceinline__ void producer_run(const uint8_t *src, uint32_t bytes,
         break;
       }
     }
-    producer_issue(src, bytes, K, g, ring, full);
+    producer_issue(ss, K, g, ring, full);
     issued = g + 1;
   }
   producer_drain(full, issued, timeout_ns);
@@ -407,8 +466,9 @@ struct GatherCtx {
 // short one with one lane, clears the zero columns of the last panel, and
 // completes the slot's sfull barrier (32 cp.async arrivals + one plain
 // arrival).  Before its first run of a pass it waits for that pass's x
-// (xready), and before its first U run of a pass for the grid barrier that
-// completes zbu (gdone).  Run records arrive kRecSlots runs ahead by cp.async.
+// (the x-ready count), and before its first U run of a pass for the grid
+// barrier that completes zbu (the zbu-ready count).  Run records arrive
+// kRecSlots runs ahead by cp.async.
 template <int kPrec, class SM>
 __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm, uint32_t gi) {
   constexpr bool kF32 = kPrec != kFP64;  // float copies of the vectors (FP32 and BF16 storage)
@@ -432,13 +492,14 @@ __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm, ui
   for (uint32_t i = 0; i < nmine && ok; ++i) {
     const uint32_t g = gi + i * kGatherWarps, k = g % c.nr, pass = g / c.nr;
     ok = warp_wait(&rfull[i % kRecSlots], (i / kRecSlots) & 1, c.timeout_ns);
-    // A parity wait only tells the current phase from the one before it, so
-    // the phases of xready and gdone are observed one pass after the other,
-    // also for passes in which this warp stages nothing.
-    for (; ok && xpass < (int)pass; ++xpass) ok = warp_wait(sm.xready, (uint32_t)(xpass + 1) & 1, c.timeout_ns);
+    if (ok && xpass < (int)pass) {
+      ok = count_wait(&sm.rsum[2], pass + 1, c.timeout_ns);
+      xpass = (int)pass;
+    }
     const bool is_u = k >= c.nr_pd;
     if (ok && is_u && upass < (int)pass) {
-      for (; ok && upass < (int)pass; ++upass) ok = warp_wait(sm.gdone, (uint32_t)(upass + 1) & 1, c.timeout_ns);
+      ok = count_wait(&sm.rsum[3], pass + 1, c.timeout_ns);
+      upass = (int)pass;
       __threadfence();
     }
     const uint32_t slot = g % kStages;

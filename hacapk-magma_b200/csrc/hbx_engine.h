@@ -48,6 +48,7 @@ struct MatvecArgs {
   int *err;
   unsigned long long timeout_ns;
   unsigned long long *prof;  // optional: per-CTA %globaltimer stamps [num_ctas][16], slots 0-5
+  uint32_t keep_frac;        // fraction (of 2^16) of each CTA's stream kept in L2 between passes; 0: no hints
 };
 
 struct BicgArgs {
@@ -70,6 +71,7 @@ struct BicgArgs {
   unsigned long long *prof;  // optional: per-CTA %globaltimer stamps [num_ctas][16], slots 8-15
   double tol;
   int max_iter;
+  uint32_t keep_frac;  // as MatvecArgs::keep_frac
 };
 
 // Multi-RHS product on the tensor cores (hbx_mrhs.cu): Y = alpha*H*X +
@@ -195,6 +197,7 @@ struct hbx_hmat {
   unsigned *d_gbar = nullptr;
   int *d_err = nullptr;
   unsigned long long timeout_ns = 2000000000ull;
+  uint32_t keep_frac = 0;  // fraction (of 2^16) of every CTA's stream kept in L2 between passes
   unsigned long long *d_prof = nullptr;  // phase stamps of the last matvec (HBX_PROFILE=1)
   double setup_seconds = 0.0;
   cudaStream_t stream = nullptr;  // used by the host-vector calls

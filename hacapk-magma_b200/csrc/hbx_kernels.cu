@@ -82,6 +82,8 @@ __device__ __forceinline__ void init_cta_part(const Smem &s, const RunLite *lite
     mbar_init(s.rdone, 1);
     s.rsum[0] = 0;
     s.rsum[1] = grid_gen0(gbar);
+    s.rsum[2] = 0;
+    s.rsum[3] = 0;
     mbar_fence_init();
   }
   if (threadIdx.x < t0) return;
@@ -112,8 +114,16 @@ __device__ __forceinline__ void sync_warp(unsigned *gbar, uint32_t npass, uint32
       atomicOr(err, kErrGridBarrier);
       return;
     }
+    st_release_s(&sm.rsum[3], p + 1);  // the gather warps' U runs of pass p may start
     mbar_arrive(sm.gdone);
   }
+}
+
+// x of the launch's pass `pass` is ready: the gather warps' count, then the
+// block-sum warp's barrier.  One thread.
+__device__ __forceinline__ void signal_xready(const Smem &sm, unsigned pass) {
+  st_release_s(&sm.rsum[2], pass + 1);
+  mbar_arrive(sm.xready);
 }
 
 // Where the block sums of one H-matvec pass go.
@@ -266,6 +276,15 @@ __device__ __forceinline__ void matvec_pass(Ring &R, uint32_t K, uint32_t nr, ui
   if (threadIdx.x < 32 && !warp_wait(sm.gdone, o.pass & 1, tmo) && threadIdx.x == 0) atomicOr(err, kErrGridBarrier);
 }
 
+// Bytes at the head of a CTA's stream read with the evict_last policy: a
+// fraction keep_frac / 2^16 of the stream, whole chunks (0: no cache hints).
+__device__ __forceinline__ uint32_t keep_bytes(uint32_t stream_bytes, uint32_t keep_frac) {
+  if (keep_frac == 0) return 0;
+  const uint64_t b = ((uint64_t)stream_bytes * keep_frac) >> 16;
+  const uint64_t r = (b + kChunkBytes - 1) & ~(uint64_t)(kChunkBytes - 1);
+  return r > 0xffffffffull ? 0xffffffffu : (uint32_t)r;
+}
+
 // kPrec: storage precision of the factors; FP32 and BF16 engines gather the
 // float copies of the vectors.
 template <int kPrec>
@@ -277,15 +296,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
   const uint64_t t_start = a.prof ? gtimer() : 0;
   uint32_t issued0 = 0;
-  if (threadIdx.x == kProducerWarp * 32)
-    issued0 = producer_start(a.stream + ci.stream_off, ci.stream_bytes, 1, sm.ring, sm.full, sm.empty);
+  const StreamSrc ss{a.stream + ci.stream_off, ci.stream_bytes, keep_bytes(ci.stream_bytes, a.keep_frac)};
+  if (threadIdx.x == kProducerWarp * 32) issued0 = producer_start(ss, 1, sm.ring, sm.full, sm.empty);
   init_cta(sm, a.lite + ci.rec_begin, nr, a.gbar);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
   if (w == kProducerWarp) {
     if (lane == 0 && K > 0)
-      producer_run(a.stream + ci.stream_off, ci.stream_bytes, 1, issued0, sm.ring, sm.full, sm.empty, a.err,
-                   a.timeout_ns);
+      producer_run(ss, 1, issued0, sm.ring, sm.full, sm.empty, a.err, a.timeout_ns);
     return;
   }
   if (w >= kGatherWarp0 && w < kSyncWarp) {
@@ -304,7 +322,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
     sum_warp(nr, 1, ci.nblk_p, &o, sm, a.err, a.timeout_ns);
     return;
   }
-  if (threadIdx.x == 0) mbar_arrive(sm.xready);  // x is an input: ready from the start
+  if (threadIdx.x == 0) signal_xready(sm, 0);  // x is an input: ready from the start
   uint32_t nb = 0;
   Ring R{sm.ring, sm.full, sm.empty, 0, 0, 0, a.timeout_ns, a.err, false};
   matvec_pass<kPrec>(R, K, nr, nb, o, sm, a.err, a.timeout_ns);
@@ -464,9 +482,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
   // the producer starts the stream of the first H-matvec, warps 4 and up set
   // up the CTA and warps 0-3 reduce the scalars
+  const StreamSrc ss{a.stream + ci.stream_off, ci.stream_bytes, keep_bytes(ci.stream_bytes, a.keep_frac)};
   uint32_t issued0 = 0;
-  if (threadIdx.x == kProducerWarp * 32)
-    issued0 = producer_start(a.stream + ci.stream_off, ci.stream_bytes, 2, sm.ring, sm.full, sm.empty);
+  if (threadIdx.x == kProducerWarp * 32) issued0 = producer_start(ss, 2, sm.ring, sm.full, sm.empty);
   init_cta_part(sm, a.lite + ci.rec_begin, nr, a.gbar, 128);
 
   // ---- S0: scalars of the previous step; stop test at the top of the loop
@@ -539,8 +557,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
   if (w == kProducerWarp) {
     if (lane == 0 && K > 0)
-      producer_run(a.stream + ci.stream_off, ci.stream_bytes, 2, issued0, sm.ring, sm.full, sm.empty, a.err,
-                   a.timeout_ns);
+      producer_run(ss, 2, issued0, sm.ring, sm.full, sm.empty, a.err, a.timeout_ns);
     return;
   }
   if (w >= kGatherWarp0 && w < kSyncWarp) {
@@ -593,7 +610,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   }
   __threadfence();
   grid_sync(a.gbar, kGridP, a.err, a.timeout_ns, sm);
-  if (threadIdx.x == 0) mbar_arrive(sm.xready);  // p complete grid-wide: pass 0 may be gathered
+  if (threadIdx.x == 0) signal_xready(sm, 0);  // p complete grid-wide: pass 0 may be gathered
   stamp(1);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.state->iter = iter + 1;
@@ -639,7 +656,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   });
   __threadfence();
   grid_sync(a.gbar, kGridT, a.err, a.timeout_ns, sm);
-  if (threadIdx.x == 0) mbar_arrive(sm.xready);  // t complete grid-wide: pass 1 may be gathered
+  if (threadIdx.x == 0) signal_xready(sm, 1);  // t complete grid-wide: pass 1 may be gathered
   stamp(4);
 
   // ---- S4: At = H t;  At . t,  At . At
