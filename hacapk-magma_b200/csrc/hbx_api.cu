@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <new>
 #include <string>
@@ -28,6 +29,22 @@ int fail(int status, const std::string &msg) {
 int cuda_fail(cudaError_t e, const char *what) {
   return fail(e == cudaErrorMemoryAllocation ? HBX_ERR_NOMEM : HBX_ERR_CUDA,
               std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Every device allocation of the library goes through dev_malloc.  A test
+// hook (hbx_debug_fail_alloc) can make the n-th one from now fail as
+// cudaMalloc does when the device is out of memory, so the error paths that
+// release a half-built engine run without exhausting a real GPU.
+std::atomic<int> g_fail_alloc{-1};
+cudaError_t dev_malloc(void *p, size_t bytes) {
+  int n = g_fail_alloc.load();
+  while (n >= 0) {
+    if (g_fail_alloc.compare_exchange_weak(n, n - 1)) {
+      if (n == 0) return cudaErrorMemoryAllocation;
+      break;
+    }
+  }
+  return cudaMalloc(reinterpret_cast<void **>(p), bytes);
 }
 
 #define HBX_CUDA(call)                               \
@@ -128,6 +145,8 @@ hbx::MatvecArgs matvec_args(hbx_hmat *h, double alpha, const double *x, double b
   a.timeout_ns = h->timeout_ns;
   a.prof = h->d_prof;
   a.keep_frac = h->keep_frac;
+  a.stall = h->stall_next;  // test hook: one launch only
+  h->stall_next = 0;
   return a;
 }
 
@@ -142,23 +161,23 @@ cudaError_t mv_launch(hbx_hmat *h, const hbx::MatvecArgs &a, cudaStream_t s) {
 
 int ensure_host_staging(hbx_hmat *h) {
   const size_t n = (size_t)h->plan.nd;
-  if (!h->d_x) HBX_CUDA(cudaMalloc(&h->d_x, n * sizeof(double)));
-  if (!h->d_y) HBX_CUDA(cudaMalloc(&h->d_y, n * sizeof(double)));
+  if (!h->d_x) HBX_CUDA(dev_malloc(&h->d_x, n * sizeof(double)));
+  if (!h->d_y) HBX_CUDA(dev_malloc(&h->d_y, n * sizeof(double)));
   if (!h->h_pin) HBX_CUDA(cudaHostAlloc(&h->h_pin, 2 * n * sizeof(double), cudaHostAllocDefault));
   return HBX_OK;
 }
 
 int ensure_solver(hbx_hmat *h, int max_iter) {
   const size_t n = (size_t)h->plan.nd;
-  if (!h->d_work) HBX_CUDA(cudaMalloc(&h->d_work, 8 * n * sizeof(double)));
-  if (!h->d_part) HBX_CUDA(cudaMalloc(&h->d_part, (size_t)h->num_ctas * hbx::kSlots * 2 * sizeof(double)));
-  if (!h->d_dot) HBX_CUDA(cudaMalloc(&h->d_dot, 4 * sizeof(double)));
-  if (!h->d_state) HBX_CUDA(cudaMalloc(&h->d_state, sizeof(hbx::BicgState)));
+  if (!h->d_work) HBX_CUDA(dev_malloc(&h->d_work, 8 * n * sizeof(double)));
+  if (!h->d_part) HBX_CUDA(dev_malloc(&h->d_part, (size_t)h->num_ctas * hbx::kSlots * 2 * sizeof(double)));
+  if (!h->d_dot) HBX_CUDA(dev_malloc(&h->d_dot, 4 * sizeof(double)));
+  if (!h->d_state) HBX_CUDA(dev_malloc(&h->d_state, sizeof(hbx::BicgState)));
   if (!h->h_state) HBX_CUDA(cudaHostAlloc(&h->h_state, sizeof(hbx::BicgState), cudaHostAllocDefault));
   if (h->hist_cap < max_iter + 1) {
     cudaFree(h->d_hist);
     h->d_hist = nullptr;
-    HBX_CUDA(cudaMalloc(&h->d_hist, (size_t)(max_iter + 1) * sizeof(double)));
+    HBX_CUDA(dev_malloc(&h->d_hist, (size_t)(max_iter + 1) * sizeof(double)));
     h->hist_cap = max_iter + 1;
   }
   return HBX_OK;
@@ -211,8 +230,8 @@ int hbx_create_batch(const stc_HACApK_leafmtxp *const *st, const int *nd, int co
   for (int k = 0; k < count; ++k)
     for (int i = cl.off[k]; i < cl.off[k + 1]; ++i) rinst[i] = k;
   cudaError_t e;
-  if ((e = cudaMalloc(&h->d_inst_off, (count + 1) * sizeof(int))) != cudaSuccess ||
-      (e = cudaMalloc(&h->d_rinst, rinst.size() * sizeof(int))) != cudaSuccess ||
+  if ((e = dev_malloc(&h->d_inst_off, (count + 1) * sizeof(int))) != cudaSuccess ||
+      (e = dev_malloc(&h->d_rinst, rinst.size() * sizeof(int))) != cudaSuccess ||
       (e = cudaMemcpy(h->d_inst_off, cl.off.data(), (count + 1) * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess ||
       (e = cudaMemcpy(h->d_rinst, rinst.data(), rinst.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess) {
     free_engine(h);
@@ -265,7 +284,7 @@ static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_option
   if (tmo) h->timeout_ns = (unsigned long long)(std::atof(tmo) * 1e6);
   const char *prof = std::getenv("HBX_PROFILE");
   if (prof && std::atoi(prof) > 0) {
-    if ((e = cudaMalloc(&h->d_prof, (size_t)nc * 16 * sizeof(unsigned long long))) != cudaSuccess)
+    if ((e = dev_malloc(&h->d_prof, (size_t)nc * 16 * sizeof(unsigned long long))) != cudaSuccess)
       return bail(cuda_fail(e, "cudaMalloc(prof)"));
     cudaMemset(h->d_prof, 0, (size_t)nc * 16 * sizeof(unsigned long long));
   }
@@ -309,26 +328,26 @@ static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_option
   cudaEventCreate(&h->ev2);
   cudaEventCreate(&h->ev3);
   cudaEventCreate(&h->ev4);
-  if ((e = cudaMalloc(&h->d_stream, P.total_bytes)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(stream)"));
-  if ((e = cudaMalloc(&h->d_recs, std::max<size_t>(1, P.recs.size()) * sizeof(hbx::RunRec))) != cudaSuccess)
+  if ((e = dev_malloc(&h->d_stream, P.total_bytes)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(stream)"));
+  if ((e = dev_malloc(&h->d_recs, std::max<size_t>(1, P.recs.size()) * sizeof(hbx::RunRec))) != cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(run records)"));
-  if ((e = cudaMalloc(&h->d_ctas, P.ctas.size() * sizeof(hbx::CtaInfo))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(ctas)"));
-  if ((e = cudaMalloc(&h->d_lite, std::max<size_t>(1, P.lite.size()) * sizeof(hbx::RunLite))) != cudaSuccess)
+  if ((e = dev_malloc(&h->d_ctas, P.ctas.size() * sizeof(hbx::CtaInfo))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(ctas)"));
+  if ((e = dev_malloc(&h->d_lite, std::max<size_t>(1, P.lite.size()) * sizeof(hbx::RunLite))) != cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(lite)"));
-  if ((e = cudaMalloc(&h->d_atoms, std::max<size_t>(1, P.atoms.size()) * sizeof(hbx::Atom))) != cudaSuccess)
+  if ((e = dev_malloc(&h->d_atoms, std::max<size_t>(1, P.atoms.size()) * sizeof(hbx::Atom))) != cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(atoms)"));
   // zbu twice: the two H-matvecs of a BiCGSTAB step write separate copies
-  if ((e = cudaMalloc(&h->d_zbu, 2 * std::max<uint64_t>(1, P.zbu_len) * sizeof(double))) != cudaSuccess)
+  if ((e = dev_malloc(&h->d_zbu, 2 * std::max<uint64_t>(1, P.zbu_len) * sizeof(double))) != cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(zbu)"));
   if (P.precision != hbx::kFP64 &&
-      (e = cudaMalloc(&h->d_f32, (3 * (size_t)nd + 2 * std::max<uint64_t>(1, P.zbu_len)) * sizeof(float))) !=
+      (e = dev_malloc(&h->d_f32, (3 * (size_t)nd + 2 * std::max<uint64_t>(1, P.zbu_len)) * sizeof(float))) !=
           cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(float copies)"));
   if (nrhs > 1 &&
-      (e = cudaMalloc(&h->d_zbum, std::max<uint64_t>(1, P.zbu_len) * hbx::kNrhs * sizeof(float))) != cudaSuccess)
+      (e = dev_malloc(&h->d_zbum, std::max<uint64_t>(1, P.zbu_len) * hbx::kNrhs * sizeof(float))) != cudaSuccess)
     return bail(cuda_fail(e, "cudaMalloc(multi-RHS zbu)"));
-  if ((e = cudaMalloc(&h->d_gbar, 4 * sizeof(unsigned))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(gbar)"));
-  if ((e = cudaMalloc(&h->d_err, sizeof(int))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(err)"));
+  if ((e = dev_malloc(&h->d_gbar, 4 * sizeof(unsigned))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(gbar)"));
+  if ((e = dev_malloc(&h->d_err, sizeof(int))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(err)"));
   if ((e = cudaMemcpy(h->d_stream, host.data(), P.total_bytes, cudaMemcpyHostToDevice)) != cudaSuccess)
     return bail(cuda_fail(e, "upload stream"));
   if (!P.recs.empty() &&
@@ -359,6 +378,17 @@ static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_option
   h->plan.pieces.shrink_to_fit();
   h->setup_seconds = now_s() - t0;
   *out = h;
+  return HBX_OK;
+}
+
+int hbx_debug_stall_next_barrier(hbx_hmat *h) {
+  if (!h) return fail(HBX_ERR_INVALID, "hbx_debug_stall_next_barrier: NULL handle");
+  h->stall_next = 1;
+  return HBX_OK;
+}
+
+int hbx_debug_fail_alloc(int n) {
+  g_fail_alloc.store(n < 0 ? -1 : n);
   return HBX_OK;
 }
 
@@ -422,8 +452,8 @@ int hbx_autotune(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *base,
   const size_t nx = (size_t)nrows * (multi ? hbx::kNrhs : 1);
   void *x = nullptr;
   double *y = nullptr;
-  HBX_CUDA(cudaMalloc(&x, nx * sizeof(double)));
-  if (cudaMalloc(&y, nx * sizeof(double)) != cudaSuccess) {
+  HBX_CUDA(dev_malloc(&x, nx * sizeof(double)));
+  if (dev_malloc(&y, nx * sizeof(double)) != cudaSuccess) {
     cudaFree(x);
     return fail(HBX_ERR_NOMEM, "hbx_autotune: vectors");
   }
@@ -792,7 +822,7 @@ static int refined_dev(hbx_hmat *h, hbx_hmat *hl, const double *b, double *u, co
   int st = ensure_solver(hl, max_iter);
   if (st != HBX_OK) return st;
   const size_t n = (size_t)h->plan.nd;
-  if (!hl->d_refine) HBX_CUDA(cudaMalloc(&hl->d_refine, 2 * n * sizeof(double)));
+  if (!hl->d_refine) HBX_CUDA(dev_malloc(&hl->d_refine, 2 * n * sizeof(double)));
   double *r = hl->d_refine, *d = hl->d_refine + n;
   cudaStream_t s = hl->stream;
   const hbx::BicgArgs a = bicg_args(hl, b, u, tol, max_iter);
@@ -969,13 +999,13 @@ struct MrPinned {
 // completes the set instead of running on a null pointer.
 int ensure_mr_workspace(hbx_hmat *hm) {
   const size_t n = (size_t)hm->plan.nd * hbx::kNrhs;
-  if (!hm->d_mrv) HBX_CUDA(cudaMalloc(&hm->d_mrv, 10 * n * sizeof(double)));
-  if (!hm->d_mr32) HBX_CUDA(cudaMalloc(&hm->d_mr32, n * sizeof(float)));
+  if (!hm->d_mrv) HBX_CUDA(dev_malloc(&hm->d_mrv, 10 * n * sizeof(double)));
+  if (!hm->d_mr32) HBX_CUDA(dev_malloc(&hm->d_mr32, n * sizeof(float)));
   if (!hm->d_mrpart)
-    HBX_CUDA(cudaMalloc(&hm->d_mrpart, (size_t)hbx::mr_row_blocks(hm->plan.nd) * 2 * hbx::kNrhs * sizeof(double)));
-  if (!hm->d_mrsc) HBX_CUDA(cudaMalloc(&hm->d_mrsc, hbx::kNrhs * sizeof(hbx::MrScal)));
-  if (!hm->d_mrint) HBX_CUDA(cudaMalloc(&hm->d_mrint, (1 + hbx::kNrhs) * sizeof(int)));
-  if (!hm->d_mrdbl) HBX_CUDA(cudaMalloc(&hm->d_mrdbl, 2 * hbx::kNrhs * sizeof(double)));
+    HBX_CUDA(dev_malloc(&hm->d_mrpart, (size_t)hbx::mr_row_blocks(hm->plan.nd) * 2 * hbx::kNrhs * sizeof(double)));
+  if (!hm->d_mrsc) HBX_CUDA(dev_malloc(&hm->d_mrsc, hbx::kNrhs * sizeof(hbx::MrScal)));
+  if (!hm->d_mrint) HBX_CUDA(dev_malloc(&hm->d_mrint, (1 + hbx::kNrhs) * sizeof(int)));
+  if (!hm->d_mrdbl) HBX_CUDA(dev_malloc(&hm->d_mrdbl, 2 * hbx::kNrhs * sizeof(double)));
   if (!hm->h_mrpin) HBX_CUDA(cudaMallocHost(&hm->h_mrpin, sizeof(MrPinned)));
   return HBX_OK;
 }
@@ -1142,7 +1172,7 @@ int hbx_bicgstab_multi_host(hbx_hmat *h, hbx_hmat *hm, const double *B, double *
   if (st != HBX_OK) return st;
   const size_t bytes = (size_t)hm->plan.nd * hbx::kNrhs * sizeof(double);
   double *dB = nullptr, *dU = nullptr;
-  HBX_CUDA(cudaMalloc(&dB, 2 * bytes));
+  HBX_CUDA(dev_malloc(&dB, 2 * bytes));
   dU = dB + (size_t)hm->plan.nd * hbx::kNrhs;
   cudaStream_t s = hm->stream;
   cudaError_t e = cudaMemcpyAsync(dB, B, bytes, cudaMemcpyHostToDevice, s);
@@ -1172,16 +1202,16 @@ int ensure_bt_workspace(hbx_hmat *h, int count) {
   const size_t n = (size_t)h->plan.nd;
   if (h->inst_off.empty()) {
     const int off[2] = {0, h->plan.nd};
-    if (!h->d_inst_off) HBX_CUDA(cudaMalloc(&h->d_inst_off, 2 * sizeof(int)));
-    if (!h->d_rinst) HBX_CUDA(cudaMalloc(&h->d_rinst, n * sizeof(int)));
+    if (!h->d_inst_off) HBX_CUDA(dev_malloc(&h->d_inst_off, 2 * sizeof(int)));
+    if (!h->d_rinst) HBX_CUDA(dev_malloc(&h->d_rinst, n * sizeof(int)));
     HBX_CUDA(cudaMemcpy(h->d_inst_off, off, 2 * sizeof(int), cudaMemcpyHostToDevice));
     HBX_CUDA(cudaMemset(h->d_rinst, 0, n * sizeof(int)));
     h->inst_off.assign(off, off + 2);
   }
-  if (!h->d_btv) HBX_CUDA(cudaMalloc(&h->d_btv, 6 * n * sizeof(double)));
-  if (!h->d_btsc) HBX_CUDA(cudaMalloc(&h->d_btsc, count * sizeof(hbx::MrScal)));
-  if (!h->d_btdbl) HBX_CUDA(cudaMalloc(&h->d_btdbl, 5 * (size_t)count * sizeof(double)));
-  if (!h->d_btany) HBX_CUDA(cudaMalloc(&h->d_btany, sizeof(int)));
+  if (!h->d_btv) HBX_CUDA(dev_malloc(&h->d_btv, 6 * n * sizeof(double)));
+  if (!h->d_btsc) HBX_CUDA(dev_malloc(&h->d_btsc, count * sizeof(hbx::MrScal)));
+  if (!h->d_btdbl) HBX_CUDA(dev_malloc(&h->d_btdbl, 5 * (size_t)count * sizeof(double)));
+  if (!h->d_btany) HBX_CUDA(dev_malloc(&h->d_btany, sizeof(int)));
   return HBX_OK;
 }
 
@@ -1267,7 +1297,7 @@ int hbx_bicgstab_batch_host(hbx_hmat *h, const double *b, double *u, const hbx_s
   if (!h || !b || !u) return fail(HBX_ERR_INVALID, "hbx_bicgstab_batch_host: NULL argument");
   const size_t bytes = (size_t)h->plan.nd * sizeof(double);
   double *d = nullptr;
-  HBX_CUDA(cudaMalloc(&d, 2 * bytes));
+  HBX_CUDA(dev_malloc(&d, 2 * bytes));
   cudaStream_t s = h->stream;
   cudaError_t e = cudaMemcpyAsync(d, b, bytes, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d + h->plan.nd, u, bytes, cudaMemcpyHostToDevice, s);
@@ -1365,6 +1395,15 @@ void c_hacapk_bicgstab_cax_lfmtx_flat_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HAC
   if (!h) {
     if (lrtrn) *lrtrn = HBX_ERR_CUDA;
     return;
+  }
+  for (int i = 0; i < *nd; ++i) {
+    if (!std::isfinite(b[i]) || !std::isfinite(u[i])) {
+      std::fprintf(stderr, "!!!! hacapk_b200: c_hacapk_bicgstab_cax_lfmtx_flat_: NaN or Inf in b or u (entry %d)\n", i);
+      if (lrtrn) *lrtrn = HBX_ERR_NONFINITE;
+      if (nstp) *nstp = 0;
+      if (own) release_for(st_leafmtxp);
+      return;
+    }
   }
   int status = HBX_OK;
   auto gpu_mv = [](void *ctx, const double *x, double *y) -> int {

@@ -113,7 +113,10 @@ __global__ void k_bt_t(size_t n, const int *rinst, const MrScal *s, const double
   }
 }
 
-// zeta = (At . t) / (At . At)
+// zeta = (At . t) / (At . At).  At . At == 0 means At = 0: zeta = 0 keeps
+// the step's BiCG half (u += alpha p, r = t); the stop test that follows
+// (k_bt_beta) then ends the instance as converged when that r is below the
+// tolerance and as a breakdown otherwise, before any further step.
 __global__ void k_bt_zeta(int count, const double *dots, MrScal *s) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= count || !s[k].active) return;

@@ -49,6 +49,8 @@ struct MatvecArgs {
   unsigned long long timeout_ns;
   unsigned long long *prof;  // optional: per-CTA %globaltimer stamps [num_ctas][16], slots 0-5
   uint32_t keep_frac;        // fraction (of 2^16) of each CTA's stream kept in L2 between passes; 0: no hints
+  uint32_t stall;            // test hook: the launch's grid barrier waits for one instance more than can
+                             // complete, so its bounded waits expire (hbx_debug_stall_next_barrier)
 };
 
 struct BicgArgs {
@@ -198,6 +200,7 @@ struct hbx_hmat {
   int *d_err = nullptr;
   unsigned long long timeout_ns = 2000000000ull;
   uint32_t keep_frac = 0;  // fraction (of 2^16) of every CTA's stream kept in L2 between passes
+  uint32_t stall_next = 0; // test hook: the next k_matvec launch's grid barrier cannot complete
   unsigned long long *d_prof = nullptr;  // phase stamps of the last matvec (HBX_PROFILE=1)
   double setup_seconds = 0.0;
   cudaStream_t stream = nullptr;  // used by the host-vector calls

@@ -5,6 +5,8 @@
 // of `mv`.  Host-only, so the loop can be checked without a GPU.
 #include "hbx_flat.h"
 
+#include "../../include/hacapk_b200.h"
+
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -45,6 +47,10 @@ int flat_bicgstab(int n, double *u, const double *b, double eps, int mstep, int 
     znorm = dot(zshdw.data(), zr.data());
     zden = dot(zshdw.data(), zakp.data());
     alpha = -znorm / zden;
+    if (!std::isfinite(alpha)) {  // r^.Ap zero (HACApK_SOLVER.c:349 divides unchecked): stop, u kept
+      if (status && *status == 0) *status = HBX_ERR_BREAKDOWN;
+      break;
+    }
     znormold = znorm;
     for (int i = 0; i < n; ++i) zt[i] = zr[i] + alpha * zakp[i];
     alpha = -alpha;
@@ -53,6 +59,10 @@ int flat_bicgstab(int n, double *u, const double *b, double eps, int mstep, int 
     znorm = dot(zakt.data(), zt.data());
     zden = dot(zakt.data(), zakt.data());
     zeta = znorm / zden;
+    if (!std::isfinite(zeta)) {  // At.At zero (HACApK_SOLVER.c:366): stop, u kept
+      if (status && *status == 0) *status = HBX_ERR_BREAKDOWN;
+      break;
+    }
     for (int i = 0; i < n; ++i) u[i] = u[i] + alpha * zkp[i];
     for (int i = 0; i < n; ++i) u[i] = u[i] + zeta * zkt[i];
     zeta = -zeta;

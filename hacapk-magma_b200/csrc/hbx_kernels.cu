@@ -101,14 +101,16 @@ __device__ __forceinline__ void init_cta(const Smem &s, const RunLite *lite, uin
 // (pdone), arrive on the grid barrier, wait for it and release the U runs
 // (gdone).  The barrier latency stays off the consumer and gather warps.
 // Pass p uses grid-barrier instance k0 + p * kstep of the launch.
+// `beyond` > 0 (a test hook) waits for an instance that no launch of this
+// grid completes, so the bounded waits of the whole CTA expire.
 __device__ __forceinline__ void sync_warp(unsigned *gbar, uint32_t npass, uint32_t k0, uint32_t kstep, const Smem &sm,
-                                          int *err, uint64_t tmo) {
+                                          int *err, uint64_t tmo, uint32_t beyond = 0) {
   for (uint32_t p = 0; p < npass; ++p) {
     if (!mbar_wait(sm.pdone, p & 1, tmo)) {
       atomicOr(err, kErrPipeline);
       return;  // the waits on gdone are bounded too
     }
-    const unsigned target = grid_target(sm.rsum[1], k0 + p * kstep, gridDim.x);
+    const unsigned target = grid_target(sm.rsum[1], k0 + p * kstep + beyond, gridDim.x);
     grid_arrive(gbar, target);  // fences first: the CTA's zbu stores are visible grid-wide
     if (!grid_wait(gbar, target, tmo)) {
       atomicOr(err, kErrGridBarrier);
@@ -314,7 +316,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
     return;
   }
   if (w == kSyncWarp) {
-    if (lane == 0) sync_warp(a.gbar, 1, 0, 0, sm, a.err, a.timeout_ns);
+    if (lane == 0) sync_warp(a.gbar, 1, 0, 0, sm, a.err, a.timeout_ns, a.stall ? 1u : 0u);
     return;
   }
   const PassOut o{a.alpha, a.beta, a.yin, a.y, a.zbu, kF32 ? a.zbu32 : nullptr, 0, ci.nblk_p};
@@ -519,6 +521,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
     double beta = 0.0;
     if (!done) {
       if (st.breakdown) { done = 1; status = HBX_ERR_BREAKDOWN; }
+      // NaN or Inf in b or x0 shows in b.b or r.r before the first step
+      else if (!isfinite(bb) || !isfinite(rr)) { done = 1; status = st.iter == 0 ? HBX_ERR_NONFINITE : HBX_ERR_BREAKDOWN; }
       else if (relres < a.tol) { done = 1; status = HBX_OK; }
       else if (!isfinite(relres)) { done = 1; status = HBX_ERR_BREAKDOWN; }
       else if (st.iter >= a.max_iter) { done = 1; status = HBX_ERR_NOT_CONVERGED; }
@@ -702,6 +706,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   stamp(6);
 
   // ---- S5: u += alpha*p + zeta*t;  r = t - zeta*At;  rh . r,  r . r
+  // A breakdown (alpha or zeta not finite: r^.Ap or At.At zero or
+  // overflowing, which HACApK_SOLVER.c:650, :694 divide by unchecked) keeps
+  // u and r of the previous step; the next launch ends the solve with
+  // HBX_ERR_BREAKDOWN.
+  if (!isfinite(alpha) || !isfinite(zeta)) {
+    stamp(7);
+    return;
+  }
   {
     Acc2 acc[2] = {{0, 0}, {0, 0}};
     if (own0) {

@@ -138,6 +138,8 @@ ENGINE_SYMBOLS = [
     ("hbx_gradient_host", C.c_int, [_VP, _VP, _DP, _DP, _DP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo),
                                     C.POINTER(SolveInfo)]),
     ("hbx_debug_phase_stamps", C.c_int, [_VP, C.POINTER(C.c_ulonglong), C.c_int]),
+    ("hbx_debug_stall_next_barrier", C.c_int, [_VP]),
+    ("hbx_debug_fail_alloc", C.c_int, [C.c_int]),
     ("hbx_status_string", C.c_char_p, [C.c_int]),
     ("hbx_last_error", C.c_char_p, []),
     ("magma_init_", None, []),

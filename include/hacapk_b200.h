@@ -342,6 +342,18 @@ int hbx_bicgstab_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_o
  * copies up to cap values into out, returns how many. */
 int hbx_debug_phase_stamps(hbx_hmat *h, unsigned long long *out, int cap);
 
+/* Test hooks of the failure paths (no counterpart in the reference).
+ * hbx_debug_stall_next_barrier: the engine's next hbx_matvec launch waits on
+ * a grid-barrier instance that cannot complete, so its bounded device waits
+ * expire after the engine's timeout (HBX_TIMEOUT_MS at create, 2 s by
+ * default) and the launch ends; hbx_sync then reports HBX_ERR_TIMEOUT and
+ * resets the barrier words, and the engine works again.
+ * hbx_debug_fail_alloc(n): the n-th device allocation made by this library
+ * from now on (n = 0: the next one) fails as cudaMalloc does on a full
+ * device; n < 0 turns the hook off. */
+int hbx_debug_stall_next_barrier(hbx_hmat *h);
+int hbx_debug_fail_alloc(int n);
+
 const char *hbx_status_string(int status);
 /* Message of the last failing hbx_* call on this host thread. */
 const char *hbx_last_error(void);

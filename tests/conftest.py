@@ -8,7 +8,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "hacapk-magma_b200"))
 sys.path.insert(0, ROOT)
 
-REFERENCE = "/root/reference"
+# The reference tree (read only by the CPU tests that pin the oracle against
+# it; absent where the GPU tests run): REFERENCE_DIR, else "reference" beside
+# the repository.
+REFERENCE = os.environ.get("REFERENCE_DIR", os.path.join(os.path.dirname(ROOT), "reference"))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def pytest_configure(config):
@@ -43,3 +47,94 @@ def gpu():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     return torch.device("cuda:0")
+
+
+_libs = {}
+
+
+def emu_lib():
+    """The test-only interpreter of the packed layout (tests/emu/plan_emu.cpp,
+    linked with the product's planner), built once per session."""
+    import ctypes as C
+    import subprocess
+    if "emu" not in _libs:
+        src = os.path.join(ROOT, "tests", "emu", "plan_emu.cpp")
+        lib = os.path.join(ROOT, "tests", "emu", "_build", "libplanemu.so")
+        os.makedirs(os.path.dirname(lib), exist_ok=True)
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", lib, src,
+                        os.path.join(ROOT, "hacapk-magma_b200", "csrc", "hbx_plan.cpp")], check=True)
+        L = C.CDLL(lib)
+        DP = C.POINTER(C.c_double)
+        L.emu_matvec_kernel_order.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, DP, C.c_double, DP, DP]
+        _libs["emu"] = L
+    return _libs["emu"]
+
+
+FLAT_MV = None
+
+
+def flat_lib():
+    """The flat solver's host loop (hbx_flat.cpp) compiled alone, callable
+    with any product (hbx_test_flat_bicgstab)."""
+    import ctypes as C
+    import subprocess
+    global FLAT_MV
+    if "flat" not in _libs:
+        src = os.path.join(ROOT, "hacapk-magma_b200", "csrc", "hbx_flat.cpp")
+        lib = os.path.join(ROOT, "tests", "emu", "_build", "libflat.so")
+        os.makedirs(os.path.dirname(lib), exist_ok=True)
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-o", lib, src],
+                       check=True)
+        L = C.CDLL(lib)
+        DP = C.POINTER(C.c_double)
+        FLAT_MV = C.CFUNCTYPE(C.c_int, C.c_void_p, DP, DP)
+        L.hbx_test_flat_bicgstab.argtypes = [C.c_int, DP, DP, C.c_double, C.c_int, FLAT_MV, C.c_void_p]
+        _libs["flat"] = L
+    return _libs["flat"]
+
+
+def kernel_order_matvec(H, num_ctas=148):
+    """y = H x in the FP64 kernel's own operation order (bit for bit what
+    k_matvec computes on num_ctas CTAs), on the CPU."""
+    import ctypes as C
+    import numpy as np
+    L = emu_lib()
+    DP = C.POINTER(C.c_double)
+
+    def mv(x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros_like(x)
+        assert L.emu_matvec_kernel_order(C.cast(H.st, C.c_void_p), H.nd, num_ctas, 1.0, x.ctypes.data_as(DP), 0.0,
+                                         None, y.ctypes.data_as(DP)) == 0
+        return y
+    return mv
+
+
+def flat_solve(H, b, mv, tol=1e-8, max_iter=1000):
+    """The flat solver's host loop driven by the product mv(x) -> H x;
+    returns (u, steps)."""
+    import ctypes as C
+    import numpy as np
+    L = flat_lib()
+    n = H.nd
+    DP = C.POINTER(C.c_double)
+
+    def cb(ctx, x, y):
+        xa = np.ctypeslib.as_array(x, shape=(n,)).copy()
+        np.ctypeslib.as_array(y, shape=(n,))[:] = mv(xa)
+        return 0
+
+    fn = FLAT_MV(cb)
+    u = np.zeros(n)
+    b = np.ascontiguousarray(b, np.float64)
+    steps = L.hbx_test_flat_bicgstab(n, u.ctypes.data_as(DP), b.ctypes.data_as(DP), tol, max_iter, fn, None)
+    return u, steps
+
+
+def reference_input_mesh():
+    """The reference's own input bem-bb_inputs/input_10ts.pbs (10,400
+    triangles) from its committed fixture (tests/golden/make_golden.py)."""
+    import numpy as np
+    from hacapk_b200 import hmatrix
+    z = np.load(os.path.join(GOLDEN, "input_10ts_mesh.npz"))
+    return hmatrix.Mesh(np.ascontiguousarray(z["xyz"]), np.ascontiguousarray(z["faces"]), None)

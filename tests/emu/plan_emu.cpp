@@ -300,3 +300,87 @@ extern "C" int emu_plan_cta_sections(const stc_HACApK_leafmtxp *st, int nd, int 
   }
   return 0;
 }
+
+// y = alpha H x + beta yin in the FP64 kernel's own operation order, so that
+// it equals k_matvec bit for bit: consumer warp w takes panels
+// j = (w - rot) mod 16, j + 16, ... of every run, four at a time (two for P
+// slabs taller than 32 rows, whose lanes also carry row lane + 32) into
+// accumulator pairs (one fma per column), folds them into its block sum at
+// the end of the run (a0 + a1, accumulators in order), and the block-sum
+// warp adds the 16 warps' sums in warp order; P blocks write zbu, D blocks
+// y = alpha s (+ beta yin), U blocks y = fma(alpha, s, y).
+extern "C" int emu_matvec_kernel_order(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, double alpha,
+                                       const double *x, double beta, const double *yin, double *y) {
+  Plan plan;
+  std::string err;
+  if (make_plan(st, nd, num_ctas, plan, err, kFP64, false, PlanCosts(), -1) != 0) return 1;
+  std::vector<uint8_t> buf(plan.total_bytes, 0);
+  pack_plan(st, plan, buf.data());
+  std::vector<double> zbu(plan.zbu_len, 0.0), stage(kStageBytes / 8);
+  constexpr int NW = kConsumerWarps;
+  std::vector<double> t0(NW * 32), t1(NW * 32);
+  auto do_pass = [&](int phase) {  // phase 0: P runs; 1: D then U runs
+    for (int c = 0; c < plan.num_ctas; ++c) {
+      const CtaInfo &ci = plan.ctas[c];
+      const uint32_t k0 = phase == 0 ? 0 : ci.nr_p, k1 = phase == 0 ? ci.nr_p : ci.nr_p + ci.nr_d + ci.nr_u;
+      std::fill(t0.begin(), t0.end(), 0.0);
+      std::fill(t1.begin(), t1.end(), 0.0);
+      for (uint32_t k = k0; k < k1; ++k) {
+        const RunRec &R = plan.recs[ci.rec_begin + k];
+        const Run &r = R.hdr;
+        const bool is_u = k >= ci.nr_p + ci.nr_d;
+        const double *vec = is_u ? zbu.data() : x;
+        for (uint32_t q = 0; q < r.nseg; ++q)
+          for (uint32_t e = 0; e < R.seg[q].len; ++e) stage[R.seg[q].dst + e] = vec[R.seg[q].src + e];
+        for (uint32_t e = r.vlen; e < 2u * r.npanel; ++e) stage[e] = 0.0;
+        const double *d = reinterpret_cast<const double *>(buf.data() + ci.stream_off + r.pos);
+        const uint32_t h = r.nrow, np = r.npanel;
+        const bool two = h > 32;
+        const uint32_t U = two ? 2 : 4;
+        for (int w = 0; w < NW; ++w)
+          for (uint32_t lane = 0; lane < 32; ++lane) {
+            const uint32_t ra = std::min(lane, h - 1), rb = std::min(lane + 32, h - 1);
+            double a0[4] = {0, 0, 0, 0}, a1[4] = {0, 0, 0, 0}, b0[4] = {0, 0, 0, 0}, b1[4] = {0, 0, 0, 0};
+            auto panel = [&](uint32_t j, uint32_t u) {
+              const double vx = stage[2 * j], vy = stage[2 * j + 1];
+              const double *ma = d + ((size_t)j * h + ra) * 2, *mb = d + ((size_t)j * h + rb) * 2;
+              a0[u] = std::fma(ma[0], vx, a0[u]);
+              a1[u] = std::fma(ma[1], vy, a1[u]);
+              if (two) {
+                b0[u] = std::fma(mb[0], vx, b0[u]);
+                b1[u] = std::fma(mb[1], vy, b1[u]);
+              }
+            };
+            uint32_t j = (w + NW - r.rot % NW) % NW;
+            for (; j + (U - 1) * NW < np; j += U * NW)
+              for (uint32_t u = 0; u < U; ++u) panel(j + u * NW, u);
+            for (; j < np; j += NW) panel(j, 0);
+            for (uint32_t u = 0; u < U; ++u) t0[w * 32 + lane] += a0[u] + a1[u];
+            if (two)
+              for (uint32_t u = 0; u < U; ++u) t1[w * 32 + lane] += b0[u] + b1[u];
+          }
+        if (!(r.flags & kLast)) continue;
+        for (uint32_t i = 0; i < h; ++i) {
+          auto part = [&](int w) { return i < 32 ? t0[w * 32 + i] : t1[w * 32 + i - 32]; };
+          double s = part(0);
+          for (int w = 1; w < NW; ++w) s += part(w);
+          const uint32_t row = r.out + i;
+          if (phase == 0) {
+            zbu[row] = s;
+          } else if (!is_u) {
+            double v = alpha * s;
+            if (beta != 0.0) v = std::fma(beta, yin[row], v);
+            y[row] = v;
+          } else {
+            y[row] = std::fma(alpha, s, y[row]);
+          }
+        }
+        std::fill(t0.begin(), t0.end(), 0.0);
+        std::fill(t1.begin(), t1.end(), 0.0);
+      }
+    }
+  };
+  do_pass(0);
+  do_pass(1);
+  return 0;
+}

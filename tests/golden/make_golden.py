@@ -3,7 +3,15 @@ H-matvec (oracle/_ref/libhacapk_ref.so, built from HACApK_MAGMA.c).
 
 Each fixture stores the inputs of one case (mesh recipe + construction
 parameters + a seeded x), a digest of the leaf list the construction produced,
-and y = H x as computed by the reference code.  Run from the repository root:
+and y = H x as computed by the reference code.
+
+It also stores the reference's own mesh input bem-bb_inputs/input_10ts.pbs
+(10,400 flat triangles) as input_10ts_mesh.npz -- the vertices and faces as
+read by hmatrix.read_pbs, and the SHA-256 of the source file -- so that the
+GPU tests, which run where the reference tree is absent, can take the
+reference's inputs through the drop-in entry points.  Run from the repository
+root (REFERENCE_DIR: the reference tree, default ../reference beside the
+repository):
     python tests/golden/make_golden.py
 """
 import hashlib
@@ -49,8 +57,24 @@ def build(case):
     return H, x
 
 
+def reference_dir() -> str:
+    return os.environ.get("REFERENCE_DIR", os.path.join(os.path.dirname(ROOT), "reference"))
+
+
+def save_reference_mesh(out: str):
+    src = os.path.join(reference_dir(), "bem-bb_inputs", "input_10ts.pbs")
+    if not os.path.exists(src):
+        print("reference mesh not found:", src)
+        return
+    m = hmatrix.read_pbs(src)
+    digest = hashlib.sha256(open(src, "rb").read()).hexdigest()
+    np.savez_compressed(os.path.join(out, "input_10ts_mesh.npz"), xyz=m.xyz, faces=m.faces, source_sha256=digest)
+    print("input_10ts_mesh", m.xyz.shape, m.faces.shape, digest)
+
+
 def main():
     out = os.path.dirname(os.path.abspath(__file__))
+    save_reference_mesh(out)
     for case in CASES:
         H, x = build(case)
         y = oracle.matvec_ref(H.st, x)

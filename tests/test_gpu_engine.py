@@ -194,3 +194,22 @@ def test_invalid_inputs_report_status(gpu, build_libs):
     assert lib.hbx_matvec(E._h, 1.0, C.c_void_p(16), 1.0, None, C.c_void_p(16), None) == 1  # beta!=0, no yin
     y, _, _ = E.matvec_host(np.ones(H.nd))  # still usable
     assert np.isfinite(y).all()
+
+
+@pytest.mark.parametrize("level", [3, 4, 5])
+def test_matvec_equals_kernel_order_emulation_bitwise(gpu, build_libs, level):
+    """k_matvec's arithmetic is fully specified: the CPU interpreter that sums
+    in the kernel's order (per-warp fma accumulators over rotated panels,
+    block sums in warp order; tests/emu) reproduces it bit for bit, on the
+    engine's own CTA count."""
+    import torch
+    from conftest import kernel_order_matvec
+    from hacapk_b200 import configs
+    from hacapk_b200.engine import Engine
+    H, _ = configs.c1(level)
+    E = Engine(H.st, H.nd)
+    x = np.random.default_rng(40 + level).standard_normal(H.nd)
+    y, _, _ = E.matvec_host(x)
+    y_emu = kernel_order_matvec(H, E.info["num_ctas"])(x)
+    assert np.array_equal(y, y_emu)
+    E.close()
