@@ -85,6 +85,16 @@ class SolveInfo(C.Structure):
                 ("launches", C.c_int), ("outer", C.c_int), ("reserved", C.c_int * 5)]
 
 
+class FillParams(C.Structure):
+    _fields_ = [("kernel", C.c_int), ("aca_eps", C.c_double), ("aca_abs_factor", C.c_double), ("kmax", C.c_int),
+                ("kmin", C.c_int), ("workspace_mb", C.c_int), ("first_cap", C.c_int), ("reserved", C.c_int * 8)]
+
+
+class FillStats(C.Structure):
+    _fields_ = [("n_lowrank", C.c_int), ("n_dense", C.c_int), ("ktmax", C.c_int), ("words", C.c_longlong),
+                ("retried", C.c_longlong), ("seconds", C.c_double), ("reserved", C.c_int * 6)]
+
+
 class BuildParams(C.Structure):
     _fields_ = [("leaf_size", C.c_int), ("eta", C.c_double), ("aca_eps", C.c_double),
                 ("aca_abs_factor", C.c_double), ("kmax", C.c_int), ("kmin", C.c_int),
@@ -138,6 +148,9 @@ ENGINE_SYMBOLS = [
     ("hbx_gradient_host", C.c_int, [_VP, _VP, _DP, _DP, _DP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo),
                                     C.POINTER(SolveInfo)]),
     ("hbx_debug_phase_stamps", C.c_int, [_VP, C.POINTER(C.c_ulonglong), C.c_int]),
+    ("hbx_fill_leaves", C.c_int, [_DP, C.c_int, _IP, C.c_int, _IP, C.POINTER(FillParams), C.POINTER(LeafMtxP),
+                                  C.POINTER(_VP), C.POINTER(FillStats)]),
+    ("hbx_fill_free", None, [_VP]),
     ("hbx_debug_stall_next_barrier", C.c_int, [_VP]),
     ("hbx_debug_fail_alloc", C.c_int, [C.c_int]),
     ("hbx_status_string", C.c_char_p, [C.c_int]),

@@ -137,9 +137,13 @@ class HostHMatrix:
 
     def __init__(self, mesh: Mesh, leaf_size: int = 15, eta: float = 2.0,
                  aca_eps: float = 1e-6, kernel: int = abi.KERNEL_LAPLACE,
-                 nthreads: int = 0, fill: bool = True):
+                 nthreads: int = 0, fill: bool | str = True):
+        """fill: True fills the leaves on the host (C++ restatement of the
+        reference's fill), "gpu" on the current CUDA device
+        (hbx_fill_leaves), False leaves only the block partition."""
         lib = abi.build_lib()
         self._lib = lib
+        self._fill = None
         self.mesh = mesh
         p = default_params()
         p.leaf_size = leaf_size
@@ -147,7 +151,7 @@ class HostHMatrix:
         p.aca_eps = aca_eps
         p.kernel = kernel
         p.nthreads = nthreads
-        p.fill = 1 if fill else 0
+        p.fill = 1 if fill is True else 0
         self.params = p
         h = C.c_void_p()
         xyz = np.ascontiguousarray(mesh.xyz, np.float64)
@@ -164,8 +168,35 @@ class HostHMatrix:
         s = abi.BuildStats()
         lib.hbx_build_get_stats(h, C.byref(s))
         self.stats = {f: getattr(s, f) for f, _ in abi.BuildStats._fields_ if f != "reserved"}
+        if fill == "gpu":
+            self.fill_stats = self._fill_gpu(xyz, faces)
+
+    def _fill_gpu(self, xyz, faces) -> dict:
+        """The ACA+ / dense fill on the GPU (hbx_fill_leaves) into this
+        partition's leaves; keeps the stats of the host fill in step."""
+        fp = abi.FillParams()
+        p = self.params
+        if p.aca_method != 2:
+            raise ValueError("the GPU fill runs ACA+ (aca_method 2) only")
+        fp.kernel, fp.aca_eps, fp.aca_abs_factor, fp.kmax, fp.kmin = p.kernel, p.aca_eps, p.aca_abs_factor, p.kmax, p.kmin
+        f = C.c_void_p()
+        fs = abi.FillStats()
+        lod = np.ascontiguousarray(self.lod, np.int32)
+        st = abi.engine_lib().hbx_fill_leaves(abi.dptr(xyz), xyz.shape[0], abi.iptr(faces), faces.shape[0],
+                                              abi.iptr(lod), C.byref(fp), self.st, C.byref(f), C.byref(fs))
+        if st != 0:
+            raise RuntimeError(f"hbx_fill_leaves failed: {abi.STATUS.get(st, st)}")
+        self._fill = f
+        d, lr = self.storage_words()
+        self.stats["ktmax"] = fs.ktmax
+        self.stats["mem_words"] = d + lr
+        self.stats["memh_words"] = d + lr + self.nlf
+        return {k: getattr(fs, k) for k, _ in abi.FillStats._fields_ if k != "reserved"}
 
     def close(self):
+        if getattr(self, "_fill", None):
+            abi.engine_lib().hbx_fill_free(self._fill)
+            self._fill = None
         if getattr(self, "_h", None):
             self._lib.hbx_build_free(self._h)
             self._h = None

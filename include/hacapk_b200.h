@@ -342,6 +342,54 @@ int hbx_bicgstab_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_o
  * copies up to cap values into out, returns how many. */
 int hbx_debug_phase_stamps(hbx_hmat *h, unsigned long long *out, int cap);
 
+/* ------------------------------------------------------------------------ */
+/* Leaf fill on the GPU                                                     */
+/* ------------------------------------------------------------------------ */
+
+/* Collocation kernel of the fill: HBX_FILL_KERNEL_PPOHBEM is face_integral of
+ * m_ppohBEM_user_func.f90:49-99 as written (single-precision literals PI and
+ * EPSILON_0 of :42-43, scale 1/(4 PI EPSILON_0)); HBX_FILL_KERNEL_LAPLACE the
+ * same analytic flat-triangle integral of 1/r scaled by 1/(4 pi) in double. */
+enum { HBX_FILL_KERNEL_PPOHBEM = 0, HBX_FILL_KERNEL_LAPLACE = 1 };
+
+typedef struct hbx_fill_params {
+  int kernel;            /* HBX_FILL_KERNEL_*                                    */
+  double aca_eps;        /* param(71): ACA+ relative tolerance                   */
+  double aca_abs_factor; /* param(72): ACA_EPS = aca_abs_factor * aca_eps        */
+  int kmax;              /* param(63): rank limit                                */
+  int kmin;              /* param(64): minimum rank                              */
+  int workspace_mb;      /* device workspace of one batch of leaves (0 = 4096)   */
+  int first_cap;         /* rank columns tried first per leaf (0 = 64); a leaf
+                            that needs more is run again with twice as many     */
+  int reserved[8];
+} hbx_fill_params;
+
+typedef struct hbx_fill_stats {
+  int n_lowrank, n_dense, ktmax;
+  long long words;       /* factor and entry words stored                       */
+  long long retried;     /* leaves run again with more rank columns            */
+  double seconds;
+  int reserved[6];
+} hbx_fill_stats;
+
+typedef struct hbx_fill hbx_fill;
+
+/* Fills the leaves of `st` on the current device, replacing
+ * HACApK_fill_leafmtx (m_HACApK_base.f90:978-1051): every dense leaf
+ * (ltmtx 2) receives its entries, every admissible leaf (ltmtx 1) the
+ * factors of HACApK_acaplus (:783-975, param(61) = 1) and its rank kt, with
+ * the collocation kernel evaluated on the GPU (collocation at the centroid of
+ * face lod(i), integration over face lod(j); xyz: 3 nond doubles, face2node:
+ * 3 nofc 0-based vertex ids, lod: nofc 1-based face ids in cluster order).
+ * On entry the leaves carry ltmtx, nstrtl, ndl, nstrtt, ndt (the block
+ * partition, e.g. from hbx_build with fill = 0); on return kt, a1size, a1 and
+ * a2 are set as the reference lays them out, st->ktmax and st->nlfkt too,
+ * and the factor storage belongs to *out until hbx_fill_free. */
+int hbx_fill_leaves(const double *xyz, int nond, const int *face2node, int nofc, const int *lod,
+                    const hbx_fill_params *params, stc_HACApK_leafmtxp *st, hbx_fill **out,
+                    hbx_fill_stats *stats);
+void hbx_fill_free(hbx_fill *f);
+
 /* Test hooks of the failure paths (no counterpart in the reference).
  * hbx_debug_stall_next_barrier: the engine's next hbx_matvec launch waits on
  * a grid-barrier instance that cannot complete, so its bounded device waits
