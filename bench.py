@@ -240,7 +240,7 @@ def run_ours(args, world, rank, local):
     mv_gbs = info["alg_bytes"] / (mv_us * 1e-6) / 1e9
     # the forms are a single-GPU report (like cpu_baseline): the scaling runs
     # time the FP64 solve only
-    forms = None if (args.no_forms or world > 1) else measure_forms(H, b, E, args, dev, stream, ms / 1e3)
+    forms = None if (args.no_forms or world > 1) else measure_forms(args, dev, stream)
     out = {
         "metric": METRIC,
         "value": ms / 1e3,
@@ -287,159 +287,73 @@ def run_ours(args, world, rank, local):
     return out
 
 
-def measure_forms(H, b, E, args, dev, stream, fp64_solve_s):
-    """The precision and batching forms beside the FP64 solve (same matrix,
-    same tolerance, verified by the FP64 residual): FP32 factors inside FP64
-    refinement, 64 right-hand sides at once on the tensor cores, and a batch
-    of uneven bodies in one block-diagonal engine."""
-    import numpy as np
+def precision_workload(args):
+    """--precision-level L: only the precision form, on C2 at level L."""
     import torch
-    from hacapk_b200 import abi
-    from hacapk_b200.engine import Engine
-    s = stream.cuda_stream
-    n = H.nd
-    reps = 3
+    dev = torch.device("cuda", 0)
+    print(json.dumps(precision_form(args, dev, torch.cuda.current_stream(dev), args.precision_level)), flush=True)
+
+
+def forms_only(args):
+    """--forms-only: only the forms on their configurations (one GPU)."""
+    import torch
+    dev = torch.device("cuda", 0)
+    print(json.dumps(measure_forms(args, dev, torch.cuda.current_stream(dev))), flush=True)
+
+
+def _timed(dev, fn, reps=3):
+    """Best host-clock time of fn() over reps runs after one untimed run, with
+    the device synchronized on both sides; returns (seconds, last result)."""
+    import torch
+    best, res = 1e9, None
+    for _ in range(reps + 1):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        res = fn()
+        torch.cuda.synchronize(dev)
+        best = min(best, time.perf_counter() - t0)
+    return best, res
+
+
+def measure_forms(args, dev, stream):
+    """The forms beside the FP64 drop-in, each on the workload its
+    configuration names, each against the FP64 solve of that same workload
+    and each verified by the FP64 residual ||b - H u||/||b|| (recomputed
+    after the solve):
+
+      precision_c2  C2: FP32 and BF16 factors inside FP64 refinement;
+      mrhs_c3       C3: 64 right-hand sides on the tensor cores, against 64
+                    FP64 solves one after another;
+      adjoint_c4    C4: dJ/dg by the adjoint solve with the transposed
+                    product, checked against central differences in 16
+                    random directions;
+      batch_c5      C5: 256 uneven bodies in one block-diagonal engine,
+                    against the same bodies solved one after another.
+
+    The H-matrices are filled on the GPU (hbx_fill_leaves)."""
     out = {}
-    bd = torch.from_numpy(b).to(dev)
-    ud = torch.zeros(n, dtype=torch.float64, device=dev)
-    # the FP64 solve timed like the forms (host clock around each call, best
-    # of the repetitions), so every speed-up below compares like with like
-    best = 1e9
-    for _ in range(reps + 1):
-        ud.zero_()
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        E.bicgstab_dev(bd.data_ptr(), ud.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
-        torch.cuda.synchronize(dev)
-        best = min(best, time.perf_counter() - t0)
-    fp64_solve_s = best
-    out["fp64_solve_s"] = best
-    # FP32 factors, FP64 refinement, single right-hand side
-    E32 = Engine(H.st, n, precision=abi.HBX_FP32)
-    best, inf = 1e9, None
-    for _ in range(reps + 1):
-        ud.zero_()
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        inf = E.bicgstab_refined_dev(E32, bd.data_ptr(), ud.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
-        torch.cuda.synchronize(dev)
-        best = min(best, time.perf_counter() - t0)
-    out["fp32_refined"] = {"solve_s": best, "true_relres": inf["true_relres"], "inner_iterations": inf["iterations"],
-                           "outer": inf["outer"], "speedup_vs_fp64": fp64_solve_s / best}
-    E32.close()
-    # 64 right-hand sides: the rhs above plus 63 seeded N(0,1) ones
-    Em = Engine(H.st, n, precision=abi.HBX_FP32, nrhs=abi.HBX_NRHS)
-    rng = np.random.default_rng(2)
-    B = rng.standard_normal((n, abi.HBX_NRHS))
-    B[:, 0] = b
-    Bd = torch.from_numpy(B).to(dev)
-    Ud = torch.zeros_like(Bd)
-    best, infos = 1e9, None
-    for _ in range(reps + 1):
-        Ud.zero_()
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        infos = E.bicgstab_multi_dev(Em, Bd.data_ptr(), Ud.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
-        torch.cuda.synchronize(dev)
-        best = min(best, time.perf_counter() - t0)
-    X = torch.randn(n, abi.HBX_NRHS, device=dev).float()
-    Y = torch.zeros(n, abi.HBX_NRHS, dtype=torch.float64, device=dev)
-    for _ in range(3):
-        Em.matmat_dev(X.data_ptr(), Y.data_ptr(), stream=s)
-    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    m0.record(stream)
-    for _ in range(20):
-        Em.matmat_dev(X.data_ptr(), Y.data_ptr(), stream=s)
-    m1.record(stream)
-    torch.cuda.synchronize(dev)
-    Em.sync(s)
-    mm_us = m0.elapsed_time(m1) / 20 * 1e3
-    its = [i["iterations"] for i in infos]
-    out["mrhs64"] = {
-        "rhs": abi.HBX_NRHS, "solve_s": best, "per_rhs_s": best / abi.HBX_NRHS,
-        "speedup_vs_fp64_per_rhs": fp64_solve_s * abi.HBX_NRHS / best,
-        "worst_true_relres": max(i["true_relres"] for i in infos), "converged": sum(i["status"] == 0 for i in infos),
-        "inner_iterations": [min(its), max(its)], "outer": infos[0]["outer"],
-        "matmat_us": mm_us, "matmat_tf32_tflops": abi.HBX_NRHS * Em.info["alg_flops"] / (mm_us * 1e-6) / 1e12,
-        "matmat_per_rhs_gbs": abi.HBX_NRHS * E.info["alg_bytes"] / 2 / (mm_us * 1e-6) / 1e9,
-    }
-    Em.close()
-    # uneven batch: a 64-instance sample of C5 (the config's 256 need a minute of
-    # host construction), solved in one block-diagonal engine and one by one
-    from hacapk_b200 import configs
-    t0 = time.time()
-    inst = configs.c5(count=args.c5_count)
-    t_build = time.time() - t0
-    Eb = Engine.batch([Hk for Hk, _ in inst])
-    bb = torch.from_numpy(np.concatenate([bk for _, bk in inst])).to(dev)
-    ub = torch.zeros_like(bb)
-    best, infos = 1e9, None
-    for _ in range(reps + 1):
-        ub.zero_()
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        infos = Eb.bicgstab_batch_dev(bb.data_ptr(), ub.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
-        torch.cuda.synchronize(dev)
-        best = min(best, time.perf_counter() - t0)
-    stream_gb = Eb.info["stream_bytes"] / 1e9
-    Eb.close()
-    one = 0.0
-    for Hk, bk in inst:
-        Ek = Engine(Hk.st, Hk.nd)
-        bd = torch.from_numpy(bk).to(dev)
-        ud = torch.zeros_like(bd)
-        tk = 1e9
-        for _ in range(2):
-            ud.zero_()
-            torch.cuda.synchronize(dev)
-            t0 = time.perf_counter()
-            Ek.bicgstab_dev(bd.data_ptr(), ud.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
-            torch.cuda.synchronize(dev)
-            tk = min(tk, time.perf_counter() - t0)
-        one += tk
-        Ek.close()
-    its = [i["iterations"] for i in infos]
-    out["batch_c5"] = {
-        "instances": len(inst), "n_total": int(sum(Hk.nd for Hk, _ in inst)), "stream_gb": stream_gb,
-        "solve_s": best, "one_by_one_s": one, "speedup": one / best,
-        "iterations": [min(its), max(its)], "worst_true_relres": max(i["true_relres"] for i in infos),
-        "converged": sum(i["status"] == 0 for i in infos), "host_build_s": t_build,
-    }
+    out["precision_c2"] = precision_form(args, dev, stream)
+    out["mrhs_c3"] = mrhs_form(args, dev, stream)
+    out["adjoint_c4"] = adjoint_form(args, dev, stream)
+    out["batch_c5"] = batch_form(args, dev, stream)
     return out
 
 
-def precision_workload(args):
-    """The precision form on its own workload (C2 at --precision-level: the
-    sphere and the seeded ellipsoid, ACA+ 1e-6), one JSON line: the FP64
-    solve, FP32 factors in FP64 refinement and, when HBX_EXPERIMENTAL_BF16=1,
-    BF16 factors in FP64 refinement (inner tolerance 1e-2); for each, the
-    standalone product's time and stream rate and the solve's time, step
-    counts and FP64 residual.  Solves are timed by the host clock around
-    each call, best of three after one untimed run."""
+def precision_form(args, dev, stream, level=7):
+    """C2 at `level` (7: the configuration): the FP64 solve, FP32 factors in
+    FP64 refinement, BF16 factors in FP64 refinement (inner tolerance 1e-2);
+    each with its product's time and stream rate."""
     import torch
     from hacapk_b200 import abi, configs
     from hacapk_b200.engine import Engine
-    dev = torch.device("cuda", 0)
-    stream = torch.cuda.current_stream(dev)
     s = stream.cuda_stream
     t0 = time.time()
-    H, b = configs.c2(args.precision_level)
+    H, b = configs.c2(level, fill="gpu")
     t_build = time.time() - t0
     n = H.nd
     bd = torch.from_numpy(b).to(dev)
     ud = torch.zeros(n, dtype=torch.float64, device=dev)
     peak, peak_kind = peaks()
-
-    def best_of(fn):
-        best, res = 1e9, None
-        for _ in range(4):
-            ud.zero_()
-            torch.cuda.synchronize(dev)
-            t = time.perf_counter()
-            res = fn()
-            torch.cuda.synchronize(dev)
-            best = min(best, time.perf_counter() - t)
-        return best, res
 
     def product(Ek):
         x = torch.randn(n, dtype=torch.float64, device=dev)
@@ -459,25 +373,174 @@ def precision_workload(args):
                 "frac_of_" + peak_kind + "_peak": Ek.info["stream_bytes"] / (us * 1e-6) / 1e9 / peak}
 
     E = Engine(H.st, n)
-    t64, inf = best_of(lambda: E.bicgstab_dev(bd.data_ptr(), ud.data_ptr(), tol=args.tol, max_iter=args.max_iter,
-                                              stream=s))
-    out = {"workload": f"C2: icosphere L{args.precision_level} + seeded ellipsoid, ACA+ 1e-6", "n": n,
-           "host_build_s": t_build,
+
+    def solve64():
+        ud.zero_()
+        return E.bicgstab_dev(bd.data_ptr(), ud.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
+    t64, inf = _timed(dev, solve64)
+    out = {"workload": f"C2: icosphere L{level} + seeded ellipsoid (semi-axes U(0.5,2), gap 3), leaf 32, eta 2, "
+                       "ACA+ 1e-6, rhs 1+N(0,1e-3^2); BiCGSTAB to an FP64-verified 1e-8",
+           "n": n, "gpu_fill_s": t_build,
            "fp64": {"solve_s": t64, "iterations": inf["iterations"], "true_relres": inf["true_relres"],
                     "product": product(E)}}
-    forms = [("fp32_refined", abi.HBX_FP32, 0.0)]
-    if os.environ.get("HBX_EXPERIMENTAL_BF16") == "1":
-        forms.append(("bf16_refined", abi.HBX_BF16, 1e-2))
-    for name, prec, inner in forms:
+    for name, prec, inner in (("fp32_refined", abi.HBX_FP32, 0.0), ("bf16_refined", abi.HBX_BF16, 1e-2)):
         El = Engine(H.st, n, precision=prec)
-        tl, inf = best_of(lambda: E.bicgstab_refined_dev(El, bd.data_ptr(), ud.data_ptr(), tol=args.tol,
-                                                         max_iter=args.max_iter, inner_tol=inner, stream=s))
+
+        def solve_l():
+            ud.zero_()
+            return E.bicgstab_refined_dev(El, bd.data_ptr(), ud.data_ptr(), tol=args.tol, max_iter=args.max_iter,
+                                          inner_tol=inner, stream=s)
+        tl, inf = _timed(dev, solve_l)
         out[name] = {"solve_s": tl, "speedup_vs_fp64": t64 / tl, "outer": inf["outer"],
                      "inner_iterations": inf["iterations"], "true_relres": inf["true_relres"],
                      "product": product(El)}
         El.close()
     E.close()
-    print(json.dumps(out), flush=True)
+    H.close()
+    return out
+
+
+def mrhs_form(args, dev, stream, level=6):
+    """C3: 64 seeded N(0,1) right-hand sides on the L6 sphere solved at once
+    (tensor-core products, FP64 refinement, per-RHS masks) against the same
+    64 solved one after another by the FP64 solver."""
+    import torch
+    from hacapk_b200 import abi, configs
+    from hacapk_b200.engine import Engine
+    s = stream.cuda_stream
+    t0 = time.time()
+    H, B = configs.c3(level, abi.HBX_NRHS, fill="gpu")
+    t_build = time.time() - t0
+    n = H.nd
+    E = Engine(H.st, n)
+    Em = Engine(H.st, n, precision=abi.HBX_FP32, nrhs=abi.HBX_NRHS)
+    Bd = torch.from_numpy(B).to(dev)
+    Ud = torch.zeros_like(Bd)
+
+    def multi():
+        Ud.zero_()
+        return E.bicgstab_multi_dev(Em, Bd.data_ptr(), Ud.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
+    t_multi, infos = _timed(dev, multi, reps=2)
+    # the 64 right-hand sides one after another (FP64 solver)
+    cols = [torch.from_numpy(np.ascontiguousarray(B[:, j])).to(dev) for j in range(abi.HBX_NRHS)]
+    u1 = torch.zeros(n, dtype=torch.float64, device=dev)
+
+    def one_by_one():
+        res = []
+        for bj in cols:
+            u1.zero_()
+            res.append(E.bicgstab_dev(bj.data_ptr(), u1.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s))
+        return res
+    t_one, res1 = _timed(dev, one_by_one, reps=1)
+    X = torch.randn(n, abi.HBX_NRHS, device=dev).float()
+    Y = torch.zeros(n, abi.HBX_NRHS, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        Em.matmat_dev(X.data_ptr(), Y.data_ptr(), stream=s)
+    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0.record(stream)
+    for _ in range(20):
+        Em.matmat_dev(X.data_ptr(), Y.data_ptr(), stream=s)
+    m1.record(stream)
+    torch.cuda.synchronize(dev)
+    Em.sync(s)
+    mm_us = m0.elapsed_time(m1) / 20 * 1e3
+    its = [i["iterations"] for i in infos]
+    out = {"workload": f"C3: icosphere L{level}, leaf 32, eta 2, ACA+ 1e-5, 64 right-hand sides N(0,1) seed 2; "
+                       "FP32 tensor-core products in FP64 refinement to an FP64-verified 1e-8",
+           "n": n, "rhs": abi.HBX_NRHS, "gpu_fill_s": t_build,
+           "solve_s": t_multi, "fp64_one_by_one_s": t_one, "speedup_vs_fp64": t_one / t_multi,
+           "worst_true_relres": max(i["true_relres"] for i in infos),
+           "converged": int(sum(i["status"] == 0 for i in infos)),
+           "inner_iterations": [min(its), max(its)], "outer": max(i["outer"] for i in infos),
+           "fp64_iterations": [min(r["iterations"] for r in res1), max(r["iterations"] for r in res1)],
+           "matmat_us": mm_us, "matmat_tf32_tflops": abi.HBX_NRHS * Em.info["alg_flops"] / (mm_us * 1e-6) / 1e12}
+    Em.close()
+    E.close()
+    H.close()
+    return out
+
+
+def adjoint_form(args, dev, stream, level=6, ndir=16, step=1e-6):
+    """C4: J(g) = 0.5 ||sigma(g) - sigma_t||^2 with H sigma = g on the L6
+    sphere (FP64); dJ/dg by the adjoint solve on the transposed engine
+    (hbx_gradient_host), checked against central differences in 16 seeded
+    random directions (step 1e-6, solves to 1e-12)."""
+    from hacapk_b200 import configs
+    from hacapk_b200.engine import Engine
+    t0 = time.time()
+    H, g, st = configs.c4(level, fill="gpu")
+    t_build = time.time() - t0
+    n = H.nd
+    E = Engine(H.st, n)
+    Et = Engine(H.st, n, transpose=True)
+    t_grad, res = _timed(dev, lambda: E.gradient_host(Et, g, st, tol=1e-12, max_iter=args.max_iter), reps=2)
+    J, grad, sigma, fi, ai = res
+
+    def J_of(gv):
+        u, _ = E.bicgstab_host(gv, tol=1e-12, max_iter=args.max_iter)
+        return 0.5 * float(np.dot(u - st, u - st))
+    t_solve, _ = _timed(dev, lambda: E.bicgstab_host(g, tol=1e-12, max_iter=args.max_iter), reps=2)
+    rng = np.random.default_rng(16)
+    errs = []
+    for _ in range(ndir):
+        d = rng.standard_normal(n)
+        d /= np.linalg.norm(d)
+        fd = (J_of(g + step * d) - J_of(g - step * d)) / (2 * step)
+        ad = float(np.dot(grad, d))
+        errs.append(abs(fd - ad) / max(abs(fd), 1e-300))
+    out = {"workload": f"C4: icosphere L{level}, leaf 32, eta 2, ACA+ 1e-5, FP64; g, sigma_t N(0,1) (seeds 3, 4); "
+                       "adjoint BiCGSTAB on the transposed H-matvec, 16 central-difference directions (step 1e-6)",
+           "n": n, "gpu_fill_s": t_build, "gradient_s": t_grad, "fp64_solve_s": t_solve,
+           "gradient_vs_two_solves": t_grad / (2 * t_solve),
+           "fd_max_rel_err": max(errs), "fd_median_rel_err": float(np.median(errs)),
+           "forward_iterations": fi["iterations"], "adjoint_iterations": ai["iterations"],
+           "adjoint_true_relres": ai["true_relres"]}
+    Et.close()
+    E.close()
+    H.close()
+    return out
+
+
+def batch_form(args, dev, stream):
+    """C5: the 256 uneven ellipsoids solved in one block-diagonal engine
+    against the same bodies solved one after another (FP64 each)."""
+    import torch
+    from hacapk_b200 import configs
+    from hacapk_b200.engine import Engine
+    s = stream.cuda_stream
+    t0 = time.time()
+    inst = configs.c5(count=args.c5_count, fill="gpu")
+    t_build = time.time() - t0
+    Eb = Engine.batch([Hk for Hk, _ in inst])
+    bb = torch.from_numpy(np.concatenate([bk for _, bk in inst])).to(dev)
+    ub = torch.zeros_like(bb)
+
+    def batch():
+        ub.zero_()
+        return Eb.bicgstab_batch_dev(bb.data_ptr(), ub.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
+    t_batch, infos = _timed(dev, batch, reps=2)
+    stream_gb = Eb.info["stream_bytes"] / 1e9
+    Eb.close()
+    engines = [(Engine(Hk.st, Hk.nd), torch.from_numpy(bk).to(dev)) for Hk, bk in inst]
+    us = [torch.zeros_like(bd) for _, bd in engines]
+
+    def one_by_one():
+        for (Ek, bd), ud in zip(engines, us):
+            ud.zero_()
+            Ek.bicgstab_dev(bd.data_ptr(), ud.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
+    t_one, _ = _timed(dev, one_by_one, reps=1)
+    for Ek, _ in engines:
+        Ek.close()
+    its = [i["iterations"] for i in infos]
+    out = {"workload": f"C5: {len(inst)} ellipsoids, semi-axes U(0.3,3), icosphere levels 2-5 (seed 5), leaf 32, "
+                       "eta 2, ACA+ 1e-5, FP64; one block-diagonal engine against one solve after another",
+           "instances": len(inst), "n_total": int(sum(Hk.nd for Hk, _ in inst)), "stream_gb": stream_gb,
+           "gpu_fill_s": t_build, "solve_s": t_batch, "one_by_one_s": t_one, "speedup": t_one / t_batch,
+           "iterations": [min(its), max(its)], "worst_true_relres": max(i["true_relres"] for i in infos),
+           "converged": int(sum(i["status"] == 0 for i in infos))}
+    for Hk, _ in inst:
+        Hk.close()
+    return out
 
 
 def profile_matmat(args):
@@ -581,8 +644,10 @@ def main():
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--max-iter", type=int, default=2000)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--no-forms", action="store_true", help="skip the FP32-refined, 64-RHS and batch forms")
-    ap.add_argument("--c5-count", type=int, default=64, help="instances of the uneven-batch sample (C5: 256)")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the forms on their configurations (C2 precision, C3 multi-RHS, C4 adjoint, C5 batch)")
+    ap.add_argument("--c5-count", type=int, default=256, help="instances of the uneven batch (C5: 256)")
+    ap.add_argument("--forms-only", action="store_true", help="only the forms on their configurations")
     ap.add_argument("--profile-matmat", action="store_true",
                     help="only run five 64-RHS tensor-core products (a short command for ncu)")
     ap.add_argument("--precision-level", type=int, default=0,
@@ -593,6 +658,9 @@ def main():
         return
     if args.precision_level > 0:
         precision_workload(args)
+        return
+    if args.forms_only:
+        forms_only(args)
         return
     world, rank, local = dist_setup()
     if args.impl == "reference":

@@ -248,11 +248,6 @@ static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_option
   if (nd <= 0) return fail(HBX_ERR_INVALID, "hbx_create: nd <= 0");
   if (opt && opt->precision != HBX_FP64 && opt->precision != HBX_FP32 && opt->precision != HBX_BF16)
     return fail(HBX_ERR_UNSUPPORTED, "hbx_create: precision must be HBX_FP64, HBX_FP32 or HBX_BF16");
-  if (opt && opt->precision == HBX_BF16) {
-    const char *on = std::getenv("HBX_EXPERIMENTAL_BF16");
-    if (!on || std::atoi(on) != 1)
-      return fail(HBX_ERR_UNSUPPORTED, "hbx_create: HBX_BF16 is experimental (set HBX_EXPERIMENTAL_BF16=1)");
-  }
   const int nrhs = (opt && opt->nrhs > 1) ? opt->nrhs : 1;
   if (nrhs != 1 && nrhs != hbx::kNrhs) return fail(HBX_ERR_UNSUPPORTED, "hbx_create: nrhs must be 0, 1 or HBX_NRHS");
   if (nrhs > 1 && opt->precision != HBX_FP32)

@@ -86,10 +86,18 @@ __device__ __forceinline__ void init_cta_part(const Smem &s, const RunLite *lite
     s.rsum[3] = 0;
     mbar_fence_init();
   }
-  if (threadIdx.x < t0) return;
+  if (threadIdx.x < t0 || s.lite == lite) return;  // summaries read where they lie (see cta_smem)
   const uint4 *src = reinterpret_cast<const uint4 *>(lite);
   uint4 *dst = reinterpret_cast<uint4 *>(s.lite);
   for (uint32_t k = threadIdx.x - t0; k < nr; k += blockDim.x - t0) dst[k] = __ldg(src + k);
+}
+
+// The CTA's shared-memory layout; a CTA with more runs than the summary
+// array holds reads its run summaries from global memory instead.
+__device__ __forceinline__ Smem cta_smem(uint8_t *base, const RunLite *lite, uint32_t nr) {
+  Smem s = smem_layout(base);
+  if (nr > (uint32_t)kMaxCtaRuns) s.lite = const_cast<RunLite *>(lite);
+  return s;
 }
 
 __device__ __forceinline__ void init_cta(const Smem &s, const RunLite *lite, uint32_t nr, const unsigned *gbar) {
@@ -293,9 +301,9 @@ template <int kPrec>
 __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   constexpr bool kF32 = kPrec != kFP64;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  const Smem sm = smem_layout(smem_raw);
   const CtaInfo ci = a.ctas[blockIdx.x];
   const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
+  const Smem sm = cta_smem(smem_raw, a.lite + ci.rec_begin, nr);
   const uint64_t t_start = a.prof ? gtimer() : 0;
   uint32_t issued0 = 0;
   const StreamSrc ss{a.stream + ci.stream_off, ci.stream_bytes, keep_bytes(ci.stream_bytes, a.keep_frac)};
@@ -459,15 +467,15 @@ template <int kPrec>
 __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   constexpr bool kF32 = kPrec != kFP64;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  const Smem sm = smem_layout(smem_raw);
   const CtaInfo ci = a.ctas[blockIdx.x];
+  const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
+  const Smem sm = cta_smem(smem_raw, a.lite + ci.rec_begin, nr);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ncta = gridDim.x;
   auto stamp = [&](int k) {
     if (a.prof && threadIdx.x == 0) a.prof[blockIdx.x * 16 + 8 + k] = gtimer();
   };
   const uint64_t t_start = a.prof ? gtimer() : 0;
-  const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
   // A consumer warp's first owned atom and this lane's row of it: its vector
   // entries stay in registers through the step, loaded while the step's
   // scalars are reduced (the rows of further atoms are read where needed).

@@ -436,9 +436,10 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
       err = "a CTA stream exceeds 4 GiB; use more CTAs";
       return HBX_ERR_INVALID;
     }
-    const int max_runs = pair_panels ? kMaxPairRuns : kMaxCtaRuns;
-    if (info.nr_p + info.nr_d + info.nr_u > (uint32_t)max_runs) {
-      err = "a CTA holds more than " + std::to_string(max_runs) + " runs; use more CTAs";
+    // the multi-RHS kernel keeps every run summary in shared memory; the
+    // single-RHS kernels read them from global memory past kMaxCtaRuns
+    if (pair_panels && info.nr_p + info.nr_d + info.nr_u > (uint32_t)kMaxPairRuns) {
+      err = "a CTA holds more than " + std::to_string(kMaxPairRuns) + " runs; use more CTAs";
       return HBX_ERR_INVALID;
     }
     info.stream_bytes = (uint32_t)pos;  // a multiple of 16 by construction

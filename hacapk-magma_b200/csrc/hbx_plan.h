@@ -41,6 +41,7 @@
 // warps; the consumer warps keep the CTA's summaries in shared memory.
 #pragma once
 
+#include <cmath>
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
@@ -85,7 +86,7 @@ constexpr int kRecBytes = 1024;    // one run record: 32-byte header + kRunSegs 
 #define HBX_STAGES 4
 #endif
 constexpr int kStages = HBX_STAGES;  // vector stage buffers: runs gathered ahead of the consumers
-constexpr int kMaxCtaRuns = 1024;    // run summaries a CTA keeps in shared memory
+constexpr int kMaxCtaRuns = 1024;    // run summaries a CTA keeps in shared memory (more: read from global memory)
 constexpr int kMaxPairRuns = 512;    // the same for the multi-RHS engine (pair-panel plans)
 
 // kRunDU: an atom's dense and low-rank columns in one block (x segments,
@@ -106,18 +107,29 @@ HBX_HD constexpr uint32_t stage_elem_bytes(int prec) { return prec == kFP64 ? 8u
 // bfloat16: the high half of a float.  Storage rounds a double to the
 // nearest bfloat16, ties to even, in one step (no intermediate float
 // rounding); bfloat16 has float's exponent range, so every factor keeps 8
-// significant bits whatever its magnitude.  Values below float's normal
-// range go through float.
+// significant bits whatever its magnitude.  Below 2^-126 the bfloat16
+// values are subnormal, multiples of 2^-133: the double is scaled to units
+// of 2^-133 (exactly) and rounded to the nearest integer, ties to even.
 inline uint16_t bf16_from_double(double v) {
   uint64_t b;
   std::memcpy(&b, &v, sizeof b);
   const uint64_t mag = b & 0x7fffffffffffffffull;
-  if (mag >= 0x7ff0000000000000ull || mag < 0x3810000000000000ull) {  // inf/nan or below 2^-126
+  const uint16_t sign = (uint16_t)((b >> 48) & 0x8000u);
+  if (mag >= 0x7ff0000000000000ull) {  // inf / nan
     const float f = (float)v;
     uint32_t u;
     std::memcpy(&u, &f, sizeof u);
     if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40u);  // quiet nan
-    return (uint16_t)((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
+    return (uint16_t)(u >> 16);
+  }
+  if (mag < 0x3810000000000000ull) {  // below 2^-126
+    double m;
+    std::memcpy(&m, &mag, sizeof m);
+    const double q = std::ldexp(m, 133);  // < 128, exact
+    double k = std::floor(q);
+    const double f = q - k;                // exact
+    if (f > 0.5 || (f == 0.5 && std::fmod(k, 2.0) != 0.0)) k += 1.0;
+    return (uint16_t)(sign | (uint16_t)k);  // k == 128 is the smallest normal, 2^-126
   }
   // keep 7 fraction bits of the 52: round the low 45 bits to nearest, ties to even
   b += (1ull << 44) - 1ull + ((b >> 45) & 1ull);

@@ -48,8 +48,7 @@ class Engine:
                  nrhs: int = 0, block_cost: int = 0, run_cost: int = 0):
         """transpose=True packs H^T: products and solves with the adjoint.
         precision=abi.HBX_FP32 stores the factors in float (half the bytes),
-        abi.HBX_BF16 in bfloat16 (a quarter; experimental: needs the
-        environment variable HBX_EXPERIMENTAL_BF16=1).
+        abi.HBX_BF16 in bfloat16 (a quarter).
         nrhs=abi.HBX_NRHS (with HBX_FP32) makes a multi-RHS engine: matmat only."""
         self.lib = abi.engine_lib()
         opt = abi.Options()

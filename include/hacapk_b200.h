@@ -119,9 +119,7 @@ typedef enum hbx_status {
  * multiplies the widened factors by float vectors in float, eight columns
  * per 16-byte load: a quarter of the FP64 bytes.  bfloat16 has float's
  * exponent range, so no per-leaf scale is needed to keep the factors in
- * range.  HBX_BF16 is experimental: hbx_create accepts it only with the
- * environment variable HBX_EXPERIMENTAL_BF16=1.  No counterpart in the
- * reference, which is FP64 throughout. */
+ * range.  No counterpart in the reference, which is FP64 throughout. */
 enum { HBX_FP64 = 0, HBX_FP32 = 1, HBX_BF16 = 2 };
 
 typedef struct hbx_hmat hbx_hmat;

@@ -69,17 +69,12 @@ def test_engine_library_has_no_cpu_compute_fallback(build_libs):
     assert "orc_" not in out and "c_hacapk_adot_body_lfmtx_" not in [l.split()[-1] for l in out.splitlines()]
 
 
-def test_bf16_engines_need_the_experimental_switch(build_libs, monkeypatch):
-    """HBX_BF16 is refused, before any CUDA call, unless
-    HBX_EXPERIMENTAL_BF16=1; an unknown precision is refused too."""
+def test_unknown_precision_is_refused(build_libs):
+    """An unknown storage precision is refused before any CUDA call."""
     from conftest import sphere
-    from hacapk_b200 import abi
     from hacapk_b200.engine import Engine, HbxError
-    monkeypatch.delenv("HBX_EXPERIMENTAL_BF16", raising=False)
+    from hacapk_b200 import abi
     H = sphere(2)
-    with pytest.raises(HbxError) as e:
-        Engine(H.st, H.nd, precision=abi.HBX_BF16)
-    assert abi.STATUS[e.value.status] == "HBX_ERR_UNSUPPORTED" and "HBX_EXPERIMENTAL_BF16" in str(e.value)
     with pytest.raises(HbxError) as e:
         Engine(H.st, H.nd, precision=7)
     assert abi.STATUS[e.value.status] == "HBX_ERR_UNSUPPORTED"

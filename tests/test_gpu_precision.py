@@ -63,12 +63,9 @@ def test_fp32_plain_bicgstab_and_rejects_mismatch(gpu, build_libs):
         E64_small.bicgstab_refined_host(E32, b2)
 
 
-# ---- BF16 storage (experimental: the engine needs HBX_EXPERIMENTAL_BF16=1) ----
-_bf16 = pytest.mark.skipif(os.environ.get("HBX_EXPERIMENTAL_BF16") != "1",
-                           reason="HBX_BF16 engines are experimental: set HBX_EXPERIMENTAL_BF16=1")
+# ---- BF16 storage ----
 
 
-@_bf16
 @pytest.mark.parametrize("level", [3, 5])
 def test_bf16_matvec_error_against_fp64_oracle(gpu, build_libs, level):
     """bfloat16 factors (8 significant bits, unit roundoff 2^-9) times the
@@ -94,7 +91,6 @@ def test_bf16_matvec_error_against_fp64_oracle(gpu, build_libs, level):
     assert np.array_equal(y, y2)
 
 
-@_bf16
 @pytest.mark.parametrize("level", [3, 4])
 def test_bf16_refined_solve_reaches_fp64_tolerance(gpu, build_libs, level):
     """BiCGSTAB on the BF16 engine inside FP64 iterative refinement reaches

@@ -243,6 +243,32 @@ def test_bf16_rounding(emu):
     assert emu.emu_bf16_from_double(-0.0) == 0x8000
 
 
+def test_bf16_rounding_below_float_normal_range(emu):
+    """Below 2^-126 bfloat16 is subnormal (multiples of 2^-133): one
+    rounding from the double, against exact rational arithmetic; rounding
+    through float first would round twice (2^-133 * (5/2 + 2^-30) rounds up
+    to 3 units here, while a float rounding would first make it an exact
+    tie, 5/2, and then round it to even, 2)."""
+    from fractions import Fraction
+    unit = Fraction(1, 2**133)
+
+    def ref(v):
+        q = abs(Fraction(v)) / unit
+        k = int(q)
+        rem = q - k
+        if rem > Fraction(1, 2) or (rem == Fraction(1, 2) and k % 2 == 1):
+            k += 1
+        return (0x8000 if np.signbit(v) else 0) | k
+
+    rng = np.random.default_rng(12)
+    v = list(rng.uniform(0, 2.0**-126, 300) * rng.choice([-1.0, 1.0], 300))
+    v += [2.0**-133 * (2.5 + 2.0**-30), 2.0**-133 * 2.5, 2.0**-133 * 3.5, 2.0**-126 * (1 - 2.0**-40),
+          2.0**-140, -2.0**-133 * 0.5, 5e-324]
+    for t in v:
+        assert emu.emu_bf16_from_double(float(t)) == ref(float(t)), t
+    assert emu.emu_bf16_from_double(2.0**-133 * (2.5 + 2.0**-30)) == 3
+
+
 @pytest.mark.parametrize("level,nc", [(3, 148), (4, 148), (3, 7), (3, 1)])
 def test_bf16_layout(emu, level, nc):
     """BF16 storage: 8-column bfloat16 panels with the same 16-byte rows,
