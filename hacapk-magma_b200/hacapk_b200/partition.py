@@ -9,12 +9,18 @@
 * Each rank keeps the leaves whose first row lies in its range
   (HACApK_generate_frame_leafmtx, m_HACApK_base.f90:511-521) and multiplies
   them on its own device.
-* One combination per product.  The reference all-gathers row segments
-  (MPI_Allgatherv, HACApK_SOLVER.c:106-251); a leaf that starts in one range
-  can reach rows of the next, so here the ranks' full-length partial products
-  are all-gathered and summed in rank order -- exact whatever the leaves'
-  extent, and the same sum on every rank and every run.  The vectors of the
-  solve are replicated, as in the reference's flat solver.
+* The combination of the ranks' products.  The reference all-gathers the
+  owned row segments (MPI_Allgatherv, HACApK_SOLVER.c:106-251).  A leaf that
+  starts in one range can reach rows below it, into the next ranges, so a
+  rank's product also holds rows it does not own (its spill, usually a few
+  leaves' worth).  Two collectives per product: the spills are all-gathered
+  (padded to the longest), every rank adds the spills that reach its own
+  rows to its own rows in rank order, and the owned segments are
+  all-gathered (padded to the longest).  Per product a rank sends and
+  receives about N + world * (longest spill) values, against world * N for
+  gathering full-length partial products, and every rank holds the same
+  vector, bit for bit, on every run.  The vectors of the solve are
+  replicated, as in the reference's flat solver.
 
 The local product is a callable built by a factory, so the same plumbing runs
 an engine per GPU over NCCL or the CPU checker over gloo.
@@ -95,20 +101,42 @@ class RowPartitionedMatvec:
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
         self.cuts = row_cuts(st, nd, self.world)
+        # reach[r]: one past the last row a leaf of rank r touches
+        self.reach = list(self.cuts[1:])
+        for ip in range(st.contents.nlf):
+            L = _leaf_ptr(st, ip)
+            r0 = L.nstrtl - 1
+            r = next(k for k in range(self.world) if self.cuts[k] <= r0 < self.cuts[k + 1])
+            self.reach[r] = max(self.reach[r], r0 + L.ndl)
+        self.spill = [self.reach[r] - self.cuts[r + 1] for r in range(self.world)]
+        self.max_spill = max(self.spill)
+        self.max_own = max(self.cuts[r + 1] - self.cuts[r] for r in range(self.world))
         self.subset = LeafSubset(st, nd, self.cuts[self.rank], self.cuts[self.rank + 1])
         self.local = local_factory(self.subset.st, nd)
         self.nd = nd
+        # values a rank sends per product (spill window, then owned segment)
+        self.exchange_values = self.max_spill + self.max_own
 
     def __call__(self, x):
         import torch
         import torch.distributed as dist
         y = self.local(x)
-        parts = [torch.empty_like(y) for _ in range(self.world)]
-        dist.all_gather(parts, y, group=self.group)
-        out = parts[0].clone()
-        for p in parts[1:]:  # rank order: the same sum on every rank
-            out += p
-        return out
+        me, c = self.rank, self.cuts
+        own = y[c[me]:c[me + 1]].clone()
+        if self.max_spill > 0:
+            mine = torch.zeros(self.max_spill, dtype=y.dtype, device=y.device)
+            mine[:self.spill[me]] = y[c[me + 1]:self.reach[me]]
+            spills = [torch.empty_like(mine) for _ in range(self.world)]
+            dist.all_gather(spills, mine, group=self.group)
+            for r in range(me):  # rank order: the same sum on every run
+                lo, hi = max(c[r + 1], c[me]), min(self.reach[r], c[me + 1])
+                if lo < hi:
+                    own[lo - c[me]:hi - c[me]] += spills[r][lo - c[r + 1]:hi - c[r + 1]]
+        seg = torch.zeros(self.max_own, dtype=y.dtype, device=y.device)
+        seg[:own.numel()] = own
+        segs = [torch.empty_like(seg) for _ in range(self.world)]
+        dist.all_gather(segs, seg, group=self.group)
+        return torch.cat([segs[r][:c[r + 1] - c[r]] for r in range(self.world)])
 
 
 def engine_product(st, nd: int):

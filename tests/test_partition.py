@@ -1,7 +1,9 @@
 """The row-partitioned product on the CPU (gloo, world sizes 2 and 3): the
 reference's MPI scheme (cuts by stored words at leaf row starts,
-m_HACApK_base.f90:511-581; one combination per product,
-HACApK_SOLVER.c:106-251) with the oracle as every rank's local product.  The
+m_HACApK_base.f90:511-581; owned row segments all-gathered per product,
+HACApK_SOLVER.c:106-251, after the rows a rank's leaves reach below its
+range are added in by their owners) with the oracle as every rank's local
+product.  The
 same plumbing runs an engine per GPU over NCCL; that form is not run here
 (one GPU per call on this pool)."""
 import multiprocessing as mp
@@ -53,7 +55,7 @@ def _rank_main(rank, world, pipelined, port, q):
     y = mv(x).numpy()
     solve = partition.bicgstab_pipelined if pipelined else partition.bicgstab
     u, steps, relres = solve(mv, torch.from_numpy(b), tol=1e-8, max_iter=500)
-    q.put((rank, y, u.numpy(), steps, relres, mv.subset.nlf))
+    q.put((rank, y, u.numpy(), steps, relres, mv.subset.nlf, mv.exchange_values))
     dist.destroy_process_group()
 
 
@@ -81,9 +83,11 @@ def test_partitioned_product_and_solve_gloo(build_libs, world, pipelined):
     H, b = _build()
     x = np.random.default_rng(3).standard_normal(H.nd)
     ref = oracle.matvec(H.st, x)
-    for rank, y, u, steps, relres, nlf in got:
+    for rank, y, u, steps, relres, nlf, sent in got:
         assert 0 < nlf < H.nlf  # each rank holds part of the leaves
         assert np.abs(y - ref).max() <= 1e-13 * np.abs(ref).max()
+        # the owned segment plus the spill window, not world full-length vectors
+        assert sent < 1.5 * H.nd / world + H.nd / 4, (sent, H.nd)
     # every rank holds the same solution (replicated vectors, same sums)
     assert all(np.array_equal(got[0][2], g[2]) and got[0][3] == g[3] for g in got[1:])
     # against the same solve with the whole product on one process
