@@ -232,8 +232,10 @@ int hbx_matvec(hbx_hmat *h, double alpha, const double *x, double beta,
  * every GPU that loads them until the process exits.  Limit: matrices whose
  * low-rank ranks sum to more than 131040 are rejected with HBX_ERR_INVALID.
  * The call allocates nothing: it clears the barrier words and launches on
- * `stream`.  The array's address is looked up on a device's first call: make
- * that first call before any stream capture.  All calls share the array, so
+ * `stream`.  The array's address is looked up on a device's first call and
+ * kept: make that first call before any stream capture, and do not use the
+ * call again in a process after cudaDeviceReset (or another teardown of the
+ * device's context), which leaves the kept address stale.  All calls share the array, so
  * calls that overlap on the GPU (other streams, other engines) race:
  * serialize them.  Device-side wait failures latch in the engine's error
  * word (hbx_sync). */
