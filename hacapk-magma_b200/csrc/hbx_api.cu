@@ -297,7 +297,15 @@ static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_option
   if (opt && opt->run_cost > 0) costs.run = (uint64_t)opt->run_cost;
   const int prec = !opt ? hbx::kFP64
                         : (opt->precision == HBX_BF16 ? hbx::kBF16 : (opt->precision == HBX_FP32 ? hbx::kFP32 : hbx::kFP64));
-  int st_plan = hbx::make_plan(st, nd, nc, h->plan, err, prec, nrhs > 1, costs);
+  // merged D+U blocks (single-vector engines): the atoms with low-rank rows
+  // that each CTA keeps split -- its first ones, whose D runs cover the wait
+  // for the zbu grid barrier -- 4 by default (C1 L5: H-matvec 50.0 -> 49.4
+  // us, BiCGSTAB step 124.9 -> 123.0 us), HBX_MERGE_KEEP overrides; < 0:
+  // none merged
+  int merge_keep = 4;
+  if (const char *mk = std::getenv("HBX_MERGE_KEEP")) merge_keep = std::atoi(mk);
+  if (nrhs > 1) merge_keep = -1;
+  int st_plan = hbx::make_plan(st, nd, nc, h->plan, err, prec, nrhs > 1, costs, merge_keep);
   if (st_plan != HBX_OK) return bail(fail(st_plan, "hbx_create: " + err));
   const hbx::Plan &P = h->plan;
   // L2 residency of the factor stream: the head of every CTA's stream, in

@@ -508,17 +508,24 @@ __device__ __forceinline__ void gather_warp(const GatherCtx &c, const SM &sm, ui
     const uint8_t *rec = recs + (i % kRecSlots) * kRecBytes;
     const Run h = *reinterpret_cast<const Run *>(rec);
     const Seg *seg = reinterpret_cast<const Seg *>(rec + sizeof(Run));
-    const uint8_t *vec =
-        static_cast<const uint8_t *>(is_u ? ((pass & 1) ? c.z1 : c.z0) : ((pass & 1) ? c.x1 : c.x0));
+    const uint8_t *xv = static_cast<const uint8_t *>((pass & 1) ? c.x1 : c.x0);
+    const uint8_t *zv = static_cast<const uint8_t *>((pass & 1) ? c.z1 : c.z0);
     constexpr uint32_t esz = kF32 ? 4u : 8u;
     uint8_t *st = sm.stage + slot * kStageBytes;
+    // a segment's source: zbu for U runs, x for P and D runs, and for the
+    // merged D+U runs of an atom zbu when kSegZbu is set in its src
+    const bool du = (h.flags & 0xffu) == kRunDU;
+    auto src_of = [&](const Seg &sg) -> const uint8_t * {
+      if (du) return (sg.src & kSegZbu) ? zv + (size_t)(sg.src & ~kSegZbu) * esz : xv + (size_t)sg.src * esz;
+      return (is_u ? zv : xv) + (size_t)sg.src * esz;
+    };
     for (uint32_t q = 0; q < h.nlong; ++q) {
       const Seg sg = seg[q];
-      stage_elems<kF32>(st, sg.dst, vec + (size_t)sg.src * esz, (uint32_t)lane, sg.len, 32);
+      stage_elems<kF32>(st, sg.dst, src_of(sg), (uint32_t)lane, sg.len, 32);
     }
     for (uint32_t q = h.nlong + lane; q < h.nseg; q += 32) {
       const Seg sg = seg[q];
-      stage_elems<kF32>(st, sg.dst, vec + (size_t)sg.src * esz, 0, sg.len, 1);
+      stage_elems<kF32>(st, sg.dst, src_of(sg), 0, sg.len, 1);
     }
     const uint32_t vend = (uint32_t)h.npanel * group_cols(kPrec);
     for (uint32_t e = h.vlen + lane; e < vend; e += 32) {

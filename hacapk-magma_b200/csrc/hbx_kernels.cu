@@ -213,7 +213,7 @@ __device__ __forceinline__ void sum_warp(uint32_t nr, uint32_t npass, uint32_t n
         if (kind == kRunP) {
           o.zbu[row] = s;
           if (o.zbu32) o.zbu32[row] = (float)s;
-        } else if (kind == kRunD) {
+        } else if (kind == kRunD || kind == kRunDU) {  // an atom's first (a merged one: only) block
           double v = o.alpha * s;
           if (o.beta != 0.0) v = fma(o.beta, o.yin[row], v);
           o.y[row] = v;

@@ -90,8 +90,8 @@ constexpr int kMaxCtaRuns = 1024;    // run summaries a CTA keeps in shared memo
 constexpr int kMaxPairRuns = 512;    // the same for the multi-RHS engine (pair-panel plans)
 
 // kRunDU: an atom's dense and low-rank columns in one block (x segments,
-// then zbu segments marked by kSegZbu), placed in the U section; only plans
-// made with merge_keep >= 0 hold it, and the kernels do not take it yet.
+// then zbu segments marked by kSegZbu), placed in the U section (its gather
+// waits for zbu); only plans made with merge_keep >= 0 hold it.
 enum RunKind : uint16_t { kRunP = 0, kRunD = 1, kRunU = 2, kRunDU = 3 };
 constexpr uint32_t kSegZbu = 0x80000000u;  // kRunDU segment source: zbu (else x)
 enum RunFlags : uint16_t { kFirst = 0x100, kLast = 0x200 };

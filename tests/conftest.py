@@ -66,6 +66,8 @@ def emu_lib():
         L = C.CDLL(lib)
         DP = C.POINTER(C.c_double)
         L.emu_matvec_kernel_order.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, DP, C.c_double, DP, DP]
+        L.emu_matvec_kernel_order_mk.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, DP, C.c_double,
+                                                 DP, DP]
         _libs["emu"] = L
     return _libs["emu"]
 
@@ -93,21 +95,30 @@ def flat_lib():
     return _libs["flat"]
 
 
-def kernel_order_matvec(H, num_ctas=148):
+def kernel_order_matvec(H, num_ctas=148, merge_keep=None):
     """y = H x in the FP64 kernel's own operation order (bit for bit what
-    k_matvec computes on num_ctas CTAs), on the CPU."""
+    k_matvec computes on num_ctas CTAs with the engine's block layout), on
+    the CPU.  merge_keep: the planner's merged-D+U setting (None: the
+    engine's default, HBX_MERGE_KEEP)."""
     import ctypes as C
     import numpy as np
     L = emu_lib()
     DP = C.POINTER(C.c_double)
+    mk = engine_merge_keep() if merge_keep is None else merge_keep
 
     def mv(x):
         x = np.ascontiguousarray(x, np.float64)
         y = np.zeros_like(x)
-        assert L.emu_matvec_kernel_order(C.cast(H.st, C.c_void_p), H.nd, num_ctas, 1.0, x.ctypes.data_as(DP), 0.0,
-                                         None, y.ctypes.data_as(DP)) == 0
+        assert L.emu_matvec_kernel_order_mk(C.cast(H.st, C.c_void_p), H.nd, num_ctas, mk, 1.0,
+                                            x.ctypes.data_as(DP), 0.0, None, y.ctypes.data_as(DP)) == 0
         return y
     return mv
+
+
+def engine_merge_keep() -> int:
+    """The merged-D+U setting the engine's planner uses (HBX_MERGE_KEEP)."""
+    v = os.environ.get("HBX_MERGE_KEEP")
+    return int(v) if v is not None else 4
 
 
 def flat_solve(H, b, mv, tol=1e-8, max_iter=1000):

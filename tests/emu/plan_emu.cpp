@@ -302,18 +302,19 @@ extern "C" int emu_plan_cta_sections(const stc_HACApK_leafmtxp *st, int nd, int 
 }
 
 // y = alpha H x + beta yin in the FP64 kernel's own operation order, so that
-// it equals k_matvec bit for bit: consumer warp w takes panels
+// it equals k_matvec bit for bit (merge_keep as make_plan's; merged D+U runs
+// gather x or zbu per segment and write like D blocks): consumer warp w takes panels
 // j = (w - rot) mod 16, j + 16, ... of every run, four at a time (two for P
 // slabs taller than 32 rows, whose lanes also carry row lane + 32) into
 // accumulator pairs (one fma per column), folds them into its block sum at
 // the end of the run (a0 + a1, accumulators in order), and the block-sum
 // warp adds the 16 warps' sums in warp order; P blocks write zbu, D blocks
 // y = alpha s (+ beta yin), U blocks y = fma(alpha, s, y).
-extern "C" int emu_matvec_kernel_order(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, double alpha,
-                                       const double *x, double beta, const double *yin, double *y) {
+extern "C" int emu_matvec_kernel_order_mk(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int merge_keep,
+                                          double alpha, const double *x, double beta, const double *yin, double *y) {
   Plan plan;
   std::string err;
-  if (make_plan(st, nd, num_ctas, plan, err, kFP64, false, PlanCosts(), -1) != 0) return 1;
+  if (make_plan(st, nd, num_ctas, plan, err, kFP64, false, PlanCosts(), merge_keep) != 0) return 1;
   std::vector<uint8_t> buf(plan.total_bytes, 0);
   pack_plan(st, plan, buf.data());
   std::vector<double> zbu(plan.zbu_len, 0.0), stage(kStageBytes / 8);
@@ -328,10 +329,14 @@ extern "C" int emu_matvec_kernel_order(const stc_HACApK_leafmtxp *st, int nd, in
       for (uint32_t k = k0; k < k1; ++k) {
         const RunRec &R = plan.recs[ci.rec_begin + k];
         const Run &r = R.hdr;
-        const bool is_u = k >= ci.nr_p + ci.nr_d;
+        const bool du = run_kind(r) == kRunDU;  // merged D+U: writes like a D block
+        const bool is_u = k >= ci.nr_p + ci.nr_d && !du;
         const double *vec = is_u ? zbu.data() : x;
-        for (uint32_t q = 0; q < r.nseg; ++q)
-          for (uint32_t e = 0; e < R.seg[q].len; ++e) stage[R.seg[q].dst + e] = vec[R.seg[q].src + e];
+        for (uint32_t q = 0; q < r.nseg; ++q) {
+          const uint32_t sv = R.seg[q].src;
+          for (uint32_t e = 0; e < R.seg[q].len; ++e)
+            stage[R.seg[q].dst + e] = du ? ((sv & kSegZbu) ? zbu[(sv & ~kSegZbu) + e] : x[sv + e]) : vec[sv + e];
+        }
         for (uint32_t e = r.vlen; e < 2u * r.npanel; ++e) stage[e] = 0.0;
         const double *d = reinterpret_cast<const double *>(buf.data() + ci.stream_off + r.pos);
         const uint32_t h = r.nrow, np = r.npanel;
@@ -383,4 +388,9 @@ extern "C" int emu_matvec_kernel_order(const stc_HACApK_leafmtxp *st, int nd, in
   do_pass(0);
   do_pass(1);
   return 0;
+}
+
+extern "C" int emu_matvec_kernel_order(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, double alpha,
+                                       const double *x, double beta, const double *yin, double *y) {
+  return emu_matvec_kernel_order_mk(st, nd, num_ctas, -1, alpha, x, beta, yin, y);
 }
