@@ -80,6 +80,10 @@ void free_engine(hbx_hmat *h) {
   cudaFree(h->d_state);
   cudaFree(h->d_hist);
   cudaFree(h->d_refine);
+  cudaFree(h->d_gcr);
+  cudaFree(h->d_gcrs);
+  cudaFree(h->d_gcrpart);
+  if (h->h_gcr) cudaFreeHost(h->h_gcr);
   cudaFree(h->d_f32);
   cudaFree(h->d_zbum);
   cudaFree(h->d_mrv);
@@ -808,6 +812,140 @@ int hbx_bicgstab_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_o
   cudaError_t e = cudaMemcpyAsync(u, du, bytes, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "hbx_bicgstab_host copy-out");
+  return st;
+}
+
+// GCR(m) of HACApK_gcrm_lfmtx (m_HACApK_solve.f90:506-571) on device vectors,
+// on h->stream; the statement order is the Fortran's (section comments).
+static int gcr_dev(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info) {
+  if (int rc = single_rhs(h, "hbx_gcr")) return rc;
+  const double tol = opts ? opts->tol : 1e-8;
+  const int mstep = opts ? opts->max_iter : 1000;
+  const int m = (opts && opts->restart > 0) ? opts->restart : 8;
+  if (mstep < 0 || !(tol >= 0.0)) return fail(HBX_ERR_INVALID, "hbx_gcr: bad tol or max_iter");
+  if (m > hbx::kMaxDots) return fail(HBX_ERR_INVALID, "hbx_gcr: restart length above " + std::to_string(hbx::kMaxDots));
+  const size_t n = (size_t)h->plan.nd;
+  if (h->gcr_m < m) {
+    cudaFree(h->d_gcr);
+    h->d_gcr = nullptr;
+    h->gcr_m = 0;
+    HBX_CUDA(dev_malloc(&h->d_gcr, (2 + 2 * (size_t)m) * n * sizeof(double)));
+    h->gcr_m = m;
+  }
+  if (!h->d_gcrs) HBX_CUDA(dev_malloc(&h->d_gcrs, (3 * (size_t)hbx::kMaxDots + 1) * sizeof(double)));
+  if (!h->d_gcrpart)
+    HBX_CUDA(dev_malloc(&h->d_gcrpart, (size_t)hbx::gcr_dot_blocks(n) * hbx::kMaxDots * 2 * sizeof(double)));
+  if (!h->h_gcr) HBX_CUDA(cudaHostAlloc(&h->h_gcr, 4 * sizeof(double), cudaHostAllocDefault));
+  cudaStream_t s = h->stream;
+  double *zr = h->d_gcr, *zar = zr + n, *zp = zar + n, *zap = zp + (size_t)m * n;
+  double *capap = h->d_gcrs, *alpha = capap + hbx::kMaxDots, *beta = alpha + 1, *dots = beta + hbx::kMaxDots;
+  double *part = h->d_gcrpart;
+  auto P = [&](int k) { return zp + (size_t)k * n; };
+  auto AP = [&](int k) { return zap + (size_t)k * n; };
+  auto dot1 = [&](const double *x, const double *y, double *out_host) -> int {
+    const double *xs[1] = {x}, *ys[1] = {y};
+    HBX_CUDA(hbx::gcr_launch_dots(1, xs, ys, n, part, dots, s));
+    HBX_CUDA(cudaMemcpyAsync(out_host, dots, sizeof(double), cudaMemcpyDeviceToHost, s));
+    HBX_CUDA(cudaStreamSynchronize(s));
+    return HBX_OK;
+  };
+  HBX_CUDA(cudaEventRecord(h->ev0, s));
+  double *hs = h->h_gcr;
+  if (int rc = dot1(b, b, &hs[0])) return rc;
+  const double bnorm = std::sqrt(hs[0]);
+  // zr = b - H u (as b - zar); zp(1) = zr
+  HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, zr), s));
+  HBX_CUDA(cudaMemcpyAsync(P(0), zr, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  if (int rc = dot1(zr, zr, &hs[1])) return rc;
+  double zrnorm = std::sqrt(hs[1]);
+  int launches = 4, nstp = 0, status = HBX_OK;
+  auto relres = [&](double rn) { return bnorm > 0.0 ? rn / bnorm : 0.0; };
+  if (!std::isfinite(zrnorm) || !std::isfinite(bnorm)) {
+    status = HBX_ERR_NONFINITE;
+  } else if (!(relres(zrnorm) < tol) && mstep > 0) {
+    {
+      HBX_CUDA(mv_launch(h, matvec_args(h, 1.0, P(0), 0.0, nullptr, AP(0)), s));  // zap(1) = H zp(1)
+      ++launches;
+      for (int in = 1; in <= mstep; ++in) {
+        const int ik = (in - 1) % m;
+        // alpha = (zq . zr) / (zq . zq), zq = zap(ik); u += alpha zp(ik); zr -= alpha zq
+        const double *xs[2] = {AP(ik), AP(ik)}, *ys[2] = {zr, AP(ik)};
+        HBX_CUDA(hbx::gcr_launch_dots(2, xs, ys, n, part, dots, s));
+        HBX_CUDA(hbx::gcr_launch_alpha(dots, ik, capap, alpha, s));
+        HBX_CUDA(hbx::gcr_launch_step(n, alpha, P(ik), AP(ik), u, zr, s));
+        if (int rc = dot1(zr, zr, &hs[1])) return rc;
+        launches += 7;
+        zrnorm = std::sqrt(hs[1]);
+        nstp = in;
+        if (!std::isfinite(zrnorm)) {
+          status = HBX_ERR_BREAKDOWN;
+          break;
+        }
+        if (relres(zrnorm) < tol || in == mstep) break;
+        // zar = H zr; the next slot holds zr / zar, orthogonalized against
+        // slots 1..ik as they are now (at a restart slot 1 is the new one)
+        HBX_CUDA(mv_launch(h, matvec_args(h, 1.0, zr, 0.0, nullptr, zar), s));
+        const int ikn = in % m;
+        HBX_CUDA(cudaMemcpyAsync(P(ikn), zr, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        HBX_CUDA(cudaMemcpyAsync(AP(ikn), zar, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        const double *qx[hbx::kMaxDots], *qy[hbx::kMaxDots];
+        for (int l = 0; l <= ik; ++l) {
+          qx[l] = AP(l);
+          qy[l] = zar;
+        }
+        HBX_CUDA(hbx::gcr_launch_dots(ik + 1, qx, qy, n, part, dots, s));
+        HBX_CUDA(hbx::gcr_launch_orth(n, ik + 1, ikn, dots, capap, beta, zp, zap, s));
+        launches += 5;
+      }
+      if (status == HBX_OK && !(relres(zrnorm) < tol)) status = HBX_ERR_NOT_CONVERGED;
+    }
+  }
+  HBX_CUDA(cudaEventRecord(h->ev1, s));
+  // true residual ||b - H u||
+  HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, zar), s));
+  if (int rc = dot1(zar, zar, &hs[2])) return rc;
+  int dst = check_device_error(h, s);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  if (info) {
+    std::memset(info, 0, sizeof(*info));
+    info->iterations = nstp;
+    info->status = dst != HBX_OK ? dst : status;
+    info->bnorm = bnorm;
+    info->relres = relres(zrnorm);
+    info->true_relres = bnorm > 0 ? std::sqrt(hs[2]) / bnorm : std::sqrt(hs[2]);
+    info->seconds = ms * 1e-3;
+    info->launches = launches + 3;
+  }
+  if (dst != HBX_OK) return dst;
+  if (status != HBX_OK) return fail(status, std::string("hbx_gcr: ") + hbx_status_string(status));
+  return HBX_OK;
+}
+
+int hbx_gcr(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info, void *stream) {
+  if (!h || !b || !u) return fail(HBX_ERR_INVALID, "hbx_gcr: NULL argument");
+  cudaStream_t us = (cudaStream_t)stream;
+  HBX_CUDA(cudaEventRecord(h->ev2, us));
+  HBX_CUDA(cudaStreamWaitEvent(h->stream, h->ev2, 0));
+  int st = gcr_dev(h, b, u, opts, info);
+  cudaEventRecord(h->ev2, h->stream);
+  cudaStreamWaitEvent(us, h->ev2, 0);
+  return st;
+}
+
+int hbx_gcr_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info) {
+  if (!h || !b || !u) return fail(HBX_ERR_INVALID, "hbx_gcr_host: NULL argument");
+  int st = ensure_solver(h, 0);
+  if (st != HBX_OK) return st;
+  const size_t n = (size_t)h->plan.nd, bytes = n * sizeof(double);
+  double *db = h->d_work + 6 * n, *du = h->d_work + 7 * n;
+  cudaStream_t s = h->stream;
+  HBX_CUDA(cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, s));
+  HBX_CUDA(cudaMemcpyAsync(du, u, bytes, cudaMemcpyHostToDevice, s));
+  st = gcr_dev(h, db, du, opts, info);
+  cudaError_t e = cudaMemcpyAsync(u, du, bytes, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "hbx_gcr_host copy-out");
   return st;
 }
 

@@ -145,6 +145,19 @@ cudaError_t bt_launch_init(int count, const double *dots, double tol, int max_it
                            int *any_active, cudaStream_t s);
 cudaError_t bt_launch_step(const BtStep &a, cudaStream_t s);
 
+// GCR(m) (hbx_gcr.cu): dot products of up to kMaxDots vector pairs per
+// launch (compensated per-block partials part[blocks][kMaxDots][2], summed
+// in block order into out[k]); the restart length is at most kMaxDots.
+constexpr int kMaxDots = 64;
+int gcr_dot_blocks(size_t n);
+cudaError_t gcr_launch_dots(int k, const double *const *x, const double *const *y, size_t n, double *part,
+                            double *out, cudaStream_t s);
+cudaError_t gcr_launch_alpha(const double *dots, int ik, double *capap, double *alpha, cudaStream_t s);
+cudaError_t gcr_launch_step(size_t n, const double *alpha, const double *p, const double *q, double *u, double *r,
+                            cudaStream_t s);
+cudaError_t gcr_launch_orth(size_t n, int k, int inew, const double *dots, const double *capap, double *beta,
+                            double *p, double *ap, cudaStream_t s);
+
 // Static scratch of hbx_matvec_noalloc (hbx_kernels.cu): 256 bytes of
 // barrier words, then room for kNoallocZbuMax zbu doubles.
 constexpr size_t kNoallocScratchBytes = size_t(1) << 20;
@@ -218,6 +231,11 @@ struct hbx_hmat {
   double *d_refine = nullptr;     // mixed-precision solve: outer residual and correction (2*nd)
   float *d_f32 = nullptr;         // FP32 engines: x, p, t (3*nd) and zbu (zbu_len) rounded to float
   int hist_cap = 0;
+  // GCR(m) workspace: r, spare, p[m], Ap[m] (nd each); scalars: capap[kMaxDots],
+  // alpha, beta[kMaxDots], dots[kMaxDots]; per-block partials; pinned readback
+  double *d_gcr = nullptr;
+  int gcr_m = 0;
+  double *d_gcrs = nullptr, *d_gcrpart = nullptr, *h_gcr = nullptr;
   // captured iteration batch
   cudaGraphExec_t graph = nullptr;
   int graph_batch = 0;

@@ -74,7 +74,7 @@ class Info(C.Structure):
 
 class SolveOpts(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iter", C.c_int), ("verbose", C.c_int),
-                ("batch", C.c_int), ("reserved0", C.c_int), ("inner_tol", C.c_double),
+                ("batch", C.c_int), ("restart", C.c_int), ("inner_tol", C.c_double),
                 ("reserved", C.c_int * 8)]
 
 
@@ -143,6 +143,8 @@ ENGINE_SYMBOLS = [
     ("hbx_matvec_host", C.c_int, [_VP, _DP, _DP, C.c_int, _DP, _DP]),
     ("hbx_bicgstab", C.c_int, [_VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
     ("hbx_bicgstab_host", C.c_int, [_VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
+    ("hbx_gcr", C.c_int, [_VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
+    ("hbx_gcr_host", C.c_int, [_VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     ("hbx_bicgstab_refined", C.c_int, [_VP, _VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
     ("hbx_bicgstab_refined_host", C.c_int, [_VP, _VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     ("hbx_gradient_host", C.c_int, [_VP, _VP, _DP, _DP, _DP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo),

@@ -220,6 +220,32 @@ class Engine:
             _check(st, "hbx_bicgstab")
         return self._info(si)
 
+    # -- GCR(m) ----------------------------------------------------------------
+    def gcr_host(self, b: np.ndarray, u0: np.ndarray | None = None, tol: float = 1e-8, max_iter: int = 1000,
+                 restart: int = 8, check: bool = True):
+        """GCR(restart) of HACApK_gcrm_lfmtx (m_HACApK_solve.f90:506-571) with
+        host vectors; returns (u, info)."""
+        b = np.ascontiguousarray(b, np.float64)
+        u = np.zeros(self.nd) if u0 is None else np.array(u0, np.float64, copy=True)
+        o = self._opts(tol, max_iter, 0, 0)
+        o.restart = restart
+        si = abi.SolveInfo()
+        st = self.lib.hbx_gcr_host(self._h, abi.dptr(b), abi.dptr(u), C.byref(o), C.byref(si))
+        if check:
+            _check(st, "hbx_gcr_host")
+        return u, self._info(si)
+
+    def gcr_dev(self, b_ptr: int, u_ptr: int, tol: float = 1e-8, max_iter: int = 1000, restart: int = 8,
+                stream: int = 0, check: bool = True) -> dict:
+        o = self._opts(tol, max_iter, 0, 0)
+        o.restart = restart
+        si = abi.SolveInfo()
+        st = self.lib.hbx_gcr(self._h, C.c_void_p(b_ptr), C.c_void_p(u_ptr), C.byref(o), C.byref(si),
+                              C.c_void_p(stream) if stream else None)
+        if check:
+            _check(st, "hbx_gcr")
+        return self._info(si)
+
     def gradient_host(self, adjoint: "Engine", g: np.ndarray, sigma_t: np.ndarray, tol: float = 1e-8,
                       max_iter: int = 1000):
         """dJ/dg for J = 0.5||sigma - sigma_t||^2 with H sigma = g (self holds H,

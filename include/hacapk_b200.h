@@ -163,7 +163,7 @@ typedef struct hbx_solve_opts {
   int max_iter;        /* iteration limit (param[82] in the drop-in)             */
   int verbose;         /* >0: print the residual history like the reference     */
   int batch;           /* iterations per graph replay between host checks (0=8) */
-  int reserved0;
+  int restart;         /* hbx_gcr: restart length m, param(87) (0 = 8; at most 64) */
   double inner_tol;    /* mixed-precision solve: relative residual reduction asked
                           of each inner solve at most (0 = 1e-6)                 */
   int reserved[8];
@@ -291,6 +291,17 @@ int hbx_bicgstab_multi(hbx_hmat *h, hbx_hmat *hm, const double *B, double *U, co
 /* The same with host arrays (copies inside, on an internal stream). */
 int hbx_bicgstab_multi_host(hbx_hmat *h, hbx_hmat *hm, const double *B, double *U, const hbx_solve_opts *opts,
                             hbx_solve_info *info);
+
+/* GCR(m) on device vectors (HACApK_gcrm_lfmtx, m_HACApK_solve.f90:506-571,
+ * which the reference runs on the host only): restarted every opts->restart
+ * steps (param(87)), the stop test ||r||/||b|| < opts->tol after each step,
+ * at most opts->max_iter steps (param(83)).  Each step is one H-matvec
+ * launch and a few vector launches; dot products are compensated and summed
+ * in a fixed order.  u: x0 in, solution out; info->iterations = nstp. */
+int hbx_gcr(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info,
+            void *stream);
+/* The same with host vectors (copies inside). */
+int hbx_gcr_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info);
 
 /* Mixed-precision BiCGSTAB (no counterpart in the reference): FP64
  * iterative refinement around BiCGSTAB on `hl`, an engine created on the same

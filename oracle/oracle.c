@@ -258,3 +258,63 @@ int orc_bicgstab(const stc_HACApK_leafmtxp *st, int nd, double *u, const double 
   free(zt); free(zr); free(zp); free(zkp); free(zakp); free(zkt); free(zakt); free(zshdw); free(wws);
   return nstp;
 }
+
+/* HACApK_gcrm_lfmtx (m_HACApK_solve.f90:506-571): GCR(m) restarted every
+ * mreset steps (param(87)), the product zau = H zu (the Fortran's
+ * HACApK_adot_lfmtx_hyp; any of the oracle's products), the sequential dot
+ * HACApK_dotp_d.  The statement order is the Fortran's, including the
+ * restart: when step `in` fills the last slot, the next direction is written
+ * into slot 1 and then orthogonalized against every slot, slot 1 (the new
+ * vector itself, with the old slot's |A p|^2) included.  u: x0 in / solution
+ * out; hist[0..nstp] receives ||r||/||b||.  Returns nstp. */
+int orc_gcrm(const stc_HACApK_leafmtxp *st, int nd, double *u, const double *b, double eps, int mstep, int mreset,
+             int mv_kind, void *mv_fn, const void *ext_st, int nthreads, double *hist, double *matvec_seconds) {
+  orc_mv mv = {mv_kind, mv_fn, ext_st, nthreads, 0.0, 0};
+  const size_t n = (size_t)nd;
+  if (mreset < 1) mreset = 1;
+  double *zr = calloc(n, 8), *zar = calloc(n, 8), *capap = calloc((size_t)mreset, 8);
+  double *zp = calloc(n * (size_t)mreset, 8), *zap = calloc(n * (size_t)mreset, 8);
+  double *wws = calloc(n > 0 ? n : 1, 8);
+  int in = 0, nstp = 0;
+  const double bnorm = sqrt(dotp_d(nd, b, b));
+  memset(zar, 0, n * 8);
+  mv_apply(&mv, zar, st, u, wws);
+  for (int i = 0; i < nd; i++) zr[i] = b[i] - zar[i];
+  memcpy(zp, zr, n * 8);
+  double zrnorm2 = dotp_d(nd, zr, zr), zrnorm = sqrt(zrnorm2);
+  if (hist) hist[0] = zrnorm / bnorm;
+  if (!(zrnorm / bnorm < eps)) {
+    memset(zap, 0, n * 8);
+    mv_apply(&mv, zap, st, zp, wws);
+    for (in = 1; in <= mstep; in++) {
+      const int ik = (in - 1) % mreset + 1;
+      const double *zq = zap + n * (size_t)(ik - 1);
+      const double znom = dotp_d(nd, zq, zr);
+      capap[ik - 1] = dotp_d(nd, zq, zq);
+      const double alpha = znom / capap[ik - 1];
+      const double *pk = zp + n * (size_t)(ik - 1);
+      for (int i = 0; i < nd; i++) u[i] = u[i] + alpha * pk[i];
+      for (int i = 0; i < nd; i++) zr[i] = zr[i] - alpha * zq[i];
+      zrnorm2 = dotp_d(nd, zr, zr);
+      zrnorm = sqrt(zrnorm2);
+      if (hist) hist[in] = zrnorm / bnorm;
+      nstp = in;
+      if (zrnorm / bnorm < eps || in == mstep) break;
+      memset(zar, 0, n * 8);
+      mv_apply(&mv, zar, st, zr, wws);
+      const int ikn = in % mreset + 1;
+      double *pn = zp + n * (size_t)(ikn - 1), *apn = zap + n * (size_t)(ikn - 1);
+      memcpy(pn, zr, n * 8);
+      memcpy(apn, zar, n * 8);
+      for (int il = 1; il <= ik; il++) {
+        const double *ql = zap + n * (size_t)(il - 1), *pl = zp + n * (size_t)(il - 1);
+        const double beta = -dotp_d(nd, ql, zar) / capap[il - 1];
+        for (int i = 0; i < nd; i++) pn[i] = pn[i] + beta * pl[i];
+        for (int i = 0; i < nd; i++) apn[i] = apn[i] + beta * ql[i];
+      }
+    }
+  }
+  if (matvec_seconds) *matvec_seconds = mv.seconds;
+  free(zr); free(zar); free(capap); free(zp); free(zap); free(wws);
+  return nstp;
+}
