@@ -81,6 +81,12 @@ void free_engine(hbx_hmat *h) {
   cudaFree(h->d_hist);
   cudaFree(h->d_refine);
   cudaFree(h->d_gcr);
+  cudaFree(h->d_pipe);
+  cudaFree(h->d_pstate);
+  cudaFree(h->d_ppart);
+  cudaFree(h->d_phist);
+  if (h->h_pstate) cudaFreeHost(h->h_pstate);
+  if (h->pgraph) cudaGraphExecDestroy(h->pgraph);
   cudaFree(h->d_gcrs);
   cudaFree(h->d_gcrpart);
   if (h->h_gcr) cudaFreeHost(h->h_gcr);
@@ -815,6 +821,180 @@ int hbx_bicgstab_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_o
   return st;
 }
 
+// Pipelined BiCGSTAB of c_hacapk_bicgstab_cax_lfmtx_pipe_ (HACApK_SOLVER_PIPE.c:144-600)
+// on device vectors, on h->stream: three products and k_pipe_init, then
+// batches of steps (k_pipe_a, v = H z, k_pipe_b, t = H w) as one captured
+// graph, the device state read back after each batch.
+static int pipe_graph(hbx_hmat *h, const hbx::PipeVecs &v, int batch) {
+  if (h->pgraph && h->pgraph_batch == batch && h->pgraph_key == v.u) return HBX_OK;
+  if (h->pgraph) {
+    cudaGraphExecDestroy(h->pgraph);
+    h->pgraph = nullptr;
+  }
+  const size_t n = (size_t)h->plan.nd;
+  cudaStream_t s = h->stream;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return HBX_ERR_CUDA;
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < batch && e == cudaSuccess; ++i) {
+    hbx::MatvecArgs av = matvec_args(h, 1.0, v.z, 0.0, nullptr, v.v);
+    av.skip = &h->d_pstate->done;
+    hbx::MatvecArgs at = matvec_args(h, 1.0, v.w, 0.0, nullptr, v.t);
+    at.skip = &h->d_pstate->done;
+    e = hbx::pipe_launch_a(v, n, h->d_pstate, h->d_ppart, s);
+    if (e == cudaSuccess) e = mv_launch(h, av, s);
+    if (e == cudaSuccess) e = hbx::pipe_launch_b(v, n, h->d_pstate, h->d_ppart, h->d_phist, s);
+    if (e == cudaSuccess) e = mv_launch(h, at, s);
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(s, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return HBX_ERR_CUDA;
+  }
+  e = cudaGraphInstantiate(&h->pgraph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    h->pgraph = nullptr;
+    return HBX_ERR_CUDA;
+  }
+  h->pgraph_batch = batch;
+  h->pgraph_key = v.u;
+  return HBX_OK;
+}
+
+static int pipe_dev(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info) {
+  if (int rc = single_rhs(h, "hbx_bicgstab_pipe")) return rc;
+  const double tol = opts ? opts->tol : 1e-8;
+  const int max_iter = opts ? opts->max_iter : 1000;
+  const int verbose = opts ? opts->verbose : 0;
+  const int batch = (opts && opts->batch > 0) ? opts->batch : 8;
+  if (max_iter < 0 || !(tol >= 0.0)) return fail(HBX_ERR_INVALID, "hbx_bicgstab_pipe: bad tol or max_iter");
+  const size_t n = (size_t)h->plan.nd;
+  if (!h->d_pipe) HBX_CUDA(dev_malloc(&h->d_pipe, (size_t)hbx::kPipeVecs * n * sizeof(double)));
+  if (!h->d_pstate) {
+    HBX_CUDA(dev_malloc(&h->d_pstate, sizeof(hbx::PipeState)));
+    HBX_CUDA(cudaMemset(h->d_pstate, 0, sizeof(hbx::PipeState)));
+  }
+  if (!h->h_pstate) HBX_CUDA(cudaHostAlloc(&h->h_pstate, sizeof(hbx::PipeState), cudaHostAllocDefault));
+  if (!h->d_ppart) HBX_CUDA(dev_malloc(&h->d_ppart, (size_t)hbx::gcr_dot_blocks(n) * hbx::kMaxDots * 2 * sizeof(double)));
+  if (h->phist_cap < max_iter + 1) {
+    cudaFree(h->d_phist);
+    h->d_phist = nullptr;
+    h->phist_cap = 0;
+    HBX_CUDA(dev_malloc(&h->d_phist, (size_t)(max_iter + 1) * sizeof(double)));
+    h->phist_cap = max_iter + 1;
+  }
+  double *V = h->d_pipe;
+  hbx::PipeVecs v{b, u, V, V + n, V + 2 * n, V + 3 * n, V + 4 * n, V + 5 * n, V + 6 * n, V + 7 * n, V + 8 * n, V + 9 * n};
+  cudaStream_t s = h->stream;
+  HBX_CUDA(cudaEventRecord(h->ev0, s));
+  // r = b - H u, r0 = r, w = H r, t = H w (HACApK_SOLVER_PIPE.c:283-356)
+  HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, v.r), s));
+  HBX_CUDA(mv_launch(h, matvec_args(h, 1.0, v.r, 0.0, nullptr, v.w), s));
+  HBX_CUDA(mv_launch(h, matvec_args(h, 1.0, v.w, 0.0, nullptr, v.t), s));
+  HBX_CUDA(hbx::pipe_launch_init(v, n, h->d_pstate, h->d_ppart, h->d_phist, tol, max_iter, s));
+  HBX_CUDA(cudaMemcpyAsync(h->h_pstate, h->d_pstate, sizeof(hbx::PipeState), cudaMemcpyDeviceToHost, s));
+  HBX_CUDA(cudaStreamSynchronize(s));
+  const bool use_graph = !h->h_pstate->done && pipe_graph(h, v, batch) == HBX_OK;
+  int launched = 0;
+  double iter_s = 0.0;
+  while (!h->h_pstate->done && launched <= max_iter + batch) {
+    HBX_CUDA(cudaEventRecord(h->ev3, s));
+    if (use_graph) {
+      HBX_CUDA(cudaGraphLaunch(h->pgraph, s));
+    } else {
+      for (int i = 0; i < batch; ++i) {
+        hbx::MatvecArgs av = matvec_args(h, 1.0, v.z, 0.0, nullptr, v.v);
+        av.skip = &h->d_pstate->done;
+        hbx::MatvecArgs at = matvec_args(h, 1.0, v.w, 0.0, nullptr, v.t);
+        at.skip = &h->d_pstate->done;
+        HBX_CUDA(hbx::pipe_launch_a(v, n, h->d_pstate, h->d_ppart, s));
+        HBX_CUDA(mv_launch(h, av, s));
+        HBX_CUDA(hbx::pipe_launch_b(v, n, h->d_pstate, h->d_ppart, h->d_phist, s));
+        HBX_CUDA(mv_launch(h, at, s));
+      }
+    }
+    HBX_CUDA(cudaEventRecord(h->ev4, s));
+    launched += batch;
+    HBX_CUDA(cudaMemcpyAsync(h->h_pstate, h->d_pstate, sizeof(hbx::PipeState), cudaMemcpyDeviceToHost, s));
+    HBX_CUDA(cudaStreamSynchronize(s));
+    float bms = 0.f;
+    cudaEventElapsedTime(&bms, h->ev3, h->ev4);
+    iter_s += bms * 1e-3;
+    int derr = 0;
+    HBX_CUDA(cudaMemcpy(&derr, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (derr) break;
+  }
+  HBX_CUDA(cudaEventRecord(h->ev1, s));
+  const hbx::PipeState S = *h->h_pstate;
+  // true residual ||b - H u||, in v.v (no longer needed)
+  HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, v.v), s));
+  const double *xs[1] = {v.v}, *ys[1] = {v.v};
+  HBX_CUDA(hbx::gcr_launch_dots(1, xs, ys, n, h->d_ppart, h->d_pipe + 8 * n, s));  // into q (free now)
+  double tr2 = 0.0;
+  HBX_CUDA(cudaMemcpyAsync(&tr2, h->d_pipe + 8 * n, sizeof(double), cudaMemcpyDeviceToHost, s));
+  HBX_CUDA(cudaStreamSynchronize(s));
+  int dst = check_device_error(h, s);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  if (info) {
+    std::memset(info, 0, sizeof(*info));
+    info->iterations = S.step;
+    info->status = dst != HBX_OK ? dst : S.status;
+    info->bnorm = S.bnorm;
+    info->relres = S.relres;
+    info->true_relres = S.bnorm > 0 ? std::sqrt(tr2) / S.bnorm : std::sqrt(tr2);
+    info->seconds = ms * 1e-3;
+    info->iter_kernel_seconds = iter_s;
+    info->iter_launches = 4 * launched;
+    info->launches = 4 * launched + 7;  // 3 setup products, init, residual product, two dot kernels
+  }
+  if (verbose > 0) {
+    std::vector<double> hist(S.step + 1, 0.0);
+    cudaMemcpy(hist.data(), h->d_phist, (S.step + 1) * sizeof(double), cudaMemcpyDeviceToHost);
+    std::printf("\n ** pipelined BICG (version 1) (B200 kernels) **\n");
+    std::printf("\nOriginal relative residual norm = %.2e\n", hist[0]);
+    for (int i = 1; i <= S.step; ++i) std::printf(" %d: log10(zrnorm/bnorm)=%.2e\n", i, std::log10(hist[i]));
+    std::printf("       BiCG        = %.5e\n", ms * 1e-3);
+    std::fflush(stdout);
+  }
+  if (dst != HBX_OK) return dst;
+  if (!S.done) return fail(HBX_ERR_NOT_CONVERGED, "hbx_bicgstab_pipe: iteration limit");
+  if (S.status != HBX_OK) return fail(S.status, std::string("hbx_bicgstab_pipe: ") + hbx_status_string(S.status));
+  return HBX_OK;
+}
+
+int hbx_bicgstab_pipe(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info,
+                      void *stream) {
+  if (!h || !b || !u) return fail(HBX_ERR_INVALID, "hbx_bicgstab_pipe: NULL argument");
+  cudaStream_t us = (cudaStream_t)stream;
+  HBX_CUDA(cudaEventRecord(h->ev2, us));
+  HBX_CUDA(cudaStreamWaitEvent(h->stream, h->ev2, 0));
+  int st = pipe_dev(h, b, u, opts, info);
+  cudaEventRecord(h->ev2, h->stream);
+  cudaStreamWaitEvent(us, h->ev2, 0);
+  return st;
+}
+
+int hbx_bicgstab_pipe_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts,
+                           hbx_solve_info *info) {
+  if (!h || !b || !u) return fail(HBX_ERR_INVALID, "hbx_bicgstab_pipe_host: NULL argument");
+  int st = ensure_solver(h, 0);
+  if (st != HBX_OK) return st;
+  const size_t n = (size_t)h->plan.nd, bytes = n * sizeof(double);
+  double *db = h->d_work + 6 * n, *du = h->d_work + 7 * n;
+  cudaStream_t s = h->stream;
+  HBX_CUDA(cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, s));
+  HBX_CUDA(cudaMemcpyAsync(du, u, bytes, cudaMemcpyHostToDevice, s));
+  st = pipe_dev(h, db, du, opts, info);
+  cudaError_t e = cudaMemcpyAsync(u, du, bytes, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "hbx_bicgstab_pipe_host copy-out");
+  return st;
+}
+
 // GCR(m) of HACApK_gcrm_lfmtx (m_HACApK_solve.f90:506-571) on device vectors,
 // on h->stream; the statement order is the Fortran's (section comments).
 static int gcr_dev(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info) {
@@ -1488,8 +1668,12 @@ static int ctl_nrank(const stc_HACApK_lcontrol *ctl) {
   return lpmd[1];
 }
 
-void c_hacapk_bicgstab_cax_lfmtx_gpu_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl, double *u,
-                                      double *b, double *param, int *nd, int *nstp, int *lrtrn) {
+typedef int (*host_solver_fn)(hbx_hmat *, const double *, double *, const hbx_solve_opts *, hbx_solve_info *);
+
+// The legacy device solvers: the engine of st_leafmtxp (made for the call
+// when there is none), param(83) steps, param(91) tolerance, one rank.
+static void legacy_device_solve(host_solver_fn solve, stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl,
+                                double *u, double *b, double *param, int *nd, int *nstp, int *lrtrn) {
   if (lrtrn) *lrtrn = HBX_OK;
   if (!st_leafmtxp || !u || !b || !param || !nd) {
     if (lrtrn) *lrtrn = HBX_ERR_INVALID;
@@ -1512,10 +1696,28 @@ void c_hacapk_bicgstab_cax_lfmtx_gpu_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACA
   o.max_iter = (int)param[82];
   o.verbose = param[0] > 0 ? 1 : 0;
   hbx_solve_info info{};
-  int rc = hbx_bicgstab_host(h, b, u, &o, &info);
+  int rc = solve(h, b, u, &o, &info);
   if (nstp) *nstp = info.iterations;
   if (lrtrn) *lrtrn = rc;
   if (own) release_for(st_leafmtxp);
+}
+
+void c_hacapk_bicgstab_cax_lfmtx_gpu_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl, double *u,
+                                      double *b, double *param, int *nd, int *nstp, int *lrtrn) {
+  legacy_device_solve(hbx_bicgstab_host, st_leafmtxp, st_ctl, u, b, param, nd, nstp, lrtrn);
+}
+
+// The two pipelined versions differ in where the reference overlaps its MPI
+// gathers with the dot products; their arithmetic is the same, and so is the
+// device sequence here (one GPU, no gathers).
+void c_hacapk_bicgstab_cax_lfmtx_pipe_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl, double *u,
+                                       double *b, double *param, int *nd, int *nstp, int *lrtrn) {
+  legacy_device_solve(hbx_bicgstab_pipe_host, st_leafmtxp, st_ctl, u, b, param, nd, nstp, lrtrn);
+}
+
+void c_hacapk_bicgstab_cax_lfmtx_pipe2_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl, double *u,
+                                        double *b, double *param, int *nd, int *nstp, int *lrtrn) {
+  legacy_device_solve(hbx_bicgstab_pipe_host, st_leafmtxp, st_ctl, u, b, param, nd, nstp, lrtrn);
 }
 
 // Host-vector BiCGSTAB with one GPU matvec per product (HACApK_SOLVER.c:254-417).

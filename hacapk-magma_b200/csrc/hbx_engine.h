@@ -51,6 +51,7 @@ struct MatvecArgs {
   uint32_t keep_frac;        // fraction (of 2^16) of each CTA's stream kept in L2 between passes; 0: no hints
   uint32_t stall;            // test hook: the launch's grid barrier waits for one instance more than can
                              // complete, so its bounded waits expire (hbx_debug_stall_next_barrier)
+  const int *skip;           // optional: the launch does nothing while *skip is set (a solver's done flag)
 };
 
 struct BicgArgs {
@@ -158,6 +159,24 @@ cudaError_t gcr_launch_step(size_t n, const double *alpha, const double *p, cons
 cudaError_t gcr_launch_orth(size_t n, int k, int inew, const double *dots, const double *capap, double *beta,
                             double *p, double *ap, cudaStream_t s);
 
+// Pipelined BiCGSTAB (hbx_pipe.cu; HACApK_SOLVER_PIPE.c:144-600).  The state
+// lives on the device so that a batch of steps runs as one captured graph.
+struct PipeState {
+  double alpha, beta, zeta, znorm, bnorm, relres, tol;
+  int step, max_iter, done, status;
+  unsigned ticket;  // last-block counter of the fused reductions
+  int pad;
+};
+struct PipeVecs {
+  const double *b;
+  double *u, *r, *r0, *w, *t, *v, *p, *s, *z, *q, *y;
+};
+constexpr int kPipeVecs = 10;  // r, r0, w, t, v, p, s, z, q, y
+cudaError_t pipe_launch_init(const PipeVecs &v, size_t n, PipeState *st, double *part, double *hist, double tol,
+                             int max_iter, cudaStream_t s);
+cudaError_t pipe_launch_a(const PipeVecs &v, size_t n, PipeState *st, double *part, cudaStream_t s);
+cudaError_t pipe_launch_b(const PipeVecs &v, size_t n, PipeState *st, double *part, double *hist, cudaStream_t s);
+
 // Static scratch of hbx_matvec_noalloc (hbx_kernels.cu): 256 bytes of
 // barrier words, then room for kNoallocZbuMax zbu doubles.
 constexpr size_t kNoallocScratchBytes = size_t(1) << 20;
@@ -236,6 +255,15 @@ struct hbx_hmat {
   double *d_gcr = nullptr;
   int gcr_m = 0;
   double *d_gcrs = nullptr, *d_gcrpart = nullptr, *h_gcr = nullptr;
+  // pipelined BiCGSTAB: vectors (kPipeVecs*nd), device state, pinned copy,
+  // per-block partials, relres history, captured step batch
+  double *d_pipe = nullptr;
+  hbx::PipeState *d_pstate = nullptr, *h_pstate = nullptr;
+  double *d_ppart = nullptr, *d_phist = nullptr;
+  int phist_cap = 0;
+  cudaGraphExec_t pgraph = nullptr;
+  int pgraph_batch = 0;
+  const void *pgraph_key = nullptr;
   // captured iteration batch
   cudaGraphExec_t graph = nullptr;
   int graph_batch = 0;

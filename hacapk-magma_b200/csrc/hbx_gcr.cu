@@ -18,13 +18,10 @@
 
 #include <algorithm>
 
-#include "hbx_device.cuh"
-#include "hbx_engine.h"
+#include "hbx_dots.cuh"
 
 namespace hbx {
 namespace {
-
-constexpr int kDotThreads = 256;
 
 struct DotPairs {
   const double *x[kMaxDots];
@@ -57,16 +54,10 @@ __global__ void __launch_bounds__(kDotThreads) k_dots(DotPairs d, int k, size_t 
 
 // out[j] = the sum of pair j's partials over nblk blocks, in block order
 __global__ void k_dots_total(const double *part, int nblk, int k, double *out) {
-  const int j = blockIdx.x, lane = threadIdx.x;
+  const int j = blockIdx.x;
   if (j >= k) return;
-  Acc2 a{0.0, 0.0};
-  for (int b0 = 0; b0 < nblk; b0 += 32) {
-    const int b = b0 + lane;
-    Acc2 v{0.0, 0.0};
-    if (b < nblk) v = Acc2{part[((size_t)b * kMaxDots + j) * 2], part[((size_t)b * kMaxDots + j) * 2 + 1]};
-    a = acc2_merge(a, warp_merge(v));
-  }
-  if (lane == 0) out[j] = a.s + a.c;
+  const double t = pair_total(part, nblk, j);
+  if (threadIdx.x == 0) out[j] = t;
 }
 
 // dots[0] = q . r, dots[1] = q . q  ->  alpha, capap[ik]
@@ -106,7 +97,7 @@ int vgrid(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
 
 }  // namespace
 
-int gcr_dot_blocks(size_t n) { return (int)std::min<size_t>((n + kDotThreads - 1) / kDotThreads, 148 * 4); }
+int gcr_dot_blocks(size_t n) { return dot_blocks(n); }
 
 cudaError_t gcr_launch_dots(int k, const double *const *x, const double *const *y, size_t n, double *part, double *out,
                             cudaStream_t s) {

@@ -301,6 +301,7 @@ template <int kPrec>
 __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   constexpr bool kF32 = kPrec != kFP64;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
+  if (a.skip && *(volatile const int *)a.skip) return;  // set by an earlier launch: the same on every CTA
   const CtaInfo ci = a.ctas[blockIdx.x];
   const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
   const Smem sm = cta_smem(smem_raw, a.lite + ci.rec_begin, nr);

@@ -145,6 +145,8 @@ ENGINE_SYMBOLS = [
     ("hbx_bicgstab_host", C.c_int, [_VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     ("hbx_gcr", C.c_int, [_VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
     ("hbx_gcr_host", C.c_int, [_VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
+    ("hbx_bicgstab_pipe", C.c_int, [_VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
+    ("hbx_bicgstab_pipe_host", C.c_int, [_VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     ("hbx_bicgstab_refined", C.c_int, [_VP, _VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
     ("hbx_bicgstab_refined_host", C.c_int, [_VP, _VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     ("hbx_gradient_host", C.c_int, [_VP, _VP, _DP, _DP, _DP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo),
@@ -168,6 +170,10 @@ ENGINE_SYMBOLS = [
     ("c_hacapk_bicgstab_cax_lfmtx_gpu_", None,
      [C.POINTER(LeafMtxP), C.POINTER(LControl), _DP, _DP, _DP, _IP, _IP, _IP]),
     ("c_hacapk_bicgstab_cax_lfmtx_flat_", None,
+     [C.POINTER(LeafMtxP), C.POINTER(LControl), _DP, _DP, _DP, _IP, _IP, _IP]),
+    ("c_hacapk_bicgstab_cax_lfmtx_pipe_", None,
+     [C.POINTER(LeafMtxP), C.POINTER(LControl), _DP, _DP, _DP, _IP, _IP, _IP]),
+    ("c_hacapk_bicgstab_cax_lfmtx_pipe2_", None,
      [C.POINTER(LeafMtxP), C.POINTER(LControl), _DP, _DP, _DP, _IP, _IP, _IP]),
 ]
 

@@ -220,6 +220,30 @@ class Engine:
             _check(st, "hbx_bicgstab")
         return self._info(si)
 
+    # -- pipelined BiCGSTAB ----------------------------------------------------
+    def bicgstab_pipe_host(self, b: np.ndarray, u0: np.ndarray | None = None, tol: float = 1e-8,
+                           max_iter: int = 1000, verbose: int = 0, batch: int = 8, check: bool = True):
+        """Pipelined BiCGSTAB (HACApK_SOLVER_PIPE.c:144-600) with host vectors;
+        returns (u, info)."""
+        b = np.ascontiguousarray(b, np.float64)
+        u = np.zeros(self.nd) if u0 is None else np.array(u0, np.float64, copy=True)
+        o = self._opts(tol, max_iter, verbose, batch)
+        si = abi.SolveInfo()
+        st = self.lib.hbx_bicgstab_pipe_host(self._h, abi.dptr(b), abi.dptr(u), C.byref(o), C.byref(si))
+        if check:
+            _check(st, "hbx_bicgstab_pipe_host")
+        return u, self._info(si)
+
+    def bicgstab_pipe_dev(self, b_ptr: int, u_ptr: int, tol: float = 1e-8, max_iter: int = 1000,
+                          verbose: int = 0, batch: int = 8, stream: int = 0, check: bool = True) -> dict:
+        o = self._opts(tol, max_iter, verbose, batch)
+        si = abi.SolveInfo()
+        st = self.lib.hbx_bicgstab_pipe(self._h, C.c_void_p(b_ptr), C.c_void_p(u_ptr), C.byref(o), C.byref(si),
+                                        C.c_void_p(stream) if stream else None)
+        if check:
+            _check(st, "hbx_bicgstab_pipe")
+        return self._info(si)
+
     # -- GCR(m) ----------------------------------------------------------------
     def gcr_host(self, b: np.ndarray, u0: np.ndarray | None = None, tol: float = 1e-8, max_iter: int = 1000,
                  restart: int = 8, check: bool = True):

@@ -303,6 +303,21 @@ int hbx_gcr(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts,
 /* The same with host vectors (copies inside). */
 int hbx_gcr_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info);
 
+/* Pipelined BiCGSTAB on device vectors (c_hacapk_bicgstab_cax_lfmtx_pipe_,
+ * HACApK_SOLVER_PIPE.c:144-600; _pipe2_, :640, is the same arithmetic): the
+ * products of p and s are carried by recurrences, so a step is two H-matvecs
+ * and two fused reduction kernels; batches of opts->batch steps (8 by
+ * default) run as one CUDA graph.  Stop test ||r||/||b|| < opts->tol before
+ * each step, at most opts->max_iter steps.  u: x0 in, solution out (the
+ * reference accumulates the iterate in an uninitialised vector and returns
+ * u unchanged, HACApK_SOLVER_PIPE.c:592).  HBX_ERR_BREAKDOWN when a
+ * denominator of the recurrences is zero or not finite. */
+int hbx_bicgstab_pipe(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info,
+                      void *stream);
+/* The same with host vectors (copies inside). */
+int hbx_bicgstab_pipe_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts,
+                           hbx_solve_info *info);
+
 /* Mixed-precision BiCGSTAB (no counterpart in the reference): FP64
  * iterative refinement around BiCGSTAB on `hl`, an engine created on the same
  * leaf list with hbx_options.precision = HBX_FP32.  Each refinement step
@@ -452,6 +467,14 @@ void c_hacapk_bicgstab_cax_lfmtx_gpu_(stc_HACApK_leafmtxp *st_leafmtxp,
 void c_hacapk_bicgstab_cax_lfmtx_flat_(stc_HACApK_leafmtxp *st_leafmtxp,
                                        stc_HACApK_lcontrol *st_ctl, double *u, double *b,
                                        double *param, int *nd, int *nstp, int *lrtrn);
+/* HACApK_SOLVER_PIPE.c:144 and :640 -- the two pipelined BiCGSTAB versions,
+ * both on hbx_bicgstab_pipe_host (same arguments as above). */
+void c_hacapk_bicgstab_cax_lfmtx_pipe_(stc_HACApK_leafmtxp *st_leafmtxp,
+                                       stc_HACApK_lcontrol *st_ctl, double *u, double *b,
+                                       double *param, int *nd, int *nstp, int *lrtrn);
+void c_hacapk_bicgstab_cax_lfmtx_pipe2_(stc_HACApK_leafmtxp *st_leafmtxp,
+                                        stc_HACApK_lcontrol *st_ctl, double *u, double *b,
+                                        double *param, int *nd, int *nstp, int *lrtrn);
 
 #ifdef __cplusplus
 }

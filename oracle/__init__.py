@@ -50,6 +50,8 @@ def lib() -> C.CDLL:
         L.orc_bicgstab.argtypes = [_VP, C.c_int, _DP, _DP, C.c_double, C.c_int, C.c_int, _VP,
                                    _VP, C.c_int, _DP, _DP]
         L.orc_bicgstab.restype = C.c_int
+        L.orc_bicgstab_pipe.argtypes = L.orc_bicgstab.argtypes
+        L.orc_bicgstab_pipe.restype = C.c_int
         L.orc_gcrm.argtypes = [_VP, C.c_int, _DP, _DP, C.c_double, C.c_int, C.c_int, C.c_int, _VP,
                                _VP, C.c_int, _DP, _DP]
         L.orc_gcrm.restype = C.c_int
@@ -175,6 +177,30 @@ def gcrm(st, b: np.ndarray, u0: np.ndarray | None = None, tol: float = 1e-8, max
         mk = MV_REF
     n = lib().orc_gcrm(_st(st), nd, _d(u), _d(b), tol, max_iter, restart, mk, fn, C.cast(C.byref(cst), _VP),
                        nthreads, _d(hist), C.byref(secs))
+    return u, int(n), hist[: n + 1].copy(), secs.value
+
+
+def bicgstab_pipe(st, b: np.ndarray, u0: np.ndarray | None = None, tol: float = 1e-8, max_iter: int = 1000,
+                  kind: str = "ref", nthreads: int = 0):
+    """Pipelined BiCGSTAB of HACApK_SOLVER_PIPE.c:144-600 on the CPU (the
+    iterate accumulates in u).  kind: 'ref', 'restated', 'omp'.  Returns (u,
+    nstp, hist[0..nstp], matvec_seconds)."""
+    nd = int(b.shape[0])
+    b = np.ascontiguousarray(b, np.float64)
+    u = np.zeros(nd) if u0 is None else np.array(u0, np.float64, copy=True)
+    hist = np.zeros(max_iter + 1)
+    secs = C.c_double(0.0)
+    fn = None
+    cst = _compact(st)
+    if kind == "ref":
+        mk = MV_EXTERNAL
+        fn = C.cast(ref_lib().c_hacapk_adot_body_lfmtx_, C.c_void_p)
+    elif kind == "omp":
+        mk = MV_OMP
+    else:
+        mk = MV_REF
+    n = lib().orc_bicgstab_pipe(_st(st), nd, _d(u), _d(b), tol, max_iter, mk, fn, C.cast(C.byref(cst), _VP),
+                                nthreads, _d(hist), C.byref(secs))
     return u, int(n), hist[: n + 1].copy(), secs.value
 
 

@@ -259,6 +259,95 @@ int orc_bicgstab(const stc_HACApK_leafmtxp *st, int nd, double *u, const double 
   return nstp;
 }
 
+/* Pipelined BiCGSTAB, c_hacapk_bicgstab_cax_lfmtx_pipe_ (HACApK_SOLVER_PIPE.c:144-600;
+ * the second version, _pipe2_ at :640-1148, runs the same arithmetic with its
+ * host gathers moved beside the dot products).  The auxiliary products
+ * s = A p and z = A s are carried by recurrences, so a step takes two products
+ * (v = A z, t = A w).  Statement order and the daxpy / dlascl roundings are
+ * the reference's (y = y + a x; x = c x); the dots are the sequential
+ * HACApK_dotp_d (the reference calls magma_ddot).  The iterate accumulates in
+ * u (x0 in / solution out): the reference adds the corrections to zx, a
+ * device vector it never initialises, and copies back the unchanged u
+ * (:592), so its own output is the initial guess.  hist[0..nstp] receives
+ * ||r||/||b||.  Returns nstp. */
+int orc_bicgstab_pipe(const stc_HACApK_leafmtxp *st, int nd, double *u, const double *b, double eps, int mstep,
+                      int mv_kind, void *mv_fn, const void *ext_st, int nthreads, double *hist,
+                      double *matvec_seconds) {
+  orc_mv mv = {mv_kind, mv_fn, ext_st, nthreads, 0.0, 0};
+  const size_t n = (size_t)nd;
+  double *zr = calloc(n, 8), *zr0 = calloc(n, 8), *zw = calloc(n, 8), *zt = calloc(n, 8), *zv = calloc(n, 8);
+  double *zp = calloc(n, 8), *zs = calloc(n, 8), *zz = calloc(n, 8), *zq = calloc(n, 8), *zy = calloc(n, 8);
+  double *wws = calloc(n > 0 ? n : 1, 8);
+  double alpha, beta = 0.0, zeta = 0.0, zden, znorm, znormold, zrnorm, zwnorm, zsnorm, zznorm;
+  int nstp = 0;
+  const double bnorm = sqrt(dotp_d(nd, b, b));
+  memset(zv, 0, n * 8);
+  mv_apply(&mv, zv, st, u, wws);
+  memcpy(zr, b, n * 8);
+  daxpy(nd, -1.0, zv, zr);
+  memcpy(zr0, zr, n * 8);
+  memset(zw, 0, n * 8);
+  mv_apply(&mv, zw, st, zr, wws);
+  memset(zt, 0, n * 8);
+  mv_apply(&mv, zt, st, zw, wws);
+  znorm = dotp_d(nd, zr, zr);
+  zrnorm = dotp_d(nd, zw, zr);
+  alpha = znorm / zrnorm;
+  zrnorm = sqrt(znorm);
+  if (hist) hist[0] = zrnorm / bnorm;
+  for (int step = 1; step <= mstep; step++) {
+    if (zrnorm / bnorm < eps) break;
+    if (step > 1) {
+      daxpy(nd, -zeta, zs, zp);
+      for (int i = 0; i < nd; i++) zp[i] = zp[i] * beta;
+      daxpy(nd, 1.0, zr, zp);
+      daxpy(nd, -zeta, zz, zs);
+      for (int i = 0; i < nd; i++) zs[i] = zs[i] * beta;
+      daxpy(nd, 1.0, zw, zs);
+      daxpy(nd, -zeta, zv, zz);
+      for (int i = 0; i < nd; i++) zz[i] = zz[i] * beta;
+      daxpy(nd, 1.0, zt, zz);
+    } else {
+      memcpy(zp, zr, n * 8);
+      memcpy(zs, zw, n * 8);
+      memcpy(zz, zt, n * 8);
+    }
+    memcpy(zq, zr, n * 8);
+    daxpy(nd, -alpha, zs, zq);
+    memcpy(zy, zw, n * 8);
+    daxpy(nd, -alpha, zz, zy);
+    zrnorm = dotp_d(nd, zy, zq);
+    zden = dotp_d(nd, zy, zy);
+    zeta = zrnorm / zden;
+    memset(zv, 0, n * 8);
+    mv_apply(&mv, zv, st, zz, wws);
+    daxpy(nd, alpha, zp, u);
+    daxpy(nd, zeta, zq, u);
+    memcpy(zr, zq, n * 8);
+    daxpy(nd, -zeta, zy, zr);
+    memcpy(zw, zt, n * 8);
+    daxpy(nd, -alpha, zv, zw);
+    for (int i = 0; i < nd; i++) zw[i] = zw[i] * -zeta;
+    daxpy(nd, 1.0, zy, zw);
+    znormold = znorm;
+    znorm = dotp_d(nd, zr, zr0);
+    zwnorm = dotp_d(nd, zw, zr0);
+    zsnorm = dotp_d(nd, zs, zr0);
+    zznorm = dotp_d(nd, zz, zr0);
+    zrnorm = dotp_d(nd, zr, zr);
+    beta = (alpha / zeta) * (znorm / znormold);
+    alpha = znorm / (zwnorm + beta * zsnorm - beta * zeta * zznorm);
+    zrnorm = sqrt(zrnorm);
+    nstp = step;
+    if (hist) hist[step] = zrnorm / bnorm;
+    memset(zt, 0, n * 8);
+    mv_apply(&mv, zt, st, zw, wws);
+  }
+  if (matvec_seconds) *matvec_seconds = mv.seconds;
+  free(zr); free(zr0); free(zw); free(zt); free(zv); free(zp); free(zs); free(zz); free(zq); free(zy); free(wws);
+  return nstp;
+}
+
 /* HACApK_gcrm_lfmtx (m_HACApK_solve.f90:506-571): GCR(m) restarted every
  * mreset steps (param(87)), the product zau = H zu (the Fortran's
  * HACApK_adot_lfmtx_hyp; any of the oracle's products), the sequential dot

@@ -7,6 +7,7 @@
 // exactly once, zbu written once before it is read), and returns y = H x.
 // With FP32 or BF16 storage it multiplies the float (bfloat16) factors by
 // the float-rounded vector, as the kernel does, but sums in double.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -393,4 +394,70 @@ extern "C" int emu_matvec_kernel_order_mk(const stc_HACApK_leafmtxp *st, int nd,
 extern "C" int emu_matvec_kernel_order(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, double alpha,
                                        const double *x, double beta, const double *yin, double *y) {
   return emu_matvec_kernel_order_mk(st, nd, num_ctas, -1, alpha, x, beta, yin, y);
+}
+
+// ---- compensated dot products in the device's reduction order -------------
+// The grid of hbx_dots.cuh: min(ceil(n/256), 592) blocks of 256 threads;
+// thread g accumulates elements g, g + G, ... as a Dot2 pair; butterfly merge
+// inside each warp, warps merged in order per block, blocks summed by one
+// warp in chunks of 32 (butterfly-merged), chunks added in order.
+namespace {
+struct A2 {
+  double s, c;
+};
+inline void a2_add(A2 &a, double p) {
+  const double s = a.s + p;
+  const double z = s - a.s;
+  a.c += (a.s - (s - z)) + (p - z);
+  a.s = s;
+}
+inline void a2_dot(A2 &a, double x, double y) {
+  const double p = x * y;
+  const double e = std::fma(x, y, -p);
+  a2_add(a, p);
+  a.c += e;
+}
+inline A2 a2_merge(A2 a, A2 b) {
+  A2 r{a.s, a.c + b.c};
+  a2_add(r, b.s);
+  return r;
+}
+A2 a2_warp(const A2 *in) {
+  A2 v[32], nv[32];
+  for (int l = 0; l < 32; ++l) v[l] = in[l];
+  for (int o = 16; o > 0; o >>= 1) {
+    for (int l = 0; l < 32; ++l) nv[l] = (l & o) ? a2_merge(v[l ^ o], v[l]) : a2_merge(v[l], v[l ^ o]);
+    for (int l = 0; l < 32; ++l) v[l] = nv[l];
+  }
+  return v[0];
+}
+}  // namespace
+
+extern "C" void emu_dots(int k, const double *const *x, const double *const *y, size_t n, double *out) {
+  const size_t nblk = std::min<size_t>((n + 255) / 256, 148 * 4), G = nblk * 256;
+  std::vector<A2> part(nblk);
+  for (int j = 0; j < k; ++j) {
+    for (size_t b = 0; b < nblk; ++b) {
+      A2 wm[8];
+      for (int w = 0; w < 8; ++w) {
+        A2 lanes[32];
+        for (int l = 0; l < 32; ++l) {
+          A2 a{0.0, 0.0};
+          for (size_t i = b * 256 + w * 32 + l; i < n; i += G) a2_dot(a, x[j][i], y[j][i]);
+          lanes[l] = a;
+        }
+        wm[w] = a2_warp(lanes);
+      }
+      A2 t = wm[0];
+      for (int w = 1; w < 8; ++w) t = a2_merge(t, wm[w]);
+      part[b] = t;
+    }
+    A2 a{0.0, 0.0};
+    for (size_t b0 = 0; b0 < nblk; b0 += 32) {
+      A2 lanes[32];
+      for (int l = 0; l < 32; ++l) lanes[l] = b0 + l < nblk ? part[b0 + l] : A2{0.0, 0.0};
+      a = a2_merge(a, a2_warp(lanes));
+    }
+    out[j] = a.s + a.c;
+  }
 }

@@ -34,6 +34,23 @@ def test_iterations_and_residual_match_oracle(gpu, build_libs, level, restart):
     assert np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref) < 1e-5
 
 
+@pytest.mark.parametrize("level,restart", [(3, 8), (4, 3), (5, 8)])
+def test_bitwise_equal_to_the_replay(gpu, build_libs, level, restart):
+    """The device solve against its CPU replay (tests/conftest.py gcr_replay:
+    the kernel-order product, the device's compensated dot order, the
+    kernels' roundings): the same iterations and u bit for bit."""
+    import torch
+    from conftest import gcr_replay
+    from hacapk_b200 import configs
+    from hacapk_b200.engine import Engine
+    H, b = configs.c1(level)
+    E = Engine(H.st, H.nd)
+    u, info = E.gcr_host(b, tol=1e-8, max_iter=1000, restart=restart)
+    num_ctas = torch.cuda.get_device_properties(0).multi_processor_count
+    ur, nr, relr = gcr_replay(H, b, tol=1e-8, max_iter=1000, restart=restart, num_ctas=num_ctas)
+    assert info["iterations"] == nr and np.array_equal(u, ur) and info["relres"] == relr
+
+
 def test_reference_input_file(gpu, build_libs):
     """The reference's own input_10ts.pbf mesh (committed fixture)."""
     import oracle

@@ -156,6 +156,167 @@ def test_oracle_bicgstab_converges(build_libs):
         assert n2 == n and np.array_equal(u2, u)
 
 
+def _gcrm_numpy(st, b, tol, mstep, m):
+    """HACApK_gcrm_lfmtx (m_HACApK_solve.f90:506-571) line by line in numpy:
+    products from the restated matvec, HACApK_dotp_d as a running sum
+    (np.cumsum accumulates in index order), 1-based slots kept as written."""
+    import oracle
+
+    def dotp(x, y):
+        return float(np.cumsum(x * y)[-1])
+
+    nd = b.shape[0]
+    u = np.zeros(nd)
+    zp, zap, capap = np.zeros((m + 1, nd)), np.zeros((m + 1, nd)), np.zeros(m + 1)
+    bnorm = np.sqrt(dotp(b, b))
+    zr = b - oracle.matvec(st, u)
+    zp[1] = zr
+    zrnorm = np.sqrt(dotp(zr, zr))
+    hist = [zrnorm / bnorm]
+    if zrnorm / bnorm < tol:
+        return u, 0, hist
+    zap[1] = oracle.matvec(st, zp[1])
+    for it in range(1, mstep + 1):
+        ik = (it - 1) % m + 1
+        znom = dotp(zap[ik], zr)
+        capap[ik] = dotp(zap[ik], zap[ik])
+        alpha = znom / capap[ik]
+        u = u + alpha * zp[ik]
+        zr = zr - alpha * zap[ik]
+        zrnorm = np.sqrt(dotp(zr, zr))
+        hist.append(zrnorm / bnorm)
+        if zrnorm / bnorm < tol or it == mstep:
+            break
+        zar = oracle.matvec(st, zr)
+        ikn = it % m + 1
+        zp[ikn] = zr
+        zap[ikn] = zar
+        for il in range(1, ik + 1):
+            beta = -dotp(zap[il], zar) / capap[il]
+            zp[ikn] = zp[ikn] + beta * zp[il]
+            zap[ikn] = zap[ikn] + beta * zap[il]
+    return u, it, hist
+
+
+@pytest.mark.parametrize("restart", [1, 3, 8])
+def test_oracle_gcrm_is_the_fortran_loop(build_libs, restart):
+    """The C restatement of GCR(m) against the Fortran loop restated in numpy:
+    the same iterations, bit for bit (restart 1 and 3 exercise the slot-1
+    aliasing at every restart)."""
+    import oracle
+    H = sphere(2)
+    b = np.random.default_rng(11).standard_normal(H.nd)
+    u, n, hist, _ = oracle.gcrm(H.st, b, tol=1e-8, max_iter=400, restart=restart, kind="restated")
+    u2, n2, hist2 = _gcrm_numpy(H.st, b, 1e-8, 400, restart)
+    assert n == n2 and np.array_equal(hist, np.array(hist2)) and np.array_equal(u, u2)
+
+
+def test_oracle_gcrm_converges_monotonically(build_libs):
+    """GCR minimises the residual over its search space, so the recorded
+    residual never grows; the solution meets the tolerance in the true
+    residual; the reference's compiled matvec gives the same iterations."""
+    import oracle
+    from hacapk_b200 import configs
+    H, b = configs.c1(3)
+    u, n, hist, _ = oracle.gcrm(H.st, b, tol=1e-8, max_iter=500, restart=8, kind="restated")
+    assert hist[-1] < 1e-8 and np.all(np.diff(hist) <= 1e-15)
+    assert np.linalg.norm(b - oracle.matvec(H.st, u)) / np.linalg.norm(b) < 1.05e-8
+    if oracle.have_ref():
+        u2, n2, _, _ = oracle.gcrm(H.st, b, tol=1e-8, max_iter=500, restart=8, kind="ref")
+        assert n2 == n and np.array_equal(u2, u)
+    _, n3, _, _ = oracle.gcrm(H.st, b, tol=1e-30, max_iter=4, restart=8, kind="restated")
+    assert n3 == 4
+
+
+def test_oracle_pipe_is_the_reference_loop(build_libs):
+    """The C restatement of the pipelined BiCGSTAB (HACApK_SOLVER_PIPE.c:144-600)
+    against the same loop in numpy (products from the restated matvec,
+    running-sum dots, daxpy / dlascl roundings): bit for bit; it converges
+    in the true residual."""
+    import oracle
+
+    def dotp(x, y):
+        return float(np.cumsum(x * y)[-1])
+
+    H = sphere(2)
+    b = np.random.default_rng(12).standard_normal(H.nd)
+    mv = lambda x: oracle.matvec(H.st, x)
+    u = np.zeros(H.nd)
+    bnorm = np.sqrt(dotp(b, b))
+    r = b + (-1.0) * mv(u)
+    r0 = r.copy()
+    w = mv(r)
+    t = mv(w)
+    znorm = dotp(r, r)
+    alpha = znorm / dotp(w, r)
+    zr = np.sqrt(znorm)
+    beta = zeta = 0.0
+    hist = [zr / bnorm]
+    for step in range(1, 401):
+        if zr / bnorm < 1e-8:
+            break
+        if step > 1:
+            p = (p + (-zeta) * s) * beta + r
+            s, z = (s + (-zeta) * z) * beta + w, (z + (-zeta) * v) * beta + t
+        else:
+            p, s, z = r.copy(), w.copy(), t.copy()
+        q = r + (-alpha) * s
+        y = w + (-alpha) * z
+        zeta = dotp(y, q) / dotp(y, y)
+        v = mv(z)
+        u = (u + alpha * p) + zeta * q
+        r = q + (-zeta) * y
+        w = (t + (-alpha) * v) * (-zeta) + y
+        znormold, znorm = znorm, dotp(r, r0)
+        zw, zs, zz, rr = dotp(w, r0), dotp(s, r0), dotp(z, r0), dotp(r, r)
+        beta = (alpha / zeta) * (znorm / znormold)
+        alpha = znorm / (zw + beta * zs - beta * zeta * zz)
+        zr = np.sqrt(rr)
+        hist.append(zr / bnorm)
+        t = mv(w)
+    u2, n2, hist2, _ = oracle.bicgstab_pipe(H.st, b, tol=1e-8, max_iter=400, kind="restated")
+    assert n2 == len(hist) - 1 and np.array_equal(hist2, np.array(hist)) and np.array_equal(u2, u)
+    assert np.linalg.norm(b - mv(u2)) / np.linalg.norm(b) < 1.05e-8
+    if oracle.have_ref():
+        u3, n3, _, _ = oracle.bicgstab_pipe(H.st, b, tol=1e-8, max_iter=400, kind="ref")
+        assert n3 == n2 and np.array_equal(u3, u2)
+
+
+def test_device_replays_against_the_oracle(build_libs):
+    """The CPU replays of the device GCR(m) and pipelined solvers (kernel-order
+    product, the device's compensated dot order) on C1 L3 / L4: GCR takes the
+    oracle's iteration count; the pipelined solver lands inside the oracle's
+    own spread under 1e-15 product noise; both meet the tolerance in the
+    true residual.  The dot emulation is checked against exact sums."""
+    import math
+    import oracle
+    from conftest import device_dots, gcr_replay, pipe_replay
+    from hacapk_b200 import configs
+    rng = np.random.default_rng(4)
+    for n in (1, 255, 256, 257, 5000, 151552, 200003):
+        x, y = rng.standard_normal(n), rng.standard_normal(n)
+        d = device_dots([(x, y)])[0]
+        # the exact dot, correctly rounded: each product split into p + e
+        # (Veltkamp / Dekker), then one exactly rounded sum of all the parts
+        p = x * y
+        c = 134217729.0
+        xh = x * c - (x * c - x)
+        yh = y * c - (y * c - y)
+        xl, yl = x - xh, y - yh
+        e = ((xh * yh - p) + xh * yl + xl * yh) + xl * yl
+        exact = math.fsum(np.concatenate([p, e]))
+        assert abs(d - exact) <= 2 * math.ulp(exact)
+    for level in (3, 4):
+        H, b = configs.c1(level)
+        tr = lambda u: np.linalg.norm(b - oracle.matvec(H.st, u)) / np.linalg.norm(b)
+        u, n, _ = gcr_replay(H, b, restart=8)
+        _, n_ref, _, _ = oracle.gcrm(H.st, b, restart=8, kind="restated")
+        assert n == n_ref and tr(u) < 1.05e-8
+        u, n, _, st = pipe_replay(H, b)
+        _, n_ref, _, _ = oracle.bicgstab_pipe(H.st, b, kind="restated")
+        assert st == 0 and n_ref - 2 <= n <= n_ref + 1 and tr(u) < 1.05e-8
+
+
 def test_two_body_precision_workload(build_libs):
     """C2 (the precision form's workload) at level 3: the sphere and the
     seeded ellipsoid are disjoint with the stated gap along x, the H-matrix
