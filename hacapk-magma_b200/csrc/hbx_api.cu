@@ -89,7 +89,8 @@ void free_engine(hbx_hmat *h) {
   if (h->pgraph) cudaGraphExecDestroy(h->pgraph);
   cudaFree(h->d_gcrs);
   cudaFree(h->d_gcrpart);
-  if (h->h_gcr) cudaFreeHost(h->h_gcr);
+  if (h->h_gcrs) cudaFreeHost(h->h_gcrs);
+  if (h->ggraph) cudaGraphExecDestroy(h->ggraph);
   cudaFree(h->d_f32);
   cudaFree(h->d_zbum);
   cudaFree(h->d_mrv);
@@ -996,7 +997,49 @@ int hbx_bicgstab_pipe_host(hbx_hmat *h, const double *b, double *u, const hbx_so
 }
 
 // GCR(m) of HACApK_gcrm_lfmtx (m_HACApK_solve.f90:506-571) on device vectors,
-// on h->stream; the statement order is the Fortran's (section comments).
+// on h->stream: r = b - H u, k_gcr_init, A p_0, k_gcr_alpha0, then whole
+// restart cycles (per step: k_gcr_update, A r, k_gcr_proj + k_gcr_orth) as
+// one captured graph, the device state read back after each graph.
+static void gcr_step(hbx_hmat *h, const hbx::GcrVecs &v, int m, int in, cudaStream_t s, cudaError_t &e) {
+  const size_t n = (size_t)h->plan.nd;
+  const int ik = (in - 1) % m, ikn = in % m;
+  if (e == cudaSuccess) e = hbx::gcr_launch_update(v, n, ik, h->d_gcrs, h->d_gcrpart, s);
+  hbx::MatvecArgs a = matvec_args(h, 1.0, v.r, 0.0, nullptr, v.ar);
+  a.skip = &h->d_gcrs->done;
+  if (e == cudaSuccess) e = mv_launch(h, a, s);
+  if (e == cudaSuccess) e = hbx::gcr_launch_orth(v, n, ik, ikn, h->d_gcrs, h->d_gcrpart, s);
+}
+
+static int gcr_graph(hbx_hmat *h, const hbx::GcrVecs &v, int m, int cycles) {
+  if (h->ggraph && h->ggraph_m == m && h->ggraph_cycles == cycles && h->ggraph_key == v.u) return HBX_OK;
+  if (h->ggraph) {
+    cudaGraphExecDestroy(h->ggraph);
+    h->ggraph = nullptr;
+  }
+  cudaStream_t s = h->stream;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return HBX_ERR_CUDA;
+  cudaError_t e = cudaSuccess;
+  for (int in = 1; in <= m * cycles; ++in) gcr_step(h, v, m, in, s, e);
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(s, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return HBX_ERR_CUDA;
+  }
+  e = cudaGraphInstantiate(&h->ggraph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    h->ggraph = nullptr;
+    return HBX_ERR_CUDA;
+  }
+  h->ggraph_m = m;
+  h->ggraph_cycles = cycles;
+  h->ggraph_key = v.u;
+  return HBX_OK;
+}
+
 static int gcr_dev(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info) {
   if (int rc = single_rhs(h, "hbx_gcr")) return rc;
   const double tol = opts ? opts->tol : 1e-8;
@@ -1011,94 +1054,77 @@ static int gcr_dev(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts
     h->gcr_m = 0;
     HBX_CUDA(dev_malloc(&h->d_gcr, (2 + 2 * (size_t)m) * n * sizeof(double)));
     h->gcr_m = m;
-  }
-  if (!h->d_gcrs) HBX_CUDA(dev_malloc(&h->d_gcrs, (3 * (size_t)hbx::kMaxDots + 1) * sizeof(double)));
-  if (!h->d_gcrpart)
-    HBX_CUDA(dev_malloc(&h->d_gcrpart, (size_t)hbx::gcr_dot_blocks(n) * hbx::kMaxDots * 2 * sizeof(double)));
-  if (!h->h_gcr) HBX_CUDA(cudaHostAlloc(&h->h_gcr, 4 * sizeof(double), cudaHostAllocDefault));
-  cudaStream_t s = h->stream;
-  double *zr = h->d_gcr, *zar = zr + n, *zp = zar + n, *zap = zp + (size_t)m * n;
-  double *capap = h->d_gcrs, *alpha = capap + hbx::kMaxDots, *beta = alpha + 1, *dots = beta + hbx::kMaxDots;
-  double *part = h->d_gcrpart;
-  auto P = [&](int k) { return zp + (size_t)k * n; };
-  auto AP = [&](int k) { return zap + (size_t)k * n; };
-  auto dot1 = [&](const double *x, const double *y, double *out_host) -> int {
-    const double *xs[1] = {x}, *ys[1] = {y};
-    HBX_CUDA(hbx::gcr_launch_dots(1, xs, ys, n, part, dots, s));
-    HBX_CUDA(cudaMemcpyAsync(out_host, dots, sizeof(double), cudaMemcpyDeviceToHost, s));
-    HBX_CUDA(cudaStreamSynchronize(s));
-    return HBX_OK;
-  };
-  HBX_CUDA(cudaEventRecord(h->ev0, s));
-  double *hs = h->h_gcr;
-  if (int rc = dot1(b, b, &hs[0])) return rc;
-  const double bnorm = std::sqrt(hs[0]);
-  // zr = b - H u (as b - zar); zp(1) = zr
-  HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, zr), s));
-  HBX_CUDA(cudaMemcpyAsync(P(0), zr, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  if (int rc = dot1(zr, zr, &hs[1])) return rc;
-  double zrnorm = std::sqrt(hs[1]);
-  int launches = 4, nstp = 0, status = HBX_OK;
-  auto relres = [&](double rn) { return bnorm > 0.0 ? rn / bnorm : 0.0; };
-  if (!std::isfinite(zrnorm) || !std::isfinite(bnorm)) {
-    status = HBX_ERR_NONFINITE;
-  } else if (!(relres(zrnorm) < tol) && mstep > 0) {
-    {
-      HBX_CUDA(mv_launch(h, matvec_args(h, 1.0, P(0), 0.0, nullptr, AP(0)), s));  // zap(1) = H zp(1)
-      ++launches;
-      for (int in = 1; in <= mstep; ++in) {
-        const int ik = (in - 1) % m;
-        // alpha = (zq . zr) / (zq . zq), zq = zap(ik); u += alpha zp(ik); zr -= alpha zq
-        const double *xs[2] = {AP(ik), AP(ik)}, *ys[2] = {zr, AP(ik)};
-        HBX_CUDA(hbx::gcr_launch_dots(2, xs, ys, n, part, dots, s));
-        HBX_CUDA(hbx::gcr_launch_alpha(dots, ik, capap, alpha, s));
-        HBX_CUDA(hbx::gcr_launch_step(n, alpha, P(ik), AP(ik), u, zr, s));
-        if (int rc = dot1(zr, zr, &hs[1])) return rc;
-        launches += 7;
-        zrnorm = std::sqrt(hs[1]);
-        nstp = in;
-        if (!std::isfinite(zrnorm)) {
-          status = HBX_ERR_BREAKDOWN;
-          break;
-        }
-        if (relres(zrnorm) < tol || in == mstep) break;
-        // zar = H zr; the next slot holds zr / zar, orthogonalized against
-        // slots 1..ik as they are now (at a restart slot 1 is the new one)
-        HBX_CUDA(mv_launch(h, matvec_args(h, 1.0, zr, 0.0, nullptr, zar), s));
-        const int ikn = in % m;
-        HBX_CUDA(cudaMemcpyAsync(P(ikn), zr, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-        HBX_CUDA(cudaMemcpyAsync(AP(ikn), zar, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-        const double *qx[hbx::kMaxDots], *qy[hbx::kMaxDots];
-        for (int l = 0; l <= ik; ++l) {
-          qx[l] = AP(l);
-          qy[l] = zar;
-        }
-        HBX_CUDA(hbx::gcr_launch_dots(ik + 1, qx, qy, n, part, dots, s));
-        HBX_CUDA(hbx::gcr_launch_orth(n, ik + 1, ikn, dots, capap, beta, zp, zap, s));
-        launches += 5;
-      }
-      if (status == HBX_OK && !(relres(zrnorm) < tol)) status = HBX_ERR_NOT_CONVERGED;
+    if (h->ggraph) {
+      cudaGraphExecDestroy(h->ggraph);
+      h->ggraph = nullptr;
     }
   }
+  if (!h->d_gcrs) {
+    HBX_CUDA(dev_malloc(&h->d_gcrs, sizeof(hbx::GcrState)));
+    HBX_CUDA(cudaMemset(h->d_gcrs, 0, sizeof(hbx::GcrState)));
+  }
+  if (!h->h_gcrs) HBX_CUDA(cudaHostAlloc(&h->h_gcrs, sizeof(hbx::GcrState), cudaHostAllocDefault));
+  if (!h->d_gcrpart)
+    HBX_CUDA(dev_malloc(&h->d_gcrpart, (size_t)hbx::gcr_dot_blocks(n) * hbx::kMaxDots * 2 * sizeof(double)));
+  cudaStream_t s = h->stream;
+  const size_t slots = (size_t)h->gcr_m;  // the workspace holds gcr_m >= m slots of p, then of A p
+  hbx::GcrVecs v{b, u, h->d_gcr, h->d_gcr + n, h->d_gcr + 2 * n, h->d_gcr + (2 + slots) * n};
+  HBX_CUDA(cudaEventRecord(h->ev0, s));
+  // zr = b - H u; zp(1) = zr; the first stop test; zap(1) = H zp(1); alpha
+  HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, v.r), s));
+  HBX_CUDA(hbx::gcr_launch_init(v, n, h->d_gcrs, h->d_gcrpart, tol, mstep, s));
+  hbx::MatvecArgs a0 = matvec_args(h, 1.0, v.p, 0.0, nullptr, v.ap);
+  a0.skip = &h->d_gcrs->done;
+  HBX_CUDA(mv_launch(h, a0, s));
+  HBX_CUDA(hbx::gcr_launch_alpha0(v, n, h->d_gcrs, h->d_gcrpart, s));
+  HBX_CUDA(cudaMemcpyAsync(h->h_gcrs, h->d_gcrs, sizeof(hbx::GcrState), cudaMemcpyDeviceToHost, s));
+  HBX_CUDA(cudaStreamSynchronize(s));
+  // steps per graph: whole cycles, at least 8 steps
+  const int cycles = (8 + m - 1) / m;
+  const bool use_graph = !h->h_gcrs->done && gcr_graph(h, v, m, cycles) == HBX_OK;
+  int launched = 0;
+  while (!h->h_gcrs->done && launched <= mstep + m * cycles) {
+    if (use_graph) {
+      HBX_CUDA(cudaGraphLaunch(h->ggraph, s));
+    } else {
+      cudaError_t e = cudaSuccess;
+      for (int in = 1; in <= m * cycles; ++in) gcr_step(h, v, m, in, s, e);
+      HBX_CUDA(e);
+    }
+    launched += m * cycles;
+    HBX_CUDA(cudaMemcpyAsync(h->h_gcrs, h->d_gcrs, sizeof(hbx::GcrState), cudaMemcpyDeviceToHost, s));
+    HBX_CUDA(cudaStreamSynchronize(s));
+    int derr = 0;
+    HBX_CUDA(cudaMemcpy(&derr, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (derr) break;
+  }
   HBX_CUDA(cudaEventRecord(h->ev1, s));
-  // true residual ||b - H u||
-  HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, zar), s));
-  if (int rc = dot1(zar, zar, &hs[2])) return rc;
+  const hbx::GcrState S = *h->h_gcrs;
+  // true residual ||b - H u|| in A r (free now)
+  HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, v.ar), s));
+  const double *xs[1] = {v.ar}, *ys[1] = {v.ar};
+  double *out = v.p;  // the search directions are no longer needed
+  HBX_CUDA(hbx::gcr_launch_dots(1, xs, ys, n, h->d_gcrpart, out, s));
+  double tr2 = 0.0;
+  HBX_CUDA(cudaMemcpyAsync(&tr2, out, sizeof(double), cudaMemcpyDeviceToHost, s));
+  HBX_CUDA(cudaStreamSynchronize(s));
   int dst = check_device_error(h, s);
   float ms = 0.f;
   cudaEventElapsedTime(&ms, h->ev0, h->ev1);
   if (info) {
     std::memset(info, 0, sizeof(*info));
-    info->iterations = nstp;
-    info->status = dst != HBX_OK ? dst : status;
-    info->bnorm = bnorm;
-    info->relres = relres(zrnorm);
-    info->true_relres = bnorm > 0 ? std::sqrt(hs[2]) / bnorm : std::sqrt(hs[2]);
+    info->iterations = S.step;
+    info->status = dst != HBX_OK ? dst : S.status;
+    info->bnorm = S.bnorm;
+    info->relres = S.relres;
+    info->true_relres = S.bnorm > 0 ? std::sqrt(tr2) / S.bnorm : std::sqrt(tr2);
     info->seconds = ms * 1e-3;
-    info->launches = launches + 3;
+    info->iter_launches = 4 * launched;
+    info->launches = 4 * launched + 7;
   }
   if (dst != HBX_OK) return dst;
-  if (status != HBX_OK) return fail(status, std::string("hbx_gcr: ") + hbx_status_string(status));
+  if (!S.done) return fail(HBX_ERR_NOT_CONVERGED, "hbx_gcr: iteration limit");
+  if (S.status != HBX_OK) return fail(S.status, std::string("hbx_gcr: ") + hbx_status_string(S.status));
   return HBX_OK;
 }
 

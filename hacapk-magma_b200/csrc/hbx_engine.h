@@ -146,18 +146,33 @@ cudaError_t bt_launch_init(int count, const double *dots, double tol, int max_it
                            int *any_active, cudaStream_t s);
 cudaError_t bt_launch_step(const BtStep &a, cudaStream_t s);
 
-// GCR(m) (hbx_gcr.cu): dot products of up to kMaxDots vector pairs per
-// launch (compensated per-block partials part[blocks][kMaxDots][2], summed
-// in block order into out[k]); the restart length is at most kMaxDots.
+// Dot products of up to kMaxDots vector pairs per launch (hbx_gcr.cu;
+// compensated per-block partials part[blocks][kMaxDots][2], summed in block
+// order into out[k]); the GCR restart length is at most kMaxDots.
 constexpr int kMaxDots = 64;
 int gcr_dot_blocks(size_t n);
 cudaError_t gcr_launch_dots(int k, const double *const *x, const double *const *y, size_t n, double *part,
                             double *out, cudaStream_t s);
-cudaError_t gcr_launch_alpha(const double *dots, int ik, double *capap, double *alpha, cudaStream_t s);
-cudaError_t gcr_launch_step(size_t n, const double *alpha, const double *p, const double *q, double *u, double *r,
+
+// GCR(m) (hbx_gcr.cu; m_HACApK_solve.f90:506-571), state on the device.
+struct GcrState {
+  double bnorm, relres, tol, alpha;
+  double capap[kMaxDots], beta[kMaxDots];
+  int step, max_iter, done, status;
+  unsigned ticket;  // last-block counter of the fused reductions
+  int pad;
+};
+struct GcrVecs {
+  const double *b;
+  double *u, *r, *ar;  // ar: A r of the current step
+  double *p, *ap;      // m slots of nd each
+};
+cudaError_t gcr_launch_init(const GcrVecs &v, size_t n, GcrState *st, double *part, double tol, int max_iter,
                             cudaStream_t s);
-cudaError_t gcr_launch_orth(size_t n, int k, int inew, const double *dots, const double *capap, double *beta,
-                            double *p, double *ap, cudaStream_t s);
+cudaError_t gcr_launch_alpha0(const GcrVecs &v, size_t n, GcrState *st, double *part, cudaStream_t s);
+cudaError_t gcr_launch_update(const GcrVecs &v, size_t n, int ik, GcrState *st, double *part, cudaStream_t s);
+cudaError_t gcr_launch_orth(const GcrVecs &v, size_t n, int ik, int ikn, GcrState *st, double *part,
+                            cudaStream_t s);
 
 // Pipelined BiCGSTAB (hbx_pipe.cu; HACApK_SOLVER_PIPE.c:144-600).  The state
 // lives on the device so that a batch of steps runs as one captured graph.
@@ -250,11 +265,15 @@ struct hbx_hmat {
   double *d_refine = nullptr;     // mixed-precision solve: outer residual and correction (2*nd)
   float *d_f32 = nullptr;         // FP32 engines: x, p, t (3*nd) and zbu (zbu_len) rounded to float
   int hist_cap = 0;
-  // GCR(m) workspace: r, spare, p[m], Ap[m] (nd each); scalars: capap[kMaxDots],
-  // alpha, beta[kMaxDots], dots[kMaxDots]; per-block partials; pinned readback
+  // GCR(m): r, A r, p[m], Ap[m] (nd each); device state and its pinned copy;
+  // per-block partials; the captured restart cycle(s)
   double *d_gcr = nullptr;
   int gcr_m = 0;
-  double *d_gcrs = nullptr, *d_gcrpart = nullptr, *h_gcr = nullptr;
+  hbx::GcrState *d_gcrs = nullptr, *h_gcrs = nullptr;
+  double *d_gcrpart = nullptr;
+  cudaGraphExec_t ggraph = nullptr;
+  int ggraph_m = 0, ggraph_cycles = 0;
+  const void *ggraph_key = nullptr;
   // pipelined BiCGSTAB: vectors (kPipeVecs*nd), device state, pinned copy,
   // per-block partials, relres history, captured step batch
   double *d_pipe = nullptr;
