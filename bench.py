@@ -328,14 +328,64 @@ def measure_forms(args, dev, stream):
                     product, checked against central differences in 16
                     random directions;
       batch_c5      C5: 256 uneven bodies in one block-diagonal engine,
-                    against the same bodies solved one after another.
+                    against the same bodies solved one after another;
+      solvers_c1    C1: the reference's other iterative solvers on the GPU
+                    (pipelined BiCGSTAB, GCR(8)), each beside its CPU loop
+                    on every host core.
 
     The H-matrices are filled on the GPU (hbx_fill_leaves)."""
-    out = {}
-    out["precision_c2"] = precision_form(args, dev, stream)
-    out["mrhs_c3"] = mrhs_form(args, dev, stream)
-    out["adjoint_c4"] = adjoint_form(args, dev, stream)
-    out["batch_c5"] = batch_form(args, dev, stream)
+    forms = {"solvers_c1": solvers_form, "precision_c2": precision_form, "mrhs_c3": mrhs_form,
+             "adjoint_c4": adjoint_form, "batch_c5": batch_form}
+    want = getattr(args, "form", "")
+    return {name: fn(args, dev, stream) for name, fn in forms.items() if not want or want == name}
+
+
+def solvers_form(args, dev, stream, level=5):
+    """C1: the pipelined BiCGSTAB (HACApK_SOLVER_PIPE.c:144, :640) and GCR(8)
+    (m_HACApK_solve.f90:506-571) to 1e-8, device vectors (CUDA-event time of
+    the solve) and host vectors (the reference-facing call with its copies,
+    host clock), each beside the same loop on the CPU (the oracle's
+    restatement with the reference's OpenMP product on every host core)."""
+    import oracle
+    import torch
+    from hacapk_b200 import configs
+    from hacapk_b200.engine import Engine
+    s = stream.cuda_stream
+    H, b = configs.c1(level, fill="gpu")
+    n = H.nd
+    E = Engine(H.st, n)
+    bd = torch.from_numpy(b).to(dev)
+    ud = torch.zeros(n, dtype=torch.float64, device=dev)
+    cores = len(os.sched_getaffinity(0))
+    out = {"workload": f"C1: icosphere L{level}, N = {n}, rhs 1+N(0,1e-3^2), to 1e-8", "n": n}
+    runs = (
+        ("bicgstab_pipe", lambda: E.bicgstab_pipe_dev(bd.data_ptr(), ud.data_ptr(), tol=args.tol,
+                                                      max_iter=args.max_iter, stream=s),
+         lambda: E.bicgstab_pipe_host(b, tol=args.tol, max_iter=args.max_iter),
+         lambda: oracle.bicgstab_pipe(H.st, b, tol=args.tol, max_iter=args.max_iter, kind="omp", nthreads=cores)),
+        ("gcr8", lambda: E.gcr_dev(bd.data_ptr(), ud.data_ptr(), tol=args.tol, max_iter=args.max_iter, restart=8,
+                                   stream=s),
+         lambda: E.gcr_host(b, tol=args.tol, max_iter=args.max_iter, restart=8),
+         lambda: oracle.gcrm(H.st, b, tol=args.tol, max_iter=args.max_iter, restart=8, kind="omp",
+                             nthreads=cores)),
+    )
+    for name, dev_solve, host_solve, cpu_solve in runs:
+        best, inf = 1e9, None
+        for _ in range(4):
+            ud.zero_()
+            inf = dev_solve()
+            best = min(best, inf["seconds"])
+        t_host, (u, hinf) = _timed(dev, host_solve)
+        t0 = time.perf_counter()
+        _, n_cpu, hist, _ = cpu_solve()
+        t_cpu = time.perf_counter() - t0
+        out[name] = {"solve_s": best, "e2e_s": t_host, "iterations": inf["iterations"],
+                     "true_relres": hinf["true_relres"], "us_per_step": best / max(inf["iterations"], 1) * 1e6,
+                     "cpu": {"solve_s": t_cpu, "iterations": n_cpu, "cores": cores, "kind": "port",
+                             "relres": float(hist[-1])},
+                     "speedup_e2e_vs_cpu": t_cpu / t_host}
+    E.close()
+    H.close()
     return out
 
 
@@ -648,6 +698,7 @@ def main():
                     help="skip the forms on their configurations (C2 precision, C3 multi-RHS, C4 adjoint, C5 batch)")
     ap.add_argument("--c5-count", type=int, default=256, help="instances of the uneven batch (C5: 256)")
     ap.add_argument("--forms-only", action="store_true", help="only the forms on their configurations")
+    ap.add_argument("--form", default="", help="with --forms-only: only this form (e.g. solvers_c1)")
     ap.add_argument("--profile-matmat", action="store_true",
                     help="only run five 64-RHS tensor-core products (a short command for ncu)")
     ap.add_argument("--precision-level", type=int, default=0,
