@@ -81,6 +81,9 @@ void free_engine(hbx_hmat *h) {
   cudaFree(h->d_hist);
   cudaFree(h->d_refine);
   cudaFree(h->d_gcr);
+  cudaFree(h->d_chunk_inst);
+  cudaFree(h->d_chunk_base);
+  cudaFree(h->d_inst_pre);
   cudaFree(h->d_pipe);
   cudaFree(h->d_pstate);
   cudaFree(h->d_ppart);
@@ -158,6 +161,11 @@ hbx::MatvecArgs matvec_args(hbx_hmat *h, double alpha, const double *x, double b
   a.keep_frac = h->keep_frac;
   a.stall = h->stall_next;  // test hook: one launch only
   h->stall_next = 0;
+  if (h->skip_inactive && h->d_chunk_inst) {
+    a.chunk_inst = h->d_chunk_inst;
+    a.chunk_base = h->d_chunk_base;
+    a.inst_pre = h->d_inst_pre;
+  }
   return a;
 }
 
@@ -218,7 +226,9 @@ const char *hbx_status_string(int status) {
 
 const char *hbx_last_error(void) { return g_last_error.c_str(); }
 
-static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hbx_hmat **out);
+static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hbx_hmat **out,
+                         bool keep_host_tables = false);
+static void release_host_tables(hbx::Plan &P);
 
 int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hbx_hmat **out) {
   return create_engine(st, nd, opt, out);
@@ -234,7 +244,7 @@ int hbx_create_batch(const stc_HACApK_leafmtxp *const *st, const int *nd, int co
   int rc = hbx::combine_leaves(st, nd, count, cl, err);
   if (rc != HBX_OK) return fail(rc, "hbx_create_batch: " + err);
   hbx_hmat *h = nullptr;
-  rc = create_engine(&cl.container, cl.off[count], opt, &h);
+  rc = create_engine(&cl.container, cl.off[count], opt, &h, true);
   if (rc != HBX_OK) return rc;
   h->inst_off = cl.off;
   std::vector<int> rinst((size_t)cl.off[count]);
@@ -248,11 +258,40 @@ int hbx_create_batch(const stc_HACApK_leafmtxp *const *st, const int *nd, int co
     free_engine(h);
     return cuda_fail(e, "hbx_create_batch: instance tables");
   }
+  std::vector<uint32_t> cinst, cbase;
+  const bool table = count < 0xffff && hbx::chunk_instances(h->plan, rinst, cinst, cbase);
+  release_host_tables(h->plan);
+  if (table) {
+    if ((e = dev_malloc(&h->d_chunk_inst, cinst.size() * sizeof(uint32_t))) != cudaSuccess ||
+        (e = dev_malloc(&h->d_chunk_base, cbase.size() * sizeof(uint32_t))) != cudaSuccess ||
+        (e = dev_malloc(&h->d_inst_pre, (count + 1) * sizeof(int))) != cudaSuccess ||
+        (e = cudaMemcpy(h->d_chunk_inst, cinst.data(), cinst.size() * sizeof(uint32_t), cudaMemcpyHostToDevice)) !=
+            cudaSuccess ||
+        (e = cudaMemcpy(h->d_chunk_base, cbase.data(), cbase.size() * sizeof(uint32_t), cudaMemcpyHostToDevice)) !=
+            cudaSuccess) {
+      free_engine(h);
+      return cuda_fail(e, "hbx_create_batch: chunk table");
+    }
+  }
   *out = h;
   return HBX_OK;
 }
 
-static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hbx_hmat **out) {
+static void release_host_tables(hbx::Plan &P) {
+  P.recs.clear();
+  P.recs.shrink_to_fit();
+  P.lite.clear();
+  P.lite.shrink_to_fit();
+  P.blocks.clear();
+  P.blocks.shrink_to_fit();
+  P.pieces.clear();
+  P.pieces.shrink_to_fit();
+}
+
+// keep_host_tables: the host copies of the run records stay (the caller
+// reads them, then calls release_host_tables).
+static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt, hbx_hmat **out,
+                         bool keep_host_tables) {
   if (!out) return fail(HBX_ERR_INVALID, "hbx_create: out is NULL");
   *out = nullptr;
   if (!st) return fail(HBX_ERR_INVALID, "hbx_create: container is NULL");
@@ -382,14 +421,7 @@ static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_option
   if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(cuda_fail(e, "hbx_create sync"));
   // host copies of the records and the packing tables are no longer needed
   h->num_runs = (long long)P.recs.size();
-  h->plan.recs.clear();
-  h->plan.recs.shrink_to_fit();
-  h->plan.lite.clear();
-  h->plan.lite.shrink_to_fit();
-  h->plan.blocks.clear();
-  h->plan.blocks.shrink_to_fit();
-  h->plan.pieces.clear();
-  h->plan.pieces.shrink_to_fit();
+  if (!keep_host_tables) release_host_tables(h->plan);
   h->setup_seconds = now_s() - t0;
   *out = h;
   return HBX_OK;
@@ -1537,6 +1569,13 @@ int hbx_bicgstab_multi_host(hbx_hmat *h, hbx_hmat *hm, const double *B, double *
 // ---- batched BiCGSTAB over the instances of a block-diagonal engine -----------
 namespace {
 
+// HBX_STREAM_ALL=1 makes the batched solves stream every instance's bytes
+// every step (the per-instance chunk skipping off), for comparisons.
+bool skip_disabled() {
+  const char *v = std::getenv("HBX_STREAM_ALL");
+  return v && std::atoi(v) != 0;
+}
+
 cudaError_t bt_matvec(void *ctx, const double *x, double *y, cudaStream_t s) {
   hbx_hmat *h = static_cast<hbx_hmat *>(ctx);
   return mv_launch(h, matvec_args(h, 1.0, x, 0.0, nullptr, y), s);
@@ -1596,15 +1635,22 @@ int hbx_bicgstab_batch(hbx_hmat *h, const double *b, double *u, const hbx_solve_
   a.r = r; a.rh = rh; a.p = p; a.ap = ap; a.t = t; a.at = at; a.u = u; a.dots = dots; a.bnorm = bnorm;
   a.matvec = bt_matvec;
   a.ctx = h;
+  // products inside the steps stream only the chunks of running instances
+  const bool skip = h->d_chunk_inst && !skip_disabled();
+  a.pre = skip ? h->d_inst_pre : nullptr;
   int any = 0, steps = 0, launches = 4;
+  h->skip_inactive = skip ? 1 : 0;
+  cudaError_t le = cudaSuccess;
   for (;;) {
-    HBX_CUDA(cudaMemcpyAsync(&any, h->d_btany, sizeof(int), cudaMemcpyDeviceToHost, s));
-    HBX_CUDA(cudaStreamSynchronize(s));
-    if (!any || steps >= max_iter) break;
-    for (int k = 0; k < batch; ++k) HBX_CUDA(hbx::bt_launch_step(a, s));
+    le = cudaMemcpyAsync(&any, h->d_btany, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (le == cudaSuccess) le = cudaStreamSynchronize(s);
+    if (le != cudaSuccess || !any || steps >= max_iter) break;
+    for (int k = 0; k < batch && le == cudaSuccess; ++k) le = hbx::bt_launch_step(a, s);
     steps += batch;
-    launches += 11 * batch;
+    launches += (skip ? 13 : 11) * batch;
   }
+  h->skip_inactive = 0;
+  HBX_CUDA(le);
   HBX_CUDA(cudaEventRecord(h->ev1, s));
   // the true residual of every instance: ||b - H u|| / ||b||
   HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, r), s));

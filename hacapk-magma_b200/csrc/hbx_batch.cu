@@ -176,7 +176,38 @@ __global__ void k_bt_beta(int count, const double *dots, const double *bnorm, in
 
 int vgrid(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
 
+// pre[k] = active instances below k (count + 1 entries), one block: each
+// thread counts a contiguous share, a block scan of the shares, then each
+// thread writes its share's prefixes.
+constexpr int kPreThreads = 1024;
+__global__ void __launch_bounds__(kPreThreads) k_bt_prefix(int count, const MrScal *s, int *pre) {
+  __shared__ int part[kPreThreads];
+  const int t = threadIdx.x, per = (count + kPreThreads - 1) / kPreThreads;
+  const int k0 = min(count, t * per), k1 = min(count, k0 + per);
+  int c = 0;
+  for (int k = k0; k < k1; ++k) c += s[k].active ? 1 : 0;
+  part[t] = c;
+  __syncthreads();
+  for (int o = 1; o < kPreThreads; o <<= 1) {
+    const int v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = part[t] - c;  // active instances below k0
+  for (int k = k0; k < k1; ++k) {
+    pre[k] = run;
+    run += s[k].active ? 1 : 0;
+  }
+  if (t == kPreThreads - 1) pre[count] = part[t];
+}
+
 }  // namespace
+
+cudaError_t bt_launch_prefix(int count, const MrScal *sc, int *pre, cudaStream_t s) {
+  k_bt_prefix<<<1, kPreThreads, 0, s>>>(count, sc, pre);
+  return cudaGetLastError();
+}
 
 cudaError_t bt_launch_dots(int nq, int count, const int *off, const double *x0, const double *y0, const double *x1,
                            const double *y1, double *out, cudaStream_t s) {
@@ -201,10 +232,12 @@ cudaError_t bt_launch_step(const BtStep &a, cudaStream_t s) {
   const int sg = (a.count + 127) / 128;
   cudaError_t e;
   k_bt_p<<<vgrid(a.n), 256, 0, s>>>(a.n, a.rinst, a.sc, a.r, a.p, a.ap);
+  if (a.pre) k_bt_prefix<<<1, kPreThreads, 0, s>>>(a.count, a.sc, a.pre);
   if ((e = a.matvec(a.ctx, a.p, a.ap, s)) != cudaSuccess) return e;
   k_bt_dots<1><<<a.count, kBt, 0, s>>>(a.off, a.rh, a.ap, nullptr, nullptr, a.dots);
   k_bt_alpha<<<sg, 128, 0, s>>>(a.count, a.dots, a.sc);
   k_bt_t<<<vgrid(a.n), 256, 0, s>>>(a.n, a.rinst, a.sc, a.r, a.ap, a.t);
+  if (a.pre) k_bt_prefix<<<1, kPreThreads, 0, s>>>(a.count, a.sc, a.pre);
   if ((e = a.matvec(a.ctx, a.t, a.at, s)) != cudaSuccess) return e;
   k_bt_dots<2><<<a.count, kBt, 0, s>>>(a.off, a.at, a.t, a.at, a.at, a.dots);
   k_bt_zeta<<<sg, 128, 0, s>>>(a.count, a.dots, a.sc);

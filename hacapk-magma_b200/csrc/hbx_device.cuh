@@ -294,13 +294,26 @@ __device__ __forceinline__ bool grid_wait(const unsigned *gbar, unsigned target,
 // byte `keep` of the CTA's stream are read with the evict_last policy (they
 // stay in L2 for the next pass), the others with evict_first; keep == 0
 // issues plain copies.
+// With `cinst` set (a block-diagonal engine inside a batched solve), a
+// chunk none of whose instances is active is not copied: its full barrier
+// completes on the producer's arrival alone and the consumers read whatever
+// the slot holds (the rows of inactive instances are left undefined).
 struct StreamSrc {
   const uint8_t *src;
   uint32_t bytes, keep;
+  const uint32_t *cinst;  // [K] instance range of each chunk (lo | hi << 16), or null
+  const int *pre;         // prefix counts of active instances
 };
 __device__ __forceinline__ void producer_issue(const StreamSrc &ss, uint32_t K, uint32_t g, uint8_t *ring,
                                                uint64_t *full) {
   const uint32_t s = g % kRingChunks;
+  if (ss.cinst) {
+    const uint32_t e = ss.cinst[g % K], lo = e & 0xffffu, hi = e >> 16;
+    if (lo > hi || ss.pre[hi + 1] == ss.pre[lo]) {
+      mbar_arrive(&full[s]);
+      return;
+    }
+  }
   const uint32_t off = (g % K) << kChunkLog;
   const uint32_t nb = min((uint32_t)kChunkBytes, ss.bytes - off);
   mbar_arrive_expect_tx(&full[s], nb);

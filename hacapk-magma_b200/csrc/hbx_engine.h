@@ -52,6 +52,13 @@ struct MatvecArgs {
   uint32_t stall;            // test hook: the launch's grid barrier waits for one instance more than can
                              // complete, so its bounded waits expire (hbx_debug_stall_next_barrier)
   const int *skip;           // optional: the launch does nothing while *skip is set (a solver's done flag)
+  // optional (block-diagonal engines): chunk g of CTA c covers instances
+  // [lo, hi] = chunk_inst[chunk_base[c] + g] (lo | hi << 16); a chunk none of
+  // whose instances is active (inst_pre: prefix counts of active instances,
+  // count + 1 entries) is not copied, and the rows of inactive instances
+  // come out undefined
+  const uint32_t *chunk_inst, *chunk_base;
+  const int *inst_pre;
 };
 
 struct BicgArgs {
@@ -132,6 +139,7 @@ cudaError_t mr_launch_add(int nd, const int *mask, const double *D, double *U, c
 struct BtStep {
   size_t n;
   int count, max_iter;
+  int *pre;  // optional: prefix counts of active instances, refreshed before each product
   const int *off, *rinst;  // instance row offsets [count + 1], instance of every row
   MrScal *sc;
   int *any_active;
@@ -145,6 +153,7 @@ cudaError_t bt_launch_setup(size_t n, const double *r, double *rh, double *p, do
 cudaError_t bt_launch_init(int count, const double *dots, double tol, int max_iter, MrScal *sc, double *bnorm,
                            int *any_active, cudaStream_t s);
 cudaError_t bt_launch_step(const BtStep &a, cudaStream_t s);
+cudaError_t bt_launch_prefix(int count, const MrScal *sc, int *pre, cudaStream_t s);
 
 // Dot products of up to kMaxDots vector pairs per launch (hbx_gcr.cu;
 // compensated per-block partials part[blocks][kMaxDots][2], summed in block
@@ -231,6 +240,12 @@ struct hbx_hmat {
   std::vector<int> inst_off;    // row offsets, count + 1 entries (empty: one instance)
   int *d_inst_off = nullptr;    // the same on the device
   int *d_rinst = nullptr;       // instance of every row
+  // per-instance stream skipping (hbx_create_batch; MatvecArgs::chunk_inst):
+  // the chunk table, each CTA's first entry, prefix counts of active
+  // instances, and whether products skip inactive instances right now
+  uint32_t *d_chunk_inst = nullptr, *d_chunk_base = nullptr;
+  int *d_inst_pre = nullptr;
+  int skip_inactive = 0;
   double *d_btv = nullptr;      // r, rh, p, ap, t, at (6 nd)
   hbx::MrScal *d_btsc = nullptr;
   double *d_btdbl = nullptr;    // dots [count][2], bnorm [count], true norms [count]

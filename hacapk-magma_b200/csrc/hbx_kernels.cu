@@ -307,7 +307,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   const Smem sm = cta_smem(smem_raw, a.lite + ci.rec_begin, nr);
   const uint64_t t_start = a.prof ? gtimer() : 0;
   uint32_t issued0 = 0;
-  const StreamSrc ss{a.stream + ci.stream_off, ci.stream_bytes, keep_bytes(ci.stream_bytes, a.keep_frac)};
+  const StreamSrc ss{a.stream + ci.stream_off, ci.stream_bytes, keep_bytes(ci.stream_bytes, a.keep_frac),
+                     a.chunk_inst ? a.chunk_inst + a.chunk_base[blockIdx.x] : nullptr, a.inst_pre};
   if (threadIdx.x == kProducerWarp * 32) issued0 = producer_start(ss, 1, sm.ring, sm.full, sm.empty);
   init_cta(sm, a.lite + ci.rec_begin, nr, a.gbar);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;

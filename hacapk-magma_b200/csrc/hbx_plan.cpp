@@ -623,4 +623,54 @@ int combine_leaves(const stc_HACApK_leafmtxp *const *st, const int *nd, int coun
   return HBX_OK;
 }
 
+// The instance range [lo, hi] of every stream chunk of every CTA of a
+// block-diagonal engine (cinst, lo | hi << 16; lo > hi: no run bytes), and
+// each CTA's first entry (cbase).  A run belongs to the instance of its
+// output rows (D, U, merged D+U) or of its columns (P); false when a run's
+// rows or x columns reach into two instances, which a block-diagonal leaf
+// list never gives, and the engine then streams every chunk.
+bool chunk_instances(const Plan &plan, const std::vector<int> &rinst, std::vector<uint32_t> &cinst,
+                            std::vector<uint32_t> &cbase) {
+  const size_t nrow = rinst.size();
+  cinst.clear();
+  cbase.assign(plan.ctas.size(), 0);
+  for (size_t c = 0; c < plan.ctas.size(); ++c) {
+    const CtaInfo &ci = plan.ctas[c];
+    const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
+    cbase[c] = (uint32_t)cinst.size();
+    std::vector<uint32_t> lo(K, 0xffffu), hi(K, 0u);
+    const uint32_t nr = ci.nr_p + ci.nr_d + ci.nr_u;
+    if ((size_t)ci.rec_begin + nr > plan.recs.size()) return false;
+    for (uint32_t r = 0; r < nr; ++r) {
+      const RunRec &rec = plan.recs[ci.rec_begin + r];
+      const Run &hd = rec.hdr;
+      const uint32_t bytes = run_bytes(hd);
+      if (bytes == 0) continue;
+      const uint32_t kind = run_kind(hd);
+      int k = -1;
+      auto same = [&](size_t row0, size_t len) {
+        if (len == 0) return true;
+        if (row0 + len > nrow) return false;
+        if (k < 0) k = rinst[row0];
+        return rinst[row0] == k && rinst[row0 + len - 1] == k;
+      };
+      if (kind != kRunP && !same(hd.out, hd.nrow)) return false;
+      for (uint32_t q = 0; q < hd.nseg; ++q) {
+        const Seg &sg = rec.seg[q];
+        if (kind == kRunU || (kind == kRunDU && (sg.src & kSegZbu))) continue;  // zbu
+        if (!same(sg.src, sg.len)) return false;
+      }
+      if (k < 0) continue;
+      for (uint32_t g = hd.pos >> kChunkLog; g <= (hd.pos + bytes - 1) >> kChunkLog && g < K; ++g) {
+        lo[g] = std::min(lo[g], (uint32_t)k);
+        hi[g] = std::max(hi[g], (uint32_t)k);
+      }
+    }
+    for (uint32_t g = 0; g < K; ++g) cinst.push_back(lo[g] | (hi[g] << 16));
+  }
+  if (cinst.empty()) cinst.push_back(0xffffu);
+  return true;
+}
+
+
 }  // namespace hbx

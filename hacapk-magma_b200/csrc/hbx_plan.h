@@ -274,6 +274,13 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
 // Writes the packed stream of every CTA into `dst` (plan.total_bytes bytes).
 void pack_plan(const stc_HACApK_leafmtxp *st, const Plan &plan, uint8_t *dst);
 
+// Block-diagonal engines: the instance range of every stream chunk of every
+// CTA (cinst[cbase[c] + g] = lo | hi << 16, lo > hi when the chunk holds no
+// run bytes), from the host run records and the instance of every row.
+// False when a run reaches into two instances.
+bool chunk_instances(const Plan &plan, const std::vector<int> &rinst, std::vector<uint32_t> &cinst,
+                     std::vector<uint32_t> &cbase);
+
 // The leaf list of H^T, in host memory owned by the object: a dense leaf
 // (ndl x ndt) becomes its transpose (ndt x ndl); a low-rank leaf U V^T becomes
 // V U^T (the factors swap places, no arithmetic), so the packed H^T streams

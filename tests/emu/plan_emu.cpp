@@ -461,3 +461,54 @@ extern "C" void emu_dots(int k, const double *const *x, const double *const *y, 
     out[j] = a.s + a.c;
   }
 }
+
+// The chunk -> instance-range table of a block-diagonal engine checked
+// against its runs: every chunk a run's bytes touch must list the run's
+// instance.  stats: [chunks, chunks holding one instance, chunks holding
+// none, runs].  Returns the number of violations, or -1 when no table is built.
+extern "C" int emu_chunk_table(const stc_HACApK_leafmtxp *const *st, const int *nd, int count, int num_ctas,
+                               int precision, int merge_keep, long long *stats) {
+  CombinedLeaves cl;
+  std::string err;
+  if (combine_leaves(st, nd, count, cl, err) != 0) return -2;
+  Plan plan;
+  if (make_plan(&cl.container, cl.off[count], num_ctas, plan, err, precision, false, PlanCosts(), merge_keep) != 0)
+    return -3;
+  std::vector<int> rinst((size_t)cl.off[count]);
+  for (int k = 0; k < count; ++k)
+    for (int i = cl.off[k]; i < cl.off[k + 1]; ++i) rinst[i] = k;
+  std::vector<uint32_t> cinst, cbase;
+  if (!chunk_instances(plan, rinst, cinst, cbase)) return -1;
+  int bad = 0;
+  long long runs = 0, one = 0, none = 0, chunks = 0;
+  for (size_t c = 0; c < plan.ctas.size(); ++c) {
+    const CtaInfo &ci = plan.ctas[c];
+    const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
+    chunks += K;
+    for (uint32_t g = 0; g < K; ++g) {
+      const uint32_t e = cinst[cbase[c] + g], lo = e & 0xffffu, hi = e >> 16;
+      one += lo == hi;
+      none += lo > hi;
+    }
+    for (uint32_t r = 0; r < ci.nr_p + ci.nr_d + ci.nr_u; ++r) {
+      const Run &hd = plan.recs[ci.rec_begin + r].hdr;
+      const uint32_t bytes = run_bytes(hd);
+      if (!bytes) continue;
+      ++runs;
+      // the run's instance from first principles: its rows, or for P runs its first column
+      const int k = run_kind(hd) == kRunP ? rinst[plan.recs[ci.rec_begin + r].seg[0].src] : rinst[hd.out];
+      for (uint32_t g = hd.pos >> kChunkLog; g <= (hd.pos + bytes - 1) >> kChunkLog; ++g) {
+        if (g >= K) { ++bad; continue; }
+        const uint32_t e = cinst[cbase[c] + g], lo = e & 0xffffu, hi = e >> 16;
+        if (!(lo <= (uint32_t)k && (uint32_t)k <= hi)) ++bad;
+      }
+    }
+  }
+  if (stats) {
+    stats[0] = chunks;
+    stats[1] = one;
+    stats[2] = none;
+    stats[3] = runs;
+  }
+  return bad;
+}

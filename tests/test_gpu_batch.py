@@ -71,3 +71,24 @@ def test_batch_masks_converged_instances(gpu, build_libs):
     assert infos[2]["iterations"] == 0 and np.all(u[off[2]:off[3]] == 0.0)
     assert all(i["status"] == 0 for i in infos)
     assert min(i["iterations"] for k, i in enumerate(infos) if k != 2) > 0
+
+
+def test_skipping_finished_instances_changes_no_bit(gpu, build_libs, monkeypatch):
+    """Inside the batched steps the products stream only the chunks of
+    instances still running (a per-CTA chunk -> instance-range table built at
+    hbx_create_batch, prefix counts of the active flags before each product).
+    The running instances' arithmetic is untouched, so the solve equals the
+    one that streams every chunk (HBX_STREAM_ALL=1) bit for bit, in every
+    instance's steps and solution."""
+    from hacapk_b200.engine import Engine
+    inst = _instances(24, 4)
+    E = Engine.batch([H for H, _ in inst])
+    b = np.concatenate([bk for _, bk in inst])
+    u1, i1 = E.bicgstab_batch_host(b, tol=1e-8, max_iter=400)
+    monkeypatch.setenv("HBX_STREAM_ALL", "1")
+    u2, i2 = E.bicgstab_batch_host(b, tol=1e-8, max_iter=400)
+    monkeypatch.delenv("HBX_STREAM_ALL")
+    assert [i["iterations"] for i in i1] == [i["iterations"] for i in i2]
+    assert len(set(i["iterations"] for i in i1)) > 3  # instances finish at different steps
+    assert np.array_equal(u1, u2)
+    assert all(i["status"] == 0 and i["true_relres"] < 1.05e-8 for i in i1)

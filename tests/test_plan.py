@@ -503,3 +503,27 @@ def test_merged_du_layout_needs_wider_stages(build_libs):
     print(f"max runs per CTA: 8 KB {split8} -> {merged8}, 16 KB {split16} -> {merged16}")
     assert merged8 == split8
     assert merged16 <= split16 - 5
+
+
+@pytest.mark.parametrize("precision,merge_keep", [(0, 4), (1, -1), (2, -1)])
+def test_batch_chunk_table_covers_every_run(build_libs, precision, merge_keep):
+    """The block-diagonal engine's chunk -> instance-range table (the batched
+    solver's products skip chunks of finished instances with it) lists, for
+    every 32 KB chunk of every CTA stream, each instance whose run bytes the
+    chunk holds (FP64 streams: ~80 % of the chunks hold one instance; the
+    smaller FP32 / BF16 streams share more chunks between instances)."""
+    import ctypes as C
+    from conftest import emu_lib
+    from hacapk_b200 import abi, configs
+    inst = configs.c5(count=24, seed=5, max_level=4)
+    L = emu_lib()
+    k = len(inst)
+    sts = (C.c_void_p * k)(*[C.cast(H.st, C.c_void_p) for H, _ in inst])
+    nds = (C.c_int * k)(*[int(H.nd) for H, _ in inst])
+    stats = (C.c_longlong * 4)()
+    bad = L.emu_chunk_table(sts, nds, k, 148, precision, merge_keep, stats)
+    assert bad == 0
+    chunks, one, none, runs = list(stats)
+    assert runs > 0 and chunks > 0
+    assert one + none <= chunks
+    print(f"precision {precision}: {chunks} chunks, {one} with one instance, {none} empty, {runs} runs")
