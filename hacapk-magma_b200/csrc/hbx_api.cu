@@ -82,6 +82,7 @@ void free_engine(hbx_hmat *h) {
   cudaFree(h->d_refine);
   cudaFree(h->d_gcr);
   cudaFree(h->d_chunk_inst);
+  cudaFree(h->d_rflag);
   cudaFree(h->d_chunk_base);
   cudaFree(h->d_inst_pre);
   cudaFree(h->d_pipe);
@@ -1603,27 +1604,24 @@ int ensure_bt_workspace(hbx_hmat *h, int count) {
 
 }  // namespace
 
-int hbx_bicgstab_batch(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info,
-                       void *stream) {
-  if (!h || !b || !u) return fail(HBX_ERR_INVALID, "hbx_bicgstab_batch: NULL argument");
-  if (int rc = single_rhs(h, "hbx_bicgstab_batch")) return rc;
-  const double tol = opts ? opts->tol : 1e-8;
-  const int max_iter = opts ? opts->max_iter : 1000;
-  const int batch = (opts && opts->batch > 0) ? opts->batch : 8;
-  if (max_iter < 0 || !(tol >= 0.0)) return fail(HBX_ERR_INVALID, "hbx_bicgstab_batch: bad tol or max_iter");
+// The batched BiCGSTAB on h's instances, on stream s.  rtol (device,
+// nullable): a tolerance per instance instead of tol.  true_res: also the
+// true residual of every instance (one more product).  Per-instance results
+// go to info (nullable, `count` entries); returns the first failing status.
+static int batch_dev(hbx_hmat *h, const double *b, double *u, double tol, const double *rtol, int max_iter, int batch,
+                     cudaStream_t s, bool true_res, hbx_solve_info *info) {
   const int count = h->inst_off.empty() ? 1 : (int)h->inst_off.size() - 1;
   int st = ensure_bt_workspace(h, count);
   if (st != HBX_OK) return st;
   const size_t n = (size_t)h->plan.nd;
   double *r = h->d_btv, *rh = r + n, *p = rh + n, *ap = p + n, *t = ap + n, *at = t + n;
   double *dots = h->d_btdbl, *bnorm = dots + 2 * (size_t)count, *tnorm = bnorm + count;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   HBX_CUDA(cudaEventRecord(h->ev0, s));
   // r = b - H u, rh = r, p = Ap = 0; the stop test of every instance
   HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, r), s));
   HBX_CUDA(hbx::bt_launch_setup(n, r, rh, p, ap, s));
   HBX_CUDA(hbx::bt_launch_dots(2, count, h->d_inst_off, r, r, b, b, dots, s));
-  HBX_CUDA(hbx::bt_launch_init(count, dots, tol, max_iter, h->d_btsc, bnorm, h->d_btany, s));
+  HBX_CUDA(hbx::bt_launch_init(count, dots, tol, rtol, max_iter, h->d_btsc, bnorm, h->d_btany, s));
   hbx::BtStep a{};
   a.n = n;
   a.count = count;
@@ -1652,9 +1650,12 @@ int hbx_bicgstab_batch(hbx_hmat *h, const double *b, double *u, const hbx_solve_
   h->skip_inactive = 0;
   HBX_CUDA(le);
   HBX_CUDA(cudaEventRecord(h->ev1, s));
-  // the true residual of every instance: ||b - H u|| / ||b||
-  HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, r), s));
-  HBX_CUDA(hbx::bt_launch_dots(1, count, h->d_inst_off, r, r, nullptr, nullptr, tnorm, s));
+  if (true_res) {
+    // the true residual of every instance: ||b - H u|| / ||b||
+    HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, r), s));
+    HBX_CUDA(hbx::bt_launch_dots(1, count, h->d_inst_off, r, r, nullptr, nullptr, tnorm, s));
+    launches += 2;
+  }
   std::vector<hbx::MrScal> sc(count);
   std::vector<double> hb(2 * (size_t)count);
   HBX_CUDA(cudaMemcpyAsync(sc.data(), h->d_btsc, count * sizeof(hbx::MrScal), cudaMemcpyDeviceToHost, s));
@@ -1675,14 +1676,151 @@ int hbx_bicgstab_batch(hbx_hmat *h, const double *b, double *u, const hbx_solve_
       I.status = stk;
       I.bnorm = bn;
       I.relres = bn > 0.0 ? std::sqrt(sc[k].rr) / bn : 0.0;
-      I.true_relres = bn > 0.0 ? tr / bn : tr;
+      I.true_relres = true_res ? (bn > 0.0 ? tr / bn : tr) : I.relres;
       I.seconds = ms * 1e-3;
       I.iter_launches = steps;
-      I.launches = launches + 2;
+      I.launches = launches;
     }
   }
-  if (worst != HBX_OK) return fail(worst, std::string("hbx_bicgstab_batch: ") + hbx_status_string(worst));
+  return worst;
+}
+
+int hbx_bicgstab_batch(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts, hbx_solve_info *info,
+                       void *stream) {
+  if (!h || !b || !u) return fail(HBX_ERR_INVALID, "hbx_bicgstab_batch: NULL argument");
+  if (int rc = single_rhs(h, "hbx_bicgstab_batch")) return rc;
+  const double tol = opts ? opts->tol : 1e-8;
+  const int max_iter = opts ? opts->max_iter : 1000;
+  const int batch = (opts && opts->batch > 0) ? opts->batch : 8;
+  if (max_iter < 0 || !(tol >= 0.0)) return fail(HBX_ERR_INVALID, "hbx_bicgstab_batch: bad tol or max_iter");
+  const int st = batch_dev(h, b, u, tol, nullptr, max_iter, batch, static_cast<cudaStream_t>(stream), true, info);
+  if (st != HBX_OK) return fail(st, std::string("hbx_bicgstab_batch: ") + hbx_status_string(st));
   return HBX_OK;
+}
+
+// Mixed-precision batched solve: the FP64 residual of every instance on h,
+// the corrections by the batched BiCGSTAB on hl (FP32 or BF16 factors of the
+// same instances), each instance's inner tolerance from its own residual;
+// an instance leaves the outer loop once its FP64 residual meets tol.
+static int batch_refined_dev(hbx_hmat *h, hbx_hmat *hl, const double *b, double *u, const hbx_solve_opts *opts,
+                             hbx_solve_info *info, cudaStream_t s) {
+  if (int rc = single_rhs(h, "hbx_bicgstab_batch_refined")) return rc;
+  if (int rc = single_rhs(hl, "hbx_bicgstab_batch_refined")) return rc;
+  const double tol = opts ? opts->tol : 1e-8;
+  const int max_iter = opts ? opts->max_iter : 1000;
+  const int batch = (opts && opts->batch > 0) ? opts->batch : 8;
+  const double floor_tol = (opts && opts->inner_tol > 0.0) ? opts->inner_tol : 1e-6;
+  if (max_iter < 0 || !(tol >= 0.0)) return fail(HBX_ERR_INVALID, "hbx_bicgstab_batch_refined: bad tol or max_iter");
+  const int count = h->inst_off.empty() ? 1 : (int)h->inst_off.size() - 1;
+  int st = ensure_bt_workspace(h, count);
+  if (st != HBX_OK) return st;
+  const size_t n = (size_t)h->plan.nd;
+  if (!hl->d_refine) HBX_CUDA(dev_malloc(&hl->d_refine, 2 * n * sizeof(double)));
+  double *r = hl->d_refine, *d = hl->d_refine + n;
+  // per-instance flags and inner tolerances (after the five per-instance
+  // doubles of h's batch scalars, a free tail is not guaranteed: own buffer)
+  if (!h->d_rflag) HBX_CUDA(dev_malloc(&h->d_rflag, (size_t)count * (sizeof(int) + sizeof(double)) + 16));
+  int *d_flag = reinterpret_cast<int *>(h->d_rflag);
+  double *d_itol = reinterpret_cast<double *>(reinterpret_cast<char *>(h->d_rflag) +
+                                              ((size_t)count * sizeof(int) + 15) / 16 * 16);
+  double *dots = h->d_btdbl;  // [count]: per-instance dots of the outer loop
+  cudaEventRecord(h->ev2, s);
+  std::vector<double> bb(count), rr(count), rel(count, 0.0), itol(count);
+  std::vector<int> flag(count), inner(count, 0), status(count, HBX_ERR_NOT_CONVERGED), outer_k(count, 0);
+  HBX_CUDA(hbx::bt_launch_dots(1, count, h->d_inst_off, b, b, nullptr, nullptr, dots, s));
+  HBX_CUDA(cudaMemcpyAsync(bb.data(), dots, count * sizeof(double), cudaMemcpyDeviceToHost, s));
+  HBX_CUDA(cudaStreamSynchronize(s));
+  std::vector<hbx_solve_info> ii(count);
+  int outer = 0, launches = 1;
+  for (;;) {
+    HBX_CUDA(mv_launch(h, matvec_args(h, -1.0, u, 1.0, b, r), s));
+    HBX_CUDA(hbx::bt_launch_dots(1, count, h->d_inst_off, r, r, nullptr, nullptr, dots, s));
+    HBX_CUDA(cudaMemcpyAsync(rr.data(), dots, count * sizeof(double), cudaMemcpyDeviceToHost, s));
+    HBX_CUDA(cudaStreamSynchronize(s));
+    launches += 2;
+    int active = 0;
+    for (int k = 0; k < count; ++k) {
+      const double bn = std::sqrt(bb[k]);
+      rel[k] = bn > 0.0 ? std::sqrt(rr[k]) / bn : std::sqrt(rr[k]);
+      flag[k] = 0;
+      if (status[k] != HBX_ERR_NOT_CONVERGED) continue;  // finished or failed earlier
+      if (!std::isfinite(rel[k])) status[k] = std::isfinite(bb[k]) ? HBX_ERR_BREAKDOWN : HBX_ERR_NONFINITE;
+      else if (rel[k] < tol) status[k] = HBX_OK;
+      else if (inner[k] < max_iter && outer < 64) {
+        flag[k] = 1;
+        itol[k] = std::max(floor_tol, 0.5 * tol / rel[k]);
+        ++active;
+      }
+      outer_k[k] = outer;
+    }
+    if (!active) break;
+    HBX_CUDA(cudaMemcpyAsync(d_flag, flag.data(), count * sizeof(int), cudaMemcpyHostToDevice, s));
+    HBX_CUDA(cudaMemcpyAsync(d_itol, itol.data(), count * sizeof(double), cudaMemcpyHostToDevice, s));
+    HBX_CUDA(hbx::bt_launch_mask(n, h->d_rinst, d_flag, r, s));
+    HBX_CUDA(cudaMemsetAsync(d, 0, n * sizeof(double), s));
+    int left = 0;
+    for (int k = 0; k < count; ++k)
+      if (flag[k]) left = std::max(left, max_iter - inner[k]);
+    const int ist = batch_dev(hl, r, d, tol, d_itol, left, batch, s, false, ii.data());
+    if (ist != HBX_OK && ist != HBX_ERR_NOT_CONVERGED && ist != HBX_ERR_BREAKDOWN) return fail(ist, "hbx_bicgstab_batch_refined: inner solve");
+    for (int k = 0; k < count; ++k) {
+      if (!flag[k]) continue;
+      inner[k] += ii[k].iterations;
+      if (ii[k].iterations == 0 && ii[k].status != HBX_OK) status[k] = ii[k].status;  // no progress possible
+    }
+    launches += ii[0].launches + 1;
+    HBX_CUDA(hbx::launch_axpy(1.0, d, u, n, s));
+    ++outer;
+  }
+  cudaEventRecord(h->ev3, s);
+  HBX_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev2, h->ev3);
+  int worst = HBX_OK;
+  for (int k = 0; k < count; ++k) {
+    if (status[k] != HBX_OK && worst == HBX_OK) worst = status[k];
+    if (info) {
+      hbx_solve_info &I = info[k];
+      std::memset(&I, 0, sizeof(I));
+      I.iterations = inner[k];
+      I.outer = outer_k[k];
+      I.status = status[k];
+      I.bnorm = std::sqrt(bb[k]);
+      I.relres = rel[k];
+      I.true_relres = rel[k];
+      I.seconds = ms * 1e-3;
+      I.launches = launches;
+    }
+  }
+  if ((st = check_device_error(h, s)) != HBX_OK) return st;
+  if (worst != HBX_OK) return fail(worst, std::string("hbx_bicgstab_batch_refined: ") + hbx_status_string(worst));
+  return HBX_OK;
+}
+
+int hbx_bicgstab_batch_refined(hbx_hmat *h, hbx_hmat *hl, const double *b, double *u, const hbx_solve_opts *opts,
+                               hbx_solve_info *info, void *stream) {
+  if (!h || !hl || !b || !u) return fail(HBX_ERR_INVALID, "hbx_bicgstab_batch_refined: NULL argument");
+  if (h->plan.nd != hl->plan.nd || h->inst_off != hl->inst_off || h->device != hl->device)
+    return fail(HBX_ERR_INVALID, "hbx_bicgstab_batch_refined: h and hl must hold the same instances on one device");
+  return batch_refined_dev(h, hl, b, u, opts, info, static_cast<cudaStream_t>(stream));
+}
+
+int hbx_bicgstab_batch_refined_host(hbx_hmat *h, hbx_hmat *hl, const double *b, double *u, const hbx_solve_opts *opts,
+                                    hbx_solve_info *info) {
+  if (!h || !hl || !b || !u) return fail(HBX_ERR_INVALID, "hbx_bicgstab_batch_refined_host: NULL argument");
+  const size_t bytes = (size_t)h->plan.nd * sizeof(double);
+  double *dv = nullptr;
+  HBX_CUDA(dev_malloc(&dv, 2 * bytes));
+  cudaStream_t s = h->stream;
+  cudaError_t e = cudaMemcpyAsync(dv, b, bytes, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dv + h->plan.nd, u, bytes, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) { cudaFree(dv); return cuda_fail(e, "hbx_bicgstab_batch_refined_host upload"); }
+  int st = hbx_bicgstab_batch_refined(h, hl, dv, dv + h->plan.nd, opts, info, s);
+  e = cudaMemcpyAsync(u, dv + h->plan.nd, bytes, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(dv);
+  if (e != cudaSuccess) return cuda_fail(e, "hbx_bicgstab_batch_refined_host download");
+  return st;
 }
 
 int hbx_bicgstab_batch_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts,

@@ -59,8 +59,8 @@ __global__ void k_bt_setup(size_t n, const double *r, double *rh, double *p, dou
 }
 
 // rho = rh.r = r.r, bnorm; an instance runs while ||r||/||b|| >= tol
-__global__ void k_bt_init(int count, const double *dots /*[k][2]: r.r, b.b*/, double tol, int max_iter, MrScal *s,
-                          double *bnorm, int *any_active) {
+__global__ void k_bt_init(int count, const double *dots /*[k][2]: r.r, b.b*/, double tol, const double *rtol,
+                          int max_iter, MrScal *s, double *bnorm, int *any_active) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= count) return;
   const double rr = dots[2 * k], bb = dots[2 * k + 1];
@@ -70,6 +70,7 @@ __global__ void k_bt_init(int count, const double *dots /*[k][2]: r.r, b.b*/, do
   q.rho = rr;
   q.rr = rr;
   const double rel = bn > 0.0 ? std::sqrt(rr) / bn : 0.0;
+  if (rtol) tol = rtol[k];  // per-instance tolerance (the inner solves of a refined batch)
   q.rtol = tol;
   q.status = 0;
   if (!isfinite(rel)) q.status = HBX_ERR_BREAKDOWN;
@@ -221,10 +222,21 @@ cudaError_t bt_launch_setup(size_t n, const double *r, double *rh, double *p, do
   return cudaGetLastError();
 }
 
-cudaError_t bt_launch_init(int count, const double *dots, double tol, int max_iter, MrScal *sc, double *bnorm,
-                           int *any_active, cudaStream_t s) {
+cudaError_t bt_launch_init(int count, const double *dots, double tol, const double *rtol, int max_iter, MrScal *sc,
+                           double *bnorm, int *any_active, cudaStream_t s) {
   cudaMemsetAsync(any_active, 0, sizeof(int), s);
-  k_bt_init<<<(count + 127) / 128, 128, 0, s>>>(count, dots, tol, max_iter, sc, bnorm, any_active);
+  k_bt_init<<<(count + 127) / 128, 128, 0, s>>>(count, dots, tol, rtol, max_iter, sc, bnorm, any_active);
+  return cudaGetLastError();
+}
+
+// r[i] = 0 for the rows of instances whose flag is 0
+__global__ void k_bt_mask(size_t n, const int *rinst, const int *flag, double *r) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    if (!flag[rinst[i]]) r[i] = 0.0;
+}
+
+cudaError_t bt_launch_mask(size_t n, const int *rinst, const int *flag, double *r, cudaStream_t s) {
+  k_bt_mask<<<vgrid(n), 256, 0, s>>>(n, rinst, flag, r);
   return cudaGetLastError();
 }
 

@@ -150,8 +150,9 @@ struct BtStep {
 cudaError_t bt_launch_dots(int nq, int count, const int *off, const double *x0, const double *y0, const double *x1,
                            const double *y1, double *out, cudaStream_t s);
 cudaError_t bt_launch_setup(size_t n, const double *r, double *rh, double *p, double *ap, cudaStream_t s);
-cudaError_t bt_launch_init(int count, const double *dots, double tol, int max_iter, MrScal *sc, double *bnorm,
-                           int *any_active, cudaStream_t s);
+cudaError_t bt_launch_init(int count, const double *dots, double tol, const double *rtol, int max_iter, MrScal *sc,
+                           double *bnorm, int *any_active, cudaStream_t s);
+cudaError_t bt_launch_mask(size_t n, const int *rinst, const int *flag, double *r, cudaStream_t s);
 cudaError_t bt_launch_step(const BtStep &a, cudaStream_t s);
 cudaError_t bt_launch_prefix(int count, const MrScal *sc, int *pre, cudaStream_t s);
 
@@ -246,6 +247,7 @@ struct hbx_hmat {
   uint32_t *d_chunk_inst = nullptr, *d_chunk_base = nullptr;
   int *d_inst_pre = nullptr;
   int skip_inactive = 0;
+  void *d_rflag = nullptr;  // refined batch: per-instance flags and inner tolerances
   double *d_btv = nullptr;      // r, rh, p, ap, t, at (6 nd)
   hbx::MrScal *d_btsc = nullptr;
   double *d_btdbl = nullptr;    // dots [count][2], bnorm [count], true norms [count]

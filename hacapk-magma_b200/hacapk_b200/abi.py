@@ -145,6 +145,8 @@ ENGINE_SYMBOLS = [
     ("hbx_bicgstab_host", C.c_int, [_VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     ("hbx_gcr", C.c_int, [_VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
     ("hbx_gcr_host", C.c_int, [_VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
+    ("hbx_bicgstab_batch_refined", C.c_int, [_VP, _VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
+    ("hbx_bicgstab_batch_refined_host", C.c_int, [_VP, _VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     ("hbx_bicgstab_pipe", C.c_int, [_VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),
     ("hbx_bicgstab_pipe_host", C.c_int, [_VP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
     ("hbx_bicgstab_refined", C.c_int, [_VP, _VP, _VP, _VP, C.POINTER(SolveOpts), C.POINTER(SolveInfo), _VP]),

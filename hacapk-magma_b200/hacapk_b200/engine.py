@@ -112,6 +112,33 @@ class Engine:
             _check(st, "hbx_bicgstab_batch")
         return [self._info(infos[j]) for j in range(k)]
 
+    def bicgstab_batch_refined_host(self, low: "Engine", b: np.ndarray, u0: np.ndarray | None = None,
+                                    tol: float = 1e-8, max_iter: int = 1000, inner_tol: float = 0.0, batch: int = 0):
+        """Every instance solved at once to an FP64-verified tol, the
+        corrections on `low` (an FP32 / BF16 batch engine of the same
+        instances); returns (u, [info per instance])."""
+        b = np.ascontiguousarray(b, np.float64)
+        u = np.zeros(self.nd) if u0 is None else np.array(u0, np.float64, copy=True)
+        k = self.info["instances"]
+        infos = (abi.SolveInfo * k)()
+        o = self._opts(tol, max_iter, 0, batch, inner_tol)
+        st = self.lib.hbx_bicgstab_batch_refined_host(self._h, low._h, abi.dptr(b), abi.dptr(u), C.byref(o), infos)
+        if st not in (0, 5, 6):
+            _check(st, "hbx_bicgstab_batch_refined_host")
+        return u, [self._info(infos[j]) for j in range(k)]
+
+    def bicgstab_batch_refined_dev(self, low: "Engine", b_ptr: int, u_ptr: int, tol: float = 1e-8,
+                                   max_iter: int = 1000, inner_tol: float = 0.0, batch: int = 0, stream: int = 0,
+                                   check: bool = True):
+        k = self.info["instances"]
+        infos = (abi.SolveInfo * k)()
+        o = self._opts(tol, max_iter, 0, batch, inner_tol)
+        st = self.lib.hbx_bicgstab_batch_refined(self._h, low._h, C.c_void_p(b_ptr), C.c_void_p(u_ptr), C.byref(o),
+                                                 infos, C.c_void_p(stream) if stream else None)
+        if check:
+            _check(st, "hbx_bicgstab_batch_refined")
+        return [self._info(infos[j]) for j in range(k)]
+
     def close(self):
         if getattr(self, "_h", None):
             self.lib.hbx_destroy(self._h)

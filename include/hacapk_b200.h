@@ -269,6 +269,19 @@ int hbx_bicgstab_batch(hbx_hmat *h, const double *b, double *u, const hbx_solve_
 /* The same with host vectors (copies inside). */
 int hbx_bicgstab_batch_host(hbx_hmat *h, const double *b, double *u, const hbx_solve_opts *opts,
                             hbx_solve_info *info);
+/* Mixed-precision batched solve (the uneven-batch form with FP32 or BF16
+ * factors): h an FP64 batch engine, hl a batch engine over the same
+ * instances with precision HBX_FP32 or HBX_BF16.  Each outer step computes
+ * every instance's FP64 residual on h; instances still above opts->tol get
+ * a correction from the batched BiCGSTAB on hl, each to its own inner
+ * tolerance max(opts->inner_tol (1e-6 when 0), tol / (2 relres)); the others
+ * are masked out (their chunks are not streamed).  info: one entry per
+ * instance (iterations = its inner steps, outer = refinement steps,
+ * true_relres = its last FP64 residual). */
+int hbx_bicgstab_batch_refined(hbx_hmat *h, hbx_hmat *hl, const double *b, double *u, const hbx_solve_opts *opts,
+                               hbx_solve_info *info, void *stream);
+int hbx_bicgstab_batch_refined_host(hbx_hmat *h, hbx_hmat *hl, const double *b, double *u,
+                                    const hbx_solve_opts *opts, hbx_solve_info *info);
 
 /* BiCGSTAB for HBX_NRHS right-hand sides at once (no counterpart in the
  * reference): FP64 iterative refinement around the algorithm of

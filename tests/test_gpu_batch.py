@@ -92,3 +92,25 @@ def test_skipping_finished_instances_changes_no_bit(gpu, build_libs, monkeypatch
     assert len(set(i["iterations"] for i in i1)) > 3  # instances finish at different steps
     assert np.array_equal(u1, u2)
     assert all(i["status"] == 0 and i["true_relres"] < 1.05e-8 for i in i1)
+
+
+@pytest.mark.parametrize("precision,inner_tol", [(1, 0.0), (2, 1e-2)])
+def test_refined_batch_meets_the_fp64_tolerance(gpu, build_libs, precision, inner_tol):
+    """The mixed-precision batched solve (FP32 or BF16 factors for the
+    corrections, FP64 residuals): every instance reaches 1e-8 in the FP64
+    residual recomputed by the oracle, in a few refinement steps."""
+    import oracle
+    from hacapk_b200.engine import Engine
+    inst = _instances(16, 4)
+    Hs = [H for H, _ in inst]
+    E = Engine.batch(Hs)
+    El = Engine.batch(Hs, precision=precision)
+    b = np.concatenate([bk for _, bk in inst])
+    u, infos = E.bicgstab_batch_refined_host(El, b, tol=1e-8, max_iter=1000, inner_tol=inner_tol)
+    off = E.offsets
+    for k, (H, bk) in enumerate(inst):
+        uk = u[off[k]:off[k + 1]]
+        rel = np.linalg.norm(bk - oracle.matvec(H.st, uk)) / np.linalg.norm(bk)
+        assert infos[k]["status"] == 0 and rel < 1.05e-8, (k, infos[k], rel)
+        assert infos[k]["true_relres"] == pytest.approx(rel, rel=1e-3, abs=1e-12)
+        assert 1 <= infos[k]["outer"] <= 8
