@@ -553,9 +553,10 @@ def adjoint_form(args, dev, stream, level=6, ndir=16, step=1e-6):
 
 def batch_form(args, dev, stream):
     """C5: the 256 uneven ellipsoids solved in one block-diagonal engine
-    against the same bodies solved one after another (FP64 each)."""
+    (FP64, and FP32 / BF16 corrections in FP64 refinement) against the same
+    bodies solved one after another (FP64 each)."""
     import torch
-    from hacapk_b200 import configs
+    from hacapk_b200 import abi, configs
     from hacapk_b200.engine import Engine
     s = stream.cuda_stream
     t0 = time.time()
@@ -570,6 +571,22 @@ def batch_form(args, dev, stream):
         return Eb.bicgstab_batch_dev(bb.data_ptr(), ub.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
     t_batch, infos = _timed(dev, batch, reps=2)
     stream_gb = Eb.info["stream_bytes"] / 1e9
+    # the configuration's mixed precision: FP32 (or BF16) factors for the
+    # corrections inside FP64 refinement, one batch engine each
+    refined = {}
+    for name, prec, inner in (("fp32_refined", abi.HBX_FP32, 0.0), ("bf16_refined", abi.HBX_BF16, 1e-2)):
+        El = Engine.batch([Hk for Hk, _ in inst], precision=prec)
+
+        def batch_ref():
+            ub.zero_()
+            return Eb.bicgstab_batch_refined_dev(El, bb.data_ptr(), ub.data_ptr(), tol=args.tol,
+                                                 max_iter=args.max_iter, inner_tol=inner, stream=s)
+        t_ref, rinf = _timed(dev, batch_ref, reps=2)
+        refined[name] = {"solve_s": t_ref, "stream_gb": El.info["stream_bytes"] / 1e9,
+                         "outer": max(i["outer"] for i in rinf), "inner_iterations_max": max(i["iterations"] for i in rinf),
+                         "worst_true_relres": max(i["true_relres"] for i in rinf),
+                         "converged": int(sum(i["status"] == 0 for i in rinf))}
+        El.close()
     Eb.close()
     engines = [(Engine(Hk.st, Hk.nd), torch.from_numpy(bk).to(dev)) for Hk, bk in inst]
     us = [torch.zeros_like(bd) for _, bd in engines]
@@ -588,6 +605,9 @@ def batch_form(args, dev, stream):
            "gpu_fill_s": t_build, "solve_s": t_batch, "one_by_one_s": t_one, "speedup": t_one / t_batch,
            "iterations": [min(its), max(its)], "worst_true_relres": max(i["true_relres"] for i in infos),
            "converged": int(sum(i["status"] == 0 for i in infos))}
+    for name, r in refined.items():
+        r["speedup_vs_one_by_one"] = t_one / r["solve_s"]
+        out[name] = r
     for Hk, _ in inst:
         Hk.close()
     return out
