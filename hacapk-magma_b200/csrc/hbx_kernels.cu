@@ -119,7 +119,7 @@ __device__ __forceinline__ void sync_warp(unsigned *gbar, uint32_t npass, uint32
       return;  // the waits on gdone are bounded too
     }
     const unsigned target = grid_target(sm.rsum[1], k0 + p * kstep + beyond, gridDim.x);
-    grid_arrive(gbar, target);  // fences first: the CTA's zbu stores are visible grid-wide
+    grid_arrive(gbar, target);  // a release: the CTA's zbu stores (before pdone) are visible grid-wide
     if (!grid_wait(gbar, target, tmo)) {
       atomicOr(err, kErrGridBarrier);
       return;
