@@ -673,7 +673,7 @@ __device__ __forceinline__ void run_rows(const RunLite &L, uint32_t stage_s, Rin
   const uint32_t lrow = 16u * min((uint32_t)lane, h - 1u);
   const uint32_t lrow2 = 16u * min((uint32_t)lane + 32u, h - 1u) - lrow;  // second row, relative
   const uint32_t ring_s = smem_u32(R.buf);
-  uint32_t j = (w + NW - L.rot) % NW;
+  uint32_t j = (w + NW - (NW == (uint32_t)kStepWarps ? (uint32_t)L.rot_step : (uint32_t)L.rot)) % NW;
   typename PM::Acc a[U], b[kTwoRows ? U : 1];
   for (; j + (U - 1) * NW < np; j += U * NW) {
     const uint32_t p0 = L.pos + j * pb;

@@ -9,7 +9,14 @@
 //               both H-matvecs, the vector updates and all dot products, with
 //               compensated (Dot2) partial sums reduced in a fixed order.
 //
-// All kernels run one CTA per SM: 16 consumer warps, a bulk-copy producer
+// The file is compiled twice: as itself (k_matvec and the small vector
+// kernels, 16 consumer warps) and with HBX_STEP_TU and HBX_CONSUMER_WARPS=13
+// (k_bicg_setup, k_bicg_iter and the dot kernels): with fewer threads per CTA
+// the step kernel gets the registers it needs without spilling, and its
+// scalar phases synchronise fewer warps (C1 step 121.4 -> 115 us, while the
+// standalone product is fastest with 16).
+//
+// All kernels run one CTA per SM: consumer warps, a bulk-copy producer
 // warp, kGatherWarps gather warps, a grid-barrier warp and a block-sum warp.
 // The producer streams the CTA's packed runs through a shared-memory ring
 // with cp.async.bulk; the consumers take every 16th panel of every run
@@ -26,7 +33,7 @@ namespace hbx {
 namespace {
 
 constexpr int NW = kConsumerWarps;
-constexpr int kConsumerThreads = NW * 32;
+[[maybe_unused]] constexpr int kConsumerThreads = NW * 32;
 
 struct Smem {
   uint8_t *ring;
@@ -100,10 +107,12 @@ __device__ __forceinline__ Smem cta_smem(uint8_t *base, const RunLite *lite, uin
   return s;
 }
 
+#ifndef HBX_STEP_TU
 __device__ __forceinline__ void init_cta(const Smem &s, const RunLite *lite, uint32_t nr, const unsigned *gbar) {
   init_cta_part(s, lite, nr, gbar, 0);
   __syncthreads();
 }
+#endif
 
 // ---- grid-barrier warp: once per pass, after the CTA's P blocks are summed
 // (pdone), arrive on the grid barrier, wait for it and release the U runs
@@ -297,6 +306,7 @@ __device__ __forceinline__ uint32_t keep_bytes(uint32_t stream_bytes, uint32_t k
 
 // kPrec: storage precision of the factors; FP32 and BF16 engines gather the
 // float copies of the vectors.
+#ifndef HBX_STEP_TU
 template <int kPrec>
 __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   constexpr bool kF32 = kPrec != kFP64;
@@ -344,6 +354,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   }
 }
 
+#endif  // !HBX_STEP_TU
+
+#ifdef HBX_STEP_TU
 // ---------------------------------------------------------------- BiCGSTAB
 template <class F>
 __device__ __forceinline__ void for_own_rows(const Atom *atoms, const CtaInfo &ci, F f) {
@@ -758,6 +771,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_dot_partial(BicgArgs a, const d
 }
 
 // y = (float)x: the input of an FP32 engine's matvec.
+#endif  // HBX_STEP_TU
+
+#ifndef HBX_STEP_TU
 __global__ void k_to_float(const double *x, float *y, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     y[i] = (float)x[i];
@@ -769,13 +785,19 @@ __global__ void k_axpy(double a, const double *x, double *y, size_t n) {
     y[i] = fma(a, x[i], y[i]);
 }
 
+#endif  // !HBX_STEP_TU
+
+#ifdef HBX_STEP_TU
 __global__ void k_dot_total(const double *part, int ncta, int slot, double *out) {
   const double v = reduce_slot(part, ncta, slot);
   if (threadIdx.x == 0) *out = v;
 }
 
+#endif  // HBX_STEP_TU
+
 }  // namespace
 
+#ifndef HBX_STEP_TU
 // ---- fixed scratch for hbx_matvec_noalloc -------------------------------
 // One 1 MiB array per device, held by every GPU that loads this library until
 // the process exits: [0, 256) barrier words, [256, end) the zbu segments.
@@ -792,13 +814,10 @@ cudaError_t configure_kernels() {
   if ((e = cudaFuncSetAttribute(k_matvec<kFP64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_matvec<kFP32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_matvec<kBF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(k_bicg_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(k_bicg_iter<kFP64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(k_bicg_iter<kFP32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(k_bicg_iter<kBF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(k_dot_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-  return cudaSuccess;
+  return configure_step_kernels();
 }
+
+#endif  // !HBX_STEP_TU
 
 template <class Args>
 static cudaError_t launch_coop(void (*kern)(Args), const Args &a, int num_ctas, cudaStream_t s) {
@@ -815,9 +834,31 @@ static cudaError_t launch_coop(void (*kern)(Args), const Args &a, int num_ctas, 
   return cudaLaunchKernelEx(&cfg, kern, a);
 }
 
+#ifndef HBX_STEP_TU
 cudaError_t launch_matvec(const MatvecArgs &a, int num_ctas, cudaStream_t s, int precision) {
   if (precision == kBF16) return launch_coop(k_matvec<kBF16>, a, num_ctas, s);
   return precision == kFP32 ? launch_coop(k_matvec<kFP32>, a, num_ctas, s) : launch_coop(k_matvec<kFP64>, a, num_ctas, s);
+}
+
+cudaError_t launch_to_float(const double *x, float *y, size_t n, cudaStream_t s) {
+  k_to_float<<<296, 256, 0, s>>>(x, y, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_axpy(double alpha, const double *x, double *y, size_t n, cudaStream_t s) {
+  k_axpy<<<296, 256, 0, s>>>(alpha, x, y, n);
+  return cudaGetLastError();
+}
+#else
+cudaError_t configure_step_kernels() {
+  const int smem = (int)SharedLayout::bytes;
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_bicg_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_bicg_iter<kFP64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_bicg_iter<kFP32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_bicg_iter<kBF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_dot_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  return cudaSuccess;
 }
 
 cudaError_t launch_bicg_setup(const BicgArgs &a, int num_ctas, cudaStream_t s) {
@@ -831,21 +872,12 @@ cudaError_t launch_bicg_iter(const BicgArgs &a, int num_ctas, cudaStream_t s, in
                             : launch_coop(k_bicg_iter<kFP64>, a, num_ctas, s);
 }
 
-cudaError_t launch_to_float(const double *x, float *y, size_t n, cudaStream_t s) {
-  k_to_float<<<296, 256, 0, s>>>(x, y, n);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_axpy(double alpha, const double *x, double *y, size_t n, cudaStream_t s) {
-  k_axpy<<<296, 256, 0, s>>>(alpha, x, y, n);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_dot(const BicgArgs &a, const double *x, const double *y, int slot, double *out, int num_ctas,
                        cudaStream_t s) {
   k_dot_partial<<<num_ctas, kThreads, SharedLayout::bytes, s>>>(a, x, y, slot);
   k_dot_total<<<1, 32, 0, s>>>(a.part, num_ctas, slot, out);
   return cudaGetLastError();
 }
+#endif  // HBX_STEP_TU
 
 }  // namespace hbx

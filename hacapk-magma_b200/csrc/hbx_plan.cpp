@@ -350,7 +350,7 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
     for (uint32_t a : split) plan.atoms.push_back(atoms[a]);
     for (uint32_t a : merged) plan.atoms.push_back(atoms[a]);
     uint64_t pos = 0;
-    uint32_t rot = 0;
+    uint32_t rot = 0, rot_step = 0;
     auto emit_block = [&](uint32_t bi) -> uint32_t {
       const Block &b = plan.blocks[bi];
       const uint32_t Wp = (b.W + RG - 1) / RG * RG;
@@ -402,11 +402,13 @@ int make_plan(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, Plan &plan, s
         L.npanel = r.npanel;
         L.nrow = (uint8_t)r.nrow;
         L.rot = (uint8_t)r.rot;
+        L.rot_step = (uint16_t)rot_step;
         L.flags = r.flags;
         plan.lite.push_back(L);
         plan.pad_bytes += (uint64_t)elem_bytes(precision) * b.h * (nc - r.vlen);
         pos += 16ull * b.h * r.npanel;
-        rot = (rot + r.npanel) % kConsumerWarps;
+        rot = (rot + r.npanel) % kProductWarps;
+        rot_step = (rot_step + r.npanel) % kStepWarps;
         col += nc;
         ++nr;
       } while (col < Wp);

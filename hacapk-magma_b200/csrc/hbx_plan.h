@@ -60,7 +60,17 @@ namespace hbx {
 
 constexpr int kAtomMax = 32;       // rows per D/U block (one lane per row)
 constexpr int kSlabMax = 64;       // rows per P slab (two rows per lane)
-constexpr int kConsumerWarps = 16; // warps that multiply (+ producer, gather, grid-barrier and block-sum warps)
+// Consumer warps of the product kernels (k_matvec) and of the BiCGSTAB step
+// kernel (k_bicg_iter, compiled in its own translation unit with fewer
+// threads, so that it keeps its registers); the planner rotates the panels of
+// consecutive runs for both counts.
+constexpr int kProductWarps = 16;
+constexpr int kStepWarps = 13;
+#ifndef HBX_CONSUMER_WARPS
+#define HBX_CONSUMER_WARPS 16
+#endif
+constexpr int kConsumerWarps = HBX_CONSUMER_WARPS; // warps that multiply (+ producer, gather, grid-barrier and block-sum warps)
+static_assert(kConsumerWarps == kProductWarps || kConsumerWarps == kStepWarps, "a planned consumer-warp count");
 #ifndef HBX_CHUNK_LOG
 #define HBX_CHUNK_LOG 15
 #endif
@@ -179,9 +189,9 @@ struct alignas(16) RunLite {
   uint32_t out;     // first output row: zbu index (P) or y row (D, U)
   uint16_t npanel;  // column-group panels
   uint8_t nrow;     // h: 1..32 (1..64 for P)
-  uint8_t rot;      // consumer warp that takes panel 0
+  uint8_t rot;      // consumer warp that takes panel 0 (kProductWarps consumers)
   uint16_t flags;   // RunKind | RunFlags
-  uint16_t pad;
+  uint16_t rot_step;  // the same for kStepWarps consumers
 };
 static_assert(sizeof(RunLite) == 16, "RunLite layout");
 

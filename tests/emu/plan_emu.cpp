@@ -64,7 +64,7 @@ static int emu_run(const stc_HACApK_leafmtxp *st, int nd, int num_ctas, int prec
           (r.npanel > 0 && r.vlen + RG <= G * r.npanel) || (pairs && r.npanel % 2 != 0))
         return "run width";
       if (r.nseg > kRunSegs) return "too many segments";
-      if (r.rot >= kConsumerWarps) return "bad rotation";
+      if (r.rot >= kProductWarps || L.rot_step >= kStepWarps) return "bad rotation";
       if (r.pos != pos || r.pos % 16 != 0) return "runs not back to back";
       pos += run_bytes(r);
       if (r.vlen != G * r.npanel && !(r.flags & kLast)) return "zero columns outside a block's last run";
