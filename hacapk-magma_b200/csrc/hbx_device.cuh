@@ -666,14 +666,25 @@ __device__ __forceinline__ void run_rows(const RunLite &L, uint32_t stage_s, Rin
   using M = typename PM::M;
   // panels per iteration: BF16 panels are twice as wide as FP32 ones, so
   // half as many give the same columns per iteration
-  constexpr uint32_t NW = kConsumerWarps, U = kTwoRows ? 2 : (kPrec == kBF16 ? kUnroll / 2 : kUnroll);
+#ifndef HBX_UNROLL_BF16
+#define HBX_UNROLL_BF16 (HBX_UNROLL / 2)
+#endif
+#ifndef HBX_UNROLL_F32
+#define HBX_UNROLL_F32 HBX_UNROLL
+#endif
+  constexpr uint32_t NW = kConsumerWarps,
+                     U = kTwoRows ? 2 : (kPrec == kBF16 ? HBX_UNROLL_BF16 : kPrec == kFP32 ? HBX_UNROLL_F32 : kUnroll);
   const int lane = threadIdx.x & 31;
   const uint32_t h = L.nrow, np = L.npanel;
   const uint32_t pb = 16u * h;
   const uint32_t lrow = 16u * min((uint32_t)lane, h - 1u);
   const uint32_t lrow2 = 16u * min((uint32_t)lane + 32u, h - 1u) - lrow;  // second row, relative
   const uint32_t ring_s = smem_u32(R.buf);
-  uint32_t j = (w + NW - (NW == (uint32_t)kStepWarps ? (uint32_t)L.rot_step : (uint32_t)L.rot)) % NW;
+  // the planned rotation for this warp count (another count: any rotation
+  // covers every panel once)
+  const uint32_t rot = NW == (uint32_t)kStepWarps ? (uint32_t)L.rot_step
+                       : NW == (uint32_t)kProductWarps ? (uint32_t)L.rot : (uint32_t)L.rot % NW;
+  uint32_t j = (w + NW - rot) % NW;
   typename PM::Acc a[U], b[kTwoRows ? U : 1];
   for (; j + (U - 1) * NW < np; j += U * NW) {
     const uint32_t p0 = L.pos + j * pb;

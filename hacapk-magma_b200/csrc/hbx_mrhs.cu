@@ -3,15 +3,22 @@
 //
 // The packed stream is the FP32 engine's (panels of 4 columns x h rows, 16
 // bytes a row) with every run an even number of panels, so two panels make
-// the K = 8 of one TF32 step.  Per CTA (one per SM), 11 warps:
+// the K = 8 of one TF32 step.  Per CTA (one per SM), 16 warps:
 //
 //   warps 0-3   epilogue: TMEM accumulator -> zbu (P blocks) or Y (D, U)
-//   warp 4      tcgen05: allocates TMEM; one thread issues the MMAs
+//   warp 4      tcgen05: allocates TMEM; one thread issues the MMAs of the
+//               even blocks
 //   warp 5      bulk-copy producer of the stream ring (16 KB chunks)
 //   warps 6-13  gather: X (or zbu) columns of a run, 64 at a time, into a
 //               K-major operand stage [4-column chunk][rhs][4] (16 KB), one
 //               stage per warp
 //   warp 14     grid barrier between the P blocks and the U runs
+//   warp 15     one thread issues the MMAs of the odd blocks
+//
+// Two issuers because one thread's issue loop (descriptors, ring and stage
+// waits, commits: ~170 cycles an MMA of M = 64, N <= 64, K = 8) paced the
+// whole CTA; each has its own two accumulators, waits for its own slices'
+// stages, and hands every ring chunk back (the empty barriers count both).
 //
 // One MMA: D[rhs][row] += Xs[rhs][k..k+8] * Panel[row][k..k+8]^T with
 // M = 64 right-hand sides, N = the block's rows rounded up to 8, A (the
@@ -45,10 +52,12 @@ constexpr uint32_t kMRingBytes = (uint32_t)kMRingChunks * kMChunkBytes;
 constexpr int kXStages = 8;
 constexpr int kMirrorBytes = 2304;  // >= 2 panels of 64 rows + 7 rows past them
 constexpr int kAccCols = 64;        // TMEM columns per accumulator (rows of a block <= 64)
-constexpr int kTmemCols = 2 * kAccCols;
-constexpr int kEpiWarps = 4, kMmaWarp = 4, kProdWarpM = 5, kGathWarp0 = 6, kGathWarps = 8, kSyncWarpM = 14;
+constexpr int kIssuers = 2;  // MMA-issuing threads (warps kMmaWarp and kMmaWarp2), alternate blocks
+constexpr int kTmemCols = 2 * kIssuers * kAccCols;  // two accumulators per issuer
+constexpr int kEpiWarps = 4, kMmaWarp = 4, kProdWarpM = 5, kGathWarp0 = 6, kGathWarps = 8, kSyncWarpM = 14,
+              kMmaWarp2 = 15;
 static_assert(kXStages == kGathWarps, "gather warp gi always fills stage gi");
-constexpr int kThreadsM = (kSyncWarpM + 1) * 32;
+constexpr int kThreadsM = (kMmaWarp2 + 1) * 32;
 
 struct MLayout {
   static constexpr uint32_t ring = 0;
@@ -60,13 +69,14 @@ struct MLayout {
   static constexpr uint32_t xfull = empty + 8 * kMRingChunks;
   static constexpr uint32_t xempty = xfull + 8 * kXStages;
   static constexpr uint32_t accfull = xempty + 8 * kXStages;
-  static constexpr uint32_t accempty = accfull + 16;
-  static constexpr uint32_t pdone = accempty + 16;
+  static constexpr uint32_t accempty = accfull + 8 * 2 * kIssuers;
+  static constexpr uint32_t pdone = accempty + 8 * 2 * kIssuers;
   static constexpr uint32_t gdone = pdone + 8;
   static constexpr uint32_t mdone = gdone + 8;
   static constexpr uint32_t tmem = mdone + 8;  // TMEM base address (tcgen05.alloc writes it)
   static constexpr uint32_t gen0 = tmem + 4;   // first grid-barrier generation of the launch
-  static constexpr uint32_t bytes = gen0 + 12;
+  static constexpr uint32_t xcnt = (gen0 + 4 + 15) / 16 * 16;  // [kXStages] slices staged per slot
+  static constexpr uint32_t bytes = xcnt + 4 * kXStages;
 };
 static_assert(MLayout::bytes <= 227 * 1024, "shared memory per CTA");
 static_assert(MLayout::xst % 1024 == 0 && MLayout::rec % 16 == 0 && MLayout::full % 8 == 0, "layout alignment");
@@ -137,7 +147,7 @@ struct MSmem {
   uint8_t *ring, *xst, *rec;
   RunLite *lite;
   uint64_t *full, *empty, *xfull, *xempty, *accfull, *accempty, *pdone, *gdone, *mdone;
-  uint32_t *tmem, *gen0;
+  uint32_t *tmem, *gen0, *xcnt;
 };
 
 __device__ __forceinline__ MSmem mlayout(uint8_t *b) {
@@ -157,6 +167,7 @@ __device__ __forceinline__ MSmem mlayout(uint8_t *b) {
   s.mdone = reinterpret_cast<uint64_t *>(b + MLayout::mdone);
   s.tmem = reinterpret_cast<uint32_t *>(b + MLayout::tmem);
   s.gen0 = reinterpret_cast<uint32_t *>(b + MLayout::gen0);
+  s.xcnt = reinterpret_cast<uint32_t *>(b + MLayout::xcnt);
   return s;
 }
 
@@ -242,7 +253,10 @@ __device__ __forceinline__ void mr_gather(const MatmatArgs &a, const CtaInfo &ci
       cp_async_wait_all();
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
       __syncwarp();
-      if (lane == 0) mbar_arrive(&sm.xfull[slot]);
+      if (lane == 0) {
+        st_release_s(&sm.xcnt[slot], qs / kXStages + 1);
+        mbar_arrive(&sm.xfull[slot]);
+      }
     }
     r = rn;
     q = qn;
@@ -252,16 +266,25 @@ __device__ __forceinline__ void mr_gather(const MatmatArgs &a, const CtaInfo &ci
   cp_async_wait_all();
 }
 
+// One thread's bounded wait until a shared counter reaches `need`.
+__device__ __forceinline__ bool thread_count_wait(const unsigned *cnt, unsigned need, uint64_t timeout_ns) {
+  if (ld_acquire_s(cnt) >= need) return true;
+  const uint64_t t0 = gtimer();
+  while (ld_acquire_s(cnt) < need)
+    if (gtimer() - t0 > timeout_ns) return false;
+  return true;
+}
+
 // ---- MMA thread ---------------------------------------------------------------
 // Per slice: wait for its X stage and for every ring chunk its panel pairs
 // touch (at most 16 KB of pairs, two chunks), then issue its MMAs back to
 // back with the descriptors advanced in place, and commit the stage back.
-__device__ __forceinline__ void mr_mma(const MatmatArgs &a, uint32_t nr, uint32_t K, const MSmem &sm) {
+__device__ __forceinline__ void mr_mma(const MatmatArgs &a, uint32_t nr, uint32_t K, const MSmem &sm, uint32_t me) {
   const RunLite *lite = sm.lite;
   const uint64_t tmo = a.timeout_ns;
   const uint32_t tbase = *sm.tmem;
   const uint32_t ring_s = smem_u32(sm.ring), xst_s = smem_u32(sm.xst);
-  uint32_t waited = 0, released = 0, q = 0, nb = 0;
+  uint32_t waited = 0, released = 0, q = 0, nb = 0, nbk = 0;  // nb: blocks so far, nbk: this issuer's
   bool ok = true, first = true;
   // Releases ring chunks below c once the MMAs issued so far are done with
   // them; a chunk is waited for (full) before its release, so the empty
@@ -280,13 +303,22 @@ __device__ __forceinline__ void mr_mma(const MatmatArgs &a, uint32_t nr, uint32_
   for (uint32_t r = 0; r < nr && ok; ++r) {
     const RunLite L = lite[r];
     if (empty_block(L)) continue;
+    if ((nb & 1u) != me) {  // the other issuer's block: count its slices
+      q += run_slices(L);
+      if (L.flags & kLast) ++nb;
+      continue;
+    }
     const uint32_t h = L.nrow, n8 = (h + 7u) & ~7u, pb = 16u * h;
     const uint32_t idesc = idesc_tf32(kNrhs, n8);
-    const uint32_t buf = nb & 1u;
+    const uint32_t buf = 2u * me + (nbk & 1u);
     const uint32_t dtm = tbase + buf * kAccCols;
     if (L.flags & kFirst) {
+      // Hand back the ring chunks below this block first: the epilogue takes
+      // the blocks in order, so the other issuer's earlier block (which may
+      // still need those chunks refilled) must not wait on this issuer.
+      release_below(L.pos >> kMChunkLog);
       // the epilogue has read this accumulator's previous block
-      if (nb >= 2 && !(ok = mbar_wait(&sm.accempty[buf], ((nb >> 1) - 1) & 1, tmo))) break;
+      if (nbk >= 2 && !(ok = mbar_wait(&sm.accempty[buf], ((nbk >> 1) - 1) & 1, tmo))) break;
       tc_fence_after();  // the epilogue's TMEM reads come before these MMAs' writes
       first = true;
     }
@@ -301,6 +333,10 @@ __device__ __forceinline__ void mr_mma(const MatmatArgs &a, uint32_t nr, uint32_
         ok = mbar_wait(&sm.full[waited % kMRingChunks], (waited / kMRingChunks) & 1, tmo);
         waited += ok ? 1u : 0u;
       }
+      // The stage's fill count first: the other issuer may not have taken
+      // the slot's previous slice yet, and a parity wait two phases ahead
+      // would return at once.
+      if (ok) ok = thread_count_wait(&sm.xcnt[slot], q / kXStages + 1, tmo);
       if (ok) ok = mbar_wait(&sm.xfull[slot], (q / kXStages) & 1, tmo);
       if (!ok) break;
       uint64_t adesc = smem_desc(xst_s + slot * kSliceBytes, kChunkXBytes, 128);
@@ -317,6 +353,7 @@ __device__ __forceinline__ void mr_mma(const MatmatArgs &a, uint32_t nr, uint32_
     }
     if (ok && (L.flags & kLast)) {
       tc_commit(&sm.accfull[buf]);
+      ++nbk;
       ++nb;
     }
   }
@@ -360,8 +397,9 @@ __device__ __forceinline__ void mr_epilogue(const MatmatArgs &a, uint32_t nr, ui
       if (kind == kRunP && ++np_done == nblk_p && lane == 0) mbar_arrive(sm.pdone);
       continue;
     }
-    const uint32_t buf = nb & 1u;
-    ok = warp_wait(&sm.accfull[buf], (nb >> 1) & 1, a.timeout_ns);
+    // block nb: issuer nb & 1, that issuer's block nbk = nb >> 1 in its accumulator nbk & 1
+    const uint32_t nbk = nb >> 1, buf = 2u * (nb & 1u) + (nbk & 1u);
+    ok = warp_wait(&sm.accfull[buf], (nbk >> 1) & 1, a.timeout_ns);
     if (!ok) break;
     tc_fence_after();
     const uint32_t taddr = *sm.tmem + tlane + buf * kAccCols;
@@ -411,19 +449,20 @@ __global__ void __launch_bounds__(kThreadsM, 1) k_matmat(MatmatArgs a) {
   if (threadIdx.x == 0) {
     for (int i = 0; i < kMRingChunks; ++i) {
       mbar_init(&sm.full[i], 1);
-      mbar_init(&sm.empty[i], 1);
+      mbar_init(&sm.empty[i], kIssuers);  // both issuers hand every chunk back
     }
     for (int i = 0; i < kXStages; ++i) {
       mbar_init(&sm.xfull[i], 1);
       mbar_init(&sm.xempty[i], 1);
+      sm.xcnt[i] = 0;
     }
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < 2 * kIssuers; ++i) {
       mbar_init(&sm.accfull[i], 1);
       mbar_init(&sm.accempty[i], kEpiWarps);
     }
     mbar_init(sm.pdone, kEpiWarps);
     mbar_init(sm.gdone, 1);
-    mbar_init(sm.mdone, 1);
+    mbar_init(sm.mdone, kIssuers);
     *sm.gen0 = grid_gen0(a.gbar);
     mbar_fence_init();
   }
@@ -466,8 +505,12 @@ __global__ void __launch_bounds__(kThreadsM, 1) k_matmat(MatmatArgs a) {
     }
     return;
   }
+  if (w == kMmaWarp2) {
+    if (lane == 0) mr_mma(a, nr, K, sm, 1);
+    return;  // its MMAs are complete (mdone) before warp kMmaWarp frees TMEM
+  }
   if (w == kMmaWarp) {
-    if (lane == 0) mr_mma(a, nr, K, sm);
+    if (lane == 0) mr_mma(a, nr, K, sm, 0);
     __syncwarp();
   } else {
     mr_epilogue(a, nr, ci.nblk_p, sm);

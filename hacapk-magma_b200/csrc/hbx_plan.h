@@ -70,7 +70,7 @@ constexpr int kStepWarps = 13;
 #define HBX_CONSUMER_WARPS 16
 #endif
 constexpr int kConsumerWarps = HBX_CONSUMER_WARPS; // warps that multiply (+ producer, gather, grid-barrier and block-sum warps)
-static_assert(kConsumerWarps == kProductWarps || kConsumerWarps == kStepWarps, "a planned consumer-warp count");
+
 #ifndef HBX_CHUNK_LOG
 #define HBX_CHUNK_LOG 15
 #endif
