@@ -160,3 +160,35 @@ def test_solvers_stop_at_a_breakdown():
         for tol in (1e-8, 0.0):
             u, steps, relres = solve(mv, torch.zeros(n, dtype=torch.float64), tol=tol)
             assert steps == 0 and relres == 0.0 and torch.all(u == 0)
+
+
+@pytest.mark.gpu
+def test_partitioned_product_and_solve_over_nccl_one_rank(gpu, build_libs):
+    """The partitioned form's device path over NCCL on the one GPU a call
+    gets: a one-rank NCCL group, the rank's engine (engine_product) on device
+    vectors, the owned segment all-gathered through NCCL; the product equals
+    the oracle's and the replicated-vector BiCGSTAB over it converges.  (More
+    ranks need more GPUs; the exchange itself is covered by the gloo tests.)"""
+    import socket
+    import torch
+    import torch.distributed as dist
+    import oracle
+    from hacapk_b200 import configs, partition
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            device_id=torch.device("cuda", 0))
+    try:
+        H, b = configs.c1(4)
+        mv = partition.RowPartitionedMatvec(H.st, H.nd, partition.engine_product)
+        x = np.random.default_rng(9).standard_normal(H.nd)
+        y = mv(torch.from_numpy(x).cuda())
+        torch.cuda.synchronize()
+        ref = oracle.matvec(H.st, x)
+        assert np.abs(y.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+        u, steps, relres = partition.bicgstab(mv, torch.from_numpy(b).cuda(), tol=1e-8)
+        r = b - oracle.matvec(H.st, u.cpu().numpy())
+        assert relres < 1e-8 and np.linalg.norm(r) / np.linalg.norm(b) < 1.05e-8
+    finally:
+        dist.destroy_process_group()
