@@ -658,7 +658,7 @@ struct PanelMath<kBF16> {
 #endif
 constexpr uint32_t kUnroll = HBX_UNROLL;
 
-template <bool kTwoRows, int kPrec>
+template <bool kTwoRows, int kPrec, int kGroupWarps>
 __device__ __forceinline__ void run_rows(const RunLite &L, uint32_t stage_s, Ring &R, uint32_t w, double &t0,
                                          double &t1) {
   using PM = PanelMath<kPrec>;
@@ -672,7 +672,8 @@ __device__ __forceinline__ void run_rows(const RunLite &L, uint32_t stage_s, Rin
 #ifndef HBX_UNROLL_F32
 #define HBX_UNROLL_F32 HBX_UNROLL
 #endif
-  constexpr uint32_t NW = kConsumerWarps,
+  // NW: the warps that share this run (a consumer group); w: the warp's index in it
+  constexpr uint32_t NW = kGroupWarps,
                      U = kTwoRows ? 2 : (kPrec == kBF16 ? HBX_UNROLL_BF16 : kPrec == kFP32 ? HBX_UNROLL_F32 : kUnroll);
   const int lane = threadIdx.x & 31;
   const uint32_t h = L.nrow, np = L.npanel;
@@ -734,11 +735,11 @@ __device__ __forceinline__ void run_rows(const RunLite &L, uint32_t stage_s, Rin
   }
 }
 
-template <int kPrec>
+template <int kPrec, int kGroupWarps>
 __device__ __forceinline__ void run_panels(const RunLite &L, uint32_t stage_s, Ring &R, uint32_t w, double &t0,
                                            double &t1) {
-  if (L.nrow > 32) run_rows<true, kPrec>(L, stage_s, R, w, t0, t1);
-  else run_rows<false, kPrec>(L, stage_s, R, w, t0, t1);
+  if (L.nrow > 32) run_rows<true, kPrec, kGroupWarps>(L, stage_s, R, w, t0, t1);
+  else run_rows<false, kPrec, kGroupWarps>(L, stage_s, R, w, t0, t1);
 }
 
 // ---- compensated (Dot2) accumulation ------------------------------------------

@@ -34,6 +34,11 @@ namespace {
 
 constexpr int NW = kConsumerWarps;
 [[maybe_unused]] constexpr int kConsumerThreads = NW * 32;
+// consumer groups of this translation unit: the product kernels split their
+// warps, the step kernels keep one group
+constexpr int kGroups = NW == kProductWarps ? kProductGroups : 1;
+constexpr int kGroupWarps = NW / kGroups;
+static_assert(kStages % kGroups == 0, "a stage slot always serves the same consumer group");
 
 struct Smem {
   uint8_t *ring;
@@ -79,7 +84,7 @@ __device__ __forceinline__ void init_cta_part(const Smem &s, const RunLite *lite
   if (threadIdx.x == t0) {
     for (int i = 0; i < kStages; ++i) {
       mbar_init(&s.sfull[i], 33);  // 32 cp.async arrivals of a gather warp + its lane 0
-      mbar_init(&s.sempty[i], NW);
+      mbar_init(&s.sempty[i], kGroupWarps);  // the slot's runs belong to one group
     }
     for (int i = 0; i < kGatherWarps * (int)kRecSlots; ++i) mbar_init(&s.rfull[i], 32);
     mbar_init(s.xready, 1);
@@ -256,21 +261,25 @@ __device__ __forceinline__ void consume_pass(Ring &R, uint32_t K, uint32_t nr, u
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   bool bad = R.bad;
   double t0 = 0.0, t1 = 0.0;  // this lane's block sums: rows lane and lane + 32
+  const uint32_t grp = kGroups == 1 ? 0u : (uint32_t)w / kGroupWarps;
+  const uint32_t wl = kGroups == 1 ? (uint32_t)w : (uint32_t)w % kGroupWarps;
   for (uint32_t r = 0; r < nr; ++r) {
     const RunLite L = sm.lite[r];
     const uint32_t g = pass * nr + r, slot = g % kStages;
     R.release_below(R.base + (L.pos >> kChunkLog));
-    // Every warp observes every phase of the slot's barrier, panels or not: a
-    // warp that skipped phases could take an older completed phase for the
-    // one it waits on.
-    if (!bad && !warp_wait(&sm.sfull[slot], (g / kStages) & 1, tmo)) {
-      bad = true;
-      if (lane == 0) atomicOr(err, kErrPipeline);
+    if (kGroups == 1 || g % kGroups == grp) {  // a run of this warp's group (the other group's: parking only)
+      // Every warp of the group observes every phase of the slot's barrier,
+      // panels or not: a warp that skipped phases could take an older
+      // completed phase for the one it waits on.
+      if (!bad && !warp_wait(&sm.sfull[slot], (g / kStages) & 1, tmo)) {
+        bad = true;
+        if (lane == 0) atomicOr(err, kErrPipeline);
+      }
+      if (!bad) run_panels<kPrec, kGroupWarps>(L, smem_u32(sm.stage + slot * kStageBytes), R, wl, t0, t1);
+      bad = bad || R.bad;
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.sempty[slot]);
     }
-    if (!bad) run_panels<kPrec>(L, smem_u32(sm.stage + slot * kStageBytes), R, (uint32_t)w, t0, t1);
-    bad = bad || R.bad;
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&sm.sempty[slot]);
     if (L.flags & kLast) {
       R.release_below(R.base + ((L.pos + 16u * L.nrow * L.npanel) >> kChunkLog));
       if (bad) ++nb;

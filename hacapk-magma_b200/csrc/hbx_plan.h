@@ -66,6 +66,15 @@ constexpr int kSlabMax = 64;       // rows per P slab (two rows per lane)
 // consecutive runs for both counts.
 constexpr int kProductWarps = 16;
 constexpr int kStepWarps = 13;
+// The product kernel splits its consumer warps into groups that take
+// alternate runs (warps [g*8, g*8+8) take runs r with r % 2 == g), so that
+// the fixed work of one run overlaps the next run's; the step kernel keeps
+// one group.
+#ifndef HBX_PRODUCT_GROUPS
+#define HBX_PRODUCT_GROUPS 2
+#endif
+constexpr int kProductGroups = HBX_PRODUCT_GROUPS;
+static_assert(kProductWarps % kProductGroups == 0, "equal consumer groups");
 #ifndef HBX_CONSUMER_WARPS
 #define HBX_CONSUMER_WARPS 16
 #endif
