@@ -34,11 +34,15 @@ namespace {
 
 constexpr int NW = kConsumerWarps;
 [[maybe_unused]] constexpr int kConsumerThreads = NW * 32;
-// consumer groups of this translation unit: the product kernels split their
-// warps, the step kernels keep one group
-constexpr int kGroups = NW == kProductWarps ? kProductGroups : 1;
-constexpr int kGroupWarps = NW / kGroups;
-static_assert(kStages % kGroups == 0, "a stage slot always serves the same consumer group");
+// Consumer groups: the FP32 and BF16 product kernels split their warps into
+// kProductGroups groups taking alternate runs; the FP64 product (whose
+// summation order the drop-in's iteration counts follow, and which a CPU
+// replay reproduces bit for bit) and the step kernels keep one group.
+template <int kPrec>
+constexpr int groups_of() {
+  return (NW == kProductWarps && kPrec != kFP64) ? kProductGroups : 1;
+}
+static_assert(kStages % kProductGroups == 0, "a stage slot always serves the same consumer group");
 
 struct Smem {
   uint8_t *ring;
@@ -80,11 +84,11 @@ __device__ __forceinline__ Smem smem_layout(uint8_t *base) {
 // nr of them) in shared memory.  Thread t0 sets up the barriers; threads t0
 // and up copy the summaries.  The caller synchronises the CTA afterwards.
 __device__ __forceinline__ void init_cta_part(const Smem &s, const RunLite *lite, uint32_t nr, const unsigned *gbar,
-                                              uint32_t t0) {
+                                              uint32_t t0, uint32_t group_warps) {
   if (threadIdx.x == t0) {
     for (int i = 0; i < kStages; ++i) {
       mbar_init(&s.sfull[i], 33);  // 32 cp.async arrivals of a gather warp + its lane 0
-      mbar_init(&s.sempty[i], kGroupWarps);  // the slot's runs belong to one group
+      mbar_init(&s.sempty[i], group_warps);  // the slot's runs belong to one consumer group
     }
     for (int i = 0; i < kGatherWarps * (int)kRecSlots; ++i) mbar_init(&s.rfull[i], 32);
     mbar_init(s.xready, 1);
@@ -113,8 +117,9 @@ __device__ __forceinline__ Smem cta_smem(uint8_t *base, const RunLite *lite, uin
 }
 
 #ifndef HBX_STEP_TU
-__device__ __forceinline__ void init_cta(const Smem &s, const RunLite *lite, uint32_t nr, const unsigned *gbar) {
-  init_cta_part(s, lite, nr, gbar, 0);
+__device__ __forceinline__ void init_cta(const Smem &s, const RunLite *lite, uint32_t nr, const unsigned *gbar,
+                                         uint32_t group_warps) {
+  init_cta_part(s, lite, nr, gbar, 0, group_warps);
   __syncthreads();
 }
 #endif
@@ -261,6 +266,7 @@ __device__ __forceinline__ void consume_pass(Ring &R, uint32_t K, uint32_t nr, u
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   bool bad = R.bad;
   double t0 = 0.0, t1 = 0.0;  // this lane's block sums: rows lane and lane + 32
+  constexpr int kGroups = groups_of<kPrec>(), kGroupWarps = NW / kGroups;
   const uint32_t grp = kGroups == 1 ? 0u : (uint32_t)w / kGroupWarps;
   const uint32_t wl = kGroups == 1 ? (uint32_t)w : (uint32_t)w % kGroupWarps;
   for (uint32_t r = 0; r < nr; ++r) {
@@ -329,7 +335,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_matvec(MatvecArgs a) {
   const StreamSrc ss{a.stream + ci.stream_off, ci.stream_bytes, keep_bytes(ci.stream_bytes, a.keep_frac),
                      a.chunk_inst ? a.chunk_inst + a.chunk_base[blockIdx.x] : nullptr, a.inst_pre};
   if (threadIdx.x == kProducerWarp * 32) issued0 = producer_start(ss, 1, sm.ring, sm.full, sm.empty);
-  init_cta(sm, a.lite + ci.rec_begin, nr, a.gbar);
+  init_cta(sm, a.lite + ci.rec_begin, nr, a.gbar, NW / groups_of<kPrec>());
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t K = (ci.stream_bytes + kChunkBytes - 1) >> kChunkLog;
   if (w == kProducerWarp) {
@@ -519,7 +525,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
   const StreamSrc ss{a.stream + ci.stream_off, ci.stream_bytes, keep_bytes(ci.stream_bytes, a.keep_frac)};
   uint32_t issued0 = 0;
   if (threadIdx.x == kProducerWarp * 32) issued0 = producer_start(ss, 2, sm.ring, sm.full, sm.empty);
-  init_cta_part(sm, a.lite + ci.rec_begin, nr, a.gbar, 128);
+  init_cta_part(sm, a.lite + ci.rec_begin, nr, a.gbar, 128, NW / groups_of<kPrec>());
 
   // ---- S0: scalars of the previous step; stop test at the top of the loop
   // (HACApK_SOLVER.c:602-603).  Every CTA computes identical values: warps

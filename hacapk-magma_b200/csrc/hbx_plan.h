@@ -66,10 +66,10 @@ constexpr int kSlabMax = 64;       // rows per P slab (two rows per lane)
 // consecutive runs for both counts.
 constexpr int kProductWarps = 16;
 constexpr int kStepWarps = 13;
-// The product kernel splits its consumer warps into groups that take
-// alternate runs (warps [g*8, g*8+8) take runs r with r % 2 == g), so that
-// the fixed work of one run overlaps the next run's; the step kernel keeps
-// one group.
+// The FP32 and BF16 product kernels split their consumer warps into groups
+// that take alternate runs (warps [g*8, g*8+8) take runs r with r % 2 == g),
+// so that the fixed work of one run overlaps the next run's; the FP64 product
+// and the step kernels keep one group.
 #ifndef HBX_PRODUCT_GROUPS
 #define HBX_PRODUCT_GROUPS 2
 #endif

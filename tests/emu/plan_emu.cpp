@@ -304,9 +304,8 @@ extern "C" int emu_plan_cta_sections(const stc_HACApK_leafmtxp *st, int nd, int 
 
 // y = alpha H x + beta yin in the FP64 kernel's own operation order, so that
 // it equals k_matvec bit for bit (merge_keep as make_plan's; merged D+U runs
-// gather x or zbu per segment and write like D blocks): run k of a CTA goes to
-// consumer group k mod 2 (warps 0-7 or 8-15), whose warp wl takes panels
-// j = (wl - rot) mod 8, j + 8, ... of the run, four at a time (two for P
+// gather x or zbu per segment and write like D blocks): consumer warp w takes panels
+// j = (w - rot) mod 16, j + 16, ... of every run, four at a time (two for P
 // slabs taller than 32 rows, whose lanes also carry row lane + 32) into
 // accumulator pairs (one fma per column), folds them into its block sum at
 // the end of the run (a0 + a1, accumulators in order), and the block-sum
@@ -344,11 +343,11 @@ extern "C" int emu_matvec_kernel_order_mk(const stc_HACApK_leafmtxp *st, int nd,
         const uint32_t h = r.nrow, np = r.npanel;
         const bool two = h > 32;
         const uint32_t U = two ? 2 : 4;
-        // consumer groups: warps [grp*GW, grp*GW+GW) take the runs k with
-        // k % kProductGroups == grp, panel j to the group's warp (j + rot) % GW
-        constexpr int GW = NW / kProductGroups;
-        const int grp = (int)(k % kProductGroups);
-        for (int w = grp * GW; w < grp * GW + GW; ++w)
+        // the FP64 product keeps one consumer group: warp w takes panel j
+        // with j = (w - rot) mod 16
+        constexpr int GW = NW;
+        const int grp = 0;
+        for (int w = 0; w < NW; ++w)
           for (uint32_t lane = 0; lane < 32; ++lane) {
             const uint32_t ra = std::min(lane, h - 1), rb = std::min(lane + 32, h - 1);
             double a0[4] = {0, 0, 0, 0}, a1[4] = {0, 0, 0, 0}, b0[4] = {0, 0, 0, 0}, b1[4] = {0, 0, 0, 0};
