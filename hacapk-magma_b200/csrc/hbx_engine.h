@@ -212,7 +212,9 @@ cudaError_t noalloc_scratch_address(void **ptr);
 // Kernel launchers (hbx_kernels.cu).
 size_t kernel_smem_bytes();
 cudaError_t configure_kernels();
-cudaError_t configure_step_kernels();  // the step kernels' translation unit
+cudaError_t configure_step_kernels();     // the step kernels' translation unit
+cudaError_t configure_step_kernels_lp();  // the FP32 / BF16 step kernels' unit
+cudaError_t launch_bicg_iter_lp(const BicgArgs &a, int num_ctas, cudaStream_t s, int precision);
 cudaError_t launch_matvec(const MatvecArgs &a, int num_ctas, cudaStream_t s, int precision);
 cudaError_t launch_bicg_setup(const BicgArgs &a, int num_ctas, cudaStream_t s);
 cudaError_t launch_bicg_iter(const BicgArgs &a, int num_ctas, cudaStream_t s, int precision);

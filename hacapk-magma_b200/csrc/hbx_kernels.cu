@@ -9,12 +9,15 @@
 //               both H-matvecs, the vector updates and all dot products, with
 //               compensated (Dot2) partial sums reduced in a fixed order.
 //
-// The file is compiled twice: as itself (k_matvec and the small vector
-// kernels, 16 consumer warps) and with HBX_STEP_TU and HBX_CONSUMER_WARPS=13
-// (k_bicg_setup, k_bicg_iter and the dot kernels): with fewer threads per CTA
-// the step kernel gets the registers it needs without spilling, and its
-// scalar phases synchronise fewer warps (C1 step 121.4 -> 115 us, while the
-// standalone product is fastest with 16).
+// The file is compiled three times: as itself (k_matvec and the small vector
+// kernels, 16 consumer warps), with HBX_STEP_TU and HBX_CONSUMER_WARPS=13
+// (k_bicg_setup, the FP64 k_bicg_iter and the dot kernels): with fewer
+// threads per CTA the step kernel gets the registers it needs without
+// spilling, and its scalar phases synchronise fewer warps (C1 step 121.4 ->
+// 115 us, while the standalone product is fastest with 16); and with
+// HBX_STEP_TU, HBX_STEP_LP and HBX_CONSUMER_WARPS=kStepWarpsLp (the FP32 and
+// BF16 k_bicg_iter, whose consumer warps form two groups like the FP32 and
+// BF16 products').
 //
 // All kernels run one CTA per SM: consumer warps, a bulk-copy producer
 // warp, kGatherWarps gather warps, a grid-barrier warp and a block-sum warp.
@@ -40,7 +43,7 @@ constexpr int NW = kConsumerWarps;
 // replay reproduces bit for bit) and the step kernels keep one group.
 template <int kPrec>
 constexpr int groups_of() {
-  return (NW == kProductWarps && kPrec != kFP64) ? kProductGroups : 1;
+  return ((NW == kProductWarps || NW == kStepWarpsLp) && kPrec != kFP64) ? kProductGroups : 1;
 }
 static_assert(kStages % kProductGroups == 0, "a stage slot always serves the same consumer group");
 
@@ -466,6 +469,7 @@ __device__ __forceinline__ bool grid_sync(unsigned *gbar, unsigned k, int *err, 
   return sm.scal[62] != 0.0;
 }
 
+#ifndef HBX_STEP_LP
 __global__ void __launch_bounds__(kThreads, 1) k_bicg_setup(BicgArgs a) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const Smem sm = smem_layout(smem_raw);
@@ -492,6 +496,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_setup(BicgArgs a) {
     *a.state = st;
   }
 }
+#endif
 
 template <int kPrec>
 __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
@@ -775,6 +780,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_bicg_iter(BicgArgs a) {
 }
 
 // part[cta][slot] over own rows, then (block 0 of a second launch) the total.
+#ifndef HBX_STEP_LP
 __global__ void __launch_bounds__(kThreads, 1) k_dot_partial(BicgArgs a, const double *x, const double *y, int slot) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const Smem sm = smem_layout(smem_raw);
@@ -784,6 +790,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_dot_partial(BicgArgs a, const d
   for_own_rows(a.atoms, ci, [&](uint32_t r) { dot2_add(acc[0], x[r], y[r]); });
   cta_partials<1>(acc, a.part, slot, sm);
 }
+#endif
 
 // y = (float)x: the input of an FP32 engine's matvec.
 #endif  // HBX_STEP_TU
@@ -803,10 +810,12 @@ __global__ void k_axpy(double a, const double *x, double *y, size_t n) {
 #endif  // !HBX_STEP_TU
 
 #ifdef HBX_STEP_TU
+#ifndef HBX_STEP_LP
 __global__ void k_dot_total(const double *part, int ncta, int slot, double *out) {
   const double v = reduce_slot(part, ncta, slot);
   if (threadIdx.x == 0) *out = v;
 }
+#endif
 
 #endif  // HBX_STEP_TU
 
@@ -864,16 +873,14 @@ cudaError_t launch_axpy(double alpha, const double *x, double *y, size_t n, cuda
   k_axpy<<<296, 256, 0, s>>>(alpha, x, y, n);
   return cudaGetLastError();
 }
-#else
+#elif !defined(HBX_STEP_LP)
 cudaError_t configure_step_kernels() {
   const int smem = (int)SharedLayout::bytes;
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(k_bicg_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_bicg_iter<kFP64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(k_bicg_iter<kFP32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(k_bicg_iter<kBF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_dot_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-  return cudaSuccess;
+  return configure_step_kernels_lp();
 }
 
 cudaError_t launch_bicg_setup(const BicgArgs &a, int num_ctas, cudaStream_t s) {
@@ -882,9 +889,8 @@ cudaError_t launch_bicg_setup(const BicgArgs &a, int num_ctas, cudaStream_t s) {
 }
 
 cudaError_t launch_bicg_iter(const BicgArgs &a, int num_ctas, cudaStream_t s, int precision) {
-  if (precision == kBF16) return launch_coop(k_bicg_iter<kBF16>, a, num_ctas, s);
-  return precision == kFP32 ? launch_coop(k_bicg_iter<kFP32>, a, num_ctas, s)
-                            : launch_coop(k_bicg_iter<kFP64>, a, num_ctas, s);
+  if (precision != kFP64) return launch_bicg_iter_lp(a, num_ctas, s, precision);
+  return launch_coop(k_bicg_iter<kFP64>, a, num_ctas, s);
 }
 
 cudaError_t launch_dot(const BicgArgs &a, const double *x, const double *y, int slot, double *out, int num_ctas,
@@ -892,6 +898,20 @@ cudaError_t launch_dot(const BicgArgs &a, const double *x, const double *y, int 
   k_dot_partial<<<num_ctas, kThreads, SharedLayout::bytes, s>>>(a, x, y, slot);
   k_dot_total<<<1, 32, 0, s>>>(a.part, num_ctas, slot, out);
   return cudaGetLastError();
+}
+#else
+// The FP32 and BF16 step kernels: kStepWarpsLp consumer warps in two groups.
+cudaError_t configure_step_kernels_lp() {
+  const int smem = (int)SharedLayout::bytes;
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_bicg_iter<kFP32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_bicg_iter<kBF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+cudaError_t launch_bicg_iter_lp(const BicgArgs &a, int num_ctas, cudaStream_t s, int precision) {
+  return precision == kBF16 ? launch_coop(k_bicg_iter<kBF16>, a, num_ctas, s)
+                            : launch_coop(k_bicg_iter<kFP32>, a, num_ctas, s);
 }
 #endif  // HBX_STEP_TU
 

@@ -66,6 +66,11 @@ constexpr int kSlabMax = 64;       // rows per P slab (two rows per lane)
 // consecutive runs for both counts.
 constexpr int kProductWarps = 16;
 constexpr int kStepWarps = 13;
+// the FP32 / BF16 step kernels (a third translation unit): two groups of 6
+#ifndef HBX_STEP_LP_WARPS
+#define HBX_STEP_LP_WARPS 12
+#endif
+constexpr int kStepWarpsLp = HBX_STEP_LP_WARPS;
 // The FP32 and BF16 product kernels split their consumer warps into groups
 // that take alternate runs (warps [g*8, g*8+8) take runs r with r % 2 == g),
 // so that the fixed work of one run overlaps the next run's; the FP64 product
