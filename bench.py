@@ -329,15 +329,47 @@ def measure_forms(args, dev, stream):
                     random directions;
       batch_c5      C5: 256 uneven bodies in one block-diagonal engine,
                     against the same bodies solved one after another;
+      autotune_c1   C1: the autotuner's schedule and layout against the
+                    defaults (product and solve);
       solvers_c1    C1: the reference's other iterative solvers on the GPU
                     (pipelined BiCGSTAB, GCR(8)), each beside its CPU loop
                     on every host core.
 
     The H-matrices are filled on the GPU (hbx_fill_leaves)."""
-    forms = {"solvers_c1": solvers_form, "precision_c2": precision_form, "mrhs_c3": mrhs_form,
-             "adjoint_c4": adjoint_form, "batch_c5": batch_form}
+    forms = {"solvers_c1": solvers_form, "autotune_c1": autotune_form, "precision_c2": precision_form,
+             "mrhs_c3": mrhs_form, "adjoint_c4": adjoint_form, "batch_c5": batch_form}
     want = getattr(args, "form", "")
     return {name: fn(args, dev, stream) for name, fn in forms.items() if not want or want == name}
+
+
+def autotune_form(args, dev, stream, level=5):
+    """C1: hbx_autotune's choice (CTA schedule, merged D+U layout, L2 budget)
+    against the defaults: the product time of each, and the BiCGSTAB solve
+    (CUDA events) with the tuned engine against the default engine."""
+    import torch
+    from hacapk_b200 import configs
+    from hacapk_b200.engine import Engine
+    s = stream.cuda_stream
+    H, b = configs.c1(level)
+    t0 = time.time()
+    kw, best_us, def_us = Engine.autotune(H.st, H.nd, reps=20)
+    t_tune = time.time() - t0
+    bd = torch.from_numpy(b).to(dev)
+    ud = torch.zeros_like(bd)
+    out = {"workload": f"C1: icosphere L{level}, N = {H.nd}", "tuned_options": kw, "tune_seconds": t_tune,
+           "matvec_us": {"tuned": best_us, "default": def_us}}
+    for name, opts in (("default", {}), ("tuned", kw)):
+        E = Engine(H.st, H.nd, **opts)
+        best = 1e9
+        for _ in range(4):
+            ud.zero_()
+            inf = E.bicgstab_dev(bd.data_ptr(), ud.data_ptr(), tol=args.tol, max_iter=args.max_iter, stream=s)
+            best = min(best, inf["seconds"])
+        out[f"solve_s_{name}"] = best
+        out[f"iterations_{name}"] = inf["iterations"]
+        E.close()
+    H.close()
+    return out
 
 
 def solvers_form(args, dev, stream, level=5):

@@ -323,9 +323,11 @@ static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_option
   if (nc > max_ctas) return bail(fail(HBX_ERR_INVALID, "hbx_create: num_ctas exceeds co-resident CTAs"));
   h->num_ctas = nc;
   // L2 budget for the factor stream's pass-to-pass residency (MB): 24 by
-  // default, HBX_L2_KEEP_MB overrides (0 turns the cache hints off)
+  // default, HBX_L2_KEEP_MB overrides it (0 turns the cache hints off), a
+  // nonzero hbx_options::l2_keep_mb overrides both (-1: no hints)
   const char *keep = std::getenv("HBX_L2_KEEP_MB");
-  const double keep_mb = keep ? std::atof(keep) : 24.0;
+  double keep_mb = keep ? std::atof(keep) : 24.0;
+  if (opt && opt->l2_keep_mb != 0) keep_mb = opt->l2_keep_mb > 0 ? (double)opt->l2_keep_mb : 0.0;
   const char *tmo = std::getenv("HBX_TIMEOUT_MS");
   if (tmo) h->timeout_ns = (unsigned long long)(std::atof(tmo) * 1e6);
   const char *prof = std::getenv("HBX_PROFILE");
@@ -355,7 +357,10 @@ static int create_engine(const stc_HACApK_leafmtxp *st, int nd, const hbx_option
   // none merged
   int merge_keep = 4;
   if (const char *mk = std::getenv("HBX_MERGE_KEEP")) merge_keep = std::atoi(mk);
+  if (opt && opt->merge != 0) merge_keep = opt->merge > 0 ? opt->merge - 1 : -1;  // the caller's choice
   if (nrhs > 1) merge_keep = -1;
+  h->merge_keep = merge_keep;
+  h->l2_keep_mb = keep_mb > 0.0 ? (int)keep_mb : 0;
   int st_plan = hbx::make_plan(st, nd, nc, h->plan, err, prec, nrhs > 1, costs, merge_keep);
   if (st_plan != HBX_OK) return bail(fail(st_plan, "hbx_create: " + err));
   const hbx::Plan &P = h->plan;
@@ -481,6 +486,8 @@ int hbx_get_info(const hbx_hmat *h, hbx_info *info) {
   info->instances = h->inst_off.empty() ? 1 : (int)h->inst_off.size() - 1;
   info->block_cost = (int)P.costs.block;
   info->run_cost = (int)P.costs.run;
+  info->merge_keep = h->merge_keep;
+  info->l2_keep_mb = h->l2_keep_mb;
   return HBX_OK;
 }
 
@@ -510,19 +517,32 @@ int hbx_autotune(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *base,
   cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  struct Cand { int block, run, ctas; };
+  // Stage 1: the CTA schedule (cost model, CTA count).  Stage 2, for
+  // single-vector engines, from the best schedule: the merged D+U layout
+  // (atoms kept split per CTA), then the L2 budget of the stream.
+  struct Cand { int block, run, ctas, merge, l2; };
   std::vector<Cand> cands;
   for (int bc : {0, 2048, 32768})
-    for (int rc : {0, 1024, 16384}) cands.push_back({bc, rc, 0});
-  cands.push_back({0, 0, std::max(1, sms - 4)});
+    for (int rc : {0, 1024, 16384}) cands.push_back({bc, rc, 0, 0, 0});
+  cands.push_back({0, 0, std::max(1, sms - 4), 0, 0});
   double t_best = 1e30, t_def = -1.0;
   hbx_options o_best = b0;
   int rc_all = HBX_OK;
-  for (const Cand &c : cands) {
+  const size_t n_stage1 = cands.size();
+  for (size_t ci = 0; ci < cands.size(); ++ci) {
+    if (ci == n_stage1 && !multi) {  // stage 2a: merged D+U runs around the best schedule
+      for (int m : {-1, 1, 3, 9}) cands.push_back({o_best.block_cost, o_best.run_cost, o_best.num_ctas, m, 0});
+    }
+    if (ci == n_stage1 + 4 && !multi) {  // stage 2b: the L2 budget around the best so far
+      for (int l2 : {-1, 12, 48}) cands.push_back({o_best.block_cost, o_best.run_cost, o_best.num_ctas, o_best.merge, l2});
+    }
+    const Cand c = cands[ci];
     hbx_options o = b0;
     o.block_cost = c.block;
     o.run_cost = c.run;
     o.num_ctas = c.ctas;
+    o.merge = c.merge;
+    o.l2_keep_mb = c.l2;
     hbx_hmat *h = nullptr;
     int rc = hbx_create(st, nd, &o, &h);
     if (rc != HBX_OK) { rc_all = rc; continue; }
@@ -540,7 +560,7 @@ int hbx_autotune(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *base,
     hbx_destroy(h);
     if (rc != HBX_OK) { rc_all = rc; continue; }
     const double us = 1e3 * ms / reps;
-    if (c.block == 0 && c.run == 0 && c.ctas == 0) t_def = us;
+    if (c.block == 0 && c.run == 0 && c.ctas == 0 && c.merge == 0 && c.l2 == 0) t_def = us;
     if (us < t_best) {
       t_best = us;
       o_best = o;

@@ -250,6 +250,8 @@ struct hbx_hmat {
   uint32_t *d_chunk_inst = nullptr, *d_chunk_base = nullptr;
   int *d_inst_pre = nullptr;
   int skip_inactive = 0;
+  int merge_keep = -1;  // the planner's merged D+U setting in use
+  int l2_keep_mb = 0;   // the L2 budget of the stream in use (MB; 0: no hints)
   void *d_rflag = nullptr;  // refined batch: per-instance flags and inner tolerances
   double *d_btv = nullptr;      // r, rh, p, ap, t, at (6 nd)
   hbx::MrScal *d_btsc = nullptr;

@@ -58,7 +58,8 @@ class LControl(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("num_ctas", C.c_int), ("transpose", C.c_int), ("nrhs", C.c_int),
-                ("block_cost", C.c_int), ("run_cost", C.c_int), ("reserved", C.c_int * 10)]
+                ("block_cost", C.c_int), ("run_cost", C.c_int), ("merge", C.c_int), ("l2_keep_mb", C.c_int),
+                ("reserved", C.c_int * 8)]
 
 
 class Info(C.Structure):
@@ -69,7 +70,8 @@ class Info(C.Structure):
                 ("zbu_len", C.c_longlong), ("dense_words", C.c_longlong),
                 ("lowrank_words", C.c_longlong), ("setup_seconds", C.c_double),
                 ("transposed", C.c_int), ("nrhs", C.c_int), ("instances", C.c_int),
-                ("block_cost", C.c_int), ("run_cost", C.c_int), ("reserved", C.c_int * 3)]
+                ("block_cost", C.c_int), ("run_cost", C.c_int), ("merge_keep", C.c_int), ("l2_keep_mb", C.c_int),
+                ("reserved", C.c_int * 1)]
 
 
 class SolveOpts(C.Structure):

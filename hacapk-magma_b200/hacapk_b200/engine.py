@@ -31,8 +31,9 @@ class Engine:
 
     @staticmethod
     def autotune(st, nd: int, precision: int = 0, nrhs: int = 0, transpose: bool = False, reps: int = 20):
-        """Times a grid of CTA schedules on the current device (hbx_autotune);
-        returns (keyword options for Engine(...) of the fastest, its us, the default's us)."""
+        """Times a grid of CTA schedules and layouts on the current device
+        (hbx_autotune); returns (keyword options for Engine(...) of the
+        fastest, its us, the default's us)."""
         lib = abi.engine_lib()
         base = abi.Options()
         base.precision = precision
@@ -41,11 +42,12 @@ class Engine:
         best = abi.Options()
         tb, td = C.c_double(0.0), C.c_double(0.0)
         _check(lib.hbx_autotune(st, nd, C.byref(base), reps, C.byref(best), C.byref(tb), C.byref(td)), "hbx_autotune")
-        kw = {"num_ctas": best.num_ctas, "block_cost": best.block_cost, "run_cost": best.run_cost}
+        kw = {"num_ctas": best.num_ctas, "block_cost": best.block_cost, "run_cost": best.run_cost,
+              "merge": best.merge, "l2_keep_mb": best.l2_keep_mb}
         return kw, tb.value, td.value
 
     def __init__(self, st, nd: int, num_ctas: int = 0, transpose: bool = False, precision: int = 0,
-                 nrhs: int = 0, block_cost: int = 0, run_cost: int = 0):
+                 nrhs: int = 0, block_cost: int = 0, run_cost: int = 0, merge: int = 0, l2_keep_mb: int = 0):
         """transpose=True packs H^T: products and solves with the adjoint.
         precision=abi.HBX_FP32 stores the factors in float (half the bytes),
         abi.HBX_BF16 in bfloat16 (a quarter).
@@ -58,6 +60,8 @@ class Engine:
         opt.nrhs = nrhs
         opt.block_cost = block_cost
         opt.run_cost = run_cost
+        opt.merge = merge  # merged D+U runs: k + 1 keeps each CTA's first k atoms split; -1 none; 0 default
+        opt.l2_keep_mb = l2_keep_mb  # L2 budget of the stream in MB; -1 no cache hints; 0 default
         h = C.c_void_p()
         _check(self.lib.hbx_create(st, nd, C.byref(opt), C.byref(h)), "hbx_create")
         self._h = h

@@ -135,7 +135,16 @@ typedef struct hbx_options {
   int block_cost;  /* balancing cost model of the CTA schedule: the fixed   */
   int run_cost;    /* cost of a block end and of a run, in bytes (0 = the
                       defaults 8192 and 4096; hbx_autotune picks them)      */
-  int reserved[10];
+  int merge;       /* single-vector engines: an atom's dense and low-rank
+                      columns in one run ("merged D+U") for every atom with
+                      low-rank rows except each CTA's first k, which stay
+                      split; merge = k + 1, -1 for no merged runs, 0 for the
+                      default k = 4 (HBX_MERGE_KEEP overrides the default) */
+  int l2_keep_mb;  /* megabytes of the factor stream kept in L2 from one
+                      product to the next (the head of every CTA's stream is
+                      read with evict_last); 0 = the default 24
+                      (HBX_L2_KEEP_MB overrides it), -1 = no cache hints   */
+  int reserved[8];
 } hbx_options;
 
 /* Right-hand sides of one hbx_matmat call on a multi-RHS engine. */
@@ -155,7 +164,9 @@ typedef struct hbx_info {
   int nrhs;                /* right-hand sides per product (1 or HBX_NRHS)   */
   int instances;           /* independent H-matrices (hbx_create_batch)     */
   int block_cost, run_cost; /* the CTA schedule's cost model in use          */
-  int reserved[3];
+  int merge_keep;           /* atoms kept split per CTA (-1: no merged runs)  */
+  int l2_keep_mb;           /* L2 budget of the stream in MB (0: no hints)    */
+  int reserved[1];
 } hbx_info;
 
 typedef struct hbx_solve_opts {
@@ -199,15 +210,17 @@ int hbx_create(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *opt,
 int hbx_create_batch(const stc_HACApK_leafmtxp *const *st, const int *nd, int count, const hbx_options *opt,
                      hbx_hmat **out);
 
-/* Autotuner of the CTA schedule (no counterpart in the reference, whose
- * size-class batches are fixed by HACApK_BATCH_SORT.c): builds engines for a
- * grid of schedules -- the planner's block and run costs, and the number of
- * CTAs -- with `base`'s precision, orientation and nrhs, times the product
- * of each on the current device (hbx_matvec, or hbx_matmat for a multi-RHS
- * base; 3 untimed and `reps` timed launches, CUDA events) and returns in
- * `best` the options of the fastest, in `best_us` its time and in
- * `default_us` the time of the defaults (both nullable).  Takes about one
- * engine build per candidate (nine to twelve). */
+/* Autotuner of the schedule and layout (no counterpart in the reference,
+ * whose size-class batches are fixed by HACApK_BATCH_SORT.c): builds engines
+ * for a grid of CTA schedules -- the planner's block and run costs, and the
+ * number of CTAs -- then, for single-vector engines and around the best
+ * schedule, for the merged D+U layout (`merge`) and then for the L2 budget of
+ * the stream (`l2_keep_mb`), with `base`'s precision, orientation and nrhs;
+ * times the product of each on the current device (hbx_matvec, or
+ * hbx_matmat for a multi-RHS base; 3 untimed and `reps` timed launches, CUDA
+ * events) and returns in `best` the options of the fastest, in `best_us` its
+ * time and in `default_us` the time of the defaults (both nullable).  Takes
+ * one engine build per candidate (10 for multi-RHS engines, 17 otherwise). */
 int hbx_autotune(const stc_HACApK_leafmtxp *st, int nd, const hbx_options *base, int reps, hbx_options *best,
                  double *best_us, double *default_us);
 
