@@ -645,6 +645,29 @@ def batch_form(args, dev, stream):
     return out
 
 
+def profile_products(args):
+    """--profile-products L: C2 at level L (GPU fill), one engine per factor
+    precision (FP64, FP32, BF16), three single-vector products each, nothing
+    timed: the command the product profiles are taken from (launch 1 + 3k of
+    k_matvec is precision k's second product)."""
+    import torch
+    from hacapk_b200 import abi, configs
+    from hacapk_b200.engine import Engine
+    H, _ = configs.c2(args.profile_products, fill="gpu")
+    x = torch.randn(H.nd, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    out = {}
+    for name, prec in (("fp64", abi.HBX_FP64), ("fp32", abi.HBX_FP32), ("bf16", abi.HBX_BF16)):
+        E = Engine(H.st, H.nd, precision=prec)
+        for _ in range(3):
+            E.matvec_dev(x.data_ptr(), y.data_ptr())
+        torch.cuda.synchronize()
+        E.sync()
+        out[name] = E.info["stream_bytes"]
+        E.close()
+    print(json.dumps({"profile_products": args.profile_products, "stream_bytes": out}), flush=True)
+
+
 def profile_matmat(args):
     """Five 64-RHS products on the C1 workload, nothing timed: the command
     the ncu summary of k_matmat is taken from."""
@@ -753,11 +776,16 @@ def main():
     ap.add_argument("--form", default="", help="with --forms-only: only this form (e.g. solvers_c1)")
     ap.add_argument("--profile-matmat", action="store_true",
                     help="only run five 64-RHS tensor-core products (a short command for ncu)")
+    ap.add_argument("--profile-products", type=int, default=0,
+                    help="only run a few FP64/FP32/BF16 products on C2 at this level (a short command for ncu)")
     ap.add_argument("--precision-level", type=int, default=0,
                     help="only time the precision form on C2 at this level (7: the config; one GPU)")
     args = ap.parse_args()
     if args.profile_matmat:
         profile_matmat(args)
+        return
+    if args.profile_products > 0:
+        profile_products(args)
         return
     if args.precision_level > 0:
         precision_workload(args)
