@@ -934,6 +934,11 @@ static int pipe_dev(hbx_hmat *h, const double *b, double *u, const hbx_solve_opt
   if (!h->h_pstate) HBX_CUDA(cudaHostAlloc(&h->h_pstate, sizeof(hbx::PipeState), cudaHostAllocDefault));
   if (!h->d_ppart) HBX_CUDA(dev_malloc(&h->d_ppart, (size_t)hbx::gcr_dot_blocks(n) * hbx::kMaxDots * 2 * sizeof(double)));
   if (h->phist_cap < max_iter + 1) {
+    if (h->pgraph) {  // the captured steps write the history being replaced
+      cudaStreamSynchronize(h->stream);
+      cudaGraphExecDestroy(h->pgraph);
+      h->pgraph = nullptr;
+    }
     cudaFree(h->d_phist);
     h->d_phist = nullptr;
     h->phist_cap = 0;

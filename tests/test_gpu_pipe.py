@@ -109,3 +109,19 @@ def test_limits_zero_rhs_nonfinite_and_not_converged(gpu, build_libs):
     assert info["status"] == 7
     u, info = E.bicgstab_pipe_host(b)  # the engine is still usable
     assert info["status"] == 0
+
+
+def test_larger_iteration_limit_after_a_captured_solve(gpu, build_libs):
+    """A second solve with a larger iteration limit replaces the residual
+    history buffer that the first solve's captured steps write; the steps are
+    captured again, and the solve is the same bit for bit."""
+    from hacapk_b200 import configs
+    from hacapk_b200.engine import Engine
+    H, b = configs.c1(3)
+    E = Engine(H.st, H.nd)
+    u1, i1 = E.bicgstab_pipe_host(b, tol=1e-8, max_iter=40)
+    u2, i2 = E.bicgstab_pipe_host(b, tol=1e-8, max_iter=4000)
+    u3, i3 = E.bicgstab_pipe_host(b, tol=1e-8, max_iter=40)
+    assert i1["status"] == i2["status"] == i3["status"] == 0
+    assert i1["iterations"] == i2["iterations"] == i3["iterations"]
+    assert np.array_equal(u1, u2) and np.array_equal(u1, u3)
