@@ -46,6 +46,13 @@ constexpr int groups_of() {
   return ((NW == kProductWarps || NW == kStepWarpsLp) && kPrec != kFP64) ? kProductGroups : 1;
 }
 static_assert(kStages % kProductGroups == 0, "a stage slot always serves the same consumer group");
+#ifdef HBX_STEP_LP
+static_assert(NW == kStepWarpsLp, "the FP32 / BF16 step unit is built with kStepWarpsLp consumer warps");
+#elif defined(HBX_STEP_TU)
+static_assert(NW == kStepWarps, "the FP64 step unit is built with kStepWarps consumer warps");
+#else
+static_assert(NW == kProductWarps, "the product unit is built with kProductWarps consumer warps");
+#endif
 
 struct Smem {
   uint8_t *ring;
