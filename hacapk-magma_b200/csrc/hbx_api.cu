@@ -1930,6 +1930,7 @@ static void legacy_device_solve(host_solver_fn solve, stc_HACApK_leafmtxp *st_le
   o.tol = param[90];
   o.max_iter = (int)param[82];
   o.verbose = param[0] > 0 ? 1 : 0;
+  o.restart = param[86] >= 1.0 && param[86] <= 64.0 ? (int)param[86] : 0;  // param(87): GCR's restart length
   hbx_solve_info info{};
   int rc = solve(h, b, u, &o, &info);
   if (nstp) *nstp = info.iterations;
@@ -1948,6 +1949,15 @@ void c_hacapk_bicgstab_cax_lfmtx_gpu_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACA
 void c_hacapk_bicgstab_cax_lfmtx_pipe_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl, double *u,
                                        double *b, double *param, int *nd, int *nstp, int *lrtrn) {
   legacy_device_solve(hbx_bicgstab_pipe_host, st_leafmtxp, st_ctl, u, b, param, nd, nstp, lrtrn);
+}
+
+// GCR(m) with the solvers' argument list (the reference's GCR is the Fortran
+// HACApK_gcrm_lfmtx, m_HACApK_solve.f90:506-571, chosen by param(85) = 2 in
+// HACApK_solve, m_HACApK_use.f90:236-241; it has no C symbol): param(87) is
+// the restart length, param(83) the step limit, param(91) the tolerance.
+void c_hacapk_gcrm_lfmtx_gpu_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl, double *u, double *b,
+                              double *param, int *nd, int *nstp, int *lrtrn) {
+  legacy_device_solve(hbx_gcr_host, st_leafmtxp, st_ctl, u, b, param, nd, nstp, lrtrn);
 }
 
 void c_hacapk_bicgstab_cax_lfmtx_pipe2_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl, double *u,

@@ -501,6 +501,13 @@ void c_hacapk_bicgstab_cax_lfmtx_pipe_(stc_HACApK_leafmtxp *st_leafmtxp,
 void c_hacapk_bicgstab_cax_lfmtx_pipe2_(stc_HACApK_leafmtxp *st_leafmtxp,
                                         stc_HACApK_lcontrol *st_ctl, double *u, double *b,
                                         double *param, int *nd, int *nstp, int *lrtrn);
+/* GCR(m) on the GPU with the same arguments, for a Fortran driver that picks
+ * GCR (param(85) = 2 in HACApK_solve, m_HACApK_use.f90:236-241): replaces the
+ * call to the Fortran HACApK_gcrm_lfmtx (m_HACApK_solve.f90:506), which has
+ * no C symbol in the reference.  param(87) is the restart length (8 when
+ * outside 1..64). */
+void c_hacapk_gcrm_lfmtx_gpu_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl,
+                              double *u, double *b, double *param, int *nd, int *nstp, int *lrtrn);
 
 #ifdef __cplusplus
 }

@@ -115,3 +115,31 @@ def test_nonfinite_rhs_is_reported(gpu, build_libs):
     b[5] = np.nan
     u, info = E.gcr_host(b, check=False)
     assert info["status"] == 7
+
+
+@pytest.mark.parametrize("restart", [8, 30])
+def test_entry_point_with_the_solvers_arguments(gpu, build_libs, restart):
+    """c_hacapk_gcrm_lfmtx_gpu_ (the solvers' argument list; param(87) the
+    restart length, param(83) the step limit, param(91) the tolerance) on the
+    reference's own input_10ts mesh: the same solution as hbx_gcr_host, bit
+    for bit, and the oracle's step count."""
+    import ctypes as C
+    import oracle
+    from hacapk_b200 import abi, hmatrix
+    from hacapk_b200.engine import Engine
+    from test_gpu_bicgstab import _control
+    lib = abi.engine_lib()
+    H = hmatrix.HostHMatrix(reference_input_mesh(), leaf_size=15, eta=2.0, aca_eps=1e-6, kernel=abi.KERNEL_PPOHBEM)
+    b = np.ones(H.nd)
+    ctl, buf = _control(maxit=1000, tol=1e-8)
+    buf[86] = restart
+    u = np.zeros(H.nd)
+    nd, nstp, lrtrn = C.c_int(H.nd), C.c_int(-1), C.c_int(-1)
+    lib.c_hacapk_gcrm_lfmtx_gpu_(H.st, C.byref(ctl), abi.dptr(u), abi.dptr(b), ctl.param, C.byref(nd),
+                                 C.byref(nstp), C.byref(lrtrn))
+    assert lrtrn.value == 0
+    E = Engine(H.st, H.nd)
+    u2, info = E.gcr_host(b, tol=1e-8, max_iter=1000, restart=restart)
+    assert nstp.value == info["iterations"] and np.array_equal(u, u2)
+    _, n_ref, _, _ = oracle.gcrm(H.st, b, tol=1e-8, max_iter=1000, restart=restart, kind=_oracle_kind())
+    assert abs(nstp.value - n_ref) <= 1
