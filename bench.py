@@ -339,7 +339,15 @@ def measure_forms(args, dev, stream):
     forms = {"solvers_c1": solvers_form, "autotune_c1": autotune_form, "precision_c2": precision_form,
              "mrhs_c3": mrhs_form, "adjoint_c4": adjoint_form, "batch_c5": batch_form}
     want = getattr(args, "form", "")
-    return {name: fn(args, dev, stream) for name, fn in forms.items() if not want or want == name}
+    out = {}
+    for name, fn in forms.items():
+        if want and want != name:
+            continue
+        try:
+            out[name] = fn(args, dev, stream)
+        except Exception as e:  # one form's failure is reported beside the others, not fatal to the line
+            out[name] = {"error": f"{type(e).__name__}: {e}"[:500]}
+    return out
 
 
 def autotune_form(args, dev, stream, level=5):

@@ -17,3 +17,24 @@ def test_host_matvecs_report_both_cpu_paths(build_libs):
     assert out["cores"] == cores
     assert out["blas_gemv_ms_1_threads"] > 0 and out[f"blas_gemv_ms_{cores}_threads"] > 0
     assert out[f"omp_ms_{cores}_threads"] > 0
+
+
+def test_a_failing_form_is_reported_beside_the_others(monkeypatch):
+    """An exception in one form (an out-of-memory on a small box, say) is
+    recorded as that form's "error" entry; the other forms still run and the
+    bench line is still printed."""
+    import argparse
+
+    import bench
+
+    def boom(args, dev, stream):
+        raise RuntimeError("hbx_create: out of device memory")
+
+    monkeypatch.setattr(bench, "solvers_form", lambda args, dev, stream: {"ok": 1})
+    monkeypatch.setattr(bench, "autotune_form", boom)
+    for name in ("precision_form", "mrhs_form", "adjoint_form", "batch_form"):
+        monkeypatch.setattr(bench, name, lambda args, dev, stream: {"ok": 2})
+    out = bench.measure_forms(argparse.Namespace(form=""), None, None)
+    assert out["solvers_c1"] == {"ok": 1} and out["batch_c5"] == {"ok": 2}
+    assert out["autotune_c1"]["error"].startswith("RuntimeError: hbx_create")
+    assert list(bench.measure_forms(argparse.Namespace(form="mrhs_c3"), None, None)) == ["mrhs_c3"]
