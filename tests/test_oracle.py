@@ -317,6 +317,51 @@ def test_device_replays_against_the_oracle(build_libs):
         assert st == 0 and n_ref - 2 <= n <= n_ref + 1 and tr(u) < 1.05e-8
 
 
+def _pipe_with_noisy_products(H, b, seed, eps=1e-15, tol=1e-8, max_iter=1000):
+    """The oracle's pipelined loop (orc_bicgstab_pipe) with every product
+    H x (the restated reference product) perturbed by eps * max|Hx| * N(0,1),
+    seeded: the loop's own sensitivity to rounding-sized changes of the
+    product.  Returns the step count."""
+    import ctypes as C
+    import oracle
+    nd = H.nd
+    rng = np.random.default_rng(seed)
+    DP = C.POINTER(C.c_double)
+
+    def product(zau, _st, zu, _zbu):
+        y = oracle.matvec(H.st, np.ctypeslib.as_array(zu, (nd,)))
+        np.ctypeslib.as_array(zau, (nd,))[:] += y + eps * np.abs(y).max() * rng.standard_normal(nd)
+
+    cb = C.CFUNCTYPE(None, DP, C.c_void_p, DP, DP)(product)
+    u, hist, secs = np.zeros(nd), np.zeros(max_iter + 1), C.c_double(0.0)
+    n = oracle.lib().orc_bicgstab_pipe(oracle._st(H.st), nd, oracle._d(u), oracle._d(np.ascontiguousarray(b)), tol,
+                                       max_iter, oracle.MV_EXTERNAL, C.cast(cb, C.c_void_p), None, 0,
+                                       oracle._d(hist), C.byref(secs))
+    return int(n)
+
+
+@pytest.mark.parametrize("level", [3, 4, 5])
+def test_pipelined_bands_are_the_oracle_spread(build_libs, level):
+    """The GPU test's step-count bands for the pipelined solver
+    (tests/test_gpu_pipe.py BANDS) come from the oracle loop's own spread:
+    over 12 seeds of 1e-15 * max|y| product noise it stops after 14-15 steps
+    at C1 L3, 19-21 at L4 and 29-34 at L5 (unperturbed: 14 / 21 / 34).  Each
+    band lies inside that spread (or +-1), and the device's step count (its
+    kernel-order replay, which the GPU test holds equal to the device bit for
+    bit) lies inside the spread too."""
+    import oracle
+    from conftest import pipe_replay
+    from hacapk_b200 import configs
+    from test_gpu_pipe import BANDS
+    H, b = configs.c1(level)
+    _, n_ref, _, _ = oracle.bicgstab_pipe(H.st, b, kind="restated")
+    spread = [_pipe_with_noisy_products(H, b, seed) for seed in range(12)]
+    lo, hi = BANDS[level]
+    assert n_ref - lo >= min(spread) and n_ref + hi <= max(max(spread), n_ref + 1)
+    _, n_dev, _, status = pipe_replay(H, b)
+    assert status == 0 and min(spread) <= n_dev <= max(spread)
+
+
 def test_two_body_precision_workload(build_libs):
     """C2 (the precision form's workload) at level 3: the sphere and the
     seeded ellipsoid are disjoint with the stated gap along x, the H-matrix
