@@ -1965,6 +1965,31 @@ void c_hacapk_bicgstab_cax_lfmtx_pipe2_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HA
   legacy_device_solve(hbx_bicgstab_pipe_host, st_leafmtxp, st_ctl, u, b, param, nd, nstp, lrtrn);
 }
 
+// The reference's multi-GPU-per-process BiCGSTAB versions (HACApK_SOLVER.c:815
+// mgpu1, :1405 mgpu2, :2137 mgpu3; its default build calls mgpu1 from
+// HACApK_solve_cax, m_HACApK_use.f90:349).  They spread one process's leaves
+// over gpus_per_proc GPUs (4 on that build), reduce the partial products by
+// peer copies and run the _gpu_ recurrence with the vector operations
+// repeated (1) or split (2, 3) over those GPUs.  Here a process drives one
+// B200, which holds the whole H-matrix, so all three are the device BiCGSTAB
+// on that GPU; several GPUs are one process each (the row-partitioned form).
+// Like the reference's, they copy H in and release it after the solve unless
+// an engine for st_leafmtxp already exists.
+void c_hacapk_bicgstab_cax_lfmtx_mgpu1_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl, double *u,
+                                        double *b, double *param, int *nd, int *nstp, int *lrtrn) {
+  legacy_device_solve(hbx_bicgstab_host, st_leafmtxp, st_ctl, u, b, param, nd, nstp, lrtrn);
+}
+
+void c_hacapk_bicgstab_cax_lfmtx_mgpu2_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl, double *u,
+                                        double *b, double *param, int *nd, int *nstp, int *lrtrn) {
+  legacy_device_solve(hbx_bicgstab_host, st_leafmtxp, st_ctl, u, b, param, nd, nstp, lrtrn);
+}
+
+void c_hacapk_bicgstab_cax_lfmtx_mgpu3_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl, double *u,
+                                        double *b, double *param, int *nd, int *nstp, int *lrtrn) {
+  legacy_device_solve(hbx_bicgstab_host, st_leafmtxp, st_ctl, u, b, param, nd, nstp, lrtrn);
+}
+
 // Host-vector BiCGSTAB with one GPU matvec per product (HACApK_SOLVER.c:254-417).
 void c_hacapk_bicgstab_cax_lfmtx_flat_(stc_HACApK_leafmtxp *st_leafmtxp, stc_HACApK_lcontrol *st_ctl, double *u,
                                        double *b, double *param, int *nd, int *nstp, int *lrtrn) {

@@ -181,6 +181,12 @@ ENGINE_SYMBOLS = [
      [C.POINTER(LeafMtxP), C.POINTER(LControl), _DP, _DP, _DP, _IP, _IP, _IP]),
     ("c_hacapk_gcrm_lfmtx_gpu_", None,
      [C.POINTER(LeafMtxP), C.POINTER(LControl), _DP, _DP, _DP, _IP, _IP, _IP]),
+    ("c_hacapk_bicgstab_cax_lfmtx_mgpu1_", None,
+     [C.POINTER(LeafMtxP), C.POINTER(LControl), _DP, _DP, _DP, _IP, _IP, _IP]),
+    ("c_hacapk_bicgstab_cax_lfmtx_mgpu2_", None,
+     [C.POINTER(LeafMtxP), C.POINTER(LControl), _DP, _DP, _DP, _IP, _IP, _IP]),
+    ("c_hacapk_bicgstab_cax_lfmtx_mgpu3_", None,
+     [C.POINTER(LeafMtxP), C.POINTER(LControl), _DP, _DP, _DP, _IP, _IP, _IP]),
 ]
 
 BUILD_SYMBOLS = [

@@ -501,6 +501,21 @@ void c_hacapk_bicgstab_cax_lfmtx_pipe_(stc_HACApK_leafmtxp *st_leafmtxp,
 void c_hacapk_bicgstab_cax_lfmtx_pipe2_(stc_HACApK_leafmtxp *st_leafmtxp,
                                         stc_HACApK_lcontrol *st_ctl, double *u, double *b,
                                         double *param, int *nd, int *nstp, int *lrtrn);
+/* HACApK_SOLVER.c:815 / :1405 / :2137 -- the multi-GPU-per-process BiCGSTAB
+ * versions (the reference's default build calls _mgpu1_ from HACApK_solve_cax,
+ * m_HACApK_use.f90:349).  The same recurrence as _gpu_; here each process
+ * drives one GPU holding the whole H, so all three run hbx_bicgstab_host on
+ * it (same arguments as above; H is copied in and released after the solve
+ * unless lfcpy already made an engine for st_leafmtxp). */
+void c_hacapk_bicgstab_cax_lfmtx_mgpu1_(stc_HACApK_leafmtxp *st_leafmtxp,
+                                        stc_HACApK_lcontrol *st_ctl, double *u, double *b,
+                                        double *param, int *nd, int *nstp, int *lrtrn);
+void c_hacapk_bicgstab_cax_lfmtx_mgpu2_(stc_HACApK_leafmtxp *st_leafmtxp,
+                                        stc_HACApK_lcontrol *st_ctl, double *u, double *b,
+                                        double *param, int *nd, int *nstp, int *lrtrn);
+void c_hacapk_bicgstab_cax_lfmtx_mgpu3_(stc_HACApK_leafmtxp *st_leafmtxp,
+                                        stc_HACApK_lcontrol *st_ctl, double *u, double *b,
+                                        double *param, int *nd, int *nstp, int *lrtrn);
 /* GCR(m) on the GPU with the same arguments, for a Fortran driver that picks
  * GCR (param(85) = 2 in HACApK_solve, m_HACApK_use.f90:236-241): replaces the
  * call to the Fortran HACApK_gcrm_lfmtx (m_HACApK_solve.f90:506), which has

@@ -132,3 +132,50 @@ def test_legacy_solver_rejects_several_ranks(gpu, build_libs):
     lib.c_hacapk_bicgstab_cax_lfmtx_gpu_(H.st, C.byref(ctl), abi.dptr(u), abi.dptr(b), ctl.param, C.byref(nd),
                                          C.byref(nstp), C.byref(lrtrn))
     assert lrtrn.value == 8
+
+
+def test_multi_gpu_per_process_entries_are_the_device_solver(gpu, build_libs):
+    """HACApK_SOLVER.c:815 / :1405 / :2137 (c_hacapk_bicgstab_cax_lfmtx_mgpu1_,
+    the solver the reference's default build calls, m_HACApK_use.f90:349, and
+    its two alternatives): one process drives one B200 here, so each is the
+    device BiCGSTAB of _gpu_.  Without an engine for the container each makes
+    one, solves and releases it (as the reference copies H in and deletes it);
+    after lfcpy they use that engine and leave it to lfdel.  Same steps and
+    the same u bit for bit as _gpu_, +-1 of the oracle, and nrank > 1
+    rejected."""
+    import oracle
+    from hacapk_b200 import abi, configs
+    lib = abi.engine_lib()
+    H, b = configs.c1(4)
+    ctl, buf = _control()
+
+    def solve(entry):
+        u = np.zeros(H.nd)
+        nd, nstp, lrtrn = C.c_int(H.nd), C.c_int(-1), C.c_int(-1)
+        getattr(lib, entry)(H.st, C.byref(ctl), abi.dptr(u), abi.dptr(b), ctl.param, C.byref(nd),
+                            C.byref(nstp), C.byref(lrtrn))
+        assert lrtrn.value == 0
+        return u, nstp.value
+
+    u_gpu, n_gpu = solve("c_hacapk_bicgstab_cax_lfmtx_gpu_")
+    _, n_ref, _, _ = oracle.bicgstab(H.st, b, tol=1e-8, max_iter=1000, kind="ref" if oracle.have_ref() else "restated")
+    assert n_ref - 1 <= n_gpu <= n_ref + 1
+    for k in (1, 2, 3):
+        u, n = solve(f"c_hacapk_bicgstab_cax_lfmtx_mgpu{k}_")
+        assert n == n_gpu and np.array_equal(u, u_gpu)
+    nd = C.c_int(H.nd)
+    lib.c_hacapk_adot_body_lfcpy_batch_sorted_(C.byref(nd), H.st)
+    u, n = solve("c_hacapk_bicgstab_cax_lfmtx_mgpu1_")
+    assert n == n_gpu and np.array_equal(u, u_gpu)
+    x = np.random.default_rng(6).standard_normal(H.nd)
+    y, t = np.zeros(H.nd), np.zeros(3)
+    lib.c_hacapk_adot_body_lfmtx_batch_(abi.dptr(y), H.st, abi.dptr(x), abi.dptr(np.zeros(H.nd)),
+                                        abi.dptr(t[0:]), abi.dptr(t[1:]), abi.dptr(t[2:]))
+    ref = oracle.matvec(H.st, x)
+    assert np.abs(y - ref).max() <= 1e-13 * np.abs(ref).max()   # the lfcpy engine is still there
+    lib.c_hacapk_adot_body_lfdel_batch_(H.st)
+    ctl2, buf2 = _control(nrank=2)
+    u2, n2, lrtrn = np.zeros(H.nd), C.c_int(-1), C.c_int(-1)
+    lib.c_hacapk_bicgstab_cax_lfmtx_mgpu1_(H.st, C.byref(ctl2), abi.dptr(u2), abi.dptr(b), ctl2.param,
+                                           C.byref(nd), C.byref(n2), C.byref(lrtrn))
+    assert lrtrn.value == 8
