@@ -7,9 +7,11 @@ Fortran driver calls them (m_HACApK_solve.f90:597-735):
   2. the CPU-vs-GPU product check with x = 1 (m_HACApK_solve.f90:705-735):
      zau = H 1 through c_hacapk_adot_body_lfmtx_batch_ against the
      reference's own compiled CPU product, relative 2-norm error;
-  3. c_hacapk_bicgstab_cax_lfmtx_gpu_ and c_hacapk_bicgstab_cax_lfmtx_flat_
-     (HACApK_SOLVER.c:421, :254) on b = 1 (unit potential), each within +-1
-     step of the oracle BiCGSTAB and below 1e-8 in the true residual;
+  3. c_hacapk_bicgstab_cax_lfmtx_gpu_, c_hacapk_bicgstab_cax_lfmtx_flat_ and
+     c_hacapk_bicgstab_cax_lfmtx_mgpu1_ (HACApK_SOLVER.c:421, :254, :815; the
+     last is what the reference's default build calls, m_HACApK_use.f90:349)
+     on b = 1 (unit potential), each within +-1 step of the oracle BiCGSTAB
+     and below 1e-8 in the true residual, _mgpu1_ equal to _gpu_ bit for bit;
   4. c_hacapk_adot_body_lfdel_batch_.
 
 The mesh comes from the committed fixture tests/golden/input_10ts_mesh.npz
@@ -46,7 +48,9 @@ def test_reference_input_through_the_drop_in_entry_points(gpu, build_libs):
     assert tb.value > 0.0
     b = H.to_cluster(np.ones(n))
     _, n_ref, _, _ = oracle.bicgstab(H.st, b, tol=1e-8, max_iter=1000, kind="ref" if oracle.have_ref() else "restated")
-    for entry in ("c_hacapk_bicgstab_cax_lfmtx_gpu_", "c_hacapk_bicgstab_cax_lfmtx_flat_"):
+    sols = {}
+    for entry in ("c_hacapk_bicgstab_cax_lfmtx_gpu_", "c_hacapk_bicgstab_cax_lfmtx_flat_",
+                  "c_hacapk_bicgstab_cax_lfmtx_mgpu1_"):
         ctl, buf = _control()
         u = np.zeros(n)
         nstp, lrtrn = C.c_int(-1), C.c_int(-1)
@@ -56,4 +60,8 @@ def test_reference_input_through_the_drop_in_entry_points(gpu, build_libs):
         assert n_ref - 1 <= nstp.value <= n_ref + 1, (entry, nstp.value, n_ref)
         r = b - oracle.matvec(H.st, u)
         assert np.linalg.norm(r) / np.linalg.norm(b) < 1.05e-8, entry
+        sols[entry] = (nstp.value, u)
+    n_gpu, u_gpu = sols["c_hacapk_bicgstab_cax_lfmtx_gpu_"]
+    n_mgpu, u_mgpu = sols["c_hacapk_bicgstab_cax_lfmtx_mgpu1_"]
+    assert n_mgpu == n_gpu and np.array_equal(u_mgpu, u_gpu)
     lib.c_hacapk_adot_body_lfdel_batch_(H.st)
