@@ -6,7 +6,8 @@ ctypes bindings to
     reference sources by oracle/Makefile;
   * oracle/liboracle.so: the C restatement in oracle.c (matvec, per-leaf BLAS
     matvec, OpenMP "_hyp" matvec, transposed matvec, BiCGSTAB of
-    HACApK_SOLVER.c:254-417).
+    HACApK_SOLVER.c:254-417, pipelined BiCGSTAB of HACApK_SOLVER_PIPE.c:144-600,
+    GCR(m) of m_HACApK_solve.f90:506-571).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it.
 The product library never links or calls anything here.

@@ -20,6 +20,13 @@
  *   orc_bicgstab .......... HACApK_SOLVER.c:254-417 (c_hacapk_bicgstab_cax_
  *                           lfmtx_flat_), same statement order, with the
  *                           sequential dot c_hacapk_dotp_d (HACApK_SOLVER.c:7-14)
+ *   orc_bicgstab_pipe ..... HACApK_SOLVER_PIPE.c:144-600 (pipelined BiCGSTAB,
+ *                           version 1; _pipe2_ at :640 has the same arithmetic)
+ *   orc_gcrm .............. m_HACApK_solve.f90:506-571 (HACApK_gcrm_lfmtx, GCR(m))
+ *
+ * The solvers take their product as a kind: the restated loops, the per-leaf
+ * BLAS form, the OpenMP form, or an external zau += H zu function (the
+ * reference's compiled c_hacapk_adot_body_lfmtx_, or a test's own product).
  *
  * Built with -ffp-contract=off.
  */
