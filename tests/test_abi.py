@@ -33,6 +33,17 @@ def test_every_declared_symbol_is_exported(build_libs, header):
     assert not missing, f"{header}: not exported by {os.path.basename(lib)}: {missing}"
 
 
+def test_engine_library_exports_only_its_c_abi(build_libs):
+    """The engine library's dynamic symbol table is exactly the functions of
+    include/hacapk_b200.h (the export map keeps the C++ internals local), so
+    a Fortran application linking it sees no other names."""
+    from hacapk_b200 import abi
+    out = subprocess.run(["nm", "-D", "--defined-only", abi.ENGINE_LIB], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    assert exported == set(declared_functions("hacapk_b200.h"))
+
+
 def test_libraries_load_without_a_gpu(build_libs):
     from hacapk_b200 import abi
     abi.engine_lib()
